@@ -1,0 +1,226 @@
+/*
+ * ufem_gpu.h -- C ABI of libufem_gpu.so, the B200 (sm_100a) implementation of
+ * uFEM's linear static solve path: element stiffness integration (4-node
+ * plane quad, 8-node brick), assembly into a block-sparse K, supports and
+ * nodal loads, Jacobi-preconditioned CG / BiCGStab / SSOR-CG, the result pass
+ * (stresses, internal forces, reactions) and the Monte Carlo plugin ABI.
+ *
+ * Plain C types only: pointers, sizes, error codes.  Every function returns
+ * the reference's AF_* codes (fem/fem.h:41-52).  There is no CPU fallback:
+ * a missing or failing GPU gives AF_ERR / AF_ERR_MEM.
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef UFEM_GPU_H
+#define UFEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes, identical to fem/fem.h:41-52 */
+#define UFEM_AF_OK       0
+#define UFEM_AF_ERR     (-1)
+#define UFEM_AF_ERR_IO  (-2)
+#define UFEM_AF_ERR_VAL (-3)
+#define UFEM_AF_ERR_MEM (-4)
+#define UFEM_AF_ERR_TYP (-5)
+#define UFEM_AF_ERR_SIZ (-9)
+#define UFEM_AF_ERR_SML (-10)
+#define UFEM_AF_ERR_BIG (-11)
+#define UFEM_AF_ERR_EMP (-12)
+#define UFEM_AF_ERR_ZER (-13)
+
+/* solver selection, as femSolve picks it (fem/fem_sol.c:1716-1730) */
+#define UFEM_SOLVER_CGWJ  0   /* femEqsCGwJ    fem/fem_eqs.c:88   */
+#define UFEM_SOLVER_SSOR  1   /* femEqsCGwSSOR fem/fem_eqs.c:1001 */
+#define UFEM_SOLVER_BICG  2   /* femEqsBiCCSwJ fem/fem_eqs.c:262  */
+
+/* stopping rules */
+#define UFEM_STOP_REFERENCE 0 /* |r| <= eps(|A||x| + |b|) with the recursive r
+                                 and |A| = max row 2-norm, fem/fem_eqs.c:202-207 */
+#define UFEM_STOP_RELRES    1 /* true residual |b - A x| / |b| <= eps (FP64)  */
+
+/* per-sample status words of the batched Monte Carlo solve */
+#define UFEM_ST_CONVERGED   0
+#define UFEM_ST_MAXIT       1 /* iteration cap reached (the reference's AF_ERR) */
+#define UFEM_ST_BREAKDOWN   2 /* p.q <= 0 or a zero pivot */
+#define UFEM_ST_NAN         3 /* non-finite residual */
+#define UFEM_ST_FALLBACK    4 /* warm start regressed; solved again from zero */
+
+/*
+ * Model tables.  Mirrors the flat global tables that femReadInput fills
+ * (fem/fem_io.c:380-590; declarations fem/fem_data.c): every index is a
+ * 0-based position, as in the reference's preparsed input.
+ */
+typedef struct ufem_tables {
+  long nLen;                 /* nodes */
+  const double *n_x, *n_y, *n_z;
+  long eLen;                 /* elements */
+  const long *eType;         /* element type: 2 (quad), 9 or 10 (brick) */
+  const long *eRS;           /* real set position per element */
+  const long *eMP;           /* material position per element */
+  const long *eFrom;         /* start of the element's nodes in eNodesL */
+  const long *eNodesL;       /* node positions */
+  long rsLen;                /* real sets */
+  const long *rsType, *rsFrom;
+  long rsLenL;
+  const double *rsValL;
+  long mpLen;                /* materials (type 1, values DENS EX NU ...) */
+  const long *mpType, *mpFrom;
+  long mpLenL;
+  const double *mpValL;
+  long nlLen;                /* nodal loads and supports */
+  const long *nlNode, *nlType, *nlDir;
+  const double *nlVal;
+} ufem_tables;
+
+typedef struct ufem_model ufem_model;
+
+/* ---- model set-up ------------------------------------------------------ */
+
+/* Builds a model from the tables: DOF numbering (fem_dofs, fem/fem_sol.c:1263),
+ * the block-sparse pattern, element colouring and the element->block scatter
+ * map; uploads everything to the current CUDA device. */
+int ufem_model_create(const ufem_tables *t, ufem_model **out);
+
+/* Reads a preparsed uFEM input file (femReadInput, fem/fem_io.c:380, with
+ * femPreparsedData = AF_YES) including its Monte Carlo section
+ * (fem_monte_read_data, fem/fem_mont.c:866), then ufem_model_create. */
+int ufem_read_input(const char *fname, ufem_model **out);
+
+void ufem_model_free(ufem_model *m);
+
+/* nDOFAct (fem/fem_sol.c:46) and nDOFfld[nLen*7] (fem/fem_sol.c:1263-1395) */
+long ufem_ndof(const ufem_model *m);
+int  ufem_get_ndoffld(const ufem_model *m, long *nDOFfld);
+
+/* The reference's row-slot pattern (fem_sol_alloc + femKhit + the first-touch
+ * column order of femMatPutAdd, fem/fem_math.c:185-236): frompos[rows],
+ * defpos[rows], pos[len] with 1-based columns and 0 in unused slots.  Call
+ * with pos == NULL to get *len. */
+int ufem_export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, long *len);
+
+/* Block-sparse pattern used on the GPU: block size b (2 quad, 3 brick),
+ * nbr block rows (= used nodes), nnzb blocks; rowptr[nbr+1], colind[nnzb]. */
+int ufem_bsr_shape(const ufem_model *m, long *b, long *nbr, long *nnzb);
+int ufem_get_bsr_pattern(const ufem_model *m, int *rowptr, int *colind);
+long ufem_num_colours(const ufem_model *m);
+
+/* ---- the static path (replaces femSolve's body, fem/fem_sol.c:1655-1760) -- */
+
+/* fem_fill_K (fem/fem_sol.c:897).  mode 0: integrate every element and
+ * assemble K on the GPU.  mode 1: the result pass -- integration-point
+ * stresses, internal forces and reactions from the current u. */
+int ufem_fill_K(ufem_model *m, long mode);
+
+/* fem_add_loads(0) (fem/fem_sol.c:1119): type-3 nodal forces into F. */
+int ufem_add_loads(ufem_model *m);
+
+/* fem_add_disps(AF_YES,0) (fem/fem_sol.c:1195): type-1 supports; zero values
+ * zero the row and column and put 1 on the diagonal (fem/fem_loads.c:158-166). */
+int ufem_add_disps(ufem_model *m);
+
+/* femEqsCGwJ / femEqsCGwSSOR / femEqsBiCCSwJ on the assembled K, F, u.
+ * maxIt <= 0 means nDOFAct (femSolve's choice).  *iters gets the count. */
+int ufem_solve(ufem_model *m, int solver, int stop_rule, double eps, long maxIt, long *iters);
+
+/* The whole femSolve sequence: fill_K(0), loads, supports, solve with the
+ * reference's stopping rule, fill_K(1). */
+int ufem_fem_solve(ufem_model *m, int solver, long *iters);
+
+/* results and intermediates (host copies) */
+int ufem_get_u(const ufem_model *m, double *u);
+int ufem_set_u(ufem_model *m, const double *u);
+int ufem_get_F(const ufem_model *m, double *F);
+int ufem_get_K_values(const ufem_model *m, double *val);  /* nnzb*b*b, BSR order */
+/* every element matrix as the element kernel computes it, eLen*s*s
+ * (s = 8 quad, 24 brick); debugging/parity aid */
+int ufem_get_element_matrices(ufem_model *m, double *Ke);
+/* integration-point stresses: quad eLen*4*3 (SX,SY,SXY), brick eLen*27*6
+ * (SX,SY,SZ,SYZ,SZX,SXY); von Mises per point: eLen*4 or eLen*27 */
+int ufem_get_stresses(const ufem_model *m, double *sig, double *von_mises);
+/* reactions in the order of fem_sol_res_alloc (fem/fem_sol.c:676-722) */
+long ufem_num_reactions(const ufem_model *m);
+int ufem_get_reactions(const ufem_model *m, long *node, long *dof, double *val);
+/* timing of the last call of each phase, milliseconds (CUDA events) */
+int ufem_get_phase_ms(const ufem_model *m, double *fill_ms, double *bc_ms, double *solve_ms,
+                      double *results_ms);
+
+/* ---- level-1 drop-in on the reference's own matrix (fem/fem_math.h:150-152) --
+ * a: the reference's MAT_SPAR tMatrix fields (rows, frompos[rows],
+ * defpos[rows], pos[] 1-based with 0 ending a row, data[]); b, x: VEC_FULL
+ * data of length rows; x is the initial guess and the result.  Same
+ * semantics and return codes as the reference functions. */
+int ufem_eqs_cgwj(long rows, const long *frompos, const long *defpos, const long *pos,
+                  const double *data, const double *b, double *x, double eps, long maxIt);
+int ufem_eqs_bicgs(long rows, const long *frompos, const long *defpos, const long *pos,
+                   const double *data, const double *b, double *x, double eps, long maxIt);
+int ufem_eqs_cgwssor(long rows, const long *frompos, const long *defpos, const long *pos,
+                     const double *data, const double *b, double *x, double eps, long maxIt);
+
+/* ---- Monte Carlo plugin ABI (fem/fem_mont.c:137-866) --------------------- */
+long  monte_dlib_interface_type(void);                                  /* :137 */
+void  monte_nums_of_vars(char *param, long *ilen, long *olen, long *ffunc); /* :146 */
+char *monte_ivar_name(char *param, long pos);                           /* :158 */
+char *monte_ovar_name(char *param, long pos);                           /* :256 */
+int   monte_init_lib_stuff(char *param);                                /* :424 */
+int   monte_clean_lib_stuff(char *param);                               /* :471 */
+int   monte_solution(char *param, double *ifld, double *ofld, long if_type); /* :694 */
+
+/* Batched extension (no reference counterpart): nsamp samples of the model
+ * loaded by monte_init_lib_stuff in one GPU launch.  ifld[nsamp*ilen],
+ * ofld[nsamp*olen], status[nsamp] (UFEM_ST_*).  Solves to the relative
+ * residual of ufem_mc_set_options (default 1e-8). */
+int monte_solution_batch(char *param, long nsamp, const double *ifld, double *ofld,
+                         long if_type, int *status);
+
+/* Options of the batched solve. precision 0: FP64 PCG; 1: FP32 inner PCG in
+ * FP64 iterative refinement.  tol: true relative residual |f-Ku|/|f|. */
+typedef struct ufem_mc_options {
+  int precision;
+  double tol;
+  double inner_tol;          /* relative reduction per refinement step (FP32) */
+  long max_iters;            /* total PCG iteration cap per sample */
+  int max_refine;            /* FP64 refinement steps */
+  int use_graphs;            /* capture the inner iteration in a CUDA graph */
+} ufem_mc_options;
+void ufem_mc_default_options(ufem_mc_options *o);
+
+/* Handle-based batched Monte Carlo over several meshes of uneven size in one
+ * launch.  models[k] must carry a Monte Carlo variable table.  For mesh k:
+ * ifld[k] is nsamp[k]*ilen_k, ofld[k] nsamp[k]*olen_k, status[k] nsamp[k],
+ * iters[k] (may be NULL) nsamp[k] iteration counts.  u_guess[k] (may be NULL,
+ * or NULL entries) gives nsamp[k]*nDOFAct initial guesses. */
+int ufem_mc_solve(int nmesh, ufem_model *const *models, const long *nsamp,
+                  const double *const *ifld, double *const *ofld, int *const *status,
+                  long *const *iters, const double *const *u_guess, const ufem_mc_options *opt);
+
+/* Same, with every input and output already in device memory (for timing the
+ * kernels without host transfers). */
+int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp,
+                         const double *const *d_ifld, double *const *d_ofld, int *const *d_status,
+                         long *const *d_iters, const double *const *d_u_guess,
+                         double *const *d_u_out, const ufem_mc_options *opt);
+
+/* Statistics of the last ufem_mc_solve*: kernel milliseconds of the inner
+ * PCG, FP64 refinement, assembly and outputs, the number of inner PCG
+ * iterations run, the algorithmic bytes moved by the PCG kernels, and the
+ * number of kernels launched. */
+typedef struct ufem_mc_stats {
+  double ms_assemble, ms_pcg, ms_refine, ms_outputs, ms_total;
+  long pcg_iterations;       /* inner iterations executed (max over samples) */
+  double pcg_bytes;          /* algorithmic bytes of all PCG iterations */
+  double spmv_bytes;         /* algorithmic bytes of the SpMV phases only */
+  long kernel_launches;
+} ufem_mc_stats;
+int ufem_mc_get_stats(ufem_mc_stats *s);
+
+/* ---- device / diagnostics ------------------------------------------------ */
+int ufem_device_info(int *sm_count, int *cc_major, int *cc_minor, long *mem_bytes);
+const char *ufem_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UFEM_GPU_H */

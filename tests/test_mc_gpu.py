@@ -1,0 +1,185 @@
+"""Monte Carlo on the GPU: the plugin ABI against the reference's own
+libfem.so outputs (golden fixture), and the batched solve against per-sample
+FP64 solves and the oracle.
+
+Tolerance: displacements and reactions within 1e-8 relative (the batched
+solves stop at true relative residual 1e-8 in FP64; the comparison allows
+the condition-number amplification seen on these beams, 1e-6 on u for the
+residual-1e-8 solves)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from golden_util import load, model_from
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def mc_fixture():
+    from ufem_b200 import meshgen as mg
+    z = load("mc_beam_4x2x2")
+    m = model_from(z)
+    d = tempfile.mkdtemp()
+    path = os.path.join(d, "mc.fem")
+    mg.write_fem(m, path)
+    return z, m, path
+
+
+def test_plugin_abi_matches_reference(mc_fixture):
+    from ufem_b200.mc import MonteLib
+    z, m, path = mc_fixture
+    lib = MonteLib(path)
+    try:
+        assert lib.interface_type() == 2
+        assert lib.ilen == int(z["mc_ilen"]) and lib.olen == int(z["mc_olen"])
+        assert lib.ovar_names() == [str(s) for s in z["onames"]]
+        nmat = len(z["inames"])
+        assert lib.ivar_names()[:nmat] == [str(s) for s in z["inames"]]
+        ref = z["ofld"]
+        prev_reac = np.zeros(ref.shape[1])
+        is_reac = np.array([n.startswith("REAC") for n in lib.ovar_names()])
+        for s in range(ref.shape[0]):
+            rv, out = lib.solution(z["ifld"][s])
+            assert rv == 0
+            # displacements: the reference's FP64 solve
+            assert relerr(out[~is_reac], ref[s, ~is_reac]) <= 1e-8
+            # reactions: the reference accumulates them across samples
+            # (resRval is never cleared in monte_linear_solver); per sample
+            # they are the difference of consecutive outputs
+            ref_reac = ref[s, is_reac] - prev_reac[is_reac]
+            prev_reac = ref[s]
+            assert relerr(out[is_reac], ref_reac) <= 1e-8
+    finally:
+        lib.close()
+
+
+def test_batch_matches_single_samples(mc_fixture):
+    from ufem_b200.mc import MonteLib
+    z, m, path = mc_fixture
+    lib = MonteLib(path)
+    try:
+        rv, ob, st = lib.solution_batch(z["ifld"])
+        assert rv == 0 and (st == 0).all()
+        for s in range(z["ifld"].shape[0]):
+            rv, o1 = lib.solution(z["ifld"][s])
+            assert relerr(ob[s], o1) <= 1e-6
+    finally:
+        lib.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_uneven_meshes_one_launch(precision):
+    """Three meshes of uneven size and sample counts (not multiples of the
+    sample group) in one launch, against per-sample FP64 oracle solves."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    from oracle.oracle import OracleModel
+    specs = [(4, 1, 1, 37), (8, 2, 2, 150), (6, 3, 2, 70)]
+    models, gms, iflds = [], [], []
+    for k, (nx, ny, nz, ns) in enumerate(specs):
+        m = mg.beam_brick(nx, ny, nz, 2.0 * nx / 4, 0.5 * ny, 0.5 * nz, per_element_material=True)
+        mg.mc_attach_vars(m, n_out_nodes=3)
+        models.append(m)
+        gms.append(GpuModel(m))
+        iflds.append(mg.mc_samples(m, mesh_id=k, nsamp=ns))
+    res, stats = mc_solve(gms, iflds, precision=precision, tol=1e-8)
+    for k, m in enumerate(models):
+        ofld, st, it = res[k]
+        assert (st == 0).all(), (k, st)
+        assert (it > 0).all()
+        for s in (0, iflds[k].shape[0] // 2, iflds[k].shape[0] - 1):
+            mm = model_from_sample(m, iflds[k][s])
+            om = OracleModel(mm)
+            o = om.run_static()
+            # RES_D outputs = u at the chosen tip nodes
+            rows = []
+            nd = o["ndoffld"]
+            for row in m.mc_vars[m.mc_ilen:]:
+                if row[1] == mg.MONTE_VTYPE_RES_D:
+                    rows.append(nd[row[2] * 7 + row[3] - 1] - 1)
+            assert relerr(ofld[s, :len(rows)], o["u"][rows]) <= 1e-6
+            reac = o["reac"]
+            reac_idx = [j for j, row in enumerate(m.mc_vars[m.mc_ilen:]) if row[1] == mg.MONTE_VTYPE_RES_R]
+            # reaction outputs: first support node, UX and UZ
+            sup = m.nl_node[np.nonzero(m.nl_type == 1)[0][0]]
+            ref_r = [reac[i] for i in range(len(reac)) if False]
+            rlist = list(zip(o_reac_nodes(m), o_reac_dofs(m)))
+            for j in reac_idx:
+                row = m.mc_vars[m.mc_ilen + j]
+                r = rlist.index((row[2], row[3]))
+                assert abs(ofld[s, j] - reac[r]) <= 1e-6 * np.abs(reac).max()
+    assert stats.pcg_iterations > 0
+
+
+def o_reac_nodes(m):
+    return [int(n) for n, t, v in zip(m.nl_node, m.nl_type, m.nl_val) if t == 1 and v == 0.0]
+
+
+def o_reac_dofs(m):
+    return [int(d) for d, t, v in zip(m.nl_dir, m.nl_type, m.nl_val) if t == 1 and v == 0.0]
+
+
+def model_from_sample(m, row):
+    """The model with one MC sample's inputs applied (E per material, forces)."""
+    import copy
+    from ufem_b200 import meshgen as mg
+    mm = copy.deepcopy(m)
+    mm.mp_vals = [v.copy() for v in m.mp_vals]
+    mm.nl_val = m.nl_val.copy()
+    for var in m.mc_vars[:m.mc_ilen]:
+        pos, ty, item, sub, it = [int(x) for x in var]
+        if ty == mg.MONTE_VTYPE_MAT and sub == mg.MAT_EX:
+            mm.mp_vals[item][1] = row[pos]
+        elif ty == mg.MONTE_VTYPE_NLD:
+            for j in range(len(mm.nl_node)):
+                if mm.nl_node[j] == item and mm.nl_type[j] == sub and mm.nl_dir[j] == it:
+                    mm.nl_val[j] = row[pos]
+                    break
+    return mm
+
+
+def test_zero_load_sample_converges_at_once():
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    m = mg.beam_brick(4, 2, 2, 2.0, 1.0, 1.0, per_element_material=True)
+    mg.mc_attach_vars(m)
+    f = mg.mc_samples(m, 5, 3)
+    f[1, len(m.mp_vals):] = 0.0          # sample 1: no load
+    res, _ = mc_solve([GpuModel(m)], [f])
+    ofld, st, it = res[0]
+    assert (st == 0).all()
+    assert it[1] == 0 and not ofld[1].any()
+    assert it[0] > 0 and it[2] > 0
+
+
+def test_batched_run_twice_identical():
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    m = mg.beam_brick(6, 2, 2, 3.0, 1.0, 1.0, per_element_material=True)
+    mg.mc_attach_vars(m)
+    f = mg.mc_samples(m, 9, 200)
+    g = GpuModel(m)
+    a, _ = mc_solve([g], [f])
+    b, _ = mc_solve([g], [f])
+    assert np.array_equal(a[0][0], b[0][0]) and np.array_equal(a[0][2], b[0][2])
+
+
+def test_iteration_cap_reports_maxit():
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import ST_MAXIT, mc_solve
+    m = mg.beam_brick(8, 2, 2, 4.0, 1.0, 1.0, per_element_material=True)
+    mg.mc_attach_vars(m)
+    f = mg.mc_samples(m, 3, 5)
+    res, _ = mc_solve([GpuModel(m)], [f], max_iters=3, max_refine=1)
+    assert (res[0][1] == ST_MAXIT).all()

@@ -1,0 +1,1313 @@
+// Batched Monte Carlo solve: many samples of several meshes (uneven sizes) in
+// one persistent launch.  Replaces the per-sample loop an external driver runs
+// over monte_solution (fem/fem_mont.c:694) -> monte_linear_solver
+// (fem/fem_mont.c:480-508), which zeroes K/F/u, re-assembles (fem_fill_K),
+// re-applies loads and supports and solves, one sample at a time.
+//
+// Layout (per mesh, S samples padded to a multiple of the sample group GS):
+//   values  V[(k*B*B + e)*S + s]   block k, entry e, sample s (sample fastest)
+//   vectors x[i*S + s]             DOF i, sample s
+// so a warp that owns one block row and GS samples reads every value and
+// every gathered neighbour with full 128-byte transactions, and one read of
+// the row's column indices serves GS samples.
+//
+// Assembly: the element matrices of one mesh are integrated once with E = 1
+// (K_e is linear in E for the isotropic D of fem/fem_pl3d.c:32-57) and kept
+// in FP64.  Per sample, K_s = sum_e E_{s,e} K_e is gathered block by block
+// through per-block contribution lists in element order -- the order of the
+// reference's femLocKM_e accumulation (fem/fem_mloc.c:163-221) -- so the FP64
+// sums are deterministic without atomics.  Supports are applied in the same
+// pass (rows/columns of fixed DOFs -> identity, fem/fem_loads.c:158-166).
+//
+// Solve: FP64 iterative refinement around an inner Jacobi PCG.  The inner
+// PCG (FP32, or FP64 when precision = 0) is one persistent cooperative
+// kernel over work tiles (mesh, sample group, block-row chunk) of every mesh;
+// two bounded grid barriers per iteration; per-sample convergence masks
+// freeze converged samples, a group of GS samples drops out when all of its
+// samples are done, and the launch ends when no group is left or at the
+// iteration cap.  Per-sample scalars come from per-tile partials reduced in
+// a fixed order (run-to-run identical); partial buffers are double-buffered
+// by iteration parity so no block overwrites what another still reads.
+// The outer loop forms r = f - K u in FP64 from FP64 values, hands r to the
+// inner solve, adds the correction to the FP64 u and stops each sample at
+// |f - K u| / |f| <= tol.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "device_util.cuh"
+#include "ufem_internal.h"
+
+namespace ufem {
+
+// ---------------------------------------------------------------------------
+// per-mesh plan (host + device), built once per model
+// ---------------------------------------------------------------------------
+struct McOut {
+  int type;    // MONTE_VTYPE_RES_*
+  int pos;     // ofld position
+  int row;     // DOF row for RES_D / RES_R (0-based) or -1
+  int elem, ip, comp;  // RES_E
+  int reac;    // reaction index
+};
+
+struct McPlan {
+  bool built = false;
+  int s = 0;                       // element matrix size (8 or 24)
+  DBuf<double> Khat;               // eLen*s*s, E = 1
+  DBuf<int> gptr, gel, gpair;      // per-block contribution lists
+  DBuf<int> elem_var;              // ifld column of each element's E, -1 = base
+  DBuf<double> F0;                 // loads that no input variable overrides
+  std::vector<int> ovr_row, ovr_var;
+  DBuf<int> d_ovr_row, d_ovr_var;
+  std::vector<McOut> outs;
+  DBuf<int> d_out_type, d_out_pos, d_out_row, d_out_elem, d_out_ip, d_out_comp;
+  DBuf<int> reac_rows;             // DOF rows of the reaction list
+  long ilen = 0, olen = 0;
+};
+
+static std::vector<std::unique_ptr<McPlan>> g_plans;
+static std::vector<const ufem_model *> g_plan_owner;
+
+McPlan *get_plan(const ufem_model *m) {
+  for (size_t i = 0; i < g_plan_owner.size(); i++)
+    if (g_plan_owner[i] == m) return g_plans[i].get();
+  g_plan_owner.push_back(m);
+  g_plans.emplace_back(new McPlan());
+  return g_plans.back().get();
+}
+
+void drop_plan(const ufem_model *m) {
+  for (size_t i = 0; i < g_plan_owner.size(); i++)
+    if (g_plan_owner[i] == m) {
+      g_plan_owner.erase(g_plan_owner.begin() + i);
+      g_plans.erase(g_plans.begin() + i);
+      return;
+    }
+}
+
+int element_matrices_unitE(ufem_model *m, double *d_out);  // kernels.cu
+
+static int build_plan(ufem_model *m, McPlan *P) {
+  int rv;
+  const int nn = m->nn, B = m->b, s = nn * B;
+  P->s = s;
+  P->ilen = m->mc_ilen;
+  P->olen = m->mc_olen;
+  if ((rv = P->Khat.alloc((size_t)m->eLen * s * s)) != UFEM_AF_OK) return rv;
+  if ((rv = element_matrices_unitE(m, P->Khat.p)) != UFEM_AF_OK) return rv;
+  // contribution lists: element order within each block
+  std::vector<int> cnt(m->nnzb + 1, 0);
+  for (long e = 0; e < m->eLen; e++)
+    for (int p = 0; p < nn * nn; p++) cnt[m->emap[(size_t)e * nn * nn + p] + 1]++;
+  for (long k = 0; k < m->nnzb; k++) cnt[k + 1] += cnt[k];
+  std::vector<int> gel(cnt[m->nnzb]), gpair(cnt[m->nnzb]), fill(cnt.begin(), cnt.end() - 1);
+  for (long e = 0; e < m->eLen; e++)
+    for (int p = 0; p < nn * nn; p++) {
+      int k = m->emap[(size_t)e * nn * nn + p];
+      gel[fill[k]] = (int)e;
+      gpair[fill[k]] = p;
+      fill[k]++;
+    }
+  if ((rv = P->gptr.upload(cnt.data(), cnt.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->gel.upload(gel.data(), gel.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->gpair.upload(gpair.data(), gpair.size())) != UFEM_AF_OK) return rv;
+  // inputs: MONTE_VTYPE_MAT (E only) and MONTE_VTYPE_NLD (fem/fem_mont.c:721-760)
+  std::vector<int> mat_var(m->mpVals.size(), -1);
+  std::vector<int> load_var(m->loads.size(), -1);
+  for (long i = 0; i < m->mc_ilen; i++) {
+    long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i], it = m->mc_iter[i];
+    int col = (int)m->mc_pos[i];
+    if (col < 0 || col >= m->mc_ilen) {
+      set_error("Monte Carlo input position out of range");
+      return UFEM_AF_ERR_VAL;
+    }
+    if (ty == 1) {  // MONTE_VTYPE_MAT
+      if (sub != 2 || item < 0 || item >= (long)m->mpVals.size()) {
+        set_error("batched Monte Carlo randomises material E (MAT_EX) only");
+        return UFEM_AF_ERR_TYP;
+      }
+      mat_var[item] = col;
+    } else if (ty == 3) {  // MONTE_VTYPE_NLD: first load with node/type/dir (fem/fem_mont.c:757-768)
+      for (size_t j = 0; j < m->loads.size(); j++)
+        if (m->loads[j].node == item && m->loads[j].type == sub && m->loads[j].dir == it) {
+          if (m->loads[j].type != 3) {
+            set_error("batched Monte Carlo randomises nodal forces (type 3) only");
+            return UFEM_AF_ERR_TYP;
+          }
+          load_var[j] = col;
+          break;
+        }
+    } else {
+      set_error("input variable type not on the batched path (MAT E and NLD forces only)");
+      return UFEM_AF_ERR_TYP;
+    }
+  }
+  std::vector<int> ev(m->eLen);
+  for (long e = 0; e < m->eLen; e++) ev[e] = mat_var[m->eMat[e]];
+  if ((rv = P->elem_var.upload(ev.data(), ev.size())) != UFEM_AF_OK) return rv;
+  std::vector<double> F0(m->nDOFAct, 0.0);
+  P->ovr_row.clear();
+  P->ovr_var.clear();
+  for (size_t j = 0; j < m->loads.size(); j++) {
+    const auto &l = m->loads[j];
+    if (l.type == 1 && l.val != 0.0) {
+      set_error("batched Monte Carlo needs zero-valued supports");
+      return UFEM_AF_ERR_TYP;
+    }
+    if (l.type != 3) continue;
+    long p = m->nDOFfld[l.node * KNOWN_DOFS + l.dir - 1];
+    if (p <= 0) continue;
+    if (load_var[j] >= 0) {
+      P->ovr_row.push_back((int)(p - 1));
+      P->ovr_var.push_back(load_var[j]);
+    } else {
+      F0[p - 1] += l.val;
+    }
+  }
+  if ((rv = P->F0.upload(F0.data(), F0.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_ovr_row.upload(P->ovr_row.data(), P->ovr_row.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_ovr_var.upload(P->ovr_var.data(), P->ovr_var.size())) != UFEM_AF_OK) return rv;
+  // outputs (fem/fem_mont.c:514-686)
+  P->outs.clear();
+  std::vector<int> ot, op, orow, oel, oip, ocomp;
+  for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
+    McOut o{(int)m->mc_type[i], (int)m->mc_pos[i - m->mc_ilen], -1, -1, 0, 0, -1};
+    if (o.pos < 0 || o.pos >= m->mc_olen) {
+      set_error("Monte Carlo output position out of range");
+      return UFEM_AF_ERR_VAL;
+    }
+    long item = m->mc_item[i], sub = m->mc_sub[i], it = m->mc_iter[i];
+    if (o.type == 8) {  // RES_D: u at node item, DOF sub
+      if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS)
+        o.row = (int)m->nDOFfld[item * KNOWN_DOFS + sub - 1] - 1;
+    } else if (o.type == 9) {  // RES_R: reaction of node item, DOF sub
+      for (size_t r = 0; r < m->reacNode.size(); r++)
+        if (m->reacNode[r] == item && m->reacDof[r] == sub) {
+          o.reac = (int)r;
+          o.row = m->reacRow[r];
+          break;
+        }
+    } else if (o.type == 10) {  // RES_E: element item, result type sub, point it
+      int nip = (m->etype == 2) ? 4 : 27;
+      int ns = (m->etype == 2) ? 3 : 6;
+      // stress result codes RES_SX.. (fem/fem_eres.h:39-44) in the element's order
+      static const int quad_map[3] = {7, 8, 10};
+      static const int brick_map[6] = {7, 8, 9, 11, 12, 10};
+      int comp = -1;
+      for (int c = 0; c < ns; c++)
+        if ((m->etype == 2 ? quad_map[c] : brick_map[c]) == sub) comp = c;
+      if (item < 0 || item >= m->eLen || it < 1 || it > nip || comp < 0) {
+        o.type = -1;  // unsupported result -> 0 (femGetEResVal returns 0, fem/fem_accs.c:269-273)
+      } else {
+        o.elem = (int)item;
+        o.ip = (int)it - 1;
+        o.comp = comp;
+      }
+    } else {
+      o.type = -1;  // other outputs report 0 on this path
+    }
+    P->outs.push_back(o);
+    ot.push_back(o.type); op.push_back(o.pos); orow.push_back(o.row);
+    oel.push_back(o.elem); oip.push_back(o.ip); ocomp.push_back(o.comp);
+  }
+  if ((rv = P->d_out_type.upload(ot.data(), ot.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_out_pos.upload(op.data(), op.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_out_row.upload(orow.data(), orow.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_out_elem.upload(oel.data(), oel.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_out_ip.upload(oip.data(), oip.size())) != UFEM_AF_OK) return rv;
+  if ((rv = P->d_out_comp.upload(ocomp.data(), ocomp.size())) != UFEM_AF_OK) return rv;
+  P->built = true;
+  return UFEM_AF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+template <typename T>
+struct VecOf;
+template <>
+struct VecOf<float> {
+  static constexpr int N = 4;
+  using V = float4;
+};
+template <>
+struct VecOf<double> {
+  static constexpr int N = 2;
+  using V = double2;
+};
+
+template <typename T>
+__device__ __forceinline__ void ldv(const T *p, T (&o)[VecOf<T>::N]);
+template <>
+__device__ __forceinline__ void ldv<float>(const float *p, float (&o)[4]) {
+  float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void ldv<double>(const double *p, double (&o)[2]) {
+  double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+  o[0] = v.x; o[1] = v.y;
+}
+// read-only for the whole kernel (matrix values): non-coherent path
+template <typename T>
+__device__ __forceinline__ void ldv_ro(const T *p, T (&o)[VecOf<T>::N]);
+template <>
+__device__ __forceinline__ void ldv_ro<float>(const float *p, float (&o)[4]) {
+  float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void ldv_ro<double>(const double *p, double (&o)[2]) {
+  double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+  o[0] = v.x; o[1] = v.y;
+}
+template <typename T>
+__device__ __forceinline__ void stv(T *p, const T (&o)[VecOf<T>::N]);
+template <>
+__device__ __forceinline__ void stv<float>(float *p, const float (&o)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+template <>
+__device__ __forceinline__ void stv<double>(double *p, const double (&o)[2]) {
+  *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
+}
+
+// E of every element for every sample: E[e*S + s]
+__global__ void k_make_E(int eLen, int S, int nsamp, long ilen, const double *__restrict__ ifld,
+                         const int *__restrict__ elem_var, const double *__restrict__ eE, double *__restrict__ E) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)eLen * S) return;
+  int e = (int)(t / S), s = (int)(t % S);
+  int v = elem_var[e];
+  E[t] = (v >= 0 && s < nsamp) ? ifld[(size_t)s * ilen + v] : eE[e];
+}
+
+// F for every sample (fem_add_loads order: fixed part, then the overridden
+// lines in input order); F at fixed DOFs is kept in Fval and zeroed.
+__global__ void k_make_F(int n, int S, int nsamp, long ilen, const double *__restrict__ ifld,
+                         const double *__restrict__ F0, int novr, const int *__restrict__ ovr_row,
+                         const int *__restrict__ ovr_var, double *__restrict__ F) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)n * S) return;
+  int i = (int)(t / S), s = (int)(t % S);
+  F[t] = (s < nsamp) ? F0[i] : 0.0;
+  if (s < nsamp)
+    for (int j = 0; j < novr; j++)
+      if (ovr_row[j] == i) F[t] += ifld[(size_t)s * ilen + ovr_var[j]];
+}
+
+__global__ void k_fix_F(int n, int S, const unsigned char *__restrict__ fixed, double *__restrict__ F) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)n * S) return;
+  if (fixed[t / S]) F[t] = 0.0;
+}
+
+// K_s = sum_e E_{s,e} K_e gathered per block; supports; FP64 and FP32 copies;
+// Jacobi diagonal.  grid (nnzb, S/128), block 128 threads = 128 samples.
+template <int B>
+__global__ void __launch_bounds__(128) k_assemble_batch(int S, int s_el, const int *__restrict__ blkrow,
+                                                        const int *__restrict__ colind,
+                                                        const int *__restrict__ gptr, const int *__restrict__ gel,
+                                                        const int *__restrict__ gpair,
+                                                        const double *__restrict__ Khat,
+                                                        const double *__restrict__ E,
+                                                        const unsigned char *__restrict__ fixed,
+                                                        double *__restrict__ V64, float *__restrict__ V32,
+                                                        double *__restrict__ M64, float *__restrict__ M32) {
+  const long k = blockIdx.x;
+  const int s = blockIdx.y * 128 + threadIdx.x;
+  const int I = blkrow[k], J = colind[k];
+  const int c0 = gptr[k], c1 = gptr[k + 1];
+  const int nn = s_el / B;
+  double acc[B * B];
+#pragma unroll
+  for (int t = 0; t < B * B; t++) acc[t] = 0.0;
+  for (int c = c0; c < c1; c++) {
+    const int e = __ldg(gel + c), p = __ldg(gpair + c);
+    const int a = p / nn, b = p % nn;
+    const double Ee = E[(size_t)e * S + s];
+    const double *kh = Khat + (size_t)e * s_el * s_el + (size_t)(a * B) * s_el + b * B;
+#pragma unroll
+    for (int i = 0; i < B; i++)
+#pragma unroll
+      for (int j = 0; j < B; j++) acc[i * B + j] += Ee * __ldg(kh + i * s_el + j);
+  }
+#pragma unroll
+  for (int i = 0; i < B; i++)
+#pragma unroll
+    for (int j = 0; j < B; j++) {
+      const int row = I * B + i, col = J * B + j;
+      double v = acc[i * B + j];
+      if (fixed[row] | fixed[col]) v = (row == col) ? 1.0 : 0.0;
+      const size_t o = ((size_t)k * B * B + i * B + j) * S + s;
+      V64[o] = v;
+      if (V32) V32[o] = (float)v;
+      if (row == col) {
+        if (M64) M64[(size_t)row * S + s] = v;
+        if (M32) M32[(size_t)row * S + s] = (float)v;
+      }
+    }
+}
+
+// r = F - K u in FP64 (and b32 = (float) r), partial |r|^2 and |F|^2 per
+// (8-row chunk, sample).  grid (ceil(nbr/8), S/64), block 256 = 8 warps.
+template <int B>
+__global__ void __launch_bounds__(kThreads) k_resid64(int nbr, int S, const int *__restrict__ rowptr,
+                                                      const int *__restrict__ colind,
+                                                      const double *__restrict__ V64,
+                                                      const double *__restrict__ F, const double *__restrict__ u,
+                                                      double *__restrict__ r, float *__restrict__ b32,
+                                                      double *__restrict__ part_rr, double *__restrict__ part_ff) {
+  __shared__ double s_rr[kWarps][64], s_ff[kWarps][64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kWarps + warp;
+  const int sb = blockIdx.y * 64 + lane * 2;
+  double rr[2] = {0, 0}, ff[2] = {0, 0};
+  if (I < nbr) {
+    double acc[B][2];
+#pragma unroll
+    for (int a = 0; a < B; a++) acc[a][0] = acc[a][1] = 0.0;
+    for (int k = rowptr[I]; k < rowptr[I + 1]; k++) {
+      const int J = colind[k];
+      double xv[B][2];
+#pragma unroll
+      for (int c = 0; c < B; c++) ldv<double>(u + (size_t)(J * B + c) * S + sb, xv[c]);
+#pragma unroll
+      for (int a = 0; a < B; a++)
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          double vv[2];
+          ldv_ro<double>(V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+          acc[a][0] += vv[0] * xv[c][0];
+          acc[a][1] += vv[1] * xv[c][1];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      const size_t o = (size_t)(I * B + a) * S + sb;
+      double f[2];
+      ldv<double>(F + o, f);
+      double rv[2] = {f[0] - acc[a][0], f[1] - acc[a][1]};
+      stv<double>(r + o, rv);
+      if (b32) {
+        b32[o] = (float)rv[0];
+        b32[o + 1] = (float)rv[1];
+      }
+      rr[0] += rv[0] * rv[0];
+      rr[1] += rv[1] * rv[1];
+      ff[0] += f[0] * f[0];
+      ff[1] += f[1] * f[1];
+    }
+  }
+  s_rr[warp][lane * 2] = rr[0];
+  s_rr[warp][lane * 2 + 1] = rr[1];
+  s_ff[warp][lane * 2] = ff[0];
+  s_ff[warp][lane * 2 + 1] = ff[1];
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    double a = 0, b = 0;
+    for (int w = 0; w < kWarps; w++) {
+      a += s_rr[w][threadIdx.x];
+      b += s_ff[w][threadIdx.x];
+    }
+    part_rr[(size_t)blockIdx.x * S + blockIdx.y * 64 + threadIdx.x] = a;
+    part_ff[(size_t)blockIdx.x * S + blockIdx.y * 64 + threadIdx.x] = b;
+  }
+}
+
+__global__ void k_sample_sum(int nchunks, int S, const double *__restrict__ part, double *__restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  double t = 0.0;
+  for (int c = 0; c < nchunks; c++) t += part[(size_t)c * S + s];
+  out[s] = t;
+}
+
+template <typename T>
+__global__ void k_correct(long n, int S, const int *__restrict__ solve, const T *__restrict__ d,
+                          double *__restrict__ u) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n * S) return;
+  if (solve[t % S]) u[t] += (double)d[t];
+}
+
+// ---------------------------------------------------------------------------
+// the persistent masked PCG over all meshes
+// ---------------------------------------------------------------------------
+enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4 };
+
+template <typename T>
+struct BMesh {
+  int nbr, S, ngroups, ntpg, rows_per_tile, B;
+  const int *rowptr, *colind;
+  const T *V, *M, *b;
+  T *x, *r, *z, *p0, *p1, *q;
+  T *part_pq, *part_rr, *part_rz;  // [ngroups*ntpg*GS], rr/rz doubled by parity
+  T *rho;                          // [2][S]
+  const T *tol2;                   // [S] squared absolute tolerance
+  int *state;                      // [S]
+  int *iters;                      // [S]
+  int *gactive;                    // [ngroups]
+};
+
+template <typename T>
+struct BArgs {
+  const BMesh<T> *meshes;
+  const int4 *tiles;  // (mesh, group, chunk, -)
+  int ntiles;
+  GridBar *bar;
+  int *active_count;
+  long maxit;
+  long *iter_out;
+};
+
+template <typename T, int B>
+__device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
+                                          T *pold, T *pnew, T (*s_red)[32 * VecOf<T>::N]) {
+  constexpr int VN = VecOf<T>::N;
+  constexpr int GS = 32 * VN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = M.S;
+  const int sb = g * GS + lane * VN;
+  const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
+  T beta[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) beta[v] = s_beta[lane * VN + v];
+  T pq[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) pq[v] = 0;
+  for (int I = row0 + warp; I < row1; I += kWarps) {
+    T acc[B][VN];
+#pragma unroll
+    for (int a = 0; a < B; a++)
+#pragma unroll
+      for (int v = 0; v < VN; v++) acc[a][v] = 0;
+    const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
+    for (int k = k0; k < k1; k++) {
+      const int J = __ldg(M.colind + k);
+      T xv[B][VN];
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
+        if (!first) {
+          T pv[VN];
+          ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
+#pragma unroll
+          for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < B; a++)
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          T vv[VN];
+          ldv_ro<T>(M.V + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+#pragma unroll
+          for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      const size_t o = (size_t)(I * B + a) * S + sb;
+      T zi[VN], pi[VN];
+      ldv<T>(M.z + o, zi);
+      if (!first) {
+        T po[VN];
+        ldv<T>(pold + o, po);
+#pragma unroll
+        for (int v = 0; v < VN; v++) pi[v] = zi[v] + beta[v] * po[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < VN; v++) pi[v] = zi[v];
+      }
+      stv<T>(pnew + o, pi);
+      stv<T>(M.q + o, acc[a]);
+#pragma unroll
+      for (int v = 0; v < VN; v++) pq[v] += pi[v] * acc[a][v];
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < VN; v++) s_red[warp][lane * VN + v] = pq[v];
+  __syncthreads();
+  if (threadIdx.x < GS) {
+    T t = 0;
+    for (int w = 0; w < kWarps; w++) t += s_red[w][threadIdx.x];
+    M.part_pq[((size_t)g * M.ntpg + chunk) * GS + threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+template <typename T, int B>
+__device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, T *pnew,
+                                            int par, bool init, T (*s_red)[32 * VecOf<T>::N],
+                                            T (*s_red2)[32 * VecOf<T>::N]) {
+  constexpr int VN = VecOf<T>::N;
+  constexpr int GS = 32 * VN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = M.S;
+  const int sb = g * GS + lane * VN;
+  const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
+  T alpha[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane * VN + v];
+  T rr[VN], rz[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
+  for (int I = row0 + warp; I < row1; I += kWarps) {
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      const size_t o = (size_t)(I * B + a) * S + sb;
+      T xi[VN], ri[VN], mi[VN], zi[VN];
+      ldv<T>(M.M + o, mi);
+      if (init) {  // x = 0, r = b, z = b / M (fem/fem_eqs.c:150-162 with x0 = 0)
+        ldv<T>(M.b + o, ri);
+#pragma unroll
+        for (int v = 0; v < VN; v++) xi[v] = 0;
+      } else {
+        T pi[VN], qi[VN];
+        ldv<T>(M.x + o, xi);
+        ldv<T>(M.r + o, ri);
+        ldv<T>(pnew + o, pi);
+        ldv<T>(M.q + o, qi);
+#pragma unroll
+        for (int v = 0; v < VN; v++) {
+          xi[v] = xi[v] + alpha[v] * pi[v];
+          ri[v] = ri[v] - alpha[v] * qi[v];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VN; v++) {
+        zi[v] = ri[v] / mi[v];
+        rr[v] += ri[v] * ri[v];
+        rz[v] += ri[v] * zi[v];
+      }
+      stv<T>(M.x + o, xi);
+      stv<T>(M.r + o, ri);
+      stv<T>(M.z + o, zi);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < VN; v++) {
+    s_red[warp][lane * VN + v] = rr[v];
+    s_red2[warp][lane * VN + v] = rz[v];
+  }
+  __syncthreads();
+  if (threadIdx.x < GS) {
+    T a = 0, b = 0;
+    for (int w = 0; w < kWarps; w++) {
+      a += s_red[w][threadIdx.x];
+      b += s_red2[w][threadIdx.x];
+    }
+    const size_t slot = (size_t)par * M.ngroups * M.ntpg * GS + ((size_t)g * M.ntpg + chunk) * GS + threadIdx.x;
+    M.part_rr[slot] = a;
+    M.part_rz[slot] = b;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ T group_total(const T *part, int g, int ntpg, int GS, int sl) {
+  T t = 0;
+  for (int c = 0; c < ntpg; c++) t += __ldcg(part + ((size_t)g * ntpg + c) * GS + sl);
+  return t;
+}
+
+template <typename T, int B>
+__global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
+  constexpr int VN = VecOf<T>::N;
+  constexpr int GS = 32 * VN;
+  __shared__ T s_red[kWarps][GS];
+  __shared__ T s_red2[kWarps][GS];
+  __shared__ T s_sc[GS];
+  __shared__ BMesh<T> s_m;
+  const int G = gridDim.x;
+  // phase 0: r = b, z = b / M, x = 0 and the partials of iteration 0
+  for (int t = blockIdx.x; t < A.ntiles; t += G) {
+    const int4 ti = A.tiles[t];
+    if (threadIdx.x == 0) s_m = A.meshes[ti.x];
+    __syncthreads();
+    const BMesh<T> &M = s_m;
+    int any = 0;
+    if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
+    any = __syncthreads_or(any);
+    if (any) tile_update<T, B>(M, ti.y, ti.z, s_sc, nullptr, 0, true, s_red, s_red2);
+    __syncthreads();
+  }
+  if (!grid_barrier(A.bar)) return;
+  long k;
+  for (k = 1;; k++) {
+    const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
+    const bool first = (k == 1);
+    // ---- phase S: convergence masks, beta, q = A p ------------------------
+    for (int t = blockIdx.x; t < A.ntiles; t += G) {
+      const int4 ti = A.tiles[t];
+      if (threadIdx.x == 0) s_m = A.meshes[ti.x];
+      __syncthreads();
+      const BMesh<T> &M = s_m;
+      const int g = ti.y;
+      int upd = 0;
+      if (threadIdx.x < GS) {
+        const int sl = threadIdx.x, s = g * GS + sl;
+        const size_t half = (size_t)M.ngroups * M.ntpg * GS;
+        const T rr = group_total(M.part_rr + (size_t)parm1 * half, g, M.ntpg, GS, sl);
+        const T rzn = group_total(M.part_rz + (size_t)parm1 * half, g, M.ntpg, GS, sl);
+        const T rzo = first ? T(1) : __ldcg(M.rho + (size_t)parm1 * M.S + s);
+        const int st = __ldcg(M.state + s);
+        int nst = st;
+        if (st == ST_ACTIVE) {
+          if (!(rr > M.tol2[s]) && rr == rr) nst = ST_CONV;
+          else if (!(rr == rr) || isinf(rr)) nst = ST_BREAK;
+          else if (k > A.maxit) nst = ST_MAXIT;
+        }
+        upd = (nst == ST_ACTIVE);
+        s_sc[sl] = upd ? (first ? T(0) : rzn / rzo) : T(0);
+        if (ti.z == 0) {  // the group's first tile records per-sample results
+          if (nst != st) {
+            M.state[s] = nst;
+            M.iters[s] = (int)(k - 1);
+          }
+          M.rho[(size_t)par * M.S + s] = rzn;
+        }
+      }
+      upd = __syncthreads_or(upd);
+      if (!upd) {
+        if (ti.z == 0 && threadIdx.x == 0 && M.gactive[g]) {
+          M.gactive[g] = 0;
+          atomicSub(A.active_count, 1);
+        }
+        __syncthreads();
+        continue;
+      }
+      T *pold = (k & 1) ? M.p0 : M.p1;
+      T *pnew = (k & 1) ? M.p1 : M.p0;
+      tile_spmv<T, B>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+    }
+    if (!grid_barrier(A.bar)) return;
+    // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
+    for (int t = blockIdx.x; t < A.ntiles; t += G) {
+      const int4 ti = A.tiles[t];
+      if (threadIdx.x == 0) s_m = A.meshes[ti.x];
+      __syncthreads();
+      const BMesh<T> &M = s_m;
+      const int g = ti.y;
+      int upd = 0;
+      if (threadIdx.x < GS) {
+        const int sl = threadIdx.x, s = g * GS + sl;
+        const int st = __ldcg(M.state + s);
+        T alpha = 0;
+        if (st == ST_ACTIVE) {
+          const T pq = group_total(M.part_pq, g, M.ntpg, GS, sl);
+          const T rho = __ldcg(M.rho + (size_t)par * M.S + s);
+          if (pq > T(0) && isfinite(pq)) {
+            alpha = rho / pq;
+            upd = 1;
+          } else if (ti.z == 0) {
+            M.state[s] = ST_BREAK;  // p.q <= 0: breakdown, the sample is frozen
+            M.iters[s] = (int)k;
+          }
+        }
+        s_sc[sl] = alpha;
+      }
+      upd = __syncthreads_or(upd);
+      // every tile of an active group writes its partials (samples with alpha = 0 keep their r)
+      int live = 0;
+      if (threadIdx.x < GS) live = (__ldcg(M.state + g * GS + threadIdx.x) == ST_ACTIVE);
+      live = __syncthreads_or(live) | upd;
+      if (!live) continue;
+      T *pnew = (k & 1) ? M.p1 : M.p0;
+      tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, false, s_red, s_red2);
+    }
+    if (!grid_barrier(A.bar)) return;
+    const int remaining = atomicAdd(A.active_count, 0);
+    if (remaining <= 0 || k > A.maxit + 1) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
+}
+
+// outputs: RES_D (u), RES_R (reaction = internal force - F at the support),
+// RES_E (stress at one integration point).  thread per (output, sample).
+template <int B>
+__global__ void k_outputs(int nout, int S, int nsamp, long olen, const int *__restrict__ otype,
+                          const int *__restrict__ opos, const int *__restrict__ orow, const int *__restrict__ oel,
+                          const int *__restrict__ oip, const int *__restrict__ ocomp, const double *__restrict__ u,
+                          const int *__restrict__ rowptr, const int *__restrict__ colind,
+                          const int *__restrict__ gptr, const int *__restrict__ gel, const int *__restrict__ gpair,
+                          int s_el, const double *__restrict__ Khat, const double *__restrict__ E,
+                          const double *__restrict__ Fraw, const double *__restrict__ xyz,
+                          const int *__restrict__ enodes, const int *__restrict__ node_rank,
+                          const double *__restrict__ eNu, const double *__restrict__ eThick, int etype,
+                          double *__restrict__ ofld) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)nout * nsamp) return;
+  const int o = (int)(t / nsamp), s = (int)(t % nsamp);
+  const int ty = otype[o];
+  double val = 0.0;
+  if (ty == 8) {
+    const int row = orow[o];
+    if (row >= 0) val = u[(size_t)row * S + s];
+  } else if (ty == 9) {
+    const int row = orow[o];
+    if (row >= 0) {
+      const int I = row / B, a = row % B, nn = s_el / B;
+      double fint = 0.0;
+      for (int k = rowptr[I]; k < rowptr[I + 1]; k++) {
+        const int J = colind[k];
+        for (int c = gptr[k]; c < gptr[k + 1]; c++) {
+          const int e = gel[c], p = gpair[c], la = p / nn, lb = p % nn;
+          const double *kh = Khat + (size_t)e * s_el * s_el + (size_t)(la * B + a) * s_el + lb * B;
+          double acc = 0.0;
+          for (int j = 0; j < B; j++) acc += kh[j] * u[(size_t)(J * B + j) * S + s];
+          fint += E[(size_t)e * S + s] * acc;
+        }
+      }
+      val = (0.0 - Fraw[(size_t)row * S + s]) + fint;
+    }
+  } else if (ty == 10) {
+    const int e = oel[o], ip = oip[o], comp = ocomp[o];
+    const double Ee = E[(size_t)e * S + s], nu = eNu[e];
+    if (etype == 9) {
+      const double gp[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+      const double nc[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                               {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+      const double x = gp[ip / 9], y = gp[(ip / 3) % 3], z = gp[ip % 3];
+      double dN[8][3], X[8][3], J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int n = 0; n < 8; n++) {
+        dN[n][0] = 0.125 * nc[n][0] * (1.0 + nc[n][1] * y) * (1.0 + nc[n][2] * z);
+        dN[n][1] = 0.125 * nc[n][1] * (1.0 + nc[n][0] * x) * (1.0 + nc[n][2] * z);
+        dN[n][2] = 0.125 * nc[n][2] * (1.0 + nc[n][0] * x) * (1.0 + nc[n][1] * y);
+        for (int d = 0; d < 3; d++) X[n][d] = xyz[3 * (size_t)enodes[(size_t)e * 8 + n] + d];
+      }
+      for (int a = 0; a < 3; a++)
+        for (int c = 0; c < 3; c++)
+          for (int n = 0; n < 8; n++) J[a][c] += dN[n][a] * X[n][c];
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double id = 1.0 / (J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02);
+      const double inv[3][3] = {{c00 * id, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id,
+                                 (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id},
+                                {c01 * id, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id,
+                                 (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id},
+                                {c02 * id, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id,
+                                 (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id}};
+      double ep[6] = {0, 0, 0, 0, 0, 0};
+      for (int n = 0; n < 8; n++) {
+        double g[3];
+        for (int d = 0; d < 3; d++) g[d] = inv[d][0] * dN[n][0] + inv[d][1] * dN[n][1] + inv[d][2] * dN[n][2];
+        const size_t r0 = (size_t)node_rank[enodes[(size_t)e * 8 + n]] * 3;
+        const double ux = u[(r0)*S + s], uy = u[(r0 + 1) * S + s], uz = u[(r0 + 2) * S + s];
+        ep[0] += g[0] * ux; ep[1] += g[1] * uy; ep[2] += g[2] * uz;
+        ep[3] += g[2] * uy + g[1] * uz; ep[4] += g[2] * ux + g[0] * uz; ep[5] += g[1] * ux + g[0] * uy;
+      }
+      const double d1 = (Ee * (1.0 - nu)) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+      const double d2 = (Ee * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+      const double d3 = Ee / (2.0 * (1 + nu));
+      const double sg[6] = {d1 * ep[0] + d2 * ep[1] + d2 * ep[2], d2 * ep[0] + d1 * ep[1] + d2 * ep[2],
+                            d2 * ep[0] + d2 * ep[1] + d1 * ep[2], d3 * ep[3], d3 * ep[4], d3 * ep[5]};
+      val = sg[comp];
+    } else {
+      const double qg = 0.577350569189626;
+      const double sx_ = (ip >> 1) ? qg : -qg, tx_ = (ip & 1) ? qg : -qg;
+      const double dS[4] = {(-1.0 + tx_) * 0.25, (1.0 - tx_) * 0.25, (1.0 + tx_) * 0.25, (-1.0 - tx_) * 0.25};
+      const double dT[4] = {(-1.0 + sx_) * 0.25, (-1.0 - sx_) * 0.25, (1.0 + sx_) * 0.25, (1.0 - sx_) * 0.25};
+      double j00 = 0, j01 = 0, j10 = 0, j11 = 0, X[4][2];
+      for (int n = 0; n < 4; n++) {
+        X[n][0] = xyz[3 * (size_t)enodes[(size_t)e * 4 + n]];
+        X[n][1] = xyz[3 * (size_t)enodes[(size_t)e * 4 + n] + 1];
+        j00 += dS[n] * X[n][0]; j01 += dS[n] * X[n][1]; j10 += dT[n] * X[n][0]; j11 += dT[n] * X[n][1];
+      }
+      const double det = j00 * j11 - j01 * j10;
+      double ex = 0, ey = 0, gxy = 0;
+      for (int n = 0; n < 4; n++) {
+        const double gx = (j11 / det) * dS[n] + (-j01 / det) * dT[n];
+        const double gy = (-j10 / det) * dS[n] + (j00 / det) * dT[n];
+        const size_t r0 = (size_t)node_rank[enodes[(size_t)e * 4 + n]] * 2;
+        const double ux = u[r0 * S + s], uy = u[(r0 + 1) * S + s];
+        ex += gx * ux; ey += gy * uy; gxy += gy * ux + gx * uy;
+      }
+      double Mul, D0, D1, D2, D3;
+      if (eThick[e] > 0.0) {
+        Mul = Ee / (1 - nu * nu); D0 = Mul; D1 = Mul * nu; D2 = Mul; D3 = Mul * 0.5 * (1 - nu);
+      } else {
+        Mul = Ee / ((1 + nu) * (1 - 2 * nu)); D0 = Mul * (1 - nu); D1 = Mul * nu; D2 = Mul * (1 - nu);
+        D3 = Mul * 0.5 * (1 - nu);
+      }
+      const double sg[3] = {D0 * ex + D1 * ey, D1 * ex + D2 * ey, D3 * gxy};
+      val = sg[comp];
+    }
+  }
+  ofld[(size_t)s * olen + opos[o]] = val;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+struct McWork {
+  int S = 0, nsamp = 0, ngroups = 0, GS = 0;
+  DBuf<double> E, F, Fraw, V64, M64, u64, r64, part_rr, part_ff, rr, ff;
+  DBuf<float> V32, M32, b32;
+  // inner vectors in the inner precision
+  DBuf<float> fx, fr, fz, fp0, fp1, fq, fpq, fprr, fprz, frho, ftol2;
+  DBuf<double> dx, dr, dz, dp0, dp1, dq, dpq, dprr, dprz, drho, dtol2, db;
+  DBuf<int> state, iters, solve;
+  DBuf<int> gactive;
+  std::vector<int> h_state, h_iters;
+  std::vector<double> h_rr, h_ff;
+};
+
+static ufem_mc_stats g_stats;
+
+extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
+  o->precision = 1;
+  o->tol = 1e-8;
+  o->inner_tol = 1e-4;
+  o->max_iters = 20000;
+  o->max_refine = 6;
+  o->use_graphs = 0;
+}
+
+extern "C" int ufem_mc_get_stats(ufem_mc_stats *s) {
+  *s = g_stats;
+  return UFEM_AF_OK;
+}
+
+namespace {
+
+struct EvTimer {
+  cudaEvent_t a, b;
+  EvTimer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+  }
+  double stop() {
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EvTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+template <typename T>
+int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, const ufem_mc_options &opt,
+              long remaining_cap, long *iters_run) {
+  constexpr int VN = VecOf<T>::N, GS = 32 * VN;
+  int rv;
+  std::vector<BMesh<T>> hm(nmesh);
+  std::vector<int4> tiles;
+  int dev = 0, nsm = 0, occ = 0;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int B = models[0]->b;
+  void (*kern)(BArgs<T>) = (B == 3) ? k_batch_pcg<T, 3> : k_batch_pcg<T, 2>;
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  if (occ < 1) {
+    set_error("batched PCG kernel does not fit on an SM");
+    return UFEM_AF_ERR;
+  }
+  const int G = nsm * std::min(occ, 2);
+  // rows per tile: about two tiles per block over the whole batch
+  long total_rows = 0;
+  for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k].S / GS);
+  int rpt = (int)std::max<long>(kWarps, (total_rows + 2L * G - 1) / (2L * G));
+  rpt = (rpt + kWarps - 1) / kWarps * kWarps;
+  int active_groups = 0;
+  for (int k = 0; k < nmesh; k++) {
+    ufem_model *m = models[k];
+    McWork &w = W[k];
+    BMesh<T> &b = hm[k];
+    b.nbr = m->nbr;
+    b.S = w.S;
+    b.ngroups = w.S / GS;
+    b.rows_per_tile = rpt;
+    b.ntpg = (m->nbr + rpt - 1) / rpt;
+    b.B = m->b;
+    b.rowptr = m->d_rowptr.p;
+    b.colind = m->d_colind.p;
+    const size_t n = (size_t)m->nDOFAct * w.S;
+    const size_t np = (size_t)b.ngroups * b.ntpg * GS;
+    if constexpr (sizeof(T) == 4) {
+      b.V = w.V32.p;
+      b.M = w.M32.p;
+      b.b = w.b32.p;
+      if ((rv = w.fx.alloc(n)) || (rv = w.fr.alloc(n)) || (rv = w.fz.alloc(n)) || (rv = w.fp0.alloc(n)) ||
+          (rv = w.fp1.alloc(n)) || (rv = w.fq.alloc(n)) || (rv = w.fpq.alloc(np)) || (rv = w.fprr.alloc(2 * np)) ||
+          (rv = w.fprz.alloc(2 * np)) || (rv = w.frho.alloc(2 * w.S)) || (rv = w.ftol2.alloc(w.S)))
+        return rv;
+      b.x = w.fx.p; b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
+      b.part_pq = w.fpq.p; b.part_rr = w.fprr.p; b.part_rz = w.fprz.p; b.rho = w.frho.p; b.tol2 = w.ftol2.p;
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.fp0.p, 0, n * sizeof(T)));
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.fp1.p, 0, n * sizeof(T)));
+    } else {
+      b.V = w.V64.p;
+      b.M = w.M64.p;
+      if ((rv = w.db.alloc(n)) != UFEM_AF_OK) return rv;
+      UFEM_CUDA_TRY(cudaMemcpyAsync(w.db.p, w.r64.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+      b.b = w.db.p;
+      if ((rv = w.dx.alloc(n)) || (rv = w.dr.alloc(n)) || (rv = w.dz.alloc(n)) || (rv = w.dp0.alloc(n)) ||
+          (rv = w.dp1.alloc(n)) || (rv = w.dq.alloc(n)) || (rv = w.dpq.alloc(np)) || (rv = w.dprr.alloc(2 * np)) ||
+          (rv = w.dprz.alloc(2 * np)) || (rv = w.drho.alloc(2 * w.S)) || (rv = w.dtol2.alloc(w.S)))
+        return rv;
+      b.x = w.dx.p; b.r = w.dr.p; b.z = w.dz.p; b.p0 = w.dp0.p; b.p1 = w.dp1.p; b.q = w.dq.p;
+      b.part_pq = w.dpq.p; b.part_rr = w.dprr.p; b.part_rz = w.dprz.p; b.rho = w.drho.p; b.tol2 = w.dtol2.p;
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.dp0.p, 0, n * sizeof(T)));
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.dp1.p, 0, n * sizeof(T)));
+    }
+    b.state = w.state.p;
+    b.iters = w.iters.p;
+    if ((rv = w.gactive.alloc(b.ngroups)) != UFEM_AF_OK) return rv;
+    b.gactive = w.gactive.p;
+    // per-sample tolerance and state on the host
+    std::vector<T> tol2(w.S);
+    std::vector<int> st(w.S), ga(b.ngroups, 0);
+    for (int s = 0; s < w.S; s++) {
+      const bool solve = w.h_state[s] == ST_ACTIVE;
+      const double rn = std::sqrt(w.h_rr[s]), fn = std::sqrt(w.h_ff[s]);
+      const double target = std::max(opt.inner_tol * rn, 0.25 * opt.tol * fn);
+      tol2[s] = (T)(target * target);
+      st[s] = solve ? ST_ACTIVE : ST_SKIP;
+      if (solve) ga[s / GS] = 1;
+    }
+    for (int g = 0; g < b.ngroups; g++) active_groups += ga[g];
+    UFEM_CUDA_TRY(cudaMemcpyAsync((void *)b.tol2, tol2.data(), w.S * sizeof(T), cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemcpyAsync(w.state.p, st.data(), w.S * sizeof(int), cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemsetAsync(w.iters.p, 0, w.S * sizeof(int)));
+    UFEM_CUDA_TRY(cudaMemcpyAsync(w.gactive.p, ga.data(), b.ngroups * sizeof(int), cudaMemcpyHostToDevice));
+    for (int g = 0; g < b.ngroups; g++)
+      for (int c = 0; c < b.ntpg; c++) tiles.push_back(make_int4(k, g, c, 0));
+  }
+  if (active_groups == 0) {
+    *iters_run = 0;
+    return UFEM_AF_OK;
+  }
+  DBuf<BMesh<T>> d_meshes;
+  DBuf<int4> d_tiles;
+  DBuf<GridBar> bar;
+  DBuf<int> cnt;
+  DBuf<long> itout;
+  if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
+      (rv = bar.alloc(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = itout.alloc(1)))
+    return rv;
+  UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
+  BArgs<T> a;
+  a.meshes = d_meshes.p;
+  a.tiles = d_tiles.p;
+  a.ntiles = (int)tiles.size();
+  a.bar = bar.p;
+  a.active_count = cnt.p;
+  a.maxit = remaining_cap;
+  a.iter_out = itout.p;
+  void *args[] = {&a};
+  const int grid = std::min<int>(G, (int)tiles.size());
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kThreads), args, 0, 0));
+  g_stats.kernel_launches += 1;
+  long its = 0;
+  GridBar hb;
+  UFEM_CUDA_TRY(cudaMemcpy(&its, itout.p, sizeof(long), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+  if (hb.err) {
+    set_error("batched PCG: grid barrier timed out");
+    return UFEM_AF_ERR;
+  }
+  *iters_run = its;
+  // algorithmic bytes of the iterations run (sample-weighted by the mesh sizes)
+  for (int k = 0; k < nmesh; k++) {
+    const ufem_model *m = models[k];
+    const double S = W[k].S, n = (double)m->nDOFAct, bb = m->b * m->b;
+    const double spmv = m->nnzb * (bb * sizeof(T) * S + 4.0) + 4.0 * (m->nbr + 1) + 2.0 * n * S * sizeof(T);
+    g_stats.spmv_bytes += spmv * its;
+    g_stats.pcg_bytes += (spmv + 11.0 * n * S * sizeof(T)) * its;
+  }
+  return UFEM_AF_OK;
+}
+
+}  // namespace
+
+int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *d_ifld,
+                    double *const *d_ofld, int *const *d_status, long *const *d_iters,
+                    const double *const *d_u_guess, double *const *d_u_out, const ufem_mc_options *opt_in) {
+  ufem_mc_options opt;
+  if (opt_in) opt = *opt_in;
+  else ufem_mc_default_options(&opt);
+  std::memset(&g_stats, 0, sizeof(g_stats));
+  int rv;
+  if (nmesh < 1) return UFEM_AF_ERR_SIZ;
+  const int B = models[0]->b;
+  for (int k = 0; k < nmesh; k++)
+    if (models[k]->b != B) {
+      set_error("all meshes of one batched launch must have the same element family");
+      return UFEM_AF_ERR_TYP;
+    }
+  EvTimer total;
+  std::vector<McWork> W(nmesh);
+  std::vector<McPlan *> plans(nmesh);
+  // ---- plans, inputs and batched assembly --------------------------------
+  {
+    EvTimer t;
+    for (int k = 0; k < nmesh; k++) {
+      ufem_model *m = models[k];
+      McPlan *P = get_plan(m);
+      if (!P->built && (rv = build_plan(m, P)) != UFEM_AF_OK) return rv;
+      plans[k] = P;
+      McWork &w = W[k];
+      const int GSf = (opt.precision == 0) ? 64 : 128;
+      w.nsamp = (int)nsamp[k];
+      w.S = std::max(GSf, (int)((nsamp[k] + 127) / 128 * 128));
+      w.GS = GSf;
+      const size_t n = (size_t)m->nDOFAct * w.S, nv = (size_t)m->nnzb * B * B * w.S;
+      if ((rv = w.E.alloc((size_t)m->eLen * w.S)) || (rv = w.F.alloc(n)) || (rv = w.Fraw.alloc(n)) ||
+          (rv = w.V64.alloc(nv)) || (rv = w.M64.alloc(n)) || (rv = w.u64.alloc(n)) || (rv = w.r64.alloc(n)) ||
+          (rv = w.state.alloc(w.S)) || (rv = w.iters.alloc(w.S)) || (rv = w.solve.alloc(w.S)) ||
+          (rv = w.rr.alloc(w.S)) || (rv = w.ff.alloc(w.S)))
+        return rv;
+      if (opt.precision != 0) {
+        if ((rv = w.V32.alloc(nv)) || (rv = w.M32.alloc(n)) || (rv = w.b32.alloc(n))) return rv;
+      }
+      const long ne = (long)m->eLen * w.S;
+      k_make_E<<<(unsigned)((ne + 255) / 256), 256>>>((int)m->eLen, w.S, w.nsamp, P->ilen, d_ifld[k],
+                                                      P->elem_var.p, m->d_eE.p, w.E.p);
+      k_make_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, w.nsamp, P->ilen, d_ifld[k], P->F0.p,
+                                                     (int)P->ovr_row.size(), P->d_ovr_row.p, P->d_ovr_var.p,
+                                                     w.Fraw.p);
+      UFEM_CUDA_TRY(cudaMemcpyAsync(w.F.p, w.Fraw.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+      k_fix_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, m->d_fixed.p, w.F.p);
+      dim3 ga((unsigned)m->nnzb, (unsigned)(w.S / 128));
+      if (B == 3)
+        k_assemble_batch<3><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
+                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, w.V32.p, w.M64.p,
+                                         w.M32.p);
+      else
+        k_assemble_batch<2><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
+                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, w.V32.p, w.M64.p,
+                                         w.M32.p);
+      g_stats.kernel_launches += 5;
+      // initial guess
+      if (d_u_guess && d_u_guess[k]) {
+        UFEM_CUDA_TRY(cudaMemcpyAsync(w.u64.p, d_u_guess[k], n * sizeof(double), cudaMemcpyDeviceToDevice));
+      } else {
+        UFEM_CUDA_TRY(cudaMemsetAsync(w.u64.p, 0, n * sizeof(double)));
+      }
+      if ((rv = w.part_rr.alloc((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)) ||
+          (rv = w.part_ff.alloc((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)))
+        return rv;
+      w.h_state.assign(w.S, ST_SKIP);
+      w.h_iters.assign(w.S, 0);
+      w.h_rr.assign(w.S, 0.0);
+      w.h_ff.assign(w.S, 0.0);
+      for (int s = 0; s < w.nsamp; s++) w.h_state[s] = ST_ACTIVE;
+    }
+    UFEM_CUDA_TRY(cudaGetLastError());
+    g_stats.ms_assemble = t.stop();
+  }
+  // ---- FP64 refinement around the inner PCG -----------------------------
+  std::vector<std::vector<long>> it_acc(nmesh);
+  std::vector<std::vector<int>> final_status(nmesh);
+  for (int k = 0; k < nmesh; k++) {
+    it_acc[k].assign(W[k].S, 0);
+    final_status[k].assign(W[k].S, UFEM_ST_MAXIT);
+  }
+  long iter_total = 0;
+  for (int step = 0; step <= opt.max_refine; step++) {
+    // r = f - K u (FP64), per-sample |r| and |f|
+    {
+      EvTimer t;
+      for (int k = 0; k < nmesh; k++) {
+        ufem_model *m = models[k];
+        McWork &w = W[k];
+        const int nch = (m->nbr + kWarps - 1) / kWarps;
+        dim3 gr((unsigned)nch, (unsigned)(w.S / 64));
+        float *b32 = (opt.precision != 0) ? w.b32.p : nullptr;
+        if (B == 3)
+          k_resid64<3><<<gr, kThreads>>>(m->nbr, w.S, m->d_rowptr.p, m->d_colind.p, w.V64.p, w.F.p, w.u64.p,
+                                         w.r64.p, b32, w.part_rr.p, w.part_ff.p);
+        else
+          k_resid64<2><<<gr, kThreads>>>(m->nbr, w.S, m->d_rowptr.p, m->d_colind.p, w.V64.p, w.F.p, w.u64.p,
+                                         w.r64.p, b32, w.part_rr.p, w.part_ff.p);
+        k_sample_sum<<<(w.S + 127) / 128, 128>>>(nch, w.S, w.part_rr.p, w.rr.p);
+        k_sample_sum<<<(w.S + 127) / 128, 128>>>(nch, w.S, w.part_ff.p, w.ff.p);
+        g_stats.kernel_launches += 3;
+        UFEM_CUDA_TRY(cudaMemcpyAsync(w.h_rr.data(), w.rr.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
+        UFEM_CUDA_TRY(cudaMemcpyAsync(w.h_ff.data(), w.ff.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
+      }
+      UFEM_CUDA_TRY(cudaDeviceSynchronize());
+      g_stats.ms_refine += t.stop();
+    }
+    bool any = false;
+    for (int k = 0; k < nmesh; k++) {
+      McWork &w = W[k];
+      for (int s = 0; s < w.nsamp; s++) {
+        if (w.h_state[s] != ST_ACTIVE) continue;
+        const double rel = (w.h_ff[s] > 0) ? std::sqrt(w.h_rr[s] / w.h_ff[s]) : 0.0;
+        if (!(rel == rel)) {
+          w.h_state[s] = ST_BREAK;
+          final_status[k][s] = UFEM_ST_NAN;
+        } else if (rel <= opt.tol) {
+          w.h_state[s] = ST_CONV;
+          final_status[k][s] = UFEM_ST_CONVERGED;
+        } else if (step == opt.max_refine || it_acc[k][s] >= opt.max_iters) {
+          w.h_state[s] = ST_MAXIT;
+          final_status[k][s] = UFEM_ST_MAXIT;
+        } else {
+          any = true;
+        }
+      }
+    }
+    if (!any) break;
+    // inner solve of K d = r for the samples still active
+    long its = 0;
+    {
+      EvTimer t;
+      long cap = opt.max_iters - iter_total;
+      if (cap < 1) cap = 1;
+      if (opt.precision != 0) rv = run_inner<float>(nmesh, models, W, opt, cap, &its);
+      else rv = run_inner<double>(nmesh, models, W, opt, cap, &its);
+      if (rv != UFEM_AF_OK) return rv;
+      g_stats.ms_pcg += t.stop();
+    }
+    iter_total += its;
+    g_stats.pcg_iterations += its;
+    {
+      EvTimer t;
+      for (int k = 0; k < nmesh; k++) {
+        ufem_model *m = models[k];
+        McWork &w = W[k];
+        std::vector<int> solve(w.S), st(w.S), itv(w.S);
+        UFEM_CUDA_TRY(cudaMemcpy(st.data(), w.state.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+        UFEM_CUDA_TRY(cudaMemcpy(itv.data(), w.iters.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < w.S; s++) {
+          solve[s] = (w.h_state[s] == ST_ACTIVE) && st[s] != ST_SKIP;
+          if (solve[s]) it_acc[k][s] += (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
+        }
+        UFEM_CUDA_TRY(cudaMemcpy(w.solve.p, solve.data(), w.S * sizeof(int), cudaMemcpyHostToDevice));
+        const long n = (long)m->nDOFAct * w.S;
+        if (opt.precision != 0)
+          k_correct<float><<<(unsigned)((n + 255) / 256), 256>>>(m->nDOFAct, w.S, w.solve.p, w.fx.p, w.u64.p);
+        else
+          k_correct<double><<<(unsigned)((n + 255) / 256), 256>>>(m->nDOFAct, w.S, w.solve.p, w.dx.p, w.u64.p);
+        g_stats.kernel_launches += 1;
+      }
+      UFEM_CUDA_TRY(cudaGetLastError());
+      g_stats.ms_refine += t.stop();
+    }
+  }
+  // ---- outputs -------------------------------------------------------------
+  {
+    EvTimer t;
+    for (int k = 0; k < nmesh; k++) {
+      ufem_model *m = models[k];
+      McWork &w = W[k];
+      McPlan *P = plans[k];
+      const int nout = (int)P->outs.size();
+      if (d_ofld && d_ofld[k] && nout > 0 && w.nsamp > 0) {
+        const long tot = (long)nout * w.nsamp;
+        if (B == 3)
+          k_outputs<3><<<(unsigned)((tot + 127) / 128), 128>>>(
+              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
+              P->d_out_ip.p, P->d_out_comp.p, w.u64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
+              P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
+              m->d_eThick.p, m->etype, d_ofld[k]);
+        else
+          k_outputs<2><<<(unsigned)((tot + 127) / 128), 128>>>(
+              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
+              P->d_out_ip.p, P->d_out_comp.p, w.u64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
+              P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
+              m->d_eThick.p, m->etype, d_ofld[k]);
+        g_stats.kernel_launches += 1;
+      }
+      if (d_u_out && d_u_out[k])
+        UFEM_CUDA_TRY(cudaMemcpyAsync(d_u_out[k], w.u64.p, (size_t)m->nDOFAct * w.S * sizeof(double),
+                                      cudaMemcpyDeviceToDevice));
+      std::vector<int> st(w.nsamp);
+      std::vector<long> it(w.nsamp);
+      for (int s = 0; s < w.nsamp; s++) {
+        st[s] = final_status[k][s];
+        it[s] = it_acc[k][s];
+      }
+      if (d_status && d_status[k] && w.nsamp > 0)
+        UFEM_CUDA_TRY(cudaMemcpy(d_status[k], st.data(), w.nsamp * sizeof(int), cudaMemcpyHostToDevice));
+      if (d_iters && d_iters[k] && w.nsamp > 0)
+        UFEM_CUDA_TRY(cudaMemcpy(d_iters[k], it.data(), w.nsamp * sizeof(long), cudaMemcpyHostToDevice));
+    }
+    UFEM_CUDA_TRY(cudaGetLastError());
+    g_stats.ms_outputs = t.stop();
+  }
+  g_stats.ms_total = total.stop();
+  return UFEM_AF_OK;
+}
+
+}  // namespace ufem
+
+using namespace ufem;
+
+extern "C" int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp,
+                                    const double *const *d_ifld, double *const *d_ofld, int *const *d_status,
+                                    long *const *d_iters, const double *const *d_u_guess,
+                                    double *const *d_u_out, const ufem_mc_options *opt) {
+  return mc_solve_device(nmesh, models, nsamp, d_ifld, d_ofld, d_status, d_iters, d_u_guess, d_u_out, opt);
+}
+
+// The same with host buffers: inputs are copied to the device, results back.
+extern "C" int ufem_mc_solve(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *ifld,
+                             double *const *ofld, int *const *status, long *const *iters,
+                             const double *const *u_guess, const ufem_mc_options *opt) {
+  int rv;
+  std::vector<std::unique_ptr<DBuf<double>>> di, dof, dg;
+  std::vector<std::unique_ptr<DBuf<int>>> ds;
+  std::vector<std::unique_ptr<DBuf<long>>> dit;
+  std::vector<const double *> pi(nmesh), pg(nmesh, nullptr);
+  std::vector<double *> po(nmesh);
+  std::vector<int *> ps(nmesh);
+  std::vector<long *> pit(nmesh);
+  for (int k = 0; k < nmesh; k++) {
+    ufem_model *m = models[k];
+    di.emplace_back(new DBuf<double>());
+    dof.emplace_back(new DBuf<double>());
+    dg.emplace_back(new DBuf<double>());
+    ds.emplace_back(new DBuf<int>());
+    dit.emplace_back(new DBuf<long>());
+    if ((rv = di[k]->upload(ifld[k], (size_t)nsamp[k] * m->mc_ilen)) != UFEM_AF_OK) return rv;
+    if ((rv = dof[k]->alloc((size_t)nsamp[k] * std::max<long>(1, m->mc_olen))) != UFEM_AF_OK) return rv;
+    if ((rv = ds[k]->alloc(nsamp[k])) != UFEM_AF_OK) return rv;
+    if ((rv = dit[k]->alloc(nsamp[k])) != UFEM_AF_OK) return rv;
+    pi[k] = di[k]->p;
+    po[k] = dof[k]->p;
+    ps[k] = ds[k]->p;
+    pit[k] = dit[k]->p;
+    if (u_guess && u_guess[k]) {
+      // host guesses are sample-major [nsamp][ndof]; the device layout is [ndof][S]
+      const int S = (int)std::max<long>(128, (nsamp[k] + 127) / 128 * 128);
+      std::vector<double> t((size_t)m->nDOFAct * S, 0.0);
+      for (long s = 0; s < nsamp[k]; s++)
+        for (long i = 0; i < m->nDOFAct; i++) t[(size_t)i * S + s] = u_guess[k][(size_t)s * m->nDOFAct + i];
+      if ((rv = dg[k]->upload(t.data(), t.size())) != UFEM_AF_OK) return rv;
+      pg[k] = dg[k]->p;
+    }
+  }
+  rv = mc_solve_device(nmesh, models, nsamp, pi.data(), po.data(), ps.data(), pit.data(), pg.data(), nullptr, opt);
+  if (rv != UFEM_AF_OK) return rv;
+  for (int k = 0; k < nmesh; k++) {
+    ufem_model *m = models[k];
+    if (ofld && ofld[k] && m->mc_olen > 0)
+      UFEM_CUDA_TRY(cudaMemcpy(ofld[k], po[k], (size_t)nsamp[k] * m->mc_olen * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+    if (status && status[k]) UFEM_CUDA_TRY(cudaMemcpy(status[k], ps[k], nsamp[k] * sizeof(int), cudaMemcpyDeviceToHost));
+    if (iters && iters[k]) UFEM_CUDA_TRY(cudaMemcpy(iters[k], pit[k], nsamp[k] * sizeof(long), cudaMemcpyDeviceToHost));
+  }
+  return UFEM_AF_OK;
+}

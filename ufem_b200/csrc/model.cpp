@@ -1,0 +1,602 @@
+// Host-side model construction for libufem_gpu.so: table checks, DOF
+// numbering, block-sparse pattern, element colouring, element->block scatter
+// map, supports/loads bookkeeping and the preparsed input reader.
+//
+// Reference interfaces restated here:
+//   femReadInput           fem/fem_io.c:380-590 (preparsed variant, fem/feminput.5)
+//   femReadInputLoads      fem/fem_io.c:86-165
+//   fem_monte_read_data    fem/fem_mont.c:866-905
+//   fem_dofs               fem/fem_sol.c:1263-1395
+//   femKhit / femKpos      fem/fem_mloc.c:52-116
+//   femMatPutAdd order     fem/fem_math.c:185-236 (first-touch column order)
+//   fem_sol_res_alloc      fem/fem_sol.c:676-722 (reaction list)
+//   femGetRepVal           fem/fem_accs.c:196-288 (value lookup by position)
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+
+#include "ufem_internal.h"
+
+namespace ufem {
+
+static std::mutex g_err_mu;
+static std::string g_err;
+
+void set_error(const std::string &msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_err = msg;
+}
+
+const char *last_error() {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return g_err.c_str();
+}
+
+static int elem_nodes(long t) { return t == 2 ? 4 : 8; }
+static int elem_dofs(long t) { return t == 2 ? 2 : 3; }
+
+// Value of entry `idx` of a record, 0 when the record is shorter: the
+// non-repeating branch of femGetRepVal (fem/fem_accs.c:236-252, :269-273).
+static double rec_val(const std::vector<double> &rec, size_t idx) {
+  return idx < rec.size() ? rec[idx] : 0.0;
+}
+
+int model_from_tables(const ufem_tables *t, ufem_model *m) {
+  if (!t || t->nLen < 2 || t->eLen < 1) {
+    set_error("model tables: fewer than 2 nodes or no elements");
+    return UFEM_AF_ERR_SML;  // fem/fem_io.c:516, :534
+  }
+  m->nLen = t->nLen;
+  m->eLen = t->eLen;
+  m->xyz.resize(3 * m->nLen);
+  for (long i = 0; i < m->nLen; i++) {
+    m->xyz[3 * i] = t->n_x[i];
+    m->xyz[3 * i + 1] = t->n_y[i];
+    m->xyz[3 * i + 2] = t->n_z ? t->n_z[i] : 0.0;
+  }
+  m->eType.assign(t->eType, t->eType + m->eLen);
+  m->eRS.assign(t->eRS, t->eRS + m->eLen);
+  m->eMP.assign(t->eMP, t->eMP + m->eLen);
+  // element types: the quad (2) or the brick (9; 10 without Winkler springs)
+  long t0 = m->eType[0];
+  bool quad = (t0 == 2);
+  for (long e = 0; e < m->eLen; e++) {
+    long te = m->eType[e];
+    bool ok = quad ? (te == 2) : (te == 9 || te == 10);
+    if (!ok) {
+      set_error("element types: only all-quad (2) or all-brick (9/10) models are on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+  }
+  m->etype = quad ? 2 : 9;
+  m->nn = elem_nodes(t0);
+  m->b = elem_dofs(t0);
+  m->enodes.resize((size_t)m->eLen * m->nn);
+  for (long e = 0; e < m->eLen; e++) {
+    for (int j = 0; j < m->nn; j++) {
+      long np = t->eNodesL[t->eFrom[e] + j];
+      if (np < 0 || np >= m->nLen) {
+        set_error("invalid node position in element");  // fem/fem_sol.c:1304-1311
+        return UFEM_AF_ERR_VAL;
+      }
+      m->enodes[(size_t)e * m->nn + j] = (int)np;
+    }
+  }
+  // materials: type 1 (linear isotropic), values DENS, EX, NU, ... (fem/fem_m001.c:38)
+  m->mpVals.resize(t->mpLen);
+  m->mpTypeH.assign(t->mpType, t->mpType + t->mpLen);
+  for (long p = 0; p < t->mpLen; p++) {
+    long from = t->mpFrom[p];
+    long to = (p + 1 < t->mpLen) ? t->mpFrom[p + 1] : t->mpLenL;
+    m->mpVals[p].assign(t->mpValL + from, t->mpValL + to);
+  }
+  m->eE.resize(m->eLen);
+  m->eNu.resize(m->eLen);
+  m->eThick.resize(m->eLen);
+  m->eMat.resize(m->eLen);
+  for (long e = 0; e < m->eLen; e++) {
+    long p = m->eMP[e];
+    if (p < 0 || p >= t->mpLen) {
+      set_error("element material position out of range");
+      return UFEM_AF_ERR_VAL;
+    }
+    if (t->mpType[p] != 1 && t->mpType[p] != 5) {
+      set_error("material types: only linear isotropic (1) is on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+    if (m->mpVals[p].size() > 7) {
+      // repeating values select the orthotropic plane D (fem/fem_stf2.c:256-266)
+      set_error("materials with repeating values are not on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+    m->eMat[e] = p;
+    m->eE[e] = rec_val(m->mpVals[p], 1);
+    m->eNu[e] = rec_val(m->mpVals[p], 2);
+    double thick = 0.0, winkler = 0.0;
+    long r = m->eRS[e];
+    if (t->rsLen > 0 && r >= 0 && r < t->rsLen) {
+      long from = t->rsFrom[r];
+      long to = (r + 1 < t->rsLen) ? t->rsFrom[r + 1] : t->rsLenL;
+      if (to > from) {
+        if (quad) thick = t->rsValL[from];       // RS_HEIGHT first, fem/fem_e002.c:1019
+        else winkler = t->rsValL[from];          // RS_WINKLER, fem/fem_e010.c:79
+      }
+    }
+    if (m->eType[e] == 10 && winkler > 0.0) {
+      set_error("brick with Winkler foundation (type 10, RS_WINKLER > 0) is not on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+    m->eThick[e] = thick;
+    if (quad && (m->eNu[e] <= 0.0 || m->eNu[e] >= 1.0)) {
+      set_error("invalid Poisson ratio");  // fem/fem_stf2.c:47-54
+      return UFEM_AF_ERR_VAL;
+    }
+  }
+  // nodal loads and supports
+  m->loads.clear();
+  for (long i = 0; i < t->nlLen; i++) {
+    NodalLoad l{t->nlNode[i], t->nlType[i], t->nlDir[i], t->nlVal[i]};
+    if (l.node < 0 || l.node >= m->nLen) {
+      set_error("load on an invalid node position");
+      return UFEM_AF_ERR_VAL;
+    }
+    if (l.type != 1 && l.type != 3) {
+      set_error("only supports (type 1) and nodal forces (type 3) are on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+    m->loads.push_back(l);
+  }
+  if (m->nID.empty()) {
+    m->nID.resize(m->nLen);
+    for (long i = 0; i < m->nLen; i++) m->nID[i] = i + 1;
+  }
+  if (m->eID.empty()) {
+    m->eID.resize(m->eLen);
+    for (long i = 0; i < m->eLen; i++) m->eID[i] = i + 1;
+  }
+  if (m->mpID.empty()) {
+    m->mpID.resize(t->mpLen);
+    for (long i = 0; i < t->mpLen; i++) m->mpID[i] = i + 1;
+  }
+  return build_model(m);
+}
+
+int build_model(ufem_model *m) {
+  const int b = m->b, nn = m->nn;
+  // ---- fem_dofs: mark used slots, number them 1..nDOFAct in slot order ----
+  m->nDOFfld.assign((size_t)m->nLen * KNOWN_DOFS, 0);
+  long act = 0;
+  for (long e = 0; e < m->eLen; e++)
+    for (int j = 0; j < nn; j++) {
+      long np = m->enodes[(size_t)e * nn + j];
+      for (int k = 0; k < b; k++) {
+        long d = np * KNOWN_DOFS + k;  // ndof = {U_X, U_Y[, U_Z]}
+        if (m->nDOFfld[d] == 0) {
+          m->nDOFfld[d] = 1;
+          act++;
+        }
+      }
+    }
+  if (act < 1) {
+    set_error("no degrees of freedom found");
+    return UFEM_AF_ERR_SIZ;
+  }
+  m->nDOFAct = act;
+  long num = 1;
+  for (size_t i = 0; i < m->nDOFfld.size(); i++)
+    if (m->nDOFfld[i] != 0) m->nDOFfld[i] = num++;
+  // block rows: used nodes in node order; DOF = b*rank + d + 1
+  m->node_rank.assign(m->nLen, -1);
+  m->rank_node.clear();
+  for (long n = 0; n < m->nLen; n++) {
+    if (m->nDOFfld[n * KNOWN_DOFS] != 0) {
+      m->node_rank[n] = (int)m->rank_node.size();
+      m->rank_node.push_back((int)n);
+      for (int d = 0; d < b; d++)
+        if (m->nDOFfld[n * KNOWN_DOFS + d] != (long)b * m->node_rank[n] + d + 1) {
+          set_error("DOF numbering is not node-uniform");
+          return UFEM_AF_ERR_TYP;
+        }
+    }
+  }
+  m->nbr = (int)m->rank_node.size();
+  // ---- block pattern: node adjacency through elements ---------------------
+  std::vector<int> n2e_ptr(m->nbr + 1, 0), n2e;
+  for (long e = 0; e < m->eLen; e++)
+    for (int j = 0; j < nn; j++) n2e_ptr[m->node_rank[m->enodes[(size_t)e * nn + j]] + 1]++;
+  for (int r = 0; r < m->nbr; r++) n2e_ptr[r + 1] += n2e_ptr[r];
+  n2e.resize(n2e_ptr[m->nbr]);
+  {
+    std::vector<int> fill(n2e_ptr.begin(), n2e_ptr.end() - 1);
+    for (long e = 0; e < m->eLen; e++)
+      for (int j = 0; j < nn; j++) n2e[fill[m->node_rank[m->enodes[(size_t)e * nn + j]]]++] = (int)e;
+  }
+  m->rowptr.assign(m->nbr + 1, 0);
+  std::vector<int> tmp;
+  std::vector<std::vector<int>> rows(m->nbr);
+  for (int r = 0; r < m->nbr; r++) {
+    tmp.clear();
+    for (int q = n2e_ptr[r]; q < n2e_ptr[r + 1]; q++) {
+      int e = n2e[q];
+      for (int j = 0; j < nn; j++) tmp.push_back(m->node_rank[m->enodes[(size_t)e * nn + j]]);
+    }
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    rows[r] = tmp;
+    m->rowptr[r + 1] = m->rowptr[r] + (int)tmp.size();
+  }
+  m->nnzb = m->rowptr[m->nbr];
+  m->colind.resize(m->nnzb);
+  m->diagblk.resize(m->nbr);
+  for (int r = 0; r < m->nbr; r++) {
+    std::copy(rows[r].begin(), rows[r].end(), m->colind.begin() + m->rowptr[r]);
+    auto it = std::lower_bound(rows[r].begin(), rows[r].end(), r);
+    m->diagblk[r] = m->rowptr[r] + (int)(it - rows[r].begin());
+  }
+  rows.clear();
+  rows.shrink_to_fit();
+  // ---- element->block scatter map ------------------------------------------
+  m->emap.resize((size_t)m->eLen * nn * nn);
+  for (long e = 0; e < m->eLen; e++)
+    for (int a = 0; a < nn; a++) {
+      int ra = m->node_rank[m->enodes[(size_t)e * nn + a]];
+      const int *beg = m->colind.data() + m->rowptr[ra];
+      const int *end = m->colind.data() + m->rowptr[ra + 1];
+      for (int c = 0; c < nn; c++) {
+        int rc = m->node_rank[m->enodes[(size_t)e * nn + c]];
+        const int *it = std::lower_bound(beg, end, rc);
+        m->emap[((size_t)e * nn + a) * nn + c] = (int)(it - m->colind.data());
+      }
+    }
+  // ---- greedy element colouring: no two elements of a colour share a node ---
+  std::vector<uint64_t> node_used(m->nbr, 0);
+  std::vector<int> ecol(m->eLen);
+  int ncol = 0;
+  for (long e = 0; e < m->eLen; e++) {
+    uint64_t busy = 0;
+    for (int j = 0; j < nn; j++) busy |= node_used[m->node_rank[m->enodes[(size_t)e * nn + j]]];
+    if (busy == ~0ull) {
+      set_error("element colouring needs more than 64 colours");
+      return UFEM_AF_ERR_BIG;
+    }
+    int c = __builtin_ctzll(~busy);
+    ecol[e] = c;
+    ncol = std::max(ncol, c + 1);
+    for (int j = 0; j < nn; j++) node_used[m->node_rank[m->enodes[(size_t)e * nn + j]]] |= (1ull << c);
+  }
+  m->ncolours = ncol;
+  m->colour_ptr.assign(ncol + 1, 0);
+  for (long e = 0; e < m->eLen; e++) m->colour_ptr[ecol[e] + 1]++;
+  for (int c = 0; c < ncol; c++) m->colour_ptr[c + 1] += m->colour_ptr[c];
+  m->colour_elems.resize(m->eLen);
+  {
+    std::vector<int> fill(m->colour_ptr.begin(), m->colour_ptr.end() - 1);
+    for (long e = 0; e < m->eLen; e++) m->colour_elems[fill[ecol[e]]++] = (int)e;
+  }
+  int rv = setup_loads(m);
+  if (rv != UFEM_AF_OK) return rv;
+  return upload_model(m);
+}
+
+
+// Loads and supports of the current tables: F after fem_add_loads
+// (femApplyNLoad type 3: F[pos] += val, fem/fem_loads.c:343-395), the
+// reaction list of fem_sol_res_alloc (fem/fem_sol.c:676-722) and the mask of
+// zero-valued supports.
+int setup_loads(ufem_model *m) {
+  // ---- loads: F after fem_add_loads (femApplyNLoad type 3: F[pos] += val) ----
+  m->F_loads.assign(m->nDOFAct, 0.0);
+  m->has_nonzero_bc = false;
+  m->reacNode.clear();
+  m->reacDof.clear();
+  m->reacRow.clear();
+  m->fixedMask.assign(m->nDOFAct, 0);
+  for (const auto &l : m->loads) {
+    long p = (l.dir >= 1 && l.dir <= KNOWN_DOFS) ? m->nDOFfld[l.node * KNOWN_DOFS + l.dir - 1] : 0;
+    if (l.type == 3) {
+      if (p > 0) m->F_loads[p - 1] += l.val;
+    } else if (l.type == 1) {
+      if (p <= 0) {
+        set_error("cannot add boundary condition on an unused DOF");  // fem/fem_loads.c:130-139
+        return UFEM_AF_ERR_VAL;
+      }
+      if (l.val != 0.0) {
+        m->has_nonzero_bc = true;
+      } else {
+        m->reacNode.push_back(l.node);
+        m->reacDof.push_back(l.dir);
+        m->reacRow.push_back((int)(p - 1));
+        m->fixedMask[p - 1] = 1;
+      }
+    }
+  }
+  m->reacVal.assign(m->reacNode.size(), 0.0);
+  return UFEM_AF_OK;
+}
+
+// The reference's row-slot K layout for this model, built on the host
+// without any values: row sizes from femKhit (fem/fem_mloc.c:83-116), starts
+// as in femMatAlloc (fem/fem_math.c:88-100) and columns in the order
+// femLocKM_e/femMatPutAdd insert them (elements in order, local rows i, local
+// columns j, a new column taking the first empty slot).
+int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, long *len) {
+  const int nn = m->nn, b = m->b, s = nn * b;
+  const long rows = m->nDOFAct;
+  std::vector<long> krows(rows, 0);
+  for (long e = 0; e < m->eLen; e++)
+    for (int j = 0; j < nn; j++)
+      for (int k = 0; k < b; k++) {
+        long p = m->nDOFfld[(long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k];
+        if (p >= 1) krows[p - 1] += s;
+      }
+  long sum = 0;
+  std::vector<long> from(rows);
+  for (long i = 0; i < rows; i++) {
+    sum += krows[i];
+    from[i] = sum - krows[i];
+  }
+  if (len) *len = sum;
+  if (frompos) std::copy(from.begin(), from.end(), frompos);
+  if (defpos) std::copy(krows.begin(), krows.end(), defpos);
+  if (!pos) return UFEM_AF_OK;
+  std::fill(pos, pos + sum, 0L);
+  std::vector<long> fill(rows, 0), lf(s);
+  for (long e = 0; e < m->eLen; e++) {
+    int q = 0;
+    for (int j = 0; j < nn; j++)
+      for (int k = 0; k < b; k++) lf[q++] = m->nDOFfld[(long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k];
+    for (int i = 0; i < s; i++) {
+      long r = lf[i] - 1;
+      for (int j = 0; j < s; j++) {
+        long c = lf[j];
+        long *row = pos + from[r];
+        long f = fill[r];
+        bool found = false;
+        for (long t = 0; t < f; t++)
+          if (row[t] == c) {
+            found = true;
+            break;
+          }
+        if (!found) {
+          if (f >= krows[r]) {
+            set_error("row-slot export: row overflow");
+            return UFEM_AF_ERR_BIG;
+          }
+          row[f] = c;
+          fill[r] = f + 1;
+        }
+      }
+    }
+  }
+  return UFEM_AF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// preparsed input reader (femReadInput, fem/fem_io.c:380-590)
+// ---------------------------------------------------------------------------
+namespace {
+struct Tok {
+  const char *p, *end;
+  bool ok = true;
+  void skip() {
+    while (p < end && (*p == ' ' || *p == '\n' || *p == '\t' || *p == '\r')) p++;
+  }
+  bool more() {
+    skip();
+    return p < end;
+  }
+  long L() {
+    skip();
+    if (p >= end) {
+      ok = false;
+      return 0;
+    }
+    char *q;
+    long v = strtol(p, &q, 10);
+    if (q == p) ok = false;
+    p = q;
+    return v;
+  }
+  double D() {
+    skip();
+    if (p >= end) {
+      ok = false;
+      return 0;
+    }
+    char *q;
+    double v = strtod(p, &q);
+    if (q == p) ok = false;
+    p = q;
+    return v;
+  }
+};
+}  // namespace
+
+int read_input_file(const char *fname, ufem_model **out) {
+  std::ifstream f(fname, std::ios::binary);
+  if (!f) {
+    set_error(std::string("cannot open input ") + fname);
+    return UFEM_AF_ERR_IO;
+  }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  std::string buf = ss.str();
+  Tok t{buf.data(), buf.data() + buf.size()};
+  // solution control data (fem/fem_io.c:408-414)
+  t.L(); t.L();
+  t.L(); t.L(); t.L();
+  // real sets (fem/fem_io.c:421-475)
+  long rsLen = t.L();
+  std::vector<long> rsID, rsType, rsFrom;
+  std::vector<double> rsVal;
+  long sum = 0;
+  for (long i = 0; i < rsLen; i++) {
+    rsID.push_back(t.L());
+    rsType.push_back(t.L());
+    long c = t.L();
+    rsFrom.push_back(sum);
+    sum += c;
+  }
+  long rsLenL = 0;
+  if (rsLen > 0) {
+    rsLenL = t.L();
+    if (rsLenL != sum) {
+      set_error("bad number of real set values");
+      return UFEM_AF_ERR_SIZ;
+    }
+    for (long i = 0; i < rsLenL; i++) rsVal.push_back(t.D());
+  }
+  // materials (fem/fem_io.c:478-521)
+  long mpLen = t.L();
+  std::vector<long> mpID, mpType, mpFrom;
+  std::vector<double> mpVal;
+  sum = 0;
+  for (long i = 0; i < mpLen; i++) {
+    mpID.push_back(t.L());
+    mpType.push_back(t.L());
+    long c = t.L();
+    mpFrom.push_back(sum);
+    sum += c;
+  }
+  long mpLenL = 0;
+  if (mpLen > 0) {
+    mpLenL = t.L();
+    if (mpLenL != sum) {
+      set_error("bad number of material property values");
+      return UFEM_AF_ERR_SIZ;
+    }
+    for (long i = 0; i < mpLenL; i++) mpVal.push_back(t.D());
+  }
+  // nodes (fem/fem_io.c:524-540)
+  long nLen = t.L();
+  if (nLen < 2) {
+    set_error("fewer than 2 nodes");
+    return UFEM_AF_ERR_SML;
+  }
+  std::vector<long> nID(nLen);
+  std::vector<double> nx(nLen), ny(nLen), nz(nLen);
+  for (long i = 0; i < nLen; i++) {
+    nID[i] = t.L();
+    nx[i] = t.D();
+    ny[i] = t.D();
+    nz[i] = t.D();
+  }
+  // elements (fem/fem_io.c:543-598)
+  long eLen = t.L();
+  if (eLen < 1) {
+    set_error("no elements");
+    return UFEM_AF_ERR_SML;
+  }
+  std::vector<long> eID(eLen), eType(eLen), eRS(eLen), eMP(eLen), eFrom(eLen);
+  sum = 0;
+  for (long i = 0; i < eLen; i++) {
+    eID[i] = t.L();
+    eType[i] = t.L();
+    eRS[i] = t.L();
+    eMP[i] = t.L();
+    long c = t.L();
+    eFrom[i] = sum;
+    sum += c;
+  }
+  long eLenL = t.L();
+  if (eLenL != sum) {
+    set_error("bad number of element nodes");
+    return UFEM_AF_ERR_SIZ;
+  }
+  std::vector<long> eNodes(eLenL);
+  for (long i = 0; i < eLenL; i++) eNodes[i] = t.L();
+  // gravity (fem/fem_io.c:604) -- only zero gravity is on this path
+  t.L();
+  double grVal = t.D();
+  if (std::fabs(grVal) > 0) {
+    set_error("gravity loads are not on this path");
+    return UFEM_AF_ERR_TYP;
+  }
+  // nodal loads (fem/fem_io.c:92-113)
+  long nlLen = t.L();
+  std::vector<long> nlNode(nlLen), nlType(nlLen), nlDir(nlLen);
+  std::vector<double> nlVal(nlLen);
+  for (long i = 0; i < nlLen; i++) {
+    nlNode[i] = t.L();
+    nlType[i] = t.L();
+    nlDir[i] = t.L();
+    nlVal[i] = t.D();
+  }
+  // element loads (fem/fem_io.c:116) -- none on this path
+  long elLen = t.L();
+  if (elLen > 0) {
+    set_error("element loads are not on this path");
+    return UFEM_AF_ERR_TYP;
+  }
+  if (!t.ok) {
+    set_error("truncated input file");
+    return UFEM_AF_ERR_IO;
+  }
+  // transient and dynamics counters (fem/fem_io.c:176, :297) and the
+  // optional Monte Carlo table (fem/fem_mont.c:873-905)
+  ufem_model *m = new ufem_model();
+  if (t.more()) {
+    long transNum = t.L(), dynNum = t.L();
+    t.D();
+    if (dynNum > 0 && transNum > 0) {
+      delete m;
+      set_error("transient data are not on this path");
+      return UFEM_AF_ERR_TYP;
+    }
+    if (t.more()) {
+      long dynNum0 = t.L();
+      if (dynNum0 > 0) {
+        delete m;
+        set_error("dynamics data are not on this path");
+        return UFEM_AF_ERR_TYP;
+      }
+      if (t.more()) {
+        long ilen = t.L(), olen = t.L();
+        if (t.ok && ilen > 0) {
+          m->mc_ilen = ilen;
+          m->mc_olen = olen;
+          for (long i = 0; i < ilen + olen; i++) {
+            m->mc_pos.push_back(t.L());
+            m->mc_type.push_back(t.L());
+            m->mc_item.push_back(t.L());
+            m->mc_sub.push_back(t.L());
+            m->mc_iter.push_back(t.L());
+          }
+          if (!t.ok) {
+            delete m;
+            set_error("incomplete or unavailable random data");  // fem/fem_mont.c:885
+            return UFEM_AF_ERR_IO;
+          }
+        }
+      }
+    }
+  }
+  m->nID = nID;
+  m->eID = eID;
+  m->mpID = mpID;
+  m->rsID = rsID;
+  ufem_tables tb{};
+  tb.nLen = nLen; tb.n_x = nx.data(); tb.n_y = ny.data(); tb.n_z = nz.data();
+  tb.eLen = eLen; tb.eType = eType.data(); tb.eRS = eRS.data(); tb.eMP = eMP.data();
+  tb.eFrom = eFrom.data(); tb.eNodesL = eNodes.data();
+  tb.rsLen = rsLen; tb.rsType = rsType.data(); tb.rsFrom = rsFrom.data(); tb.rsLenL = rsLenL;
+  tb.rsValL = rsVal.data();
+  tb.mpLen = mpLen; tb.mpType = mpType.data(); tb.mpFrom = mpFrom.data(); tb.mpLenL = mpLenL;
+  tb.mpValL = mpVal.data();
+  tb.nlLen = nlLen; tb.nlNode = nlNode.data(); tb.nlType = nlType.data(); tb.nlDir = nlDir.data();
+  tb.nlVal = nlVal.data();
+  int rv = model_from_tables(&tb, m);
+  if (rv != UFEM_AF_OK) {
+    delete m;
+    return rv;
+  }
+  *out = m;
+  return UFEM_AF_OK;
+}
+
+}  // namespace ufem

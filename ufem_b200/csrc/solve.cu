@@ -1,0 +1,765 @@
+// Single-system FP64 solvers on the GPU block-sparse K (block size B = 1, 2
+// or 3; B = 1 is plain CSR):
+//
+//   Jacobi PCG      femEqsCGwJ    fem/fem_eqs.c:88-247   (one persistent kernel)
+//   Jacobi BiCGStab femEqsBiCCSwJ fem/fem_eqs.c:262-468  (stream of kernels)
+//   SSOR PCG        femEqsCGwSSOR fem/fem_eqs.c:1001-1217 (multicolour sweeps)
+//
+// Jacobi PCG: one cooperative launch runs every iteration; the grid meets at
+// a bounded barrier twice per iteration.  Phase S computes q = A p with
+// p = z + beta p_old formed on the fly from the gathered neighbours (p needs
+// no pass of its own) and the partial p.q; phase U updates x and r, forms
+// z = r / diag(A) and the partials of r.r, x.x and r.z.  Every block sums the
+// per-block partials in the same fixed order, so all blocks take the same
+// convergence decision and results are identical run to run.  Vectors that
+// other blocks write during the kernel are read with ld.global.cg (L2), never
+// from the non-coherent L1.
+//
+// SpMV mapping: one warp per block row; L = 32 - 32 % B lanes walk the row's
+// (block, row-in-block) items with stride L, so a lane's row-in-block
+// a = lane % B is fixed; each lane reads the B consecutive values of its block
+// row (contiguous across the warp) and the B gathered neighbour values; the B
+// sums are combined in a fixed order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "device_util.cuh"
+#include "ufem_internal.h"
+
+namespace ufem {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+struct CgResult {
+  long iters;
+  int status;
+  int pad;
+  double normRes, normX;
+};
+
+struct CgArgs {
+  int nbr;
+  const int *rowptr, *colind;
+  const double *val;
+  const double *b;
+  double *x;
+  const double *M;
+  double *r, *z, *p0, *p1, *q;
+  double *part;  // [grid][4]: slots 0..2 = r.r, x.x, r.z ; slot 3 = p.q
+  GridBar *bar;
+  CgResult *res;
+  double eps, normA, normB;
+  long maxIt;
+  int stop_rule;
+};
+
+// One block row of y = A (z + beta p) (use_p) or y = A z: the B row sums come
+// back on lanes < B.
+template <int B>
+__device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ rowptr,
+                                                const int *__restrict__ colind, const double *__restrict__ val,
+                                                const double *z, const double *p, double beta, bool use_p,
+                                                double *s_acc) {
+  constexpr int L = 32 - (32 % B);
+  const int lane = threadIdx.x & 31;
+  const int k0 = __ldg(rowptr + I), k1 = __ldg(rowptr + I + 1);
+  const int nitems = (k1 - k0) * B;
+  double acc = 0.0;
+  if (lane < L) {
+    const int a = lane % B;
+    for (int t = lane; t < nitems; t += L) {
+      const int k = k0 + t / B;
+      const int J = __ldg(colind + k);
+      const double *v = val + (size_t)k * B * B + a * B;
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        double xj = __ldcg(z + (size_t)J * B + c);
+        if (use_p) xj = xj + beta * __ldcg(p + (size_t)J * B + c);
+        acc += __ldg(v + c) * xj;
+      }
+    }
+  }
+  if (B == 1) {
+    return warp_sum(acc);
+  } else if (B == 2) {
+#pragma unroll
+    for (int o = 16; o >= 2; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    return acc;
+  } else {
+    s_acc[lane] = acc;
+    __syncwarp();
+    double y = 0.0;
+    if (lane < B)
+      for (int l = lane; l < L; l += B) y += s_acc[l];
+    __syncwarp();
+    return y;
+  }
+}
+
+// Fixed-order sum of slot `off` of the per-block partials (all blocks agree).
+__device__ __forceinline__ double part_total(const double *part, int G, int off) {
+  __shared__ double s_t;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int g = lane; g < G; g += 32) t += __ldcg(part + (size_t)g * 4 + off);
+    t = warp_sum(t);
+    if (lane == 0) s_t = t;
+  }
+  __syncthreads();
+  double v = s_t;
+  __syncthreads();
+  return v;
+}
+
+template <int B>
+__global__ void __launch_bounds__(kThreads) k_cg_fp64(CgArgs A) {
+  __shared__ double s_acc[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
+  const int rpw = (A.nbr + nw - 1) / nw;
+  const int I0 = min(A.nbr, gw * rpw), I1 = min(A.nbr, I0 + rpw);
+  const int G = gridDim.x;
+  double *mypart = A.part + (size_t)blockIdx.x * 4;
+  // phase 0: r = b - A x; z = r / M (fem/fem_eqs.c:150-162)
+  {
+    double rr = 0.0, xx = 0.0, rz = 0.0;
+    for (int I = I0; I < I1; I++) {
+      double y = warp_row_spmv<B>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
+      if (lane < B) {
+        size_t i = (size_t)I * B + lane;
+        double ri = A.b[i] - y;
+        double zi = ri / A.M[i];
+        A.r[i] = ri;
+        A.z[i] = zi;
+        rr += ri * ri;
+        xx += A.x[i] * A.x[i];
+        rz += ri * zi;
+      }
+    }
+    double v[3] = {rr, xx, rz};
+    block_partials<3>(v, mypart);
+  }
+  if (!grid_barrier(A.bar)) return;
+  double rho = part_total(A.part, G, 2), rhoold = 1.0;
+  double normRes = sqrt(part_total(A.part, G, 0)), normX = sqrt(part_total(A.part, G, 1));
+  int status = UFEM_AF_ERR;
+  long it = 0;
+  for (it = 1; it <= A.maxIt; it++) {
+    const bool first = (it == 1);
+    const double beta = first ? 0.0 : rho / rhoold;  // fem/fem_eqs.c:172
+    const double *pold = (it & 1) ? A.p0 : A.p1;
+    double *pnew = (it & 1) ? A.p1 : A.p0;
+    // phase S: q = A p, p = z + beta p_old (fem/fem_eqs.c:168-186), partial p.q
+    {
+      double pq = 0.0;
+      for (int I = I0; I < I1; I++) {
+        double y = warp_row_spmv<B>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
+        if (lane < B) {
+          size_t i = (size_t)I * B + lane;
+          double zi = A.z[i];
+          double pi = first ? zi : (zi + (beta * pold[i]));
+          pnew[i] = pi;
+          A.q[i] = y;
+          pq += pi * y;
+        }
+      }
+      double v[1] = {pq};
+      block_partials<1>(v, mypart + 3);
+    }
+    if (!grid_barrier(A.bar)) return;
+    const double pq = part_total(A.part, G, 3);
+    if (!(pq > 0.0) || !isfinite(pq)) {  // breakdown: p.q <= 0 or not finite
+      status = UFEM_AF_ERR;
+      it = -it;
+      break;
+    }
+    const double alpha = rho / pq;  // fem/fem_eqs.c:188
+    // phase U: x += alpha p, r -= alpha q (fem/fem_eqs.c:194-198), z = r / M
+    {
+      double rr = 0.0, xx = 0.0, rz = 0.0;
+      const size_t i0 = (size_t)I0 * B, i1 = (size_t)I1 * B;
+      for (size_t i = i0 + lane; i < i1; i += 32) {
+        double xi = A.x[i] + (alpha * pnew[i]);
+        double ri = A.r[i] - (alpha * A.q[i]);
+        double zi = ri / A.M[i];
+        A.x[i] = xi;
+        A.r[i] = ri;
+        A.z[i] = zi;
+        rr += ri * ri;
+        xx += xi * xi;
+        rz += ri * zi;
+      }
+      double v[3] = {rr, xx, rz};
+      block_partials<3>(v, mypart);
+    }
+    if (!grid_barrier(A.bar)) return;
+    normRes = sqrt(part_total(A.part, G, 0));
+    normX = sqrt(part_total(A.part, G, 1));
+    const double rhonew = part_total(A.part, G, 2);
+    bool conv;
+    if (A.stop_rule == UFEM_STOP_REFERENCE)
+      conv = normRes <= (A.eps * ((A.normA * normX) + A.normB));  // fem/fem_eqs.c:207
+    else
+      conv = normRes <= A.eps * A.normB;
+    if (!isfinite(normRes)) {
+      status = UFEM_AF_ERR;
+      break;
+    }
+    if (conv) {
+      status = UFEM_AF_OK;
+      break;
+    }
+    rhoold = rho;
+    rho = rhonew;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.res->iters = it > A.maxIt ? A.maxIt : it;
+    A.res->status = status;
+    A.res->normRes = normRes;
+    A.res->normX = normX;
+  }
+}
+
+// ---- small kernels shared by the host-driven solvers ------------------------
+
+template <int B>
+__global__ void __launch_bounds__(kThreads) k_spmv(int nbr, const int *__restrict__ rowptr,
+                                                   const int *__restrict__ colind, const double *__restrict__ val,
+                                                   const double *__restrict__ x, double *__restrict__ y) {
+  __shared__ double s_acc[kWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kWarps + warp;
+  if (I >= nbr) return;
+  double v = warp_row_spmv<B>(I, rowptr, colind, val, x, nullptr, 0.0, false, s_acc[warp]);
+  if (lane < B) y[(size_t)I * B + lane] = v;
+}
+
+// Diagonal of A and its smallest magnitude check (fem/fem_eqs.c:134-145).
+template <int B>
+__global__ void k_diag(int nbr, const int *__restrict__ rowptr, const int *__restrict__ colind,
+                       const double *__restrict__ val, double *__restrict__ M, int *__restrict__ zero_row) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbr * B) return;
+  int I = t / B, a = t % B;
+  double d = 0.0;
+  for (int k = rowptr[I]; k < rowptr[I + 1]; k++)
+    if (colind[k] == I) d = val[(size_t)k * B * B + a * B + a];
+  M[t] = d;
+  if (fabs(d) < FEM_ZERO) atomicMin(zero_row, t);
+}
+
+// max over rows of the row 2-norm (femMatNormBig, fem/fem_math.c:1856-1952)
+template <int B>
+__global__ void k_row_norm_max(int nbr, const int *__restrict__ rowptr, const double *__restrict__ val,
+                               unsigned long long *__restrict__ out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbr * B) return;
+  int I = t / B, a = t % B;
+  double s = 0.0;
+  for (int k = rowptr[I]; k < rowptr[I + 1]; k++)
+    for (int c = 0; c < B; c++) {
+      double v = val[(size_t)k * B * B + a * B + c];
+      s += v * v;
+    }
+  s = sqrt(s);
+  atomicMax(out, (unsigned long long)__double_as_longlong(s));  // order-free for s >= 0
+}
+
+// deterministic two-stage dot products
+constexpr int kDotBlocks = 296;
+__global__ void __launch_bounds__(kThreads) k_dot_part(long n, const double *__restrict__ a,
+                                                       const double *__restrict__ b, double *__restrict__ part) {
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  double v[1] = {s};
+  block_partials<1>(v, part + blockIdx.x);
+}
+__global__ void k_dot_final(const double *__restrict__ part, int nb, double *__restrict__ out) {
+  double t = 0.0;
+  for (int g = threadIdx.x; g < nb; g += 32) t += part[g];
+  t = warp_sum(t);
+  if (threadIdx.x == 0) *out = t;
+}
+
+struct Dots {
+  DBuf<double> part, vals;
+  int init(int nslots) {
+    int rv = part.alloc(kDotBlocks);
+    if (rv != UFEM_AF_OK) return rv;
+    return vals.alloc(nslots);
+  }
+  void dot(long n, const double *a, const double *b, int slot, cudaStream_t s = 0) {
+    k_dot_part<<<kDotBlocks, kThreads, 0, s>>>(n, a, b, part.p);
+    k_dot_final<<<1, 32, 0, s>>>(part.p, kDotBlocks, vals.p + slot);
+  }
+};
+
+int setup_common(const DevMatrix &A, DBuf<double> &M, double *normA, int *zero_row_out) {
+  const long n = (long)A.nbr * A.B;
+  int rv;
+  if ((rv = M.alloc(n)) != UFEM_AF_OK) return rv;
+  DBuf<int> zr;
+  DBuf<unsigned long long> nm;
+  if ((rv = zr.alloc(1)) != UFEM_AF_OK) return rv;
+  if ((rv = nm.alloc(1)) != UFEM_AF_OK) return rv;
+  int big = 0x7fffffff;
+  UFEM_CUDA_TRY(cudaMemcpy(zr.p, &big, sizeof(int), cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemset(nm.p, 0, sizeof(unsigned long long)));
+  unsigned g = (unsigned)((n + 255) / 256);
+  switch (A.B) {
+    case 1: k_diag<1><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M.p, zr.p);
+            k_row_norm_max<1><<<g, 256>>>(A.nbr, A.rowptr, A.val, nm.p); break;
+    case 2: k_diag<2><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M.p, zr.p);
+            k_row_norm_max<2><<<g, 256>>>(A.nbr, A.rowptr, A.val, nm.p); break;
+    default: k_diag<3><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M.p, zr.p);
+             k_row_norm_max<3><<<g, 256>>>(A.nbr, A.rowptr, A.val, nm.p); break;
+  }
+  UFEM_CUDA_TRY(cudaGetLastError());
+  unsigned long long nb = 0;
+  UFEM_CUDA_TRY(cudaMemcpy(&nb, nm.p, sizeof(nb), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(zero_row_out, zr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  double d;
+  memcpy(&d, &nb, sizeof(d));
+  *normA = d;
+  return UFEM_AF_OK;
+}
+
+double host_norm(long n, const double *d_v) {
+  Dots d;
+  if (d.init(1) != UFEM_AF_OK) return NAN;
+  d.dot(n, d_v, d_v, 0);
+  double h = 0;
+  cudaMemcpy(&h, d.vals.p, sizeof(double), cudaMemcpyDeviceToHost);
+  return std::sqrt(h);
+}
+
+void spmv_launch(const DevMatrix &A, const double *x, double *y, cudaStream_t s = 0) {
+  unsigned g = (unsigned)((A.nbr + kWarps - 1) / kWarps);
+  switch (A.B) {
+    case 1: k_spmv<1><<<g, kThreads, 0, s>>>(A.nbr, A.rowptr, A.colind, A.val, x, y); break;
+    case 2: k_spmv<2><<<g, kThreads, 0, s>>>(A.nbr, A.rowptr, A.colind, A.val, x, y); break;
+    default: k_spmv<3><<<g, kThreads, 0, s>>>(A.nbr, A.rowptr, A.colind, A.val, x, y); break;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, int stop_rule,
+                   long *iters, float *ms) {
+  const long n = (long)A.nbr * A.B;
+  int rv;
+  if (iters) *iters = 0;
+  double normA = 0.0;
+  int zero_row = 0;
+  DBuf<double> M;
+  if ((rv = setup_common(A, M, &normA, &zero_row)) != UFEM_AF_OK) return rv;
+  double normB = host_norm(n, d_b);
+  if (!(normB > 0.0)) {  // zero load: x = 0 without iterating (fem/fem_eqs.c:108-116)
+    UFEM_CUDA_TRY(cudaMemset(d_x, 0, n * sizeof(double)));
+    return UFEM_AF_OK;
+  }
+  if (zero_row != 0x7fffffff) {
+    set_error("matrix member on the diagonal has zero size");  // fem/fem_eqs.c:134-145
+    return UFEM_AF_ERR_ZER;
+  }
+  DBuf<double> r, z, p0, p1, q, part;
+  DBuf<GridBar> bar;
+  DBuf<CgResult> res;
+  if ((rv = r.alloc(n)) || (rv = z.alloc(n)) || (rv = p0.alloc(n)) || (rv = p1.alloc(n)) || (rv = q.alloc(n)))
+    return rv;
+  UFEM_CUDA_TRY(cudaMemset(p0.p, 0, n * sizeof(double)));
+  UFEM_CUDA_TRY(cudaMemset(p1.p, 0, n * sizeof(double)));
+  int dev = 0, nsm = 0, occ = 0;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  void (*kern)(CgArgs) = A.B == 1 ? k_cg_fp64<1> : (A.B == 2 ? k_cg_fp64<2> : k_cg_fp64<3>);
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  if (occ < 1) {
+    set_error("persistent CG kernel does not fit on an SM");
+    return UFEM_AF_ERR;
+  }
+  // at least two block rows per warp; never more blocks than are co-resident
+  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  G = std::max(G, 1);
+  if ((rv = part.alloc((size_t)G * 4)) != UFEM_AF_OK) return rv;
+  if ((rv = bar.alloc(1)) != UFEM_AF_OK) return rv;
+  if ((rv = res.alloc(1)) != UFEM_AF_OK) return rv;
+  UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
+  UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
+  CgArgs a;
+  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
+  a.M = M.p; a.r = r.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
+  a.bar = bar.p; a.res = res.p; a.eps = eps; a.normA = normA; a.normB = normB;
+  a.maxIt = maxIt; a.stop_rule = stop_rule;
+  void *args[] = {&a};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
+  cudaEventRecord(e1);
+  UFEM_CUDA_TRY(cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  GridBar hb;
+  CgResult hr;
+  UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
+  if (hb.err) {
+    set_error("persistent CG: grid barrier timed out");
+    return UFEM_AF_ERR;
+  }
+  if (iters) *iters = hr.iters < 0 ? -hr.iters : hr.iters;
+  if (hr.status != UFEM_AF_OK) set_error("unconverged solution");  // fem/fem_eqs.c:230-236
+  return hr.status;
+}
+
+// ---- BiCGStab (femEqsBiCCSwJ) ------------------------------------------------
+
+namespace {
+struct BiScal {  // device scalars
+  double ro, roro, alpha, omega, beta, rrv, ts, tt;
+};
+
+__global__ void k_bicg_p(long n, int first, const double *__restrict__ dv, const double *__restrict__ r,
+                         double *__restrict__ p, const double *__restrict__ v, const double *__restrict__ M,
+                         double *__restrict__ pp) {
+  // dv: [0]=ro [1]=roro [2]=alpha [3]=omega
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double pi;
+  if (first) {
+    pi = r[i];
+  } else {
+    double beta = (dv[0] / dv[1]) * (dv[2] / dv[3]);  // fem/fem_eqs.c:386
+    pi = r[i] + beta * (p[i] - (dv[3] * v[i]));
+  }
+  p[i] = pi;
+  pp[i] = pi / M[i];
+}
+__global__ void k_bicg_s(long n, const double *__restrict__ dv, const double *__restrict__ r,
+                         const double *__restrict__ v, const double *__restrict__ M, double *__restrict__ s,
+                         double *__restrict__ ss) {
+  // dv[2] = alpha = ro / (rr.v) computed by k_bicg_alpha
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double si = r[i] - (dv[2] * v[i]);
+  s[i] = si;
+  ss[i] = si / M[i];
+}
+__global__ void k_bicg_alpha(double *dv, const double *rrv) { dv[2] = dv[0] / *rrv; }
+__global__ void k_bicg_omega(double *dv, const double *ts, const double *tt) { dv[3] = *ts / *tt; }
+__global__ void k_bicg_xr(long n, const double *__restrict__ dv, double *__restrict__ x, double *__restrict__ r,
+                          const double *__restrict__ pp, const double *__restrict__ ss,
+                          const double *__restrict__ s, const double *__restrict__ t) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] += dv[2] * pp[i] + (dv[3] * ss[i]);
+  r[i] = s[i] - (dv[3] * t[i]);
+}
+__global__ void k_axpy_last(long n, const double *__restrict__ dv, double *__restrict__ x,
+                            const double *__restrict__ pp) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += dv[2] * pp[i];
+}
+__global__ void k_sub(long n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) c[i] = a[i] - b[i];
+}
+__global__ void k_copy_scalar(double *dst, const double *src) { *dst = *src; }
+}  // namespace
+
+int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, int stop_rule,
+                         long *iters, float *ms) {
+  const long n = (long)A.nbr * A.B;
+  int rv;
+  if (iters) *iters = 0;
+  double normA = 0.0;
+  int zero_row = 0;
+  DBuf<double> M;
+  if ((rv = setup_common(A, M, &normA, &zero_row)) != UFEM_AF_OK) return rv;
+  double normB = host_norm(n, d_b);
+  // the reference leaves through memFree and still returns AF_OK (fem/fem_eqs.c:352-360, :467)
+  if (zero_row != 0x7fffffff) return UFEM_AF_OK;
+  DBuf<double> r, rr, p, pp, s, ss, t, v, res;
+  if ((rv = r.alloc(n)) || (rv = rr.alloc(n)) || (rv = p.alloc(n)) || (rv = pp.alloc(n)) || (rv = s.alloc(n)) ||
+      (rv = ss.alloc(n)) || (rv = t.alloc(n)) || (rv = v.alloc(n)) || (rv = res.alloc(n)))
+    return rv;
+  Dots D;
+  if ((rv = D.init(8)) != UFEM_AF_OK) return rv;
+  DBuf<double> dv;
+  if ((rv = dv.alloc(4)) != UFEM_AF_OK) return rv;
+  UFEM_CUDA_TRY(cudaMemset(dv.p, 0, 4 * sizeof(double)));
+  unsigned g = (unsigned)((n + 255) / 256);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  spmv_launch(A, d_x, r.p);
+  k_sub<<<g, 256>>>(n, d_b, r.p, r.p);
+  UFEM_CUDA_TRY(cudaMemcpy(rr.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+  long it = 0;
+  if (!(host_norm(n, r.p) <= FEM_ZERO)) {
+    for (it = 1; it <= maxIt; it++) {
+      D.dot(n, rr.p, r.p, 0);                       // ro
+      k_copy_scalar<<<1, 1>>>(dv.p + 0, D.vals.p + 0);
+      double ro = 0;
+      UFEM_CUDA_TRY(cudaMemcpy(&ro, D.vals.p, sizeof(double), cudaMemcpyDeviceToHost));
+      if (fabs(ro) <= 0.0) break;                   // fem/fem_eqs.c:373-379
+      k_bicg_p<<<g, 256>>>(n, it == 1, dv.p, r.p, p.p, v.p, M.p, pp.p);
+      spmv_launch(A, pp.p, v.p);
+      D.dot(n, rr.p, v.p, 1);
+      k_bicg_alpha<<<1, 1>>>(dv.p, D.vals.p + 1);
+      k_bicg_s<<<g, 256>>>(n, dv.p, r.p, v.p, M.p, s.p, ss.p);
+      if (host_norm(n, s.p) <= FEM_ZERO) {          // fem/fem_eqs.c:407-417
+        k_axpy_last<<<g, 256>>>(n, dv.p, d_x, pp.p);
+        break;
+      }
+      spmv_launch(A, ss.p, t.p);
+      D.dot(n, t.p, s.p, 2);
+      D.dot(n, t.p, t.p, 3);
+      k_bicg_omega<<<1, 1>>>(dv.p, D.vals.p + 2, D.vals.p + 3);
+      k_bicg_xr<<<g, 256>>>(n, dv.p, d_x, r.p, pp.p, ss.p, s.p, t.p);
+      k_copy_scalar<<<1, 1>>>(dv.p + 1, dv.p + 0);  // roro = ro
+      double normRes;
+      if (stop_rule == UFEM_STOP_REFERENCE) {
+        // eqsCompResid(a, b, x, &res) as called at fem/fem_eqs.c:425: the
+        // arguments are swapped against its prototype, so res = A b - x
+        spmv_launch(A, d_b, res.p);
+        k_sub<<<g, 256>>>(n, res.p, d_x, res.p);
+        normRes = host_norm(n, res.p);
+        double normX = host_norm(n, d_x);
+        if (normRes < (eps * ((normA * normX) + normB))) break;
+      } else {
+        spmv_launch(A, d_x, res.p);
+        k_sub<<<g, 256>>>(n, d_b, res.p, res.p);
+        normRes = host_norm(n, res.p);
+        if (normRes <= eps * normB) break;
+      }
+    }
+  }
+  UFEM_CUDA_TRY(cudaGetLastError());
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float tm = 0;
+  cudaEventElapsedTime(&tm, e0, e1);
+  if (ms) *ms = tm;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (iters) *iters = it > maxIt ? maxIt : it;
+  return UFEM_AF_OK;  // the reference always returns AF_OK (fem/fem_eqs.c:467)
+}
+
+// ---- SSOR PCG (femEqsCGwSSOR) with multicolour Gauss-Seidel sweeps -----------
+//
+// The reference sweeps rows in natural order (fem/fem_eqs.c:1077-1129), a
+// sequential recurrence.  Here block rows are coloured so that no two rows
+// of a colour are coupled; the forward sweep visits colours in order and the
+// backward sweep in reverse, rows of a colour in parallel, the B DOFs of a
+// node in order.  This is symmetric Gauss-Seidel for a permuted ordering: an
+// SPD preconditioner like the reference's, with different iterates.
+
+namespace {
+template <int B, bool FWD>
+__global__ void k_sgs_sweep(int nrows, const int *__restrict__ rows, const int *__restrict__ colour_of,
+                            int colour, const int *__restrict__ rowptr, const int *__restrict__ colind,
+                            const double *__restrict__ val, const double *__restrict__ Minv,
+                            const double *__restrict__ rhs, double *__restrict__ out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int I = rows[t];
+  double loc[B];
+#pragma unroll
+  for (int a = 0; a < B; a++) loc[a] = 0.0;
+  // coupling to other rows of earlier (FWD) or later (!FWD) colours
+  for (int k = rowptr[I]; k < rowptr[I + 1]; k++) {
+    const int J = colind[k];
+    if (J == I) continue;
+    const int cj = colour_of[J];
+    if (FWD ? (cj < colour) : (cj > colour)) {
+#pragma unroll
+      for (int a = 0; a < B; a++)
+#pragma unroll
+        for (int c = 0; c < B; c++) loc[a] += val[(size_t)k * B * B + a * B + c] * out[(size_t)J * B + c];
+    }
+  }
+  int kd = rowptr[I];
+  while (colind[kd] != I) kd++;
+  const double *D = val + (size_t)kd * B * B;
+  if (FWD) {
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      double s = loc[a];
+      for (int c = 0; c < a; c++) s += D[a * B + c] * out[(size_t)I * B + c];
+      out[(size_t)I * B + a] = Minv[(size_t)I * B + a] * (rhs[(size_t)I * B + a] - s);
+    }
+  } else {
+#pragma unroll
+    for (int a = B - 1; a >= 0; a--) {
+      double s = loc[a];
+      for (int c = a + 1; c < B; c++) s += D[a * B + c] * out[(size_t)I * B + c];
+      out[(size_t)I * B + a] = rhs[(size_t)I * B + a] - Minv[(size_t)I * B + a] * s;
+    }
+  }
+}
+__global__ void k_recip(long n, const double *__restrict__ M, double *__restrict__ Minv) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) Minv[i] = 1.0 / M[i];
+}
+__global__ void k_cg_p(long n, int first, const double *__restrict__ sc, const double *__restrict__ z,
+                       double *__restrict__ p) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  p[i] = first ? z[i] : (z[i] + ((sc[0] / sc[1]) * p[i]));
+}
+__global__ void k_cg_xr(long n, const double *__restrict__ sc, const double *__restrict__ pq,
+                        double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
+                        const double *__restrict__ q) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double alpha = sc[0] / *pq;
+  x[i] = x[i] + (alpha * p[i]);
+  r[i] = r[i] - (alpha * q[i]);
+}
+}  // namespace
+
+int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, int stop_rule,
+                 long *iters, float *ms) {
+  const long n = (long)A.nbr * A.B;
+  int rv;
+  if (iters) *iters = 0;
+  double normA = 0.0;
+  int zero_row = 0;
+  DBuf<double> M;
+  if ((rv = setup_common(A, M, &normA, &zero_row)) != UFEM_AF_OK) return rv;
+  double normB = host_norm(n, d_b);
+  if (!(normB > 0.0)) {
+    UFEM_CUDA_TRY(cudaMemset(d_x, 0, n * sizeof(double)));
+    return UFEM_AF_OK;
+  }
+  if (zero_row != 0x7fffffff) {
+    set_error("matrix member on the diagonal has zero size");
+    return UFEM_AF_ERR_ZER;
+  }
+  // greedy colouring of block rows on the host
+  std::vector<int> rp(A.nbr + 1), ci(A.nnzb);
+  UFEM_CUDA_TRY(cudaMemcpy(rp.data(), A.rowptr, (A.nbr + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(ci.data(), A.colind, A.nnzb * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<int> col(A.nbr, -1);
+  int ncol = 0;
+  std::vector<char> used;
+  for (int I = 0; I < A.nbr; I++) {
+    used.assign(ncol + 1, 0);
+    for (int k = rp[I]; k < rp[I + 1]; k++)
+      if (ci[k] != I && col[ci[k]] >= 0) used[col[ci[k]]] = 1;
+    int c = 0;
+    while (used[c]) c++;
+    col[I] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  std::vector<int> cptr(ncol + 1, 0), crow(A.nbr);
+  for (int I = 0; I < A.nbr; I++) cptr[col[I] + 1]++;
+  for (int c = 0; c < ncol; c++) cptr[c + 1] += cptr[c];
+  {
+    std::vector<int> f(cptr.begin(), cptr.end() - 1);
+    for (int I = 0; I < A.nbr; I++) crow[f[col[I]]++] = I;
+  }
+  DBuf<int> d_col, d_crow;
+  DBuf<double> Minv, r, z, zz, p, q, sc;
+  if ((rv = d_col.upload(col.data(), col.size())) || (rv = d_crow.upload(crow.data(), crow.size()))) return rv;
+  if ((rv = Minv.alloc(n)) || (rv = r.alloc(n)) || (rv = z.alloc(n)) || (rv = zz.alloc(n)) || (rv = p.alloc(n)) ||
+      (rv = q.alloc(n)) || (rv = sc.alloc(2)))
+    return rv;
+  Dots D;
+  if ((rv = D.init(4)) != UFEM_AF_OK) return rv;
+  unsigned g = (unsigned)((n + 255) / 256);
+  k_recip<<<g, 256>>>(n, M.p, Minv.p);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  spmv_launch(A, d_x, r.p);
+  k_sub<<<g, 256>>>(n, d_b, r.p, r.p);
+  long it;
+  int status = UFEM_AF_ERR;
+  for (it = 1; it <= maxIt; it++) {
+    for (int c = 0; c < ncol; c++) {
+      int nr = cptr[c + 1] - cptr[c];
+      unsigned gg = (unsigned)((nr + 127) / 128);
+      if (A.B == 3)
+        k_sgs_sweep<3, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                           r.p, zz.p);
+      else if (A.B == 2)
+        k_sgs_sweep<2, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                           r.p, zz.p);
+      else
+        k_sgs_sweep<1, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                           r.p, zz.p);
+    }
+    for (int c = ncol - 1; c >= 0; c--) {
+      int nr = cptr[c + 1] - cptr[c];
+      unsigned gg = (unsigned)((nr + 127) / 128);
+      if (A.B == 3)
+        k_sgs_sweep<3, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                            zz.p, z.p);
+      else if (A.B == 2)
+        k_sgs_sweep<2, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                            zz.p, z.p);
+      else
+        k_sgs_sweep<1, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
+                                            zz.p, z.p);
+    }
+    D.dot(n, r.p, z.p, 0);  // ro
+    if (it > 1) k_copy_scalar<<<1, 1>>>(sc.p + 1, sc.p + 0);
+    k_copy_scalar<<<1, 1>>>(sc.p + 0, D.vals.p + 0);
+    // sc[0] = ro, sc[1] = roro (beta = ro/roro)
+    k_cg_p<<<g, 256>>>(n, it == 1, sc.p, z.p, p.p);
+    spmv_launch(A, p.p, q.p);
+    D.dot(n, p.p, q.p, 1);
+    k_cg_xr<<<g, 256>>>(n, sc.p, D.vals.p + 1, d_x, r.p, p.p, q.p);
+    double normRes = host_norm(n, r.p);
+    double normX = host_norm(n, d_x);
+    bool conv = stop_rule == UFEM_STOP_REFERENCE ? normRes <= (eps * ((normA * normX) + normB))
+                                                 : normRes <= eps * normB;
+    if (!std::isfinite(normRes)) break;
+    if (conv) {
+      status = UFEM_AF_OK;
+      break;
+    }
+  }
+  UFEM_CUDA_TRY(cudaGetLastError());
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float tm = 0;
+  cudaEventElapsedTime(&tm, e0, e1);
+  if (ms) *ms = tm;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (iters) *iters = it > maxIt ? maxIt : it;
+  return status;
+}
+
+// true residual |b - A x| / |b| in FP64 (host helper for the RELRES rule)
+double true_relres(const DevMatrix &A, const double *d_b, const double *d_x) {
+  const long n = (long)A.nbr * A.B;
+  DBuf<double> t;
+  if (t.alloc(n) != UFEM_AF_OK) return NAN;
+  spmv_launch(A, d_x, t.p);
+  unsigned g = (unsigned)((n + 255) / 256);
+  k_sub<<<g, 256>>>(n, d_b, t.p, t.p);
+  return host_norm(n, t.p) / host_norm(n, d_b);
+}
+
+}  // namespace ufem

@@ -1,0 +1,171 @@
+// Internal definitions shared by the host model code and the CUDA kernels of
+// libufem_gpu.so.  Not part of the public ABI (include/ufem_gpu.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ufem_gpu.h"
+
+namespace ufem {
+
+constexpr int KNOWN_DOFS = 7;             // DOF slots per node, fem/fem_elem.h:43
+constexpr double FEM_ZERO = 1e-17;        // fem/fem.h:59
+
+void set_error(const std::string &msg);
+
+#define UFEM_CUDA_TRY(call)                                                          \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      ::ufem::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));        \
+      return (e_ == cudaErrorMemoryAllocation) ? UFEM_AF_ERR_MEM : UFEM_AF_ERR;      \
+    }                                                                                \
+  } while (0)
+
+// A device allocation owned by the model.
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return UFEM_AF_ERR_MEM;
+    }
+    n = count;
+    return UFEM_AF_OK;
+  }
+  int upload(const T *h, size_t count) {
+    int rv = alloc(count);
+    if (rv != UFEM_AF_OK) return rv;
+    if (count) {
+      cudaError_t e = cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        set_error(std::string("cudaMemcpy H2D: ") + cudaGetErrorString(e));
+        return UFEM_AF_ERR;
+      }
+    }
+    return UFEM_AF_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+};
+
+// One support or nodal load line of the input (fem/fem_io.c:97-107).
+struct NodalLoad {
+  long node, type, dir;
+  double val;
+};
+
+}  // namespace ufem
+
+// The model: host copies of the reference tables, the derived GPU layout and
+// the device state.  Block-sparse layout: block size b = DOFs per node (2 for
+// quads, 3 for bricks); block row r = r-th node used by an element (the
+// reference numbers DOFs node-major over used nodes, so DOF = b*r + d + 1).
+struct ufem_model {
+  // ---- host tables -------------------------------------------------------
+  long nLen = 0, eLen = 0;
+  std::vector<double> xyz;            // nLen*3
+  std::vector<long> eType, eRS, eMP;  // eLen
+  std::vector<int> enodes;            // eLen*nn node positions
+  int nn = 0;                         // nodes per element (4 or 8)
+  int b = 0;                          // DOFs per node (2 or 3)
+  int etype = 0;                      // 2 = quad, 9 = brick
+  std::vector<double> eE, eNu, eThick;  // per-element E, nu, thickness
+  std::vector<long> eMat;             // material position per element (for MC)
+  std::vector<std::vector<double>> mpVals;  // material records
+  std::vector<long> mpTypeH;
+  std::vector<long> nID, eID;         // identifiers (names), for MC variable names
+  std::vector<long> mpID, rsID;
+  std::vector<ufem::NodalLoad> loads;
+
+  // ---- DOF map and pattern -------------------------------------------------
+  long nDOFAct = 0;
+  std::vector<long> nDOFfld;          // nLen*7, 1-based DOF numbers, 0 unused
+  std::vector<int> node_rank;         // nLen, block row of a node or -1
+  std::vector<int> rank_node;         // nbr
+  int nbr = 0;                        // block rows
+  long nnzb = 0;                      // blocks
+  std::vector<int> rowptr, colind, diagblk;
+  int ncolours = 0;
+  std::vector<int> colour_ptr, colour_elems;  // elements grouped by colour
+  std::vector<int> emap;              // eLen*nn*nn block index per node pair
+
+  // ---- supports / loads ----------------------------------------------------
+  std::vector<double> F_loads;        // F after fem_add_loads (host, reference order)
+  bool has_nonzero_bc = false;
+  std::vector<long> reacNode, reacDof;  // fem_sol_res_alloc order
+  std::vector<int> reacRow;           // 0-based DOF index or -1
+  std::vector<double> reacFval;       // F value at the time each support was applied
+  std::vector<unsigned char> fixedMask;  // nDOFAct, zero-valued supports
+
+  // ---- Monte Carlo variable table (fem/fem_mont.c:866) ---------------------
+  long mc_ilen = 0, mc_olen = 0;
+  std::vector<long> mc_pos, mc_type, mc_item, mc_sub, mc_iter;
+
+  // ---- device state --------------------------------------------------------
+  int device = 0;
+  ufem::DBuf<double> d_xyz;
+  ufem::DBuf<int> d_enodes, d_emap, d_colour_elems, d_rowptr, d_colind, d_diagblk;
+  ufem::DBuf<int> d_blkrow;           // block -> block row
+  ufem::DBuf<int> d_noderank;         // node -> block row or -1
+  ufem::DBuf<double> d_eE, d_eNu, d_eThick;
+  ufem::DBuf<double> d_val;           // nnzb*b*b FP64 K
+  ufem::DBuf<double> d_F, d_u;
+  ufem::DBuf<unsigned char> d_fixed;
+  ufem::DBuf<double> d_sig, d_vm, d_fint;
+  bool assembled = false, bcs_applied = false;
+  double ms_fill = 0, ms_bc = 0, ms_solve = 0, ms_results = 0;
+  std::vector<double> reacVal;
+};
+
+namespace ufem {
+
+// host model construction (model.cpp)
+int build_model(ufem_model *m);
+int setup_loads(ufem_model *m);
+int read_input_file(const char *fname, ufem_model **out);
+int model_from_tables(const ufem_tables *t, ufem_model *m);
+int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, long *len);
+
+// device work (kernels.cu)
+int upload_model(ufem_model *m);
+int gpu_fill_K(ufem_model *m);
+int gpu_element_matrices(ufem_model *m, double *hKe);
+int gpu_add_loads(ufem_model *m);
+int gpu_add_disps(ufem_model *m);
+int gpu_results(ufem_model *m);
+int gpu_solve(ufem_model *m, int solver, int stop_rule, double eps, long maxIt, long *iters);
+
+// generic solvers on a CSR matrix already on the device (solve.cu)
+struct DevMatrix {
+  int B;            // block size (1 = scalar CSR)
+  int nbr;          // block rows
+  long nnzb;
+  const int *rowptr, *colind;
+  const double *val;
+};
+int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
+                   int stop_rule, long *iters, float *ms);
+int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
+                         int stop_rule, long *iters, float *ms);
+int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
+                 int stop_rule, long *iters, float *ms);
+
+}  // namespace ufem
