@@ -91,6 +91,12 @@ int ufem_read_input(const char *fname, ufem_model **out);
 
 void ufem_model_free(ufem_model *m);
 
+/* Attaches a Monte Carlo variable table to a model built from tables: the
+ * rows of the input file's Monte Carlo section (fem_monte_read_data,
+ * fem/fem_mont.c:866-905), vars[(ilen+olen)*5] = (position, type, item,
+ * subitem, subitem iteration) per variable, inputs first. */
+int ufem_model_set_mc_vars(ufem_model *m, long ilen, long olen, const long *vars);
+
 /* nDOFAct (fem/fem_sol.c:46) and nDOFfld[nLen*7] (fem/fem_sol.c:1263-1395) */
 long ufem_ndof(const ufem_model *m);
 int  ufem_get_ndoffld(const ufem_model *m, long *nDOFfld);
@@ -196,6 +202,14 @@ int ufem_mc_solve(int nmesh, ufem_model *const *models, const long *nsamp,
                   const double *const *ifld, double *const *ofld, int *const *status,
                   long *const *iters, const double *const *u_guess, const ufem_mc_options *opt);
 
+/* The plain method: the same samples solved one at a time, each by FP64
+ * assembly (fem_fill_K), supports and the persistent FP64 Jacobi PCG to the
+ * true relative residual tol -- what monte_solution does per call
+ * (fem/fem_mont.c:694), kept as the comparison baseline of the batched
+ * solve.  Arguments as ufem_mc_solve for one mesh. */
+int ufem_mc_solve_serial(ufem_model *m, long nsamp, const double *ifld, double *ofld, int *status, long *iters,
+                         double tol);
+
 /* Same, with every input and output already in device memory (for timing the
  * kernels without host transfers). */
 int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp,
@@ -213,6 +227,8 @@ typedef struct ufem_mc_stats {
   double pcg_bytes;          /* algorithmic bytes of all PCG iterations */
   double spmv_bytes;         /* algorithmic bytes of the SpMV phases only */
   long kernel_launches;
+  long pcg_launches;         /* persistent PCG launches (one per refinement step) */
+  double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 

@@ -39,7 +39,8 @@ class McOptions(C.Structure):
 class McStats(C.Structure):
     _fields_ = [("ms_assemble", C.c_double), ("ms_pcg", C.c_double), ("ms_refine", C.c_double),
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
-                ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long)]
+                ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long),
+                ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16)]
 
 
 _SIGS = {
@@ -48,6 +49,7 @@ _SIGS = {
     "ufem_model_create": (C.c_int, [C.POINTER(Tables), C.POINTER(C.c_void_p)]),
     "ufem_read_input": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "ufem_model_free": (None, [C.c_void_p]),
+    "ufem_model_set_mc_vars": (C.c_int, [C.c_void_p, C.c_long, C.c_long, _l]),
     "ufem_ndof": (C.c_long, [C.c_void_p]),
     "ufem_get_ndoffld": (C.c_int, [C.c_void_p, _l]),
     "ufem_export_rowslot": (C.c_int, [C.c_void_p, _l, _l, _l, _l]),
@@ -86,6 +88,7 @@ _SIGS = {
                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(McOptions)]),
     "ufem_mc_get_stats": (C.c_int, [C.POINTER(McStats)]),
+    "ufem_mc_solve_serial": (C.c_int, [C.c_void_p, C.c_long, _d, _d, _i, _l, C.c_double]),
 }
 
 # every symbol include/ufem_gpu.h declares (checked by the CPU test suite)

@@ -78,6 +78,13 @@ class GpuModel:
             t, self._keep = tables_of(model)
             _lib.check("ufem_model_create", L.ufem_model_create(C.byref(t), C.byref(h)))
         self.h = h
+        if model is not None and model.mc_vars is not None and model.mc_ilen > 0:
+            self.set_mc_vars(model.mc_ilen, model.mc_olen, model.mc_vars)
+
+    def set_mc_vars(self, ilen: int, olen: int, table):
+        """Attach a Monte Carlo variable table (rows: pos, type, item, sub, iter)."""
+        v = np.ascontiguousarray(np.asarray(table, np.int64).ravel())
+        _lib.check("ufem_model_set_mc_vars", _lib.load().ufem_model_set_mc_vars(self.h, ilen, olen, _lp(v)))
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

@@ -81,7 +81,10 @@ McPlan *get_plan(const ufem_model *m) {
   return g_plans.back().get();
 }
 
+void drop_work(const ufem_model *m);
+
 void drop_plan(const ufem_model *m) {
+  drop_work(m);
   for (size_t i = 0; i < g_plan_owner.size(); i++)
     if (g_plan_owner[i] == m) {
       g_plan_owner.erase(g_plan_owner.begin() + i);
@@ -693,6 +696,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       tile_spmv<T, B>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
+    // The group counter only changes in phase S; every block reads it here,
+    // between the two barriers, so all blocks take the same exit decision.
+    const int remaining = atomicAdd(A.active_count, 0);
     // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
     for (int t = blockIdx.x; t < A.ntiles; t += G) {
       const int4 ti = A.tiles[t];
@@ -728,7 +734,6 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, false, s_red, s_red2);
     }
     if (!grid_barrier(A.bar)) return;
-    const int remaining = atomicAdd(A.active_count, 0);
     if (remaining <= 0 || k > A.maxit + 1) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
@@ -868,6 +873,33 @@ struct McWork {
 
 static ufem_mc_stats g_stats;
 
+// Workspaces are kept per model between calls, so repeated batches reuse
+// their device buffers instead of allocating gigabytes each time.
+static std::vector<std::pair<const ufem_model *, std::unique_ptr<McWork>>> g_work;
+
+McWork *get_work(const ufem_model *m) {
+  for (auto &w : g_work)
+    if (w.first == m) return w.second.get();
+  g_work.emplace_back(m, std::unique_ptr<McWork>(new McWork()));
+  return g_work.back().second.get();
+}
+
+void drop_work(const ufem_model *m) {
+  for (size_t i = 0; i < g_work.size(); i++)
+    if (g_work[i].first == m) {
+      g_work.erase(g_work.begin() + i);
+      return;
+    }
+}
+
+// vector-of-pointers view with the indexing of a vector of workspaces
+struct WorkRef {
+  std::vector<McWork *> &v;
+  explicit WorkRef(std::vector<McWork *> &x) : v(x) {}
+  McWork &operator[](size_t i) { return *v[i]; }
+  const McWork &operator[](size_t i) const { return *v[i]; }
+};
+
 extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->precision = 1;
   o->tol = 1e-8;
@@ -905,7 +937,7 @@ struct EvTimer {
 };
 
 template <typename T>
-int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, const ufem_mc_options &opt,
+int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_options &opt,
               long remaining_cap, long *iters_run) {
   constexpr int VN = VecOf<T>::N, GS = 32 * VN;
   int rv;
@@ -946,9 +978,9 @@ int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, cons
       b.V = w.V32.p;
       b.M = w.M32.p;
       b.b = w.b32.p;
-      if ((rv = w.fx.alloc(n)) || (rv = w.fr.alloc(n)) || (rv = w.fz.alloc(n)) || (rv = w.fp0.alloc(n)) ||
-          (rv = w.fp1.alloc(n)) || (rv = w.fq.alloc(n)) || (rv = w.fpq.alloc(np)) || (rv = w.fprr.alloc(2 * np)) ||
-          (rv = w.fprz.alloc(2 * np)) || (rv = w.frho.alloc(2 * w.S)) || (rv = w.ftol2.alloc(w.S)))
+      if ((rv = w.fx.ensure(n)) || (rv = w.fr.ensure(n)) || (rv = w.fz.ensure(n)) || (rv = w.fp0.ensure(n)) ||
+          (rv = w.fp1.ensure(n)) || (rv = w.fq.ensure(n)) || (rv = w.fpq.ensure(np)) || (rv = w.fprr.ensure(2 * np)) ||
+          (rv = w.fprz.ensure(2 * np)) || (rv = w.frho.ensure(2 * w.S)) || (rv = w.ftol2.ensure(w.S)))
         return rv;
       b.x = w.fx.p; b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
       b.part_pq = w.fpq.p; b.part_rr = w.fprr.p; b.part_rz = w.fprz.p; b.rho = w.frho.p; b.tol2 = w.ftol2.p;
@@ -957,12 +989,12 @@ int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, cons
     } else {
       b.V = w.V64.p;
       b.M = w.M64.p;
-      if ((rv = w.db.alloc(n)) != UFEM_AF_OK) return rv;
+      if ((rv = w.db.ensure(n)) != UFEM_AF_OK) return rv;
       UFEM_CUDA_TRY(cudaMemcpyAsync(w.db.p, w.r64.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
       b.b = w.db.p;
-      if ((rv = w.dx.alloc(n)) || (rv = w.dr.alloc(n)) || (rv = w.dz.alloc(n)) || (rv = w.dp0.alloc(n)) ||
-          (rv = w.dp1.alloc(n)) || (rv = w.dq.alloc(n)) || (rv = w.dpq.alloc(np)) || (rv = w.dprr.alloc(2 * np)) ||
-          (rv = w.dprz.alloc(2 * np)) || (rv = w.drho.alloc(2 * w.S)) || (rv = w.dtol2.alloc(w.S)))
+      if ((rv = w.dx.ensure(n)) || (rv = w.dr.ensure(n)) || (rv = w.dz.ensure(n)) || (rv = w.dp0.ensure(n)) ||
+          (rv = w.dp1.ensure(n)) || (rv = w.dq.ensure(n)) || (rv = w.dpq.ensure(np)) || (rv = w.dprr.ensure(2 * np)) ||
+          (rv = w.dprz.ensure(2 * np)) || (rv = w.drho.ensure(2 * w.S)) || (rv = w.dtol2.ensure(w.S)))
         return rv;
       b.x = w.dx.p; b.r = w.dr.p; b.z = w.dz.p; b.p0 = w.dp0.p; b.p1 = w.dp1.p; b.q = w.dq.p;
       b.part_pq = w.dpq.p; b.part_rr = w.dprr.p; b.part_rz = w.dprz.p; b.rho = w.drho.p; b.tol2 = w.dtol2.p;
@@ -971,7 +1003,7 @@ int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, cons
     }
     b.state = w.state.p;
     b.iters = w.iters.p;
-    if ((rv = w.gactive.alloc(b.ngroups)) != UFEM_AF_OK) return rv;
+    if ((rv = w.gactive.ensure(b.ngroups)) != UFEM_AF_OK) return rv;
     b.gactive = w.gactive.p;
     // per-sample tolerance and state on the host
     std::vector<T> tol2(w.S);
@@ -1015,24 +1047,55 @@ int run_inner(int nmesh, ufem_model *const *models, std::vector<McWork> &W, cons
   a.iter_out = itout.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0);
   UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kThreads), args, 0, 0));
+  cudaEventRecord(ev1);
   g_stats.kernel_launches += 1;
   long its = 0;
   GridBar hb;
   UFEM_CUDA_TRY(cudaMemcpy(&its, itout.p, sizeof(long), cudaMemcpyDeviceToHost));
   UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+  float kms = 0;
+  cudaEventElapsedTime(&kms, ev0, ev1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  g_stats.ms_pcg += kms;
+  g_stats.pcg_launch_ms[std::min<long>(g_stats.pcg_launches, 15)] = kms;
+  g_stats.pcg_launches += 1;
   if (hb.err) {
     set_error("batched PCG: grid barrier timed out");
     return UFEM_AF_ERR;
   }
   *iters_run = its;
-  // algorithmic bytes of the iterations run (sample-weighted by the mesh sizes)
+  // Algorithmic bytes of the iterations run.  A group of GS samples stops
+  // moving data once all of its samples are done, so each group is counted
+  // for the iterations it was live; the index arrays once per mesh-iteration.
   for (int k = 0; k < nmesh; k++) {
     const ufem_model *m = models[k];
-    const double S = W[k].S, n = (double)m->nDOFAct, bb = m->b * m->b;
-    const double spmv = m->nnzb * (bb * sizeof(T) * S + 4.0) + 4.0 * (m->nbr + 1) + 2.0 * n * S * sizeof(T);
-    g_stats.spmv_bytes += spmv * its;
-    g_stats.pcg_bytes += (spmv + 11.0 * n * S * sizeof(T)) * its;
+    const McWork &w = W[k];
+    std::vector<int> st(w.S), itv(w.S);
+    UFEM_CUDA_TRY(cudaMemcpy(st.data(), w.state.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+    UFEM_CUDA_TRY(cudaMemcpy(itv.data(), w.iters.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+    const double n = (double)m->nDOFAct, bb = m->b * m->b;
+    long mesh_its = 0;
+    for (int g = 0; g < w.S / GS; g++) {
+      long gi = 0;
+      for (int s = g * GS; s < (g + 1) * GS; s++) {
+        if (st[s] == ST_SKIP) continue;
+        long si = (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
+        gi = std::max(gi, si);
+      }
+      mesh_its = std::max(mesh_its, gi);
+      const double vals = m->nnzb * bb * sizeof(T) * GS, vec = n * GS * sizeof(T);
+      g_stats.spmv_bytes += (vals + 2.0 * vec) * gi;
+      g_stats.pcg_bytes += (vals + 13.0 * vec) * gi;
+    }
+    const double idx = m->nnzb * 4.0 + 4.0 * (m->nbr + 1);
+    g_stats.spmv_bytes += idx * mesh_its;
+    g_stats.pcg_bytes += idx * mesh_its;
   }
   return UFEM_AF_OK;
 }
@@ -1055,7 +1118,9 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       return UFEM_AF_ERR_TYP;
     }
   EvTimer total;
-  std::vector<McWork> W(nmesh);
+  std::vector<McWork *> Wp(nmesh);
+  for (int k = 0; k < nmesh; k++) Wp[k] = get_work(models[k]);
+  WorkRef W(Wp);
   std::vector<McPlan *> plans(nmesh);
   // ---- plans, inputs and batched assembly --------------------------------
   {
@@ -1071,13 +1136,13 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       w.S = std::max(GSf, (int)((nsamp[k] + 127) / 128 * 128));
       w.GS = GSf;
       const size_t n = (size_t)m->nDOFAct * w.S, nv = (size_t)m->nnzb * B * B * w.S;
-      if ((rv = w.E.alloc((size_t)m->eLen * w.S)) || (rv = w.F.alloc(n)) || (rv = w.Fraw.alloc(n)) ||
-          (rv = w.V64.alloc(nv)) || (rv = w.M64.alloc(n)) || (rv = w.u64.alloc(n)) || (rv = w.r64.alloc(n)) ||
-          (rv = w.state.alloc(w.S)) || (rv = w.iters.alloc(w.S)) || (rv = w.solve.alloc(w.S)) ||
-          (rv = w.rr.alloc(w.S)) || (rv = w.ff.alloc(w.S)))
+      if ((rv = w.E.ensure((size_t)m->eLen * w.S)) || (rv = w.F.ensure(n)) || (rv = w.Fraw.ensure(n)) ||
+          (rv = w.V64.ensure(nv)) || (rv = w.M64.ensure(n)) || (rv = w.u64.ensure(n)) || (rv = w.r64.ensure(n)) ||
+          (rv = w.state.ensure(w.S)) || (rv = w.iters.ensure(w.S)) || (rv = w.solve.ensure(w.S)) ||
+          (rv = w.rr.ensure(w.S)) || (rv = w.ff.ensure(w.S)))
         return rv;
       if (opt.precision != 0) {
-        if ((rv = w.V32.alloc(nv)) || (rv = w.M32.alloc(n)) || (rv = w.b32.alloc(n))) return rv;
+        if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n)) || (rv = w.b32.ensure(n))) return rv;
       }
       const long ne = (long)m->eLen * w.S;
       k_make_E<<<(unsigned)((ne + 255) / 256), 256>>>((int)m->eLen, w.S, w.nsamp, P->ilen, d_ifld[k],
@@ -1103,8 +1168,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       } else {
         UFEM_CUDA_TRY(cudaMemsetAsync(w.u64.p, 0, n * sizeof(double)));
       }
-      if ((rv = w.part_rr.alloc((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)) ||
-          (rv = w.part_ff.alloc((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)))
+      if ((rv = w.part_rr.ensure((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)) ||
+          (rv = w.part_ff.ensure((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)))
         return rv;
       w.h_state.assign(w.S, ST_SKIP);
       w.h_iters.assign(w.S, 0);
@@ -1172,13 +1237,11 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
     // inner solve of K d = r for the samples still active
     long its = 0;
     {
-      EvTimer t;
       long cap = opt.max_iters - iter_total;
       if (cap < 1) cap = 1;
       if (opt.precision != 0) rv = run_inner<float>(nmesh, models, W, opt, cap, &its);
       else rv = run_inner<double>(nmesh, models, W, opt, cap, &its);
       if (rv != UFEM_AF_OK) return rv;
-      g_stats.ms_pcg += t.stop();
     }
     iter_total += its;
     g_stats.pcg_iterations += its;

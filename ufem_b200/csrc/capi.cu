@@ -81,6 +81,26 @@ void ufem_model_free(ufem_model *m) {
   delete m;
 }
 
+int ufem_model_set_mc_vars(ufem_model *m, long ilen, long olen, const long *vars) {
+  if (!m || ilen < 0 || olen < 0) return UFEM_AF_ERR_VAL;
+  m->mc_ilen = ilen;
+  m->mc_olen = olen;
+  m->mc_pos.clear();
+  m->mc_type.clear();
+  m->mc_item.clear();
+  m->mc_sub.clear();
+  m->mc_iter.clear();
+  for (long i = 0; i < ilen + olen; i++) {
+    m->mc_pos.push_back(vars[5 * i]);
+    m->mc_type.push_back(vars[5 * i + 1]);
+    m->mc_item.push_back(vars[5 * i + 2]);
+    m->mc_sub.push_back(vars[5 * i + 3]);
+    m->mc_iter.push_back(vars[5 * i + 4]);
+  }
+  drop_plan(m);
+  return UFEM_AF_OK;
+}
+
 long ufem_ndof(const ufem_model *m) { return m ? m->nDOFAct : 0; }
 
 int ufem_get_ndoffld(const ufem_model *m, long *nDOFfld) {

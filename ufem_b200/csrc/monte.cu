@@ -303,6 +303,52 @@ int monte_solution(char *param, double *ifld, double *ofld, long if_type) {
   return UFEM_AF_OK;
 }
 
+int ufem_mc_solve_serial(ufem_model *m, long nsamp, const double *ifld, double *ofld, int *status, long *iters,
+                         double tol) {
+  if (!m) return UFEM_AF_ERR;
+  int rv;
+  const int nip = m->etype == 2 ? 4 : 27, ns = m->etype == 2 ? 3 : 6;
+  std::vector<double> u(m->nDOFAct), sig;
+  for (long s = 0; s < nsamp; s++) {
+    const double *in = ifld + s * m->mc_ilen;
+    double *out = ofld + s * m->mc_olen;
+    for (long i = 0; i < m->mc_olen; i++) out[m->mc_pos[m->mc_ilen + i]] = 0;
+    if ((rv = apply_inputs(m, in)) != UFEM_AF_OK) return rv;
+    long it = 0;
+    if ((rv = ufem_fill_K(m, 0)) != UFEM_AF_OK) return rv;
+    if ((rv = ufem_add_loads(m)) != UFEM_AF_OK) return rv;
+    UFEM_CUDA_TRY(cudaMemset(m->d_u.p, 0, m->nDOFAct * sizeof(double)));
+    if ((rv = ufem_add_disps(m)) != UFEM_AF_OK) return rv;
+    int srv = ufem_solve(m, UFEM_SOLVER_CGWJ, UFEM_STOP_RELRES, tol, 10 * m->nDOFAct, &it);
+    if (status) status[s] = srv == UFEM_AF_OK ? UFEM_ST_CONVERGED : UFEM_ST_MAXIT;
+    if (iters) iters[s] = it;
+    if ((rv = ufem_fill_K(m, 1)) != UFEM_AF_OK) return rv;
+    if ((rv = ufem_get_u(m, u.data())) != UFEM_AF_OK) return rv;
+    for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
+      const long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i], itr = m->mc_iter[i];
+      double &o = out[m->mc_pos[i - m->mc_ilen]];
+      if (ty == 8 && item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS) {
+        long p = m->nDOFfld[item * KNOWN_DOFS + sub - 1];
+        o = p > 0 ? u[p - 1] : 0.0;
+      } else if (ty == 9) {
+        for (size_t r = 0; r < m->reacNode.size(); r++)
+          if (m->reacNode[r] == item && m->reacDof[r] == sub) {
+            o = m->reacVal[r];
+            break;
+          }
+      } else if (ty == 10) {
+        const int c = stress_comp(m, sub);
+        if (c >= 0 && item >= 0 && item < m->eLen && itr >= 1 && itr <= nip) {
+          if (sig.empty()) sig.resize((size_t)m->eLen * nip * ns);
+          if ((rv = ufem_get_stresses(m, sig.data(), nullptr)) != UFEM_AF_OK) return rv;
+          o = sig[((size_t)item * nip + itr - 1) * ns + c];
+        }
+      }
+    }
+  }
+  return UFEM_AF_OK;
+}
+
 int monte_solution_batch(char *param, long nsamp, const double *ifld, double *ofld, long if_type, int *status) {
   (void)param;
   if (!g_mc) return UFEM_AF_ERR;

@@ -43,8 +43,13 @@ struct DBuf {
     n = count;
     return UFEM_AF_OK;
   }
+  // keeps the allocation when it is already large enough (workspace reuse)
+  int ensure(size_t count) {
+    if (p && n >= count && count > 0) return UFEM_AF_OK;
+    return alloc(count);
+  }
   int upload(const T *h, size_t count) {
-    int rv = alloc(count);
+    int rv = ensure(count);
     if (rv != UFEM_AF_OK) return rv;
     if (count) {
       cudaError_t e = cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice);

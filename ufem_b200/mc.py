@@ -115,3 +115,16 @@ def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1
 
 def stats_dict(s) -> dict:
     return {f: getattr(s, f) for f, _ in s._fields_}
+
+
+def mc_solve_serial(model: GpuModel, ifld: np.ndarray, tol: float = 1e-8):
+    """The plain method: one sample at a time, FP64 assembly + FP64 Jacobi PCG."""
+    L = _lib.load()
+    f = np.ascontiguousarray(ifld, np.float64)
+    n = f.shape[0]
+    olen = model.model.mc_olen
+    o = np.zeros((n, max(olen, 1)))
+    st = np.zeros(n, np.int32)
+    it = np.zeros(n, np.int64)
+    _lib.check("ufem_mc_solve_serial", L.ufem_mc_solve_serial(model.h, n, _dp(f), _dp(o), _ip(st), _lp(it), tol))
+    return o[:, :olen], st, it
