@@ -165,6 +165,24 @@ int ufem_eqs_bicgs(long rows, const long *frompos, const long *defpos, const lon
 int ufem_eqs_cgwssor(long rows, const long *frompos, const long *defpos, const long *pos,
                      const double *data, const double *b, double *x, double eps, long maxIt);
 
+/* Jacobi PCG that allocates nothing.  No counterpart in the reference: it
+ * serves callers that may not allocate device memory while they solve -- an
+ * application whose own allocator owns the device pool, a solve issued from
+ * inside another GPU library's callback, a loop that must avoid cudaMalloc's
+ * implicit synchronisation.  Same algorithm, stopping rule and return codes
+ * as ufem_eqs_cgwj, but the matrix is the GPU block-sparse form already in
+ * device memory: block size B (1 = plain CSR), nbr block rows, d_rowptr
+ * [nbr+1] and d_colind (0-based, int32), d_val (nnzb*B*B doubles, row-major
+ * blocks); d_b and d_x (initial guess in, solution out) are device vectors
+ * of nbr*B doubles.  All scratch lives in one array built into the library:
+ * at most 131,072 rows (larger systems return AF_ERR_SIZ), about 6.3 MB held
+ * on every GPU that loads the library until the process exits.  Calls share
+ * that array: calls that overlap on the GPU race and must be serialised.
+ * The first call on each device looks the array up (make it before any
+ * stream capture). */
+int ufem_eqs_cgwj_noalloc(int B, int nbr, const int *d_rowptr, const int *d_colind, const double *d_val,
+                          const double *d_b, double *d_x, double eps, long maxIt, long *iters);
+
 /* ---- Monte Carlo plugin ABI (fem/fem_mont.c:137-866) --------------------- */
 long  monte_dlib_interface_type(void);                                  /* :137 */
 void  monte_nums_of_vars(char *param, long *ilen, long *olen, long *ffunc); /* :146 */

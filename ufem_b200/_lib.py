@@ -73,6 +73,8 @@ _SIGS = {
     "ufem_eqs_cgwj": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),
     "ufem_eqs_bicgs": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),
     "ufem_eqs_cgwssor": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),
+    "ufem_eqs_cgwj_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_double, C.c_long, _l]),
     "monte_dlib_interface_type": (C.c_long, []),
     "monte_nums_of_vars": (None, [C.c_char_p, _l, _l, _l]),
     "monte_ivar_name": (C.c_char_p, [C.c_char_p, C.c_long]),

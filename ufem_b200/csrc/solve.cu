@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "device_util.cuh"
@@ -762,4 +764,155 @@ double true_relres(const DevMatrix &A, const double *d_b, const double *d_x) {
   return host_norm(n, t.p) / host_norm(n, d_b);
 }
 
+// ---------------------------------------------------------------------------
+// Jacobi PCG without any allocation (ufem_eqs_cgwj_noalloc)
+//
+// Some callers cannot allocate device memory at solve time: code running
+// inside a framework that owns the whole device pool (an embedding
+// application with its own allocator, a solver called from a callback of
+// another GPU library), or a real-time loop that must not hit cudaMalloc's
+// implicit device synchronisation.  For them the persistent Jacobi PCG above
+// runs with all of its scratch -- the diagonal, the five work vectors, the
+// per-block partial sums, the grid barrier and the result words -- placed in
+// one fixed array compiled into this library.  The caller passes the matrix,
+// the right-hand side and the solution in device memory.
+//
+// Limits: at most kNoallocMaxRows scalar rows (131,072) and kNoallocMaxGrid
+// blocks; the array takes about 6.3 MB on every GPU that loads the library,
+// until the process exits.  All calls share the one array, so calls that
+// overlap on the GPU (two host threads, or two streams) race; serialise
+// them.  The first call on a device looks the array's device address up
+// (once per device, with that device current) and should come before any
+// stream capture.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long kNoallocMaxRows = 131072;
+constexpr int kNoallocMaxGrid = 1024;
+constexpr int kNoallocHeader = 64;  // doubles: barrier, result, norms, flags
+constexpr long kNoallocDoubles = kNoallocHeader + (long)kDotBlocks + 4L * kNoallocMaxGrid + 6L * kNoallocMaxRows;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
+
+struct NoallocHeader {  // overlays the first kNoallocHeader doubles
+  GridBar bar;
+  CgResult res;
+  unsigned long long normA_bits;
+  int zero_row;
+  int pad;
+  double normB2;
+};
+static_assert(sizeof(NoallocHeader) <= kNoallocHeader * sizeof(double), "scratch header too large");
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[64] = {nullptr};
+
+}  // namespace
+
+int cg_jacobi_fp64_noalloc(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
+                           long *iters) {
+  const long n = (long)A.nbr * A.B;
+  if (iters) *iters = 0;
+  if (A.B < 1 || A.B > 3 || A.nbr < 1) {
+    set_error("ufem_eqs_cgwj_noalloc: block size must be 1, 2 or 3 and the matrix non-empty");
+    return UFEM_AF_ERR_SIZ;
+  }
+  if (n > kNoallocMaxRows) {
+    set_error("ufem_eqs_cgwj_noalloc: more than 131072 rows; use ufem_eqs_cgwj or ufem_solve");
+    return UFEM_AF_ERR_SIZ;
+  }
+  int dev = 0, nsm = 0, occ = 0;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("ufem_eqs_cgwj_noalloc: device index out of range");
+    return UFEM_AF_ERR;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("ufem_eqs_cgwj_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return UFEM_AF_ERR;
+    }
+    g_noalloc_addr[dev] = static_cast<double *>(p);
+  }
+  double *base = g_noalloc_addr[dev];
+  NoallocHeader *hdr = reinterpret_cast<NoallocHeader *>(base);
+  double *dots = base + kNoallocHeader;
+  double *part = dots + kDotBlocks;
+  double *M = part + 4L * kNoallocMaxGrid;
+  double *r = M + kNoallocMaxRows, *z = r + kNoallocMaxRows, *p0 = z + kNoallocMaxRows;
+  double *p1 = p0 + kNoallocMaxRows, *q = p1 + kNoallocMaxRows;
+  // what must start at zero: the barrier, the result, the norm maximum;
+  // the zero-diagonal flag starts at INT_MAX (atomicMin target)
+  UFEM_CUDA_TRY(cudaMemset(base, 0, kNoallocHeader * sizeof(double)));
+  const int big = 0x7fffffff;
+  UFEM_CUDA_TRY(cudaMemcpy(&hdr->zero_row, &big, sizeof(int), cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemset(p0, 0, n * sizeof(double)));
+  UFEM_CUDA_TRY(cudaMemset(p1, 0, n * sizeof(double)));
+  const unsigned g = (unsigned)((n + 255) / 256);
+  switch (A.B) {
+    case 1: k_diag<1><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M, &hdr->zero_row);
+            k_row_norm_max<1><<<g, 256>>>(A.nbr, A.rowptr, A.val, &hdr->normA_bits); break;
+    case 2: k_diag<2><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M, &hdr->zero_row);
+            k_row_norm_max<2><<<g, 256>>>(A.nbr, A.rowptr, A.val, &hdr->normA_bits); break;
+    default: k_diag<3><<<g, 256>>>(A.nbr, A.rowptr, A.colind, A.val, M, &hdr->zero_row);
+             k_row_norm_max<3><<<g, 256>>>(A.nbr, A.rowptr, A.val, &hdr->normA_bits); break;
+  }
+  k_dot_part<<<kDotBlocks, kThreads>>>(n, d_b, d_b, dots);
+  k_dot_final<<<1, 32>>>(dots, kDotBlocks, &hdr->normB2);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  NoallocHeader h;
+  UFEM_CUDA_TRY(cudaMemcpy(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost));
+  double normA;
+  memcpy(&normA, &h.normA_bits, sizeof(normA));
+  const double normB = std::sqrt(h.normB2);
+  if (!(normB > 0.0)) {  // zero load: x = 0 (fem/fem_eqs.c:108-116)
+    UFEM_CUDA_TRY(cudaMemset(d_x, 0, n * sizeof(double)));
+    return UFEM_AF_OK;
+  }
+  if (h.zero_row != big) {
+    set_error("matrix member on the diagonal has zero size");
+    return UFEM_AF_ERR_ZER;
+  }
+  UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  void (*kern)(CgArgs) = A.B == 1 ? k_cg_fp64<1> : (A.B == 2 ? k_cg_fp64<2> : k_cg_fp64<3>);
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  if (occ < 1) {
+    set_error("persistent CG kernel does not fit on an SM");
+    return UFEM_AF_ERR;
+  }
+  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  G = std::max(1, std::min(G, kNoallocMaxGrid));
+  CgArgs a;
+  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
+  a.M = M; a.r = r; a.z = z; a.p0 = p0; a.p1 = p1; a.q = q; a.part = part;
+  a.bar = &hdr->bar; a.res = &hdr->res; a.eps = eps; a.normA = normA; a.normB = normB;
+  a.maxIt = maxIt; a.stop_rule = UFEM_STOP_REFERENCE;
+  void *args[] = {&a};
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
+  UFEM_CUDA_TRY(cudaMemcpy(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h.bar.err) {
+    set_error("persistent CG: grid barrier timed out");
+    return UFEM_AF_ERR;
+  }
+  if (iters) *iters = h.res.iters < 0 ? -h.res.iters : h.res.iters;
+  if (h.res.status != UFEM_AF_OK) set_error("unconverged solution");
+  return h.res.status;
+}
+
 }  // namespace ufem
+
+// The allocation-free Jacobi PCG (declared in include/ufem_gpu.h).
+extern "C" int ufem_eqs_cgwj_noalloc(int B, int nbr, const int *d_rowptr, const int *d_colind, const double *d_val,
+                                     const double *d_b, double *d_x, double eps, long maxIt, long *iters) {
+  ufem::DevMatrix A;
+  A.B = B;
+  A.nbr = nbr;
+  A.nnzb = 0;
+  A.rowptr = d_rowptr;
+  A.colind = d_colind;
+  A.val = d_val;
+  return ufem::cg_jacobi_fp64_noalloc(A, d_b, d_x, eps, maxIt, iters);
+}
