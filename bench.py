@@ -46,9 +46,29 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nsamp", type=int, default=NSAMP)
     p.add_argument("--plain-samples", type=int, default=16, help="samples per mesh timed by the plain method")
-    p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of the bounded CPU sample")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
+    p.add_argument("--profile-case", action="store_true",
+                   help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
     return p.parse_args()
+
+
+def profile_case():
+    """A bounded case of the same kernels for profiler captures: the 60x15x15
+    mesh, 128 samples (values 1.76 GB FP32 > L2), the inner PCG capped at 40
+    iterations and one refinement step, run twice (warm + captured)."""
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    from ufem_b200 import meshgen as mg
+    m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
+    mg.mc_attach_vars(m)
+    f = mg.mc_samples(m, mesh_id=2, nsamp=128)
+    g = GpuModel(m)
+    for _ in range(2):
+        res, st = mc_solve([g], [f], max_iters=40, max_refine=1)
+    print(json.dumps({"profile_case": "60x15x15 x 128 samples, 40 iterations", "pcg_ms": st.ms_pcg,
+                      "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
+                      "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))
 
 
 def build_meshes(nsamp, rank=0):
@@ -359,7 +379,7 @@ def ours(a):
                 traffic = None
         # ---- CPU baseline: the reference on a bounded sample ------------------
         cpu = None
-        if os.path.exists(REF_LIB):
+        if os.path.exists(REF_LIB) and not a.no_cpu:
             procs = host_cores()
             with tempfile.TemporaryDirectory() as d:
                 files = ref_files(models, [f[:max(1, procs)] for f in iflds], d)
@@ -398,6 +418,9 @@ def main():
     a = parse()
     if a.ref_worker:
         ref_worker(a.ref_worker)
+        return
+    if a.profile_case:
+        profile_case()
         return
     if a.impl == "reference":
         reference_arm(a)
