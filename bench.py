@@ -65,7 +65,7 @@ def profile_case():
     f = mg.mc_samples(m, mesh_id=2, nsamp=128)
     g = GpuModel(m)
     for _ in range(2):
-        res, st = mc_solve([g], [f], max_iters=40, max_refine=1)
+        res, st = mc_solve([g], [f], max_iters=40)
     print(json.dumps({"profile_case": "60x15x15 x 128 samples, 40 iterations", "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
                       "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))

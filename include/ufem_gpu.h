@@ -199,15 +199,17 @@ int   monte_solution(char *param, double *ifld, double *ofld, long if_type); /* 
 int monte_solution_batch(char *param, long nsamp, const double *ifld, double *ofld,
                          long if_type, int *status);
 
-/* Options of the batched solve. precision 0: FP64 PCG; 1: FP32 inner PCG in
- * FP64 iterative refinement.  tol: true relative residual |f-Ku|/|f|. */
+/* Options of the batched solve.  precision 0: FP64 PCG; 1: FP32 PCG (FP32
+ * matrix and work vectors) with the solution kept in FP64 and the residual
+ * replaced by the true FP64 residual f - K u from time to time.  A sample
+ * converges when its true relative residual |f - K u| / |f| <= tol. */
 typedef struct ufem_mc_options {
   int precision;
   double tol;
-  double inner_tol;          /* relative reduction per refinement step (FP32) */
-  long max_iters;            /* total PCG iteration cap per sample */
-  int max_refine;            /* FP64 refinement steps */
-  int use_graphs;            /* capture the inner iteration in a CUDA graph */
+  long max_iters;            /* PCG iteration cap per sample */
+  long replace_every;        /* at most this many iterations between FP64 residual replacements */
+  double replace_near;       /* also replace when the recursive residual reaches replace_near * tol */
+  int use_graphs;            /* reserved */
 } ufem_mc_options;
 void ufem_mc_default_options(ufem_mc_options *o);
 

@@ -109,8 +109,6 @@ def test_uneven_meshes_one_launch(precision):
             reac = o["reac"]
             reac_idx = [j for j, row in enumerate(m.mc_vars[m.mc_ilen:]) if row[1] == mg.MONTE_VTYPE_RES_R]
             # reaction outputs: first support node, UX and UZ
-            sup = m.nl_node[np.nonzero(m.nl_type == 1)[0][0]]
-            ref_r = [reac[i] for i in range(len(reac)) if False]
             rlist = list(zip(o_reac_nodes(m), o_reac_dofs(m)))
             for j in reac_idx:
                 row = m.mc_vars[m.mc_ilen + j]
@@ -181,5 +179,5 @@ def test_iteration_cap_reports_maxit():
     m = mg.beam_brick(8, 2, 2, 4.0, 1.0, 1.0, per_element_material=True)
     mg.mc_attach_vars(m)
     f = mg.mc_samples(m, 3, 5)
-    res, _ = mc_solve([GpuModel(m)], [f], max_iters=3, max_refine=1)
+    res, _ = mc_solve([GpuModel(m)], [f], max_iters=3)
     assert (res[0][1] == ST_MAXIT).all()

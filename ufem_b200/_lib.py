@@ -32,8 +32,8 @@ class Tables(C.Structure):
 
 
 class McOptions(C.Structure):
-    _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("inner_tol", C.c_double),
-                ("max_iters", C.c_long), ("max_refine", C.c_int), ("use_graphs", C.c_int)]
+    _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iters", C.c_long),
+                ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int)]
 
 
 class McStats(C.Structure):

@@ -19,18 +19,21 @@
 // sums are deterministic without atomics.  Supports are applied in the same
 // pass (rows/columns of fixed DOFs -> identity, fem/fem_loads.c:158-166).
 //
-// Solve: FP64 iterative refinement around an inner Jacobi PCG.  The inner
-// PCG (FP32, or FP64 when precision = 0) is one persistent cooperative
-// kernel over work tiles (mesh, sample group, block-row chunk) of every mesh;
-// two bounded grid barriers per iteration; per-sample convergence masks
-// freeze converged samples, a group of GS samples drops out when all of its
-// samples are done, and the launch ends when no group is left or at the
+// Solve: Jacobi PCG with the FP32 matrix and FP32 work vectors (FP64 when
+// precision = 0), one persistent cooperative kernel over work tiles (mesh,
+// sample group, block-row chunk) of every mesh.  The solution is kept in
+// FP64 (x += alpha p in FP64), and the recursive residual is replaced by the
+// true residual f - K x, computed in FP64 from the FP64 values, every
+// replace_every iterations and whenever it falls to replace_near * tol: the
+// CG keeps its search direction across replacements (no restart), so FP32
+// costs about the FP64 iteration count.  A sample converges only on a true
+// residual, |f - K x| / |f| <= tol.  Two bounded grid barriers per
+// iteration (three when a replacement runs); per-sample masks freeze
+// converged samples, a group of GS samples drops out when all of its
+// samples are done, the launch ends when no group is left or at the
 // iteration cap.  Per-sample scalars come from per-tile partials reduced in
 // a fixed order (run-to-run identical); partial buffers are double-buffered
 // by iteration parity so no block overwrites what another still reads.
-// The outer loop forms r = f - K u in FP64 from FP64 values, hands r to the
-// inner solve, adds the correction to the FP64 u and stops each sample at
-// |f - K u| / |f| <= tol.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -285,6 +288,45 @@ __device__ __forceinline__ void stv<double>(double *p, const double (&o)[2]) {
   *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
 }
 
+// streaming (evict-first) loads for data read once per iteration: the
+// matrix values, so that L2 keeps the gathered vectors instead
+template <typename T>
+__device__ __forceinline__ void ldv_stream(const T *p, T (&o)[VecOf<T>::N]);
+template <>
+__device__ __forceinline__ void ldv_stream<float>(const float *p, float (&o)[4]) {
+  float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void ldv_stream<double>(const double *p, double (&o)[2]) {
+  double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+  o[0] = v.x; o[1] = v.y;
+}
+// VN doubles (VN = 2 or 4) at a 16-byte aligned address
+template <int VN>
+__device__ __forceinline__ void ldv_d(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    double2 v = __ldcg(reinterpret_cast<const double2 *>(p) + h);
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
+template <int VN>
+__device__ __forceinline__ void ldv_d_stream(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    double2 v = __ldcs(reinterpret_cast<const double2 *>(p) + h);
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
+template <int VN>
+__device__ __forceinline__ void stv_d(double *p, const double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) reinterpret_cast<double2 *>(p)[h] = make_double2(o[2 * h], o[2 * h + 1]);
+}
+
 // E of every element for every sample: E[e*S + s]
 __global__ void k_make_E(int eLen, int S, int nsamp, long ilen, const double *__restrict__ ifld,
                          const int *__restrict__ elem_var, const double *__restrict__ eE, double *__restrict__ E) {
@@ -362,90 +404,9 @@ __global__ void __launch_bounds__(128) k_assemble_batch(int S, int s_el, const i
     }
 }
 
-// r = F - K u in FP64 (and b32 = (float) r), partial |r|^2 and |F|^2 per
-// (8-row chunk, sample).  grid (ceil(nbr/8), S/64), block 256 = 8 warps.
-template <int B>
-__global__ void __launch_bounds__(kThreads) k_resid64(int nbr, int S, const int *__restrict__ rowptr,
-                                                      const int *__restrict__ colind,
-                                                      const double *__restrict__ V64,
-                                                      const double *__restrict__ F, const double *__restrict__ u,
-                                                      double *__restrict__ r, float *__restrict__ b32,
-                                                      double *__restrict__ part_rr, double *__restrict__ part_ff) {
-  __shared__ double s_rr[kWarps][64], s_ff[kWarps][64];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * kWarps + warp;
-  const int sb = blockIdx.y * 64 + lane * 2;
-  double rr[2] = {0, 0}, ff[2] = {0, 0};
-  if (I < nbr) {
-    double acc[B][2];
-#pragma unroll
-    for (int a = 0; a < B; a++) acc[a][0] = acc[a][1] = 0.0;
-    for (int k = rowptr[I]; k < rowptr[I + 1]; k++) {
-      const int J = colind[k];
-      double xv[B][2];
-#pragma unroll
-      for (int c = 0; c < B; c++) ldv<double>(u + (size_t)(J * B + c) * S + sb, xv[c]);
-#pragma unroll
-      for (int a = 0; a < B; a++)
-#pragma unroll
-        for (int c = 0; c < B; c++) {
-          double vv[2];
-          ldv_ro<double>(V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
-          acc[a][0] += vv[0] * xv[c][0];
-          acc[a][1] += vv[1] * xv[c][1];
-        }
-    }
-#pragma unroll
-    for (int a = 0; a < B; a++) {
-      const size_t o = (size_t)(I * B + a) * S + sb;
-      double f[2];
-      ldv<double>(F + o, f);
-      double rv[2] = {f[0] - acc[a][0], f[1] - acc[a][1]};
-      stv<double>(r + o, rv);
-      if (b32) {
-        b32[o] = (float)rv[0];
-        b32[o + 1] = (float)rv[1];
-      }
-      rr[0] += rv[0] * rv[0];
-      rr[1] += rv[1] * rv[1];
-      ff[0] += f[0] * f[0];
-      ff[1] += f[1] * f[1];
-    }
-  }
-  s_rr[warp][lane * 2] = rr[0];
-  s_rr[warp][lane * 2 + 1] = rr[1];
-  s_ff[warp][lane * 2] = ff[0];
-  s_ff[warp][lane * 2 + 1] = ff[1];
-  __syncthreads();
-  if (threadIdx.x < 64) {
-    double a = 0, b = 0;
-    for (int w = 0; w < kWarps; w++) {
-      a += s_rr[w][threadIdx.x];
-      b += s_ff[w][threadIdx.x];
-    }
-    part_rr[(size_t)blockIdx.x * S + blockIdx.y * 64 + threadIdx.x] = a;
-    part_ff[(size_t)blockIdx.x * S + blockIdx.y * 64 + threadIdx.x] = b;
-  }
-}
-
-__global__ void k_sample_sum(int nchunks, int S, const double *__restrict__ part, double *__restrict__ out) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S) return;
-  double t = 0.0;
-  for (int c = 0; c < nchunks; c++) t += part[(size_t)c * S + s];
-  out[s] = t;
-}
-
-template <typename T>
-__global__ void k_correct(long n, int S, const int *__restrict__ solve, const T *__restrict__ d,
-                          double *__restrict__ u) {
-  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= n * S) return;
-  if (solve[t % S]) u[t] += (double)d[t];
-}
-
 // ---------------------------------------------------------------------------
-// the persistent masked PCG over all meshes
+// ---------------------------------------------------------------------------
+// the persistent masked PCG over all meshes, with residual replacement
 // ---------------------------------------------------------------------------
 enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4 };
 
@@ -453,14 +414,21 @@ template <typename T>
 struct BMesh {
   int nbr, S, ngroups, ntpg, rows_per_tile, B;
   const int *rowptr, *colind;
-  const T *V, *M, *b;
-  T *x, *r, *z, *p0, *p1, *q;
-  T *part_pq, *part_rr, *part_rz;  // [ngroups*ntpg*GS], rr/rz doubled by parity
-  T *rho;                          // [2][S]
-  const T *tol2;                   // [S] squared absolute tolerance
-  int *state;                      // [S]
-  int *iters;                      // [S]
-  int *gactive;                    // [ngroups]
+  const T *V;           // inner-precision values [nnzb*B*B][S]
+  const double *V64;    // FP64 values, for the true residual
+  const T *M;           // diagonal [n][S]
+  const double *F;      // right-hand side (supports applied) [n][S]
+  double *x;            // solution, FP64 [n][S] (in: initial guess)
+  T *r, *z, *p0, *p1, *q;
+  T *part_pq;           // [ngroups*ntpg*GS]
+  T *part_rr, *part_rz; // [2][ngroups*ntpg*GS] by iteration parity
+  T *rho;               // [2][S]
+  const double *tol2;   // [S] (tol |F_s|)^2
+  int *state, *iters;   // [S]
+  int *gactive;         // [ngroups]
+  int *gtrue;           // [ngroups] the group's latest rr partials are true residuals
+  int *gneed;           // [ngroups] a replacement is due after this iteration
+  int *glast;           // [ngroups] iteration of the last replacement
 };
 
 template <typename T>
@@ -469,14 +437,19 @@ struct BArgs {
   const int4 *tiles;  // (mesh, group, chunk, -)
   int ntiles;
   GridBar *bar;
-  int *active_count;
+  int *active_count;  // groups still iterating (changes only in phase S)
+  int *rcount;        // groups due for replacement (changes only in phase U)
   long maxit;
+  long rr_every;      // at most this many iterations between replacements
+  double near2;       // recursive |r|^2 <= near2 * tol2 asks for a replacement
   long *iter_out;
 };
 
+// y = A (z + beta p_old) on the block rows of one tile for GS samples;
+// pnew = z + beta p_old on the own rows; partial p.q per sample.
 template <typename T, int B>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
-                                          T *pold, T *pnew, T (*s_red)[32 * VecOf<T>::N]) {
+                                          const T *pold, T *pnew, T (*s_red)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -496,28 +469,35 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
-    for (int k = k0; k < k1; k++) {
-      const int J = __ldg(M.colind + k);
-      T xv[B][VN];
+    for (int kb = k0; kb < k1; kb += 32) {
+      // the row's column indices, one per lane, then broadcast by shuffle:
+      // the neighbour gathers no longer wait on a dependent index load
+      const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+      const int cnt = min(32, k1 - kb);
+      for (int j = 0; j < cnt; j++) {
+        const int k = kb + j;
+        T vv[B * B][VN];
 #pragma unroll
-      for (int c = 0; c < B; c++) {
-        ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
-        if (!first) {
-          T pv[VN];
-          ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
-#pragma unroll
-          for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < B; a++)
+        for (int e = 0; e < B * B; e++) ldv_stream<T>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
+        const int J = __shfl_sync(0xffffffffu, myJ, j);
+        T xv[B][VN];
 #pragma unroll
         for (int c = 0; c < B; c++) {
-          T vv[VN];
-          ldv_ro<T>(M.V + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+          ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
+          if (!first) {
+            T pv[VN];
+            ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
 #pragma unroll
-          for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
+            for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
+          }
         }
+#pragma unroll
+        for (int a = 0; a < B; a++)
+#pragma unroll
+          for (int c = 0; c < B; c++)
+#pragma unroll
+            for (int v = 0; v < VN; v++) acc[a][v] += vv[a * B + c][v] * xv[c][v];
+      }
     }
 #pragma unroll
     for (int a = 0; a < B; a++) {
@@ -550,55 +530,14 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   __syncthreads();
 }
 
-template <typename T, int B>
-__device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, T *pnew,
-                                            int par, bool init, T (*s_red)[32 * VecOf<T>::N],
-                                            T (*s_red2)[32 * VecOf<T>::N]) {
+// Writes the tile's r.r and r.z partials of parity slot `par`.
+template <typename T>
+__device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const T (&rr)[VecOf<T>::N],
+                                              const T (&rz)[VecOf<T>::N], T (*s_red)[32 * VecOf<T>::N],
+                                              T (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = M.S;
-  const int sb = g * GS + lane * VN;
-  const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
-  T alpha[VN];
-#pragma unroll
-  for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane * VN + v];
-  T rr[VN], rz[VN];
-#pragma unroll
-  for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
-  for (int I = row0 + warp; I < row1; I += kWarps) {
-#pragma unroll
-    for (int a = 0; a < B; a++) {
-      const size_t o = (size_t)(I * B + a) * S + sb;
-      T xi[VN], ri[VN], mi[VN], zi[VN];
-      ldv<T>(M.M + o, mi);
-      if (init) {  // x = 0, r = b, z = b / M (fem/fem_eqs.c:150-162 with x0 = 0)
-        ldv<T>(M.b + o, ri);
-#pragma unroll
-        for (int v = 0; v < VN; v++) xi[v] = 0;
-      } else {
-        T pi[VN], qi[VN];
-        ldv<T>(M.x + o, xi);
-        ldv<T>(M.r + o, ri);
-        ldv<T>(pnew + o, pi);
-        ldv<T>(M.q + o, qi);
-#pragma unroll
-        for (int v = 0; v < VN; v++) {
-          xi[v] = xi[v] + alpha[v] * pi[v];
-          ri[v] = ri[v] - alpha[v] * qi[v];
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < VN; v++) {
-        zi[v] = ri[v] / mi[v];
-        rr[v] += ri[v] * ri[v];
-        rz[v] += ri[v] * zi[v];
-      }
-      stv<T>(M.x + o, xi);
-      stv<T>(M.r + o, ri);
-      stv<T>(M.z + o, zi);
-    }
-  }
 #pragma unroll
   for (int v = 0; v < VN; v++) {
     s_red[warp][lane * VN + v] = rr[v];
@@ -618,6 +557,112 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
   __syncthreads();
 }
 
+// x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z.
+template <typename T, int B>
+__device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, const T *pnew,
+                                            int par, T (*s_red)[32 * VecOf<T>::N], T (*s_red2)[32 * VecOf<T>::N]) {
+  constexpr int VN = VecOf<T>::N;
+  constexpr int GS = 32 * VN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = M.S;
+  const int sb = g * GS + lane * VN;
+  const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
+  T alpha[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane * VN + v];
+  T rr[VN], rz[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
+  for (int I = row0 + warp; I < row1; I += kWarps) {
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      const size_t o = (size_t)(I * B + a) * S + sb;
+      T ri[VN], mi[VN], pi[VN], qi[VN], zi[VN];
+      double xi[VN];
+      ldv<T>(M.M + o, mi);
+      ldv<T>(M.r + o, ri);
+      ldv<T>(pnew + o, pi);
+      ldv<T>(M.q + o, qi);
+      ldv_d<VN>(M.x + o, xi);
+#pragma unroll
+      for (int v = 0; v < VN; v++) {
+        xi[v] += (double)alpha[v] * (double)pi[v];
+        ri[v] = ri[v] - alpha[v] * qi[v];
+        zi[v] = ri[v] / mi[v];
+        rr[v] += ri[v] * ri[v];
+        rz[v] += ri[v] * zi[v];
+      }
+      stv_d<VN>(M.x + o, xi);
+      stv<T>(M.r + o, ri);
+      stv<T>(M.z + o, zi);
+    }
+  }
+  tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
+}
+
+// Residual replacement: r = F - K x in FP64 from the FP64 values, then
+// r (inner precision), z = r / M and the partials of the true residual.
+template <typename T, int B>
+__device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
+                                                   T (*s_red)[32 * VecOf<T>::N], T (*s_red2)[32 * VecOf<T>::N]) {
+  constexpr int VN = VecOf<T>::N;
+  constexpr int GS = 32 * VN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = M.S;
+  const int sb = g * GS + lane * VN;
+  const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
+  T rr[VN], rz[VN];
+#pragma unroll
+  for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
+  for (int I = row0 + warp; I < row1; I += kWarps) {
+    double acc[B][VN];
+#pragma unroll
+    for (int a = 0; a < B; a++)
+#pragma unroll
+      for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
+    const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+      const int cnt = min(32, k1 - kb);
+      for (int j = 0; j < cnt; j++) {
+        const int k = kb + j;
+        const int J = __shfl_sync(0xffffffffu, myJ, j);
+        double xv[B][VN];
+#pragma unroll
+        for (int c = 0; c < B; c++) ldv_d<VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
+#pragma unroll
+        for (int a = 0; a < B; a++)
+#pragma unroll
+          for (int c = 0; c < B; c++) {
+            double vv[VN];
+            ldv_d_stream<VN>(M.V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+#pragma unroll
+            for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
+          }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < B; a++) {
+      const size_t o = (size_t)(I * B + a) * S + sb;
+      double f[VN];
+      T ri[VN], mi[VN], zi[VN];
+      ldv_d<VN>(M.F + o, f);
+      ldv<T>(M.M + o, mi);
+#pragma unroll
+      for (int v = 0; v < VN; v++) {
+        const double r64 = f[v] - acc[a][v];
+        ri[v] = (T)r64;
+        zi[v] = ri[v] / mi[v];
+        rr[v] += (T)(r64 * r64);
+        rz[v] += ri[v] * zi[v];
+      }
+      stv<T>(M.r + o, ri);
+      stv<T>(M.z + o, zi);
+    }
+  }
+  tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
+}
+
 template <typename T>
 __device__ __forceinline__ T group_total(const T *part, int g, int ntpg, int GS, int sl) {
   T t = 0;
@@ -633,8 +678,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
   __shared__ T s_red2[kWarps][GS];
   __shared__ T s_sc[GS];
   __shared__ BMesh<T> s_m;
+  __shared__ int s_flag;
   const int G = gridDim.x;
-  // phase 0: r = b, z = b / M, x = 0 and the partials of iteration 0
+  // phase 0: the true residual of the initial guess (parity slot 0)
   for (int t = blockIdx.x; t < A.ntiles; t += G) {
     const int4 ti = A.tiles[t];
     if (threadIdx.x == 0) s_m = A.meshes[ti.x];
@@ -643,7 +689,13 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
     int any = 0;
     if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
     any = __syncthreads_or(any);
-    if (any) tile_update<T, B>(M, ti.y, ti.z, s_sc, nullptr, 0, true, s_red, s_red2);
+    if (any) {
+      tile_true_residual<T, B>(M, ti.y, ti.z, 0, s_red, s_red2);
+      if (ti.z == 0 && threadIdx.x == 0) {
+        M.gtrue[ti.y] = 1;
+        M.glast[ti.y] = 0;
+      }
+    }
     __syncthreads();
   }
   if (!grid_barrier(A.bar)) return;
@@ -651,28 +703,34 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
   for (k = 1;; k++) {
     const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
     const bool first = (k == 1);
-    // ---- phase S: convergence masks, beta, q = A p ------------------------
+    // ---- phase S: convergence on true residuals, beta, q = A p -------------
     for (int t = blockIdx.x; t < A.ntiles; t += G) {
       const int4 ti = A.tiles[t];
-      if (threadIdx.x == 0) s_m = A.meshes[ti.x];
+      if (threadIdx.x == 0) {
+        s_m = A.meshes[ti.x];
+        s_flag = __ldcg(A.meshes[ti.x].gtrue + ti.y);
+      }
       __syncthreads();
       const BMesh<T> &M = s_m;
       const int g = ti.y;
-      int upd = 0;
+      const bool is_true = s_flag != 0;
+      int upd = 0, near = 0;
       if (threadIdx.x < GS) {
         const int sl = threadIdx.x, s = g * GS + sl;
         const size_t half = (size_t)M.ngroups * M.ntpg * GS;
         const T rr = group_total(M.part_rr + (size_t)parm1 * half, g, M.ntpg, GS, sl);
         const T rzn = group_total(M.part_rz + (size_t)parm1 * half, g, M.ntpg, GS, sl);
         const T rzo = first ? T(1) : __ldcg(M.rho + (size_t)parm1 * M.S + s);
+        const double tol2 = M.tol2[s];
         const int st = __ldcg(M.state + s);
         int nst = st;
         if (st == ST_ACTIVE) {
-          if (!(rr > M.tol2[s]) && rr == rr) nst = ST_CONV;
-          else if (!(rr == rr) || isinf(rr)) nst = ST_BREAK;
+          if (!(rr == rr) || isinf(rr)) nst = ST_BREAK;
+          else if (is_true && (double)rr <= tol2) nst = ST_CONV;
           else if (k > A.maxit) nst = ST_MAXIT;
         }
         upd = (nst == ST_ACTIVE);
+        near = upd && !is_true && (double)rr <= A.near2 * tol2;
         s_sc[sl] = upd ? (first ? T(0) : rzn / rzo) : T(0);
         if (ti.z == 0) {  // the group's first tile records per-sample results
           if (nst != st) {
@@ -683,21 +741,25 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
         }
       }
       upd = __syncthreads_or(upd);
-      if (!upd) {
-        if (ti.z == 0 && threadIdx.x == 0 && M.gactive[g]) {
+      near = __syncthreads_or(near);
+      if (ti.z == 0 && threadIdx.x == 0) {
+        if (!upd && M.gactive[g]) {
           M.gactive[g] = 0;
           atomicSub(A.active_count, 1);
         }
+        M.gneed[g] = upd && (near || (k - M.glast[g] >= A.rr_every));
+      }
+      if (!upd) {
         __syncthreads();
         continue;
       }
-      T *pold = (k & 1) ? M.p0 : M.p1;
+      const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
       tile_spmv<T, B>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
-    // The group counter only changes in phase S; every block reads it here,
-    // between the two barriers, so all blocks take the same exit decision.
+    // The group counter changes only in phase S: read between the barriers,
+    // every block takes the same exit decision.
     const int remaining = atomicAdd(A.active_count, 0);
     // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
     for (int t = blockIdx.x; t < A.ntiles; t += G) {
@@ -725,15 +787,42 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
         s_sc[sl] = alpha;
       }
       upd = __syncthreads_or(upd);
-      // every tile of an active group writes its partials (samples with alpha = 0 keep their r)
       int live = 0;
       if (threadIdx.x < GS) live = (__ldcg(M.state + g * GS + threadIdx.x) == ST_ACTIVE);
       live = __syncthreads_or(live) | upd;
       if (!live) continue;
-      T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, false, s_red, s_red2);
+      const T *pnew = (k & 1) ? M.p1 : M.p0;
+      tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
+      if (ti.z == 0 && threadIdx.x == 0) {
+        M.gtrue[g] = 0;
+        if (__ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
+      }
     }
     if (!grid_barrier(A.bar)) return;
+    // ---- phase R (when a group asked): replace the recursive residual -------
+    const int nrep = atomicAdd(A.rcount, 0);  // changes only in phase U
+    if (nrep > 0) {
+      for (int t = blockIdx.x; t < A.ntiles; t += G) {
+        const int4 ti = A.tiles[t];
+        if (threadIdx.x == 0) {
+          s_m = A.meshes[ti.x];
+          s_flag = __ldcg(A.meshes[ti.x].gneed + ti.y);
+        }
+        __syncthreads();
+        const BMesh<T> &M = s_m;
+        if (!s_flag) {
+          __syncthreads();  // thread 0 rewrites s_m / s_flag for the next tile
+          continue;
+        }
+        tile_true_residual<T, B>(M, ti.y, ti.z, par, s_red, s_red2);
+        if (ti.z == 0 && threadIdx.x == 0) {
+          M.gtrue[ti.y] = 1;
+          M.glast[ti.y] = (int)k;
+        }
+      }
+      if (!grid_barrier(A.bar)) return;
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(A.rcount, 0);  // read again only after the next U
+    }
     if (remaining <= 0 || k > A.maxit + 1) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
@@ -853,22 +942,34 @@ __global__ void k_outputs(int nout, int S, int nsamp, long olen, const int *__re
   ofld[(size_t)s * olen + opos[o]] = val;
 }
 
+// (|F_s| tol)^2 per sample and |F_s|^2 (rows summed in order: deterministic)
+__global__ void k_tol2(long n, int S, const double *__restrict__ F, double tol, double *__restrict__ tol2,
+                       double *__restrict__ ff) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  double t = 0.0;
+  for (long i = 0; i < n; i++) {
+    double f = F[(size_t)i * S + s];
+    t += f * f;
+  }
+  ff[s] = t;
+  tol2[s] = tol * tol * t;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
 struct McWork {
-  int S = 0, nsamp = 0, ngroups = 0, GS = 0;
-  DBuf<double> E, F, Fraw, V64, M64, u64, r64, part_rr, part_ff, rr, ff;
-  DBuf<float> V32, M32, b32;
-  // inner vectors in the inner precision
-  DBuf<float> fx, fr, fz, fp0, fp1, fq, fpq, fprr, fprz, frho, ftol2;
-  DBuf<double> dx, dr, dz, dp0, dp1, dq, dpq, dprr, dprz, drho, dtol2, db;
-  DBuf<int> state, iters, solve;
-  DBuf<int> gactive;
-  std::vector<int> h_state, h_iters;
-  std::vector<double> h_rr, h_ff;
+  int S = 0, nsamp = 0;
+  DBuf<double> E, F, Fraw, V64, M64, x64, tol2, ff;
+  DBuf<float> V32, M32;
+  // inner vectors, FP32 or FP64
+  DBuf<float> fr, fz, fp0, fp1, fq, fpq, fprr, fprz, frho;
+  DBuf<double> dr, dz, dp0, dp1, dq, dpq, dprr, dprz, drho;
+  DBuf<int> state, iters, gactive, gtrue, gneed, glast;
+  std::vector<double> h_ff;
 };
 
 static ufem_mc_stats g_stats;
@@ -892,20 +993,12 @@ void drop_work(const ufem_model *m) {
     }
 }
 
-// vector-of-pointers view with the indexing of a vector of workspaces
-struct WorkRef {
-  std::vector<McWork *> &v;
-  explicit WorkRef(std::vector<McWork *> &x) : v(x) {}
-  McWork &operator[](size_t i) { return *v[i]; }
-  const McWork &operator[](size_t i) const { return *v[i]; }
-};
-
 extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->precision = 1;
   o->tol = 1e-8;
-  o->inner_tol = 1e-4;
   o->max_iters = 20000;
-  o->max_refine = 6;
+  o->replace_every = 50;
+  o->replace_near = 0.5;
   o->use_graphs = 0;
 }
 
@@ -937,8 +1030,8 @@ struct EvTimer {
 };
 
 template <typename T>
-int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_options &opt,
-              long remaining_cap, long *iters_run) {
+int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, const ufem_mc_options &opt,
+            long *iters_run) {
   constexpr int VN = VecOf<T>::N, GS = 32 * VN;
   int rv;
   std::vector<BMesh<T>> hm(nmesh);
@@ -953,16 +1046,16 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
     set_error("batched PCG kernel does not fit on an SM");
     return UFEM_AF_ERR;
   }
-  const int G = nsm * std::min(occ, 2);
-  // rows per tile: about two tiles per block over the whole batch
+  const int G = nsm * occ;
+  // rows per tile: about three tiles per block over the whole batch
   long total_rows = 0;
-  for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k].S / GS);
-  int rpt = (int)std::max<long>(kWarps, (total_rows + 2L * G - 1) / (2L * G));
+  for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
+  int rpt = (int)std::max<long>(kWarps, (total_rows + 3L * G - 1) / (3L * G));
   rpt = (rpt + kWarps - 1) / kWarps * kWarps;
   int active_groups = 0;
   for (int k = 0; k < nmesh; k++) {
     ufem_model *m = models[k];
-    McWork &w = W[k];
+    McWork &w = *W[k];
     BMesh<T> &b = hm[k];
     b.nbr = m->nbr;
     b.S = w.S;
@@ -972,57 +1065,60 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
     b.B = m->b;
     b.rowptr = m->d_rowptr.p;
     b.colind = m->d_colind.p;
+    b.V64 = w.V64.p;
+    b.F = w.F.p;
+    b.x = w.x64.p;
+    b.tol2 = w.tol2.p;
     const size_t n = (size_t)m->nDOFAct * w.S;
     const size_t np = (size_t)b.ngroups * b.ntpg * GS;
     if constexpr (sizeof(T) == 4) {
       b.V = w.V32.p;
       b.M = w.M32.p;
-      b.b = w.b32.p;
-      if ((rv = w.fx.ensure(n)) || (rv = w.fr.ensure(n)) || (rv = w.fz.ensure(n)) || (rv = w.fp0.ensure(n)) ||
-          (rv = w.fp1.ensure(n)) || (rv = w.fq.ensure(n)) || (rv = w.fpq.ensure(np)) || (rv = w.fprr.ensure(2 * np)) ||
-          (rv = w.fprz.ensure(2 * np)) || (rv = w.frho.ensure(2 * w.S)) || (rv = w.ftol2.ensure(w.S)))
+      if ((rv = w.fr.ensure(n)) || (rv = w.fz.ensure(n)) || (rv = w.fp0.ensure(n)) || (rv = w.fp1.ensure(n)) ||
+          (rv = w.fq.ensure(n)) || (rv = w.fpq.ensure(np)) || (rv = w.fprr.ensure(2 * np)) ||
+          (rv = w.fprz.ensure(2 * np)) || (rv = w.frho.ensure(2 * w.S)))
         return rv;
-      b.x = w.fx.p; b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
-      b.part_pq = w.fpq.p; b.part_rr = w.fprr.p; b.part_rz = w.fprz.p; b.rho = w.frho.p; b.tol2 = w.ftol2.p;
-      UFEM_CUDA_TRY(cudaMemsetAsync(w.fp0.p, 0, n * sizeof(T)));
-      UFEM_CUDA_TRY(cudaMemsetAsync(w.fp1.p, 0, n * sizeof(T)));
+      b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
+      b.part_pq = w.fpq.p; b.part_rr = w.fprr.p; b.part_rz = w.fprz.p; b.rho = w.frho.p;
     } else {
       b.V = w.V64.p;
       b.M = w.M64.p;
-      if ((rv = w.db.ensure(n)) != UFEM_AF_OK) return rv;
-      UFEM_CUDA_TRY(cudaMemcpyAsync(w.db.p, w.r64.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
-      b.b = w.db.p;
-      if ((rv = w.dx.ensure(n)) || (rv = w.dr.ensure(n)) || (rv = w.dz.ensure(n)) || (rv = w.dp0.ensure(n)) ||
-          (rv = w.dp1.ensure(n)) || (rv = w.dq.ensure(n)) || (rv = w.dpq.ensure(np)) || (rv = w.dprr.ensure(2 * np)) ||
-          (rv = w.dprz.ensure(2 * np)) || (rv = w.drho.ensure(2 * w.S)) || (rv = w.dtol2.ensure(w.S)))
+      if ((rv = w.dr.ensure(n)) || (rv = w.dz.ensure(n)) || (rv = w.dp0.ensure(n)) || (rv = w.dp1.ensure(n)) ||
+          (rv = w.dq.ensure(n)) || (rv = w.dpq.ensure(np)) || (rv = w.dprr.ensure(2 * np)) ||
+          (rv = w.dprz.ensure(2 * np)) || (rv = w.drho.ensure(2 * w.S)))
         return rv;
-      b.x = w.dx.p; b.r = w.dr.p; b.z = w.dz.p; b.p0 = w.dp0.p; b.p1 = w.dp1.p; b.q = w.dq.p;
-      b.part_pq = w.dpq.p; b.part_rr = w.dprr.p; b.part_rz = w.dprz.p; b.rho = w.drho.p; b.tol2 = w.dtol2.p;
-      UFEM_CUDA_TRY(cudaMemsetAsync(w.dp0.p, 0, n * sizeof(T)));
-      UFEM_CUDA_TRY(cudaMemsetAsync(w.dp1.p, 0, n * sizeof(T)));
+      b.r = w.dr.p; b.z = w.dz.p; b.p0 = w.dp0.p; b.p1 = w.dp1.p; b.q = w.dq.p;
+      b.part_pq = w.dpq.p; b.part_rr = w.dprr.p; b.part_rz = w.dprz.p; b.rho = w.drho.p;
     }
+    UFEM_CUDA_TRY(cudaMemsetAsync(b.p0, 0, n * sizeof(T)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(b.p1, 0, n * sizeof(T)));
+    if ((rv = w.gactive.ensure(b.ngroups)) || (rv = w.gtrue.ensure(b.ngroups)) || (rv = w.gneed.ensure(b.ngroups)) ||
+        (rv = w.glast.ensure(b.ngroups)))
+      return rv;
     b.state = w.state.p;
     b.iters = w.iters.p;
-    if ((rv = w.gactive.ensure(b.ngroups)) != UFEM_AF_OK) return rv;
     b.gactive = w.gactive.p;
-    // per-sample tolerance and state on the host
-    std::vector<T> tol2(w.S);
+    b.gtrue = w.gtrue.p;
+    b.gneed = w.gneed.p;
+    b.glast = w.glast.p;
+    UFEM_CUDA_TRY(cudaMemsetAsync(w.gtrue.p, 0, b.ngroups * sizeof(int)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(w.gneed.p, 0, b.ngroups * sizeof(int)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(w.glast.p, 0, b.ngroups * sizeof(int)));
+    // per-sample state: solve the real samples with a nonzero load
     std::vector<int> st(w.S), ga(b.ngroups, 0);
     for (int s = 0; s < w.S; s++) {
-      const bool solve = w.h_state[s] == ST_ACTIVE;
-      const double rn = std::sqrt(w.h_rr[s]), fn = std::sqrt(w.h_ff[s]);
-      const double target = std::max(opt.inner_tol * rn, 0.25 * opt.tol * fn);
-      tol2[s] = (T)(target * target);
-      st[s] = solve ? ST_ACTIVE : ST_SKIP;
-      if (solve) ga[s / GS] = 1;
+      if (s >= w.nsamp) st[s] = ST_SKIP;
+      else if (!(w.h_ff[s] > 0.0)) st[s] = ST_CONV;  // zero load: u = 0 at once
+      else st[s] = ST_ACTIVE;
+      if (st[s] == ST_ACTIVE) ga[s / GS] = 1;
     }
     for (int g = 0; g < b.ngroups; g++) active_groups += ga[g];
-    UFEM_CUDA_TRY(cudaMemcpyAsync((void *)b.tol2, tol2.data(), w.S * sizeof(T), cudaMemcpyHostToDevice));
     UFEM_CUDA_TRY(cudaMemcpyAsync(w.state.p, st.data(), w.S * sizeof(int), cudaMemcpyHostToDevice));
     UFEM_CUDA_TRY(cudaMemsetAsync(w.iters.p, 0, w.S * sizeof(int)));
     UFEM_CUDA_TRY(cudaMemcpyAsync(w.gactive.p, ga.data(), b.ngroups * sizeof(int), cudaMemcpyHostToDevice));
     for (int g = 0; g < b.ngroups; g++)
-      for (int c = 0; c < b.ntpg; c++) tiles.push_back(make_int4(k, g, c, 0));
+      if (ga[g])
+        for (int c = 0; c < b.ntpg; c++) tiles.push_back(make_int4(k, g, c, 0));
   }
   if (active_groups == 0) {
     *iters_run = 0;
@@ -1031,10 +1127,12 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
   DBuf<BMesh<T>> d_meshes;
   DBuf<int4> d_tiles;
   DBuf<GridBar> bar;
-  DBuf<int> cnt;
+  DBuf<int> cnt, rcnt;
   DBuf<long> itout;
+  const int zero = 0;
   if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
-      (rv = bar.alloc(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = itout.alloc(1)))
+      (rv = bar.alloc(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
+      (rv = itout.alloc(1)))
     return rv;
   UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
   BArgs<T> a;
@@ -1043,7 +1141,10 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
   a.ntiles = (int)tiles.size();
   a.bar = bar.p;
   a.active_count = cnt.p;
-  a.maxit = remaining_cap;
+  a.rcount = rcnt.p;
+  a.maxit = opt.max_iters;
+  a.rr_every = std::max<long>(1, opt.replace_every);
+  a.near2 = opt.replace_near * opt.replace_near;
   a.iter_out = itout.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
@@ -1070,12 +1171,12 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
     return UFEM_AF_ERR;
   }
   *iters_run = its;
-  // Algorithmic bytes of the iterations run.  A group of GS samples stops
-  // moving data once all of its samples are done, so each group is counted
-  // for the iterations it was live; the index arrays once per mesh-iteration.
+  // Algorithmic bytes.  A group of GS samples moves data only while it is
+  // live, so each group counts the iterations it ran; the index arrays count
+  // once per mesh-iteration.
   for (int k = 0; k < nmesh; k++) {
     const ufem_model *m = models[k];
-    const McWork &w = W[k];
+    const McWork &w = *W[k];
     std::vector<int> st(w.S), itv(w.S);
     UFEM_CUDA_TRY(cudaMemcpy(st.data(), w.state.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
     UFEM_CUDA_TRY(cudaMemcpy(itv.data(), w.iters.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
@@ -1084,14 +1185,16 @@ int run_inner(int nmesh, ufem_model *const *models, WorkRef &W, const ufem_mc_op
     for (int g = 0; g < w.S / GS; g++) {
       long gi = 0;
       for (int s = g * GS; s < (g + 1) * GS; s++) {
-        if (st[s] == ST_SKIP) continue;
+        if (st[s] == ST_SKIP || s >= w.nsamp) continue;
         long si = (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
         gi = std::max(gi, si);
       }
       mesh_its = std::max(mesh_its, gi);
       const double vals = m->nnzb * bb * sizeof(T) * GS, vec = n * GS * sizeof(T);
       g_stats.spmv_bytes += (vals + 2.0 * vec) * gi;
-      g_stats.pcg_bytes += (vals + 13.0 * vec) * gi;
+      // S phase: values, 2 gathered and 2 own vectors in, 2 out; U phase:
+      // M, r, p, q in, r, z out, x (FP64) in and out
+      g_stats.pcg_bytes += (vals + 11.0 * vec + 2.0 * n * GS * sizeof(double)) * gi;
     }
     const double idx = m->nnzb * 4.0 + 4.0 * (m->nbr + 1);
     g_stats.spmv_bytes += idx * mesh_its;
@@ -1118,11 +1221,9 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       return UFEM_AF_ERR_TYP;
     }
   EvTimer total;
-  std::vector<McWork *> Wp(nmesh);
-  for (int k = 0; k < nmesh; k++) Wp[k] = get_work(models[k]);
-  WorkRef W(Wp);
+  std::vector<McWork *> W(nmesh);
   std::vector<McPlan *> plans(nmesh);
-  // ---- plans, inputs and batched assembly --------------------------------
+  // ---- plans, inputs, batched assembly, tolerances ------------------------
   {
     EvTimer t;
     for (int k = 0; k < nmesh; k++) {
@@ -1130,19 +1231,17 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       McPlan *P = get_plan(m);
       if (!P->built && (rv = build_plan(m, P)) != UFEM_AF_OK) return rv;
       plans[k] = P;
-      McWork &w = W[k];
-      const int GSf = (opt.precision == 0) ? 64 : 128;
+      W[k] = get_work(m);
+      McWork &w = *W[k];
       w.nsamp = (int)nsamp[k];
-      w.S = std::max(GSf, (int)((nsamp[k] + 127) / 128 * 128));
-      w.GS = GSf;
+      w.S = std::max(128, (int)((nsamp[k] + 127) / 128 * 128));
       const size_t n = (size_t)m->nDOFAct * w.S, nv = (size_t)m->nnzb * B * B * w.S;
       if ((rv = w.E.ensure((size_t)m->eLen * w.S)) || (rv = w.F.ensure(n)) || (rv = w.Fraw.ensure(n)) ||
-          (rv = w.V64.ensure(nv)) || (rv = w.M64.ensure(n)) || (rv = w.u64.ensure(n)) || (rv = w.r64.ensure(n)) ||
-          (rv = w.state.ensure(w.S)) || (rv = w.iters.ensure(w.S)) || (rv = w.solve.ensure(w.S)) ||
-          (rv = w.rr.ensure(w.S)) || (rv = w.ff.ensure(w.S)))
+          (rv = w.V64.ensure(nv)) || (rv = w.M64.ensure(n)) || (rv = w.x64.ensure(n)) || (rv = w.state.ensure(w.S)) ||
+          (rv = w.iters.ensure(w.S)) || (rv = w.tol2.ensure(w.S)) || (rv = w.ff.ensure(w.S)))
         return rv;
       if (opt.precision != 0) {
-        if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n)) || (rv = w.b32.ensure(n))) return rv;
+        if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n))) return rv;
       }
       const long ne = (long)m->eLen * w.S;
       k_make_E<<<(unsigned)((ne + 255) / 256), 256>>>((int)m->eLen, w.S, w.nsamp, P->ilen, d_ifld[k],
@@ -1153,128 +1252,43 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       UFEM_CUDA_TRY(cudaMemcpyAsync(w.F.p, w.Fraw.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
       k_fix_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, m->d_fixed.p, w.F.p);
       dim3 ga((unsigned)m->nnzb, (unsigned)(w.S / 128));
+      float *v32 = opt.precision != 0 ? w.V32.p : nullptr;
+      float *m32 = opt.precision != 0 ? w.M32.p : nullptr;
       if (B == 3)
         k_assemble_batch<3><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
-                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, w.V32.p, w.M64.p,
-                                         w.M32.p);
+                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
       else
         k_assemble_batch<2><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
-                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, w.V32.p, w.M64.p,
-                                         w.M32.p);
-      g_stats.kernel_launches += 5;
-      // initial guess
+                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
+      k_tol2<<<(w.S + 127) / 128, 128>>>((long)m->nDOFAct, w.S, w.F.p, opt.tol, w.tol2.p, w.ff.p);
+      g_stats.kernel_launches += 6;
       if (d_u_guess && d_u_guess[k]) {
-        UFEM_CUDA_TRY(cudaMemcpyAsync(w.u64.p, d_u_guess[k], n * sizeof(double), cudaMemcpyDeviceToDevice));
+        UFEM_CUDA_TRY(cudaMemcpyAsync(w.x64.p, d_u_guess[k], n * sizeof(double), cudaMemcpyDeviceToDevice));
       } else {
-        UFEM_CUDA_TRY(cudaMemsetAsync(w.u64.p, 0, n * sizeof(double)));
+        UFEM_CUDA_TRY(cudaMemsetAsync(w.x64.p, 0, n * sizeof(double)));
       }
-      if ((rv = w.part_rr.ensure((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)) ||
-          (rv = w.part_ff.ensure((size_t)((m->nbr + kWarps - 1) / kWarps) * w.S)))
-        return rv;
-      w.h_state.assign(w.S, ST_SKIP);
-      w.h_iters.assign(w.S, 0);
-      w.h_rr.assign(w.S, 0.0);
       w.h_ff.assign(w.S, 0.0);
-      for (int s = 0; s < w.nsamp; s++) w.h_state[s] = ST_ACTIVE;
+      UFEM_CUDA_TRY(cudaMemcpy(w.h_ff.data(), w.ff.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
+      // a sample without load has u = 0, whatever its guess (fem/fem_eqs.c:108-116)
+      for (int s = 0; s < w.nsamp; s++)
+        if (!(w.h_ff[s] > 0.0))
+          UFEM_CUDA_TRY(cudaMemset2DAsync(w.x64.p + s, w.S * sizeof(double), 0, sizeof(double), m->nDOFAct));
     }
     UFEM_CUDA_TRY(cudaGetLastError());
     g_stats.ms_assemble = t.stop();
   }
-  // ---- FP64 refinement around the inner PCG -----------------------------
-  std::vector<std::vector<long>> it_acc(nmesh);
-  std::vector<std::vector<int>> final_status(nmesh);
-  for (int k = 0; k < nmesh; k++) {
-    it_acc[k].assign(W[k].S, 0);
-    final_status[k].assign(W[k].S, UFEM_ST_MAXIT);
-  }
-  long iter_total = 0;
-  for (int step = 0; step <= opt.max_refine; step++) {
-    // r = f - K u (FP64), per-sample |r| and |f|
-    {
-      EvTimer t;
-      for (int k = 0; k < nmesh; k++) {
-        ufem_model *m = models[k];
-        McWork &w = W[k];
-        const int nch = (m->nbr + kWarps - 1) / kWarps;
-        dim3 gr((unsigned)nch, (unsigned)(w.S / 64));
-        float *b32 = (opt.precision != 0) ? w.b32.p : nullptr;
-        if (B == 3)
-          k_resid64<3><<<gr, kThreads>>>(m->nbr, w.S, m->d_rowptr.p, m->d_colind.p, w.V64.p, w.F.p, w.u64.p,
-                                         w.r64.p, b32, w.part_rr.p, w.part_ff.p);
-        else
-          k_resid64<2><<<gr, kThreads>>>(m->nbr, w.S, m->d_rowptr.p, m->d_colind.p, w.V64.p, w.F.p, w.u64.p,
-                                         w.r64.p, b32, w.part_rr.p, w.part_ff.p);
-        k_sample_sum<<<(w.S + 127) / 128, 128>>>(nch, w.S, w.part_rr.p, w.rr.p);
-        k_sample_sum<<<(w.S + 127) / 128, 128>>>(nch, w.S, w.part_ff.p, w.ff.p);
-        g_stats.kernel_launches += 3;
-        UFEM_CUDA_TRY(cudaMemcpyAsync(w.h_rr.data(), w.rr.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
-        UFEM_CUDA_TRY(cudaMemcpyAsync(w.h_ff.data(), w.ff.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
-      }
-      UFEM_CUDA_TRY(cudaDeviceSynchronize());
-      g_stats.ms_refine += t.stop();
-    }
-    bool any = false;
-    for (int k = 0; k < nmesh; k++) {
-      McWork &w = W[k];
-      for (int s = 0; s < w.nsamp; s++) {
-        if (w.h_state[s] != ST_ACTIVE) continue;
-        const double rel = (w.h_ff[s] > 0) ? std::sqrt(w.h_rr[s] / w.h_ff[s]) : 0.0;
-        if (!(rel == rel)) {
-          w.h_state[s] = ST_BREAK;
-          final_status[k][s] = UFEM_ST_NAN;
-        } else if (rel <= opt.tol) {
-          w.h_state[s] = ST_CONV;
-          final_status[k][s] = UFEM_ST_CONVERGED;
-        } else if (step == opt.max_refine || it_acc[k][s] >= opt.max_iters) {
-          w.h_state[s] = ST_MAXIT;
-          final_status[k][s] = UFEM_ST_MAXIT;
-        } else {
-          any = true;
-        }
-      }
-    }
-    if (!any) break;
-    // inner solve of K d = r for the samples still active
-    long its = 0;
-    {
-      long cap = opt.max_iters - iter_total;
-      if (cap < 1) cap = 1;
-      if (opt.precision != 0) rv = run_inner<float>(nmesh, models, W, opt, cap, &its);
-      else rv = run_inner<double>(nmesh, models, W, opt, cap, &its);
-      if (rv != UFEM_AF_OK) return rv;
-    }
-    iter_total += its;
-    g_stats.pcg_iterations += its;
-    {
-      EvTimer t;
-      for (int k = 0; k < nmesh; k++) {
-        ufem_model *m = models[k];
-        McWork &w = W[k];
-        std::vector<int> solve(w.S), st(w.S), itv(w.S);
-        UFEM_CUDA_TRY(cudaMemcpy(st.data(), w.state.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
-        UFEM_CUDA_TRY(cudaMemcpy(itv.data(), w.iters.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
-        for (int s = 0; s < w.S; s++) {
-          solve[s] = (w.h_state[s] == ST_ACTIVE) && st[s] != ST_SKIP;
-          if (solve[s]) it_acc[k][s] += (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
-        }
-        UFEM_CUDA_TRY(cudaMemcpy(w.solve.p, solve.data(), w.S * sizeof(int), cudaMemcpyHostToDevice));
-        const long n = (long)m->nDOFAct * w.S;
-        if (opt.precision != 0)
-          k_correct<float><<<(unsigned)((n + 255) / 256), 256>>>(m->nDOFAct, w.S, w.solve.p, w.fx.p, w.u64.p);
-        else
-          k_correct<double><<<(unsigned)((n + 255) / 256), 256>>>(m->nDOFAct, w.S, w.solve.p, w.dx.p, w.u64.p);
-        g_stats.kernel_launches += 1;
-      }
-      UFEM_CUDA_TRY(cudaGetLastError());
-      g_stats.ms_refine += t.stop();
-    }
-  }
+  // ---- one persistent launch over every mesh -----------------------------
+  long its = 0;
+  if (opt.precision != 0) rv = run_pcg<float>(nmesh, models, W, opt, &its);
+  else rv = run_pcg<double>(nmesh, models, W, opt, &its);
+  if (rv != UFEM_AF_OK) return rv;
+  g_stats.pcg_iterations = its;
   // ---- outputs -------------------------------------------------------------
   {
     EvTimer t;
     for (int k = 0; k < nmesh; k++) {
       ufem_model *m = models[k];
-      McWork &w = W[k];
+      McWork &w = *W[k];
       McPlan *P = plans[k];
       const int nout = (int)P->outs.size();
       if (d_ofld && d_ofld[k] && nout > 0 && w.nsamp > 0) {
@@ -1282,30 +1296,37 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
         if (B == 3)
           k_outputs<3><<<(unsigned)((tot + 127) / 128), 128>>>(
               nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
-              P->d_out_ip.p, P->d_out_comp.p, w.u64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
+              P->d_out_ip.p, P->d_out_comp.p, w.x64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
               P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
               m->d_eThick.p, m->etype, d_ofld[k]);
         else
           k_outputs<2><<<(unsigned)((tot + 127) / 128), 128>>>(
               nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
-              P->d_out_ip.p, P->d_out_comp.p, w.u64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
+              P->d_out_ip.p, P->d_out_comp.p, w.x64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
               P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
               m->d_eThick.p, m->etype, d_ofld[k]);
         g_stats.kernel_launches += 1;
       }
       if (d_u_out && d_u_out[k])
-        UFEM_CUDA_TRY(cudaMemcpyAsync(d_u_out[k], w.u64.p, (size_t)m->nDOFAct * w.S * sizeof(double),
+        UFEM_CUDA_TRY(cudaMemcpyAsync(d_u_out[k], w.x64.p, (size_t)m->nDOFAct * w.S * sizeof(double),
                                       cudaMemcpyDeviceToDevice));
-      std::vector<int> st(w.nsamp);
-      std::vector<long> it(w.nsamp);
+      std::vector<int> st(w.S), itv(w.S);
+      UFEM_CUDA_TRY(cudaMemcpy(st.data(), w.state.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+      UFEM_CUDA_TRY(cudaMemcpy(itv.data(), w.iters.p, w.S * sizeof(int), cudaMemcpyDeviceToHost));
+      std::vector<int> hs(w.nsamp);
+      std::vector<long> hi(w.nsamp);
       for (int s = 0; s < w.nsamp; s++) {
-        st[s] = final_status[k][s];
-        it[s] = it_acc[k][s];
+        switch (st[s]) {
+          case ST_CONV: hs[s] = UFEM_ST_CONVERGED; break;
+          case ST_BREAK: hs[s] = UFEM_ST_BREAKDOWN; break;
+          default: hs[s] = UFEM_ST_MAXIT; break;
+        }
+        hi[s] = (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
       }
       if (d_status && d_status[k] && w.nsamp > 0)
-        UFEM_CUDA_TRY(cudaMemcpy(d_status[k], st.data(), w.nsamp * sizeof(int), cudaMemcpyHostToDevice));
+        UFEM_CUDA_TRY(cudaMemcpy(d_status[k], hs.data(), w.nsamp * sizeof(int), cudaMemcpyHostToDevice));
       if (d_iters && d_iters[k] && w.nsamp > 0)
-        UFEM_CUDA_TRY(cudaMemcpy(d_iters[k], it.data(), w.nsamp * sizeof(long), cudaMemcpyHostToDevice));
+        UFEM_CUDA_TRY(cudaMemcpy(d_iters[k], hi.data(), w.nsamp * sizeof(long), cudaMemcpyHostToDevice));
     }
     UFEM_CUDA_TRY(cudaGetLastError());
     g_stats.ms_outputs = t.stop();
@@ -1325,7 +1346,6 @@ extern "C" int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const 
   return mc_solve_device(nmesh, models, nsamp, d_ifld, d_ofld, d_status, d_iters, d_u_guess, d_u_out, opt);
 }
 
-// The same with host buffers: inputs are copied to the device, results back.
 extern "C" int ufem_mc_solve(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *ifld,
                              double *const *ofld, int *const *status, long *const *iters,
                              const double *const *u_guess, const ufem_mc_options *opt) {

@@ -64,7 +64,7 @@ def default_options():
 
 
 def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1, tol: float = 1e-8,
-             inner_tol: float | None = None, max_iters: int | None = None, max_refine: int | None = None,
+             max_iters: int | None = None, replace_every: int | None = None, replace_near: float | None = None,
              u_guess: list[np.ndarray | None] | None = None, olens: list[int] | None = None):
     """Batched solve of every sample of every mesh in one launch.
 
@@ -75,12 +75,12 @@ def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1
     opt = default_options()
     opt.precision = precision
     opt.tol = tol
-    if inner_tol is not None:
-        opt.inner_tol = inner_tol
     if max_iters is not None:
         opt.max_iters = max_iters
-    if max_refine is not None:
-        opt.max_refine = max_refine
+    if replace_every is not None:
+        opt.replace_every = replace_every
+    if replace_near is not None:
+        opt.replace_near = replace_near
     keep = []
     hs = (C.c_void_p * nm)(*[m.h.value for m in models])
     ns = np.array([f.shape[0] for f in iflds], np.int64)
