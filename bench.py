@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--nsamp", type=int, default=NSAMP)
     p.add_argument("--plain-samples", type=int, default=16, help="samples per mesh timed by the plain method")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
+    p.add_argument("--precision", type=int, default=1,
+                   help="1: FP32 PCG with FP64 solution and residual replacement; 0: FP64 PCG")
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
     p.add_argument("--profile-case", action="store_true",
                    help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
@@ -270,7 +272,7 @@ def ours(a):
     gms = [GpuModel(m) for m in models]
     nm = len(gms)
     opt = default_options()
-    opt.precision = 1
+    opt.precision = a.precision
     opt.tol = 1e-8
     dev = torch.device("cuda", local)
     d_in = [torch.from_numpy(f).to(dev) for f in iflds]
@@ -325,7 +327,25 @@ def ours(a):
     solves_step = int(ns.sum()) * world
     value = solves_step / (ms_step / 1000.0)
     st_ok = all(bool((s == 0).all()) for s in d_st)
-    iters = [int(x.max().item()) for x in d_it]
+    iters_main = [int(x.max().item()) for x in d_it]
+
+    # ---- the other precision, one step, for comparison ----------------------
+    alt = None
+    if rank == 0:
+        opt_main = opt.precision
+        opt.precision = 1 - opt_main
+        step_device()  # builds its buffers
+        torch.cuda.synchronize()
+        e0.record()
+        step_device()
+        e1.record()
+        torch.cuda.synchronize()
+        alt = {"precision": "FP64 PCG" if opt.precision == 0 else "FP32 PCG + FP64 replacement",
+               "value": int(ns.sum()) / (e0.elapsed_time(e1) / 1000.0), "unit": "solves/s",
+               "all_converged": all(bool((s == 0).all()) for s in d_st),
+               "max_iters_per_mesh": [int(x.max().item()) for x in d_it]}
+        opt.precision = opt_main
+    iters = iters_main
 
     # ---- e2e: host (pinned) inputs through the public C ABI call -------------
     h_in = [torch.from_numpy(f).pin_memory() for f in iflds]
@@ -405,7 +425,7 @@ def ours(a):
                          "pcg_iterations_per_step": pcg_its / a.steps},
             "e2e": {"value": solves_step / (e2e_ms / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "matches_device_run": bool(e2e_ok)},
-            "gpu_launches": launches, "clocks": clk.summary(local),
+            "gpu_launches": launches, "clocks": clk.summary(local), "other_precision": alt,
             "cpu_baseline": cpu,
         }
         print(json.dumps(result))

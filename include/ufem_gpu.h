@@ -208,7 +208,8 @@ typedef struct ufem_mc_options {
   double tol;
   long max_iters;            /* PCG iteration cap per sample */
   long replace_every;        /* at most this many iterations between FP64 residual replacements */
-  double replace_near;       /* also replace when the recursive residual reaches replace_near * tol */
+  double replace_near;       /* also replace once the recursive residual has dropped by this factor
+                                since the last replacement, and when it reaches tol */
   int use_graphs;            /* reserved */
 } ufem_mc_options;
 void ufem_mc_default_options(ufem_mc_options *o);

@@ -420,9 +420,10 @@ struct BMesh {
   const double *F;      // right-hand side (supports applied) [n][S]
   double *x;            // solution, FP64 [n][S] (in: initial guess)
   T *r, *z, *p0, *p1, *q;
-  T *part_pq;           // [ngroups*ntpg*GS]
-  T *part_rr, *part_rz; // [2][ngroups*ntpg*GS] by iteration parity
-  T *rho;               // [2][S]
+  double *part_pq;      // [ngroups*ntpg*GS] (dot products accumulate in FP64)
+  double *part_rr, *part_rz;  // [2][ngroups*ntpg*GS] by iteration parity
+  double *rho;          // [2][S]
+  double *rrlast;       // [S] true |r|^2 at the last replacement
   const double *tol2;   // [S] (tol |F_s|)^2
   int *state, *iters;   // [S]
   int *gactive;         // [ngroups]
@@ -441,7 +442,7 @@ struct BArgs {
   int *rcount;        // groups due for replacement (changes only in phase U)
   long maxit;
   long rr_every;      // at most this many iterations between replacements
-  double near2;       // recursive |r|^2 <= near2 * tol2 asks for a replacement
+  double near2;       // recursive |r|^2 <= near2 * (true |r|^2 at the last replacement) asks for one
   long *iter_out;
 };
 
@@ -449,7 +450,7 @@ struct BArgs {
 // pnew = z + beta p_old on the own rows; partial p.q per sample.
 template <typename T, int B>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
-                                          const T *pold, T *pnew, T (*s_red)[32 * VecOf<T>::N]) {
+                                          const T *pold, T *pnew, double (*s_red)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -459,7 +460,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   T beta[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) beta[v] = s_beta[lane * VN + v];
-  T pq[VN];
+  double pq[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) pq[v] = 0;
   for (int I = row0 + warp; I < row1; I += kWarps) {
@@ -516,14 +517,14 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       stv<T>(pnew + o, pi);
       stv<T>(M.q + o, acc[a]);
 #pragma unroll
-      for (int v = 0; v < VN; v++) pq[v] += pi[v] * acc[a][v];
+      for (int v = 0; v < VN; v++) pq[v] += (double)pi[v] * (double)acc[a][v];
     }
   }
 #pragma unroll
   for (int v = 0; v < VN; v++) s_red[warp][lane * VN + v] = pq[v];
   __syncthreads();
   if (threadIdx.x < GS) {
-    T t = 0;
+    double t = 0;
     for (int w = 0; w < kWarps; w++) t += s_red[w][threadIdx.x];
     M.part_pq[((size_t)g * M.ntpg + chunk) * GS + threadIdx.x] = t;
   }
@@ -532,9 +533,9 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
 
 // Writes the tile's r.r and r.z partials of parity slot `par`.
 template <typename T>
-__device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const T (&rr)[VecOf<T>::N],
-                                              const T (&rz)[VecOf<T>::N], T (*s_red)[32 * VecOf<T>::N],
-                                              T (*s_red2)[32 * VecOf<T>::N]) {
+__device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const double (&rr)[VecOf<T>::N],
+                                              const double (&rz)[VecOf<T>::N], double (*s_red)[32 * VecOf<T>::N],
+                                              double (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -545,7 +546,7 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
   }
   __syncthreads();
   if (threadIdx.x < GS) {
-    T a = 0, b = 0;
+    double a = 0, b = 0;
     for (int w = 0; w < kWarps; w++) {
       a += s_red[w][threadIdx.x];
       b += s_red2[w][threadIdx.x];
@@ -560,7 +561,7 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
 // x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z.
 template <typename T, int B>
 __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, const T *pnew,
-                                            int par, T (*s_red)[32 * VecOf<T>::N], T (*s_red2)[32 * VecOf<T>::N]) {
+                                            int par, double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -570,7 +571,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
   T alpha[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane * VN + v];
-  T rr[VN], rz[VN];
+  double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
   for (int I = row0 + warp; I < row1; I += kWarps) {
@@ -589,8 +590,8 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
         xi[v] += (double)alpha[v] * (double)pi[v];
         ri[v] = ri[v] - alpha[v] * qi[v];
         zi[v] = ri[v] / mi[v];
-        rr[v] += ri[v] * ri[v];
-        rz[v] += ri[v] * zi[v];
+        rr[v] += (double)ri[v] * (double)ri[v];
+        rz[v] += (double)ri[v] * (double)zi[v];
       }
       stv_d<VN>(M.x + o, xi);
       stv<T>(M.r + o, ri);
@@ -604,14 +605,14 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
 // r (inner precision), z = r / M and the partials of the true residual.
 template <typename T, int B>
 __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
-                                                   T (*s_red)[32 * VecOf<T>::N], T (*s_red2)[32 * VecOf<T>::N]) {
+                                                   double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
   const int sb = g * GS + lane * VN;
   const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
-  T rr[VN], rz[VN];
+  double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
   for (int I = row0 + warp; I < row1; I += kWarps) {
@@ -653,8 +654,8 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
         const double r64 = f[v] - acc[a][v];
         ri[v] = (T)r64;
         zi[v] = ri[v] / mi[v];
-        rr[v] += (T)(r64 * r64);
-        rz[v] += ri[v] * zi[v];
+        rr[v] += r64 * r64;
+        rz[v] += (double)ri[v] * (double)zi[v];
       }
       stv<T>(M.r + o, ri);
       stv<T>(M.z + o, zi);
@@ -663,9 +664,8 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
-template <typename T>
-__device__ __forceinline__ T group_total(const T *part, int g, int ntpg, int GS, int sl) {
-  T t = 0;
+__device__ __forceinline__ double group_total(const double *part, int g, int ntpg, int GS, int sl) {
+  double t = 0;
   for (int c = 0; c < ntpg; c++) t += __ldcg(part + ((size_t)g * ntpg + c) * GS + sl);
   return t;
 }
@@ -674,8 +674,8 @@ template <typename T, int B>
 __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
-  __shared__ T s_red[kWarps][GS];
-  __shared__ T s_red2[kWarps][GS];
+  __shared__ double s_red[kWarps][GS];
+  __shared__ double s_red2[kWarps][GS];
   __shared__ T s_sc[GS];
   __shared__ BMesh<T> s_m;
   __shared__ int s_flag;
@@ -718,9 +718,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       if (threadIdx.x < GS) {
         const int sl = threadIdx.x, s = g * GS + sl;
         const size_t half = (size_t)M.ngroups * M.ntpg * GS;
-        const T rr = group_total(M.part_rr + (size_t)parm1 * half, g, M.ntpg, GS, sl);
-        const T rzn = group_total(M.part_rz + (size_t)parm1 * half, g, M.ntpg, GS, sl);
-        const T rzo = first ? T(1) : __ldcg(M.rho + (size_t)parm1 * M.S + s);
+        const double rr = group_total(M.part_rr + (size_t)parm1 * half, g, M.ntpg, GS, sl);
+        const double rzn = group_total(M.part_rz + (size_t)parm1 * half, g, M.ntpg, GS, sl);
+        const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
         const double tol2 = M.tol2[s];
         const int st = __ldcg(M.state + s);
         int nst = st;
@@ -730,14 +730,17 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
           else if (k > A.maxit) nst = ST_MAXIT;
         }
         upd = (nst == ST_ACTIVE);
-        near = upd && !is_true && (double)rr <= A.near2 * tol2;
-        s_sc[sl] = upd ? (first ? T(0) : rzn / rzo) : T(0);
+        // replace once the recursive residual has dropped by the factor
+        // near since the last replacement, and to verify convergence
+        near = upd && !is_true && (rr <= A.near2 * __ldcg(M.rrlast + s) || rr <= 0.25 * tol2);
+        s_sc[sl] = upd ? (first ? T(0) : (T)(rzn / rzo)) : T(0);
         if (ti.z == 0) {  // the group's first tile records per-sample results
           if (nst != st) {
             M.state[s] = nst;
             M.iters[s] = (int)(k - 1);
           }
           M.rho[(size_t)par * M.S + s] = rzn;
+          if (is_true) M.rrlast[s] = rr;
         }
       }
       upd = __syncthreads_or(upd);
@@ -774,10 +777,10 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
         const int st = __ldcg(M.state + s);
         T alpha = 0;
         if (st == ST_ACTIVE) {
-          const T pq = group_total(M.part_pq, g, M.ntpg, GS, sl);
-          const T rho = __ldcg(M.rho + (size_t)par * M.S + s);
-          if (pq > T(0) && isfinite(pq)) {
-            alpha = rho / pq;
+          const double pq = group_total(M.part_pq, g, M.ntpg, GS, sl);
+          const double rho = __ldcg(M.rho + (size_t)par * M.S + s);
+          if (pq > 0.0 && isfinite(pq)) {
+            alpha = (T)(rho / pq);
             upd = 1;
           } else if (ti.z == 0) {
             M.state[s] = ST_BREAK;  // p.q <= 0: breakdown, the sample is frozen
@@ -966,8 +969,8 @@ struct McWork {
   DBuf<double> E, F, Fraw, V64, M64, x64, tol2, ff;
   DBuf<float> V32, M32;
   // inner vectors, FP32 or FP64
-  DBuf<float> fr, fz, fp0, fp1, fq, fpq, fprr, fprz, frho;
-  DBuf<double> dr, dz, dp0, dp1, dq, dpq, dprr, dprz, drho;
+  DBuf<float> fr, fz, fp0, fp1, fq;
+  DBuf<double> dr, dz, dp0, dp1, dq, pq, prr, prz, rho, rrlast;
   DBuf<int> state, iters, gactive, gtrue, gneed, glast;
   std::vector<double> h_ff;
 };
@@ -998,7 +1001,7 @@ extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->tol = 1e-8;
   o->max_iters = 20000;
   o->replace_every = 50;
-  o->replace_near = 0.5;
+  o->replace_near = 1e-2;
   o->use_graphs = 0;
 }
 
@@ -1075,21 +1078,21 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       b.V = w.V32.p;
       b.M = w.M32.p;
       if ((rv = w.fr.ensure(n)) || (rv = w.fz.ensure(n)) || (rv = w.fp0.ensure(n)) || (rv = w.fp1.ensure(n)) ||
-          (rv = w.fq.ensure(n)) || (rv = w.fpq.ensure(np)) || (rv = w.fprr.ensure(2 * np)) ||
-          (rv = w.fprz.ensure(2 * np)) || (rv = w.frho.ensure(2 * w.S)))
+          (rv = w.fq.ensure(n)))
         return rv;
       b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
-      b.part_pq = w.fpq.p; b.part_rr = w.fprr.p; b.part_rz = w.fprz.p; b.rho = w.frho.p;
     } else {
       b.V = w.V64.p;
       b.M = w.M64.p;
       if ((rv = w.dr.ensure(n)) || (rv = w.dz.ensure(n)) || (rv = w.dp0.ensure(n)) || (rv = w.dp1.ensure(n)) ||
-          (rv = w.dq.ensure(n)) || (rv = w.dpq.ensure(np)) || (rv = w.dprr.ensure(2 * np)) ||
-          (rv = w.dprz.ensure(2 * np)) || (rv = w.drho.ensure(2 * w.S)))
+          (rv = w.dq.ensure(n)))
         return rv;
       b.r = w.dr.p; b.z = w.dz.p; b.p0 = w.dp0.p; b.p1 = w.dp1.p; b.q = w.dq.p;
-      b.part_pq = w.dpq.p; b.part_rr = w.dprr.p; b.part_rz = w.dprz.p; b.rho = w.drho.p;
     }
+    if ((rv = w.pq.ensure(np)) || (rv = w.prr.ensure(2 * np)) || (rv = w.prz.ensure(2 * np)) ||
+        (rv = w.rho.ensure(2 * w.S)) || (rv = w.rrlast.ensure(w.S)))
+      return rv;
+    b.part_pq = w.pq.p; b.part_rr = w.prr.p; b.part_rz = w.prz.p; b.rho = w.rho.p; b.rrlast = w.rrlast.p;
     UFEM_CUDA_TRY(cudaMemsetAsync(b.p0, 0, n * sizeof(T)));
     UFEM_CUDA_TRY(cudaMemsetAsync(b.p1, 0, n * sizeof(T)));
     if ((rv = w.gactive.ensure(b.ngroups)) || (rv = w.gtrue.ensure(b.ngroups)) || (rv = w.gneed.ensure(b.ngroups)) ||
