@@ -253,6 +253,28 @@ typedef struct ufem_mc_stats {
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 
+/* ---- learned warm start: the MLP (no counterpart in the reference; the
+ * closest hook is the disabled warm start of monte_linear_solver,
+ * fem/fem_mont.c:493-504) ---------------------------------------------------
+ * n_in -> n_hidden -> n_hidden -> n_out, GELU, mean-squared-error training
+ * with Adam.  Every product runs on the tensor cores (tcgen05, BF16 operands,
+ * FP32 accumulation); master weights FP32.  Parameters flat: W1 [n_hidden]
+ * [32] (inputs zero-padded to 32), b1, W2 [n_hidden][n_hidden], b2,
+ * W3 [n_out][n_hidden], b3.  d_* are device pointers, row-major FP32. */
+typedef struct ufem_mlp ufem_mlp;
+int  ufem_mlp_create(int n_in, int n_hidden, int n_out, unsigned long long seed, ufem_mlp **out);
+void ufem_mlp_free(ufem_mlp *p);
+long ufem_mlp_num_params(const ufem_mlp *p);
+int  ufem_mlp_get_params(const ufem_mlp *p, float *h_params);
+int  ufem_mlp_set_params(ufem_mlp *p, const float *h_params);
+int  ufem_mlp_forward(ufem_mlp *p, long nbatch, const float *d_x, float *d_y);
+int  ufem_mlp_gradients(ufem_mlp *p, long nbatch, const float *d_x, const float *d_t, float *h_grad, float *loss);
+int  ufem_mlp_train_step(ufem_mlp *p, long nbatch, const float *d_x, const float *d_t, float lr, float *loss);
+/* C [M x N] = A [M x K] . B [N x K]^T, BF16 in, FP32 out, on the tensor
+ * cores (the GEMM of the MLP, exposed for its tests); N a multiple of 16,
+ * at most 256. */
+int  ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, float *d_C);
+
 /* ---- device / diagnostics ------------------------------------------------ */
 int ufem_device_info(int *sm_count, int *cc_major, int *cc_minor, long *mem_bytes);
 const char *ufem_last_error(void);

@@ -91,6 +91,17 @@ _SIGS = {
                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(McOptions)]),
     "ufem_mc_get_stats": (C.c_int, [C.POINTER(McStats)]),
     "ufem_mc_solve_serial": (C.c_int, [C.c_void_p, C.c_long, _d, _d, _i, _l, C.c_double]),
+    "ufem_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "ufem_mlp_free": (None, [C.c_void_p]),
+    "ufem_mlp_num_params": (C.c_long, [C.c_void_p]),
+    "ufem_mlp_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "ufem_mlp_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "ufem_mlp_forward": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p]),
+    "ufem_mlp_gradients": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float)]),
+    "ufem_mlp_train_step": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_float,
+                                      C.POINTER(C.c_float)]),
+    "ufem_tc_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 # every symbol include/ufem_gpu.h declares (checked by the CPU test suite)

@@ -1,0 +1,561 @@
+// The warm-start network: a 3-layer GELU MLP (n_in -> H -> H -> n_out) that
+// maps a Monte Carlo sample's random parameters to coefficients on a POD
+// basis of earlier solutions.  No counterpart in the reference (the closest
+// hook is the disabled warm start of monte_linear_solver, fem/fem_mont.c:493-504).
+//
+// Every matrix product, forward and backward, runs on the 5th-generation
+// tensor cores through one hand-written kernel, k_gemm_tc:
+//   C[M x N] = A[M x K] . B[N x K]^T   (BF16 operands, FP32 accumulation)
+// * A and B are staged from global memory (any element strides, so the
+//   backward products read transposed operands without copies) into shared
+//   memory in the canonical no-swizzle K-major layout of the UMMA
+//   descriptors: 8-row x 16-byte core matrices, K-adjacent core matrices
+//   128 B apart (LBO), 8-row groups KC/8 * 128 B apart (SBO);
+// * one elected thread issues tcgen05.mma.cta_group::1.kind::f16 (M = 128,
+//   N <= 256, K = 16 per instruction) into an FP32 accumulator in tensor
+//   memory (TMEM) and tcgen05.commit arrives on an mbarrier; all waits are
+//   bounded (an iteration limit sets an error flag and the kernel still
+//   frees its TMEM);
+// * the epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
+//   TMEM lanes 32w..32w+31 = rows of the tile) and applies bias, GELU or the
+//   GELU derivative.
+// Master weights and Adam moments are FP32; BF16 copies feed the GEMMs.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "ufem_internal.h"
+
+namespace ufem {
+namespace {
+
+constexpr int kTileM = 128;   // UMMA M (TMEM lanes)
+constexpr int kMaxN = 256;    // UMMA N per CTA (TMEM columns)
+constexpr int kKC = 64;       // K chunk staged per round
+constexpr int kGemmThreads = 128;
+constexpr long kSpinLimit = 1L << 26;
+
+struct GemmArgs {
+  int M, N, K;
+  const __nv_bfloat16 *A;
+  long a_sm, a_sk;  // A(m, k) = A[m * a_sm + k * a_sk]
+  const __nv_bfloat16 *B;
+  long b_sn, b_sk;  // B(n, k) = B[n * b_sn + k * b_sk]
+  int epi;          // 0: C = acc; 1: Z = acc + bias, H = gelu(Z); 2: C = acc + bias;
+                    // 3: D = acc * gelu'(Zin) -> C (FP32) and H (BF16)
+  float *C;
+  long ldc;
+  const float *bias;
+  float *Z;         // epi 1: pre-activation out; epi 3: pre-activation in
+  __nv_bfloat16 *H; // epi 1/3: BF16 copy of the output
+  long ldh;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// canonical K-major, no-swizzle UMMA shared-memory descriptor (version 1)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;               // base offset 0, legacy LBO mode, SWIZZLE_NONE
+}
+
+// instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// byte offset of element (r, k) of an R x KC tile in the core-matrix layout
+__device__ __forceinline__ uint32_t cm_offset(int r, int k) {
+  return (uint32_t)(((r >> 3) * (kKC / 8) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sA = smem;                              // 128 x KC bf16 = 16 KB
+  uint8_t *sB = smem + kTileM * kKC * 2;           // 256 x KC bf16 = 32 KB
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_bad;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * kTileM;
+  const int N = g.N;
+  const int ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  if (threadIdx.x == 0) {
+    s_bad = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = umma_idesc(kTileM, N);
+  const uint32_t sbo = (kKC / 8) * 128;
+  uint32_t phase = 0;
+  const int nchunks = (g.K + kKC - 1) / kKC;
+  for (int c = 0; c < nchunks; c++) {
+    const int k0 = c * kKC;
+    // stage A (128 x KC) and B (N x KC), zero-padded
+    for (int i = threadIdx.x; i < kTileM * kKC; i += kGemmThreads) {
+      const int r = i / kKC, k = i % kKC;
+      const int m = m0 + r, kk = k0 + k;
+      __nv_bfloat16 v = __float2bfloat16(0.0f);
+      if (m < g.M && kk < g.K) v = g.A[(long)m * g.a_sm + (long)kk * g.a_sk];
+      *reinterpret_cast<__nv_bfloat16 *>(sA + cm_offset(r, k)) = v;
+    }
+    for (int i = threadIdx.x; i < N * kKC; i += kGemmThreads) {
+      const int r = i / kKC, k = i % kKC;
+      const int kk = k0 + k;
+      __nv_bfloat16 v = __float2bfloat16(0.0f);
+      if (kk < g.K) v = g.B[(long)r * g.b_sn + (long)kk * g.b_sk];
+      *reinterpret_cast<__nv_bfloat16 *>(sB + cm_offset(r, k)) = v;
+    }
+    // make the generic-proxy shared stores visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      for (int ks = 0; ks < kKC / 16; ks++) {
+        const uint64_t da = umma_desc(smem_u32(sA) + ks * 256, 128, sbo);
+        const uint64_t db = umma_desc(smem_u32(sB) + ks * 256, 128, sbo);
+        const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(&mbar)));
+    }
+    // wait for the MMAs of this chunk (they also release the staged tiles)
+    {
+      uint32_t done = 0;
+      long spins = 0;
+      while (!done) {
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.b32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(phase));
+        if (!done && ++spins > kSpinLimit) {
+          s_bad = 1;
+          break;
+        }
+      }
+      phase ^= 1u;
+    }
+    __syncthreads();
+    if (s_bad) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (!s_bad) {
+    // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows m0+32w+lane
+    const int m = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+            "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+            "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;");
+      if (m < g.M) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int n = c0 + j;
+          if (n >= N) break;
+          float a = __uint_as_float(v[j]);
+          switch (g.epi) {
+            case 0:
+              g.C[(long)m * g.ldc + n] = a;
+              break;
+            case 1: {
+              const float z = a + g.bias[n];
+              g.Z[(long)m * g.ldc + n] = z;
+              g.H[(long)m * g.ldh + n] = __float2bfloat16(gelu(z));
+              break;
+            }
+            case 2:
+              g.C[(long)m * g.ldc + n] = a + g.bias[n];
+              break;
+            default: {
+              const float d = a * gelu_grad(g.Z[(long)m * g.ldc + n]);
+              g.C[(long)m * g.ldc + n] = d;
+              g.H[(long)m * g.ldh + n] = __float2bfloat16(d);
+              break;
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  if (threadIdx.x == 0 && s_bad) atomicExch(g.err, 1);
+}
+
+// The operand tiles take 48 KB; the request is padded to 100 KB so that at
+// most two CTAs share an SM, which keeps their TMEM allocations (<= 256
+// columns each) within the SM's 512 columns without any CTA waiting.
+constexpr size_t kGemmSmem = 100 * 1024;
+static_assert((size_t)(kTileM + kMaxN) * kKC * 2 <= kGemmSmem, "operand tiles exceed the shared-memory request");
+
+// ---- small elementwise kernels ---------------------------------------------
+__global__ void k_to_bf16_pad(long rows, int cols, int ld_out, const float *__restrict__ x,
+                              __nv_bfloat16 *__restrict__ y) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= rows * ld_out) return;
+  long r = t / ld_out;
+  int c = (int)(t % ld_out);
+  y[t] = __float2bfloat16(c < cols ? x[r * cols + c] : 0.0f);
+}
+
+__global__ void k_f32_to_bf16(long n, const float *__restrict__ x, __nv_bfloat16 *__restrict__ y) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t < n) y[t] = __float2bfloat16(x[t]);
+}
+
+// dY = 2 (Y - T) / (B * n_out) and the per-row squared error
+__global__ void k_loss_grad(long B, int n_out, const float *__restrict__ Y, const float *__restrict__ T,
+                            float *__restrict__ dY, __nv_bfloat16 *__restrict__ dYb, float *__restrict__ rowloss) {
+  long b = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const float scale = 2.0f / (float)(B * n_out);
+  float s = 0.0f;
+  for (int o = 0; o < n_out; o++) {
+    const float d = Y[b * n_out + o] - T[b * n_out + o];
+    s += d * d;
+    dY[b * n_out + o] = scale * d;
+    dYb[b * n_out + o] = __float2bfloat16(scale * d);
+  }
+  rowloss[b] = s;
+}
+
+// column sums of a row-major [B][n] matrix (bias gradients), fixed order
+__global__ void k_colsum(long B, int n, const float *__restrict__ x, float *__restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  float s = 0.0f;
+  for (long b = 0; b < B; b++) s += x[b * n + c];
+  out[c] = s;
+}
+
+__global__ void k_sum(long n, const float *__restrict__ x, float *__restrict__ out) {
+  __shared__ float sh[256];
+  float s = 0.0f;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s += x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_adam(long n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                       float *__restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2,
+                       const unsigned char *__restrict__ frozen) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n || (frozen && frozen[i])) return;
+  const float gi = g[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+}  // namespace
+}  // namespace ufem
+
+using namespace ufem;
+
+// ---------------------------------------------------------------------------
+struct ufem_mlp {
+  int n_in = 0, n_inp = 0, H = 0, n_out = 0;  // n_inp: n_in padded to 32
+  long nparam = 0;
+  // FP32 master parameters (flat: W1 [H][n_inp], b1, W2 [H][H], b2, W3 [n_out][H], b3)
+  DBuf<float> w, grad, m1, m2;
+  DBuf<unsigned char> frozen;  // padded input columns of W1 stay zero
+  DBuf<__nv_bfloat16> wb;      // BF16 copies of W1, W2, W3
+  long oW1 = 0, ob1 = 0, oW2 = 0, ob2 = 0, oW3 = 0, ob3 = 0;
+  long step = 0;
+  // activations for a batch
+  long cap = 0;
+  DBuf<__nv_bfloat16> X, H1, H2, dYb, dZ2b, dZ1b;
+  DBuf<float> Z1, Z2, Y, dY, dZ2, dZ1, dH, rowloss, scal;
+  DBuf<int> err;
+};
+
+namespace {
+
+int launch_gemm(const GemmArgs &a) {
+  if (a.N > kMaxN || a.N % 16 != 0) {
+    set_error("tensor-core GEMM: N must be a multiple of 16 up to 256");
+    return UFEM_AF_ERR_SIZ;
+  }
+  static bool configured = false;
+  if (!configured) {
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    configured = true;
+  }
+  dim3 grid((unsigned)((a.M + kTileM - 1) / kTileM));
+  k_gemm_tc<<<grid, kGemmThreads, kGemmSmem>>>(a);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+int ensure_batch(ufem_mlp *p, long B) {
+  if (B <= p->cap) return UFEM_AF_OK;
+  int rv;
+  const long H = p->H;
+  if ((rv = p->X.alloc(B * p->n_inp)) || (rv = p->H1.alloc(B * H)) || (rv = p->H2.alloc(B * H)) ||
+      (rv = p->dYb.alloc(B * p->n_out)) || (rv = p->dZ2b.alloc(B * H)) || (rv = p->dZ1b.alloc(B * H)) ||
+      (rv = p->Z1.alloc(B * H)) || (rv = p->Z2.alloc(B * H)) || (rv = p->Y.alloc(B * p->n_out)) ||
+      (rv = p->dY.alloc(B * p->n_out)) || (rv = p->dZ2.alloc(B * H)) || (rv = p->dZ1.alloc(B * H)) ||
+      (rv = p->dH.alloc(B * H)) || (rv = p->rowloss.alloc(B)) || (rv = p->scal.alloc(4)))
+    return rv;
+  p->cap = B;
+  return UFEM_AF_OK;
+}
+
+int refresh_bf16(ufem_mlp *p) {
+  const long n1 = (long)p->H * p->n_inp, n2 = (long)p->H * p->H, n3 = (long)p->n_out * p->H;
+  k_f32_to_bf16<<<(unsigned)((n1 + 255) / 256), 256>>>(n1, p->w.p + p->oW1, p->wb.p);
+  k_f32_to_bf16<<<(unsigned)((n2 + 255) / 256), 256>>>(n2, p->w.p + p->oW2, p->wb.p + n1);
+  k_f32_to_bf16<<<(unsigned)((n3 + 255) / 256), 256>>>(n3, p->w.p + p->oW3, p->wb.p + n1 + n2);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+GemmArgs gemm(int M, int N, int K, const __nv_bfloat16 *A, long a_sm, long a_sk, const __nv_bfloat16 *B, long b_sn,
+              long b_sk, int epi, float *C, long ldc, const float *bias, float *Z, __nv_bfloat16 *H, long ldh,
+              int *err) {
+  GemmArgs a;
+  a.M = M; a.N = N; a.K = K; a.A = A; a.a_sm = a_sm; a.a_sk = a_sk; a.B = B; a.b_sn = b_sn; a.b_sk = b_sk;
+  a.epi = epi; a.C = C; a.ldc = ldc; a.bias = bias; a.Z = Z; a.H = H; a.ldh = ldh; a.err = err;
+  return a;
+}
+
+int forward(ufem_mlp *p, long B, const float *d_x) {
+  int rv;
+  const int H = p->H;
+  const __nv_bfloat16 *W1 = p->wb.p, *W2 = W1 + (long)H * p->n_inp, *W3 = W2 + (long)H * H;
+  k_to_bf16_pad<<<(unsigned)((B * p->n_inp + 255) / 256), 256>>>(B, p->n_in, p->n_inp, d_x, p->X.p);
+  // Z1 = X W1^T + b1, H1 = gelu(Z1)
+  if ((rv = launch_gemm(gemm((int)B, H, p->n_inp, p->X.p, p->n_inp, 1, W1, p->n_inp, 1, 1, nullptr, H,
+                             p->w.p + p->ob1, p->Z1.p, p->H1.p, H, p->err.p))))
+    return rv;
+  // Z2 = H1 W2^T + b2, H2 = gelu(Z2)
+  if ((rv = launch_gemm(gemm((int)B, H, H, p->H1.p, H, 1, W2, H, 1, 1, nullptr, H, p->w.p + p->ob2, p->Z2.p,
+                             p->H2.p, H, p->err.p))))
+    return rv;
+  // Y = H2 W3^T + b3
+  return launch_gemm(gemm((int)B, p->n_out, H, p->H2.p, H, 1, W3, H, 1, 2, p->Y.p, p->n_out, p->w.p + p->ob3,
+                          nullptr, nullptr, 0, p->err.p));
+}
+
+// gradients of the mean squared error into p->grad; the loss into p->scal[0]
+int backward(ufem_mlp *p, long B, const float *d_t) {
+  int rv;
+  const int H = p->H, O = p->n_out;
+  const __nv_bfloat16 *W2 = p->wb.p + (long)H * p->n_inp, *W3 = W2 + (long)H * H;
+  k_loss_grad<<<(unsigned)((B + 127) / 128), 128>>>(B, O, p->Y.p, d_t, p->dY.p, p->dYb.p, p->rowloss.p);
+  k_sum<<<1, 256>>>(B, p->rowloss.p, p->scal.p);
+  float *gW1 = p->grad.p + p->oW1, *gb1 = p->grad.p + p->ob1, *gW2 = p->grad.p + p->oW2;
+  float *gb2 = p->grad.p + p->ob2, *gW3 = p->grad.p + p->oW3, *gb3 = p->grad.p + p->ob3;
+  // dW3 = dY^T H2 (O x H, K = B); db3 = colsum(dY)
+  if ((rv = launch_gemm(gemm(O, H, (int)B, p->dYb.p, 1, O, p->H2.p, 1, H, 0, gW3, H, nullptr, nullptr, nullptr, 0,
+                             p->err.p))))
+    return rv;
+  k_colsum<<<(O + 127) / 128, 128>>>(B, O, p->dY.p, gb3);
+  // dZ2 = (dY W3) * gelu'(Z2)   (B x H, K = O)
+  if ((rv = launch_gemm(gemm((int)B, H, O, p->dYb.p, O, 1, W3, 1, H, 3, p->dZ2.p, H, nullptr, p->Z2.p, p->dZ2b.p,
+                             H, p->err.p))))
+    return rv;
+  // dW2 = dZ2^T H1 (H x H, K = B); db2
+  if ((rv = launch_gemm(gemm(H, H, (int)B, p->dZ2b.p, 1, H, p->H1.p, 1, H, 0, gW2, H, nullptr, nullptr, nullptr, 0,
+                             p->err.p))))
+    return rv;
+  k_colsum<<<(H + 127) / 128, 128>>>(B, H, p->dZ2.p, gb2);
+  // dZ1 = (dZ2 W2) * gelu'(Z1)   (B x H, K = H)
+  if ((rv = launch_gemm(gemm((int)B, H, H, p->dZ2b.p, H, 1, W2, 1, H, 3, p->dZ1.p, H, nullptr, p->Z1.p, p->dZ1b.p,
+                             H, p->err.p))))
+    return rv;
+  // dW1 = dZ1^T X (H x n_inp, K = B); db1
+  if ((rv = launch_gemm(gemm(H, p->n_inp, (int)B, p->dZ1b.p, 1, H, p->X.p, 1, p->n_inp, 0, gW1, p->n_inp, nullptr,
+                             nullptr, nullptr, 0, p->err.p))))
+    return rv;
+  k_colsum<<<(H + 127) / 128, 128>>>(B, H, p->dZ1.p, gb1);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+int check_mlp_err(ufem_mlp *p) {
+  int h = 0;
+  UFEM_CUDA_TRY(cudaMemcpy(&h, p->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    set_error("tensor-core GEMM: MMA completion wait timed out");
+    return UFEM_AF_ERR;
+  }
+  return UFEM_AF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ufem_mlp_create(int n_in, int n_hidden, int n_out, unsigned long long seed, ufem_mlp **out) {
+  if (n_in < 1 || n_in > 32 || n_hidden < 16 || n_hidden > 256 || n_hidden % 16 || n_out < 16 || n_out > 256 ||
+      n_out % 16) {
+    set_error("ufem_mlp_create: n_in <= 32; n_hidden and n_out multiples of 16 up to 256");
+    return UFEM_AF_ERR_SIZ;
+  }
+  ufem_mlp *p = new ufem_mlp();
+  p->n_in = n_in;
+  p->n_inp = 32;
+  p->H = n_hidden;
+  p->n_out = n_out;
+  const long H = n_hidden;
+  p->oW1 = 0;
+  p->ob1 = p->oW1 + H * p->n_inp;
+  p->oW2 = p->ob1 + H;
+  p->ob2 = p->oW2 + H * H;
+  p->oW3 = p->ob2 + H;
+  p->ob3 = p->oW3 + (long)n_out * H;
+  p->nparam = p->ob3 + n_out;
+  // He-style uniform initialisation, seeded; padded input columns zero and frozen
+  std::mt19937_64 rng(seed);
+  std::vector<float> w(p->nparam, 0.0f);
+  std::vector<unsigned char> fr(p->nparam, 0);
+  auto fill = [&](long off, long rows, long cols, long fan_in, long valid_cols) {
+    const float lim = std::sqrt(6.0f / (float)fan_in);
+    std::uniform_real_distribution<float> u(-lim, lim);
+    for (long r = 0; r < rows; r++)
+      for (long c = 0; c < cols; c++) {
+        if (c < valid_cols) w[off + r * cols + c] = u(rng);
+        else fr[off + r * cols + c] = 1;
+      }
+  };
+  fill(p->oW1, H, p->n_inp, n_in, n_in);
+  fill(p->oW2, H, H, H, H);
+  fill(p->oW3, n_out, H, H, H);
+  int rv;
+  if ((rv = p->w.upload(w.data(), w.size())) || (rv = p->grad.alloc(p->nparam)) || (rv = p->m1.alloc(p->nparam)) ||
+      (rv = p->m2.alloc(p->nparam)) || (rv = p->frozen.upload(fr.data(), fr.size())) ||
+      (rv = p->wb.alloc(H * p->n_inp + H * H + (long)n_out * H)) || (rv = p->err.alloc(1))) {
+    delete p;
+    return rv;
+  }
+  cudaMemset(p->m1.p, 0, p->nparam * sizeof(float));
+  cudaMemset(p->m2.p, 0, p->nparam * sizeof(float));
+  cudaMemset(p->err.p, 0, sizeof(int));
+  if ((rv = refresh_bf16(p)) != UFEM_AF_OK) {
+    delete p;
+    return rv;
+  }
+  *out = p;
+  return UFEM_AF_OK;
+}
+
+void ufem_mlp_free(ufem_mlp *p) { delete p; }
+
+long ufem_mlp_num_params(const ufem_mlp *p) { return p->nparam; }
+
+int ufem_mlp_get_params(const ufem_mlp *p, float *h) {
+  UFEM_CUDA_TRY(cudaMemcpy(h, p->w.p, p->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+  return UFEM_AF_OK;
+}
+
+int ufem_mlp_set_params(ufem_mlp *p, const float *h) {
+  UFEM_CUDA_TRY(cudaMemcpy(p->w.p, h, p->nparam * sizeof(float), cudaMemcpyHostToDevice));
+  return refresh_bf16(p);
+}
+
+int ufem_mlp_forward(ufem_mlp *p, long nbatch, const float *d_x, float *d_y) {
+  int rv;
+  if ((rv = ensure_batch(p, nbatch)) || (rv = forward(p, nbatch, d_x))) return rv;
+  UFEM_CUDA_TRY(cudaMemcpy(d_y, p->Y.p, nbatch * p->n_out * sizeof(float), cudaMemcpyDeviceToDevice));
+  return check_mlp_err(p);
+}
+
+int ufem_mlp_gradients(ufem_mlp *p, long nbatch, const float *d_x, const float *d_t, float *h_grad, float *loss) {
+  int rv;
+  if ((rv = ensure_batch(p, nbatch)) || (rv = forward(p, nbatch, d_x)) || (rv = backward(p, nbatch, d_t))) return rv;
+  if ((rv = check_mlp_err(p)) != UFEM_AF_OK) return rv;
+  if (h_grad) UFEM_CUDA_TRY(cudaMemcpy(h_grad, p->grad.p, p->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) {
+    float s = 0;
+    UFEM_CUDA_TRY(cudaMemcpy(&s, p->scal.p, sizeof(float), cudaMemcpyDeviceToHost));
+    *loss = s / (float)(nbatch * p->n_out);
+  }
+  return UFEM_AF_OK;
+}
+
+int ufem_mlp_train_step(ufem_mlp *p, long nbatch, const float *d_x, const float *d_t, float lr, float *loss) {
+  int rv;
+  if ((rv = ensure_batch(p, nbatch)) || (rv = forward(p, nbatch, d_x)) || (rv = backward(p, nbatch, d_t))) return rv;
+  p->step++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, (float)p->step), c2 = 1.0f - std::pow(b2, (float)p->step);
+  k_adam<<<(unsigned)((p->nparam + 255) / 256), 256>>>(p->nparam, p->w.p, p->grad.p, p->m1.p, p->m2.p, lr, b1, b2,
+                                                       1e-8f, c1, c2, p->frozen.p);
+  if ((rv = refresh_bf16(p)) != UFEM_AF_OK) return rv;
+  if (loss) {
+    float s = 0;
+    UFEM_CUDA_TRY(cudaMemcpy(&s, p->scal.p, sizeof(float), cudaMemcpyDeviceToHost));
+    *loss = s / (float)(nbatch * p->n_out);
+  }
+  return check_mlp_err(p);
+}
+
+// C = A . B^T on the tensor cores, for tests of the GEMM itself: A [M x K]
+// and B [N x K] row-major BF16, C [M x N] row-major FP32 (device pointers).
+int ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, float *d_C) {
+  DBuf<int> err;
+  int rv;
+  if ((rv = err.alloc(1)) != UFEM_AF_OK) return rv;
+  UFEM_CUDA_TRY(cudaMemset(err.p, 0, sizeof(int)));
+  GemmArgs a = gemm(M, N, K, (const __nv_bfloat16 *)d_A, K, 1, (const __nv_bfloat16 *)d_B, K, 1, 0, d_C, N, nullptr,
+                    nullptr, nullptr, 0, err.p);
+  if ((rv = launch_gemm(a)) != UFEM_AF_OK) return rv;
+  int h = 0;
+  UFEM_CUDA_TRY(cudaMemcpy(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    set_error("tensor-core GEMM: MMA completion wait timed out");
+    return UFEM_AF_ERR;
+  }
+  return UFEM_AF_OK;
+}
+
+}  // extern "C"
