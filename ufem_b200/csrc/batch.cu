@@ -945,16 +945,40 @@ __global__ void k_outputs(int nout, int S, int nsamp, long olen, const int *__re
   ofld[(size_t)s * olen + opos[o]] = val;
 }
 
-// (|F_s| tol)^2 per sample and |F_s|^2 (rows summed in order: deterministic)
-__global__ void k_tol2(long n, int S, const double *__restrict__ F, double tol, double *__restrict__ tol2,
+// |F_s|^2 per sample in two passes with a fixed summation order (run-to-run
+// identical): k_ff_part sums one chunk of rows for 32 samples per block (the
+// lane is the sample, so each row read is one 256-byte transaction; 8 warps
+// stride the chunk and are combined in warp order), k_tol2 adds the chunks in
+// order and forms (|F_s| tol)^2.
+constexpr int kFfChunks = 64;
+
+__global__ void __launch_bounds__(256) k_ff_part(long n, int S, const double *__restrict__ F,
+                                                 double *__restrict__ part) {
+  __shared__ double sh[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int s = blockIdx.x * 32 + lane;  // S is a multiple of 128
+  const long per = (n + gridDim.y - 1) / gridDim.y;
+  const long i0 = (long)blockIdx.y * per, i1 = min(n, i0 + per);
+  double t = 0.0;
+  for (long i = i0 + w; i < i1; i += 8) {
+    const double f = F[(size_t)i * S + s];
+    t += f * f;
+  }
+  sh[w][lane] = t;
+  __syncthreads();
+  if (w == 0) {
+    double a = 0.0;
+    for (int k = 0; k < 8; k++) a += sh[k][lane];
+    part[(size_t)blockIdx.y * S + s] = a;
+  }
+}
+
+__global__ void k_tol2(int nch, int S, const double *__restrict__ part, double tol, double *__restrict__ tol2,
                        double *__restrict__ ff) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
   double t = 0.0;
-  for (long i = 0; i < n; i++) {
-    double f = F[(size_t)i * S + s];
-    t += f * f;
-  }
+  for (int c = 0; c < nch; c++) t += part[(size_t)c * S + s];
   ff[s] = t;
   tol2[s] = tol * tol * t;
 }
@@ -966,7 +990,7 @@ __global__ void k_tol2(long n, int S, const double *__restrict__ F, double tol, 
 // ---------------------------------------------------------------------------
 struct McWork {
   int S = 0, nsamp = 0;
-  DBuf<double> E, F, Fraw, V64, M64, x64, tol2, ff;
+  DBuf<double> E, F, Fraw, V64, M64, x64, tol2, ff, ffpart;
   DBuf<float> V32, M32;
   // inner vectors, FP32 or FP64
   DBuf<float> fr, fz, fp0, fp1, fq;
@@ -1241,7 +1265,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       const size_t n = (size_t)m->nDOFAct * w.S, nv = (size_t)m->nnzb * B * B * w.S;
       if ((rv = w.E.ensure((size_t)m->eLen * w.S)) || (rv = w.F.ensure(n)) || (rv = w.Fraw.ensure(n)) ||
           (rv = w.V64.ensure(nv)) || (rv = w.M64.ensure(n)) || (rv = w.x64.ensure(n)) || (rv = w.state.ensure(w.S)) ||
-          (rv = w.iters.ensure(w.S)) || (rv = w.tol2.ensure(w.S)) || (rv = w.ff.ensure(w.S)))
+          (rv = w.iters.ensure(w.S)) || (rv = w.tol2.ensure(w.S)) || (rv = w.ff.ensure(w.S)) ||
+          (rv = w.ffpart.ensure((size_t)kFfChunks * w.S)))
         return rv;
       if (opt.precision != 0) {
         if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n))) return rv;
@@ -1263,8 +1288,9 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       else
         k_assemble_batch<2><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
                                          P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
-      k_tol2<<<(w.S + 127) / 128, 128>>>((long)m->nDOFAct, w.S, w.F.p, opt.tol, w.tol2.p, w.ff.p);
-      g_stats.kernel_launches += 6;
+      k_ff_part<<<dim3((unsigned)(w.S / 32), kFfChunks), 256>>>((long)m->nDOFAct, w.S, w.F.p, w.ffpart.p);
+      k_tol2<<<(w.S + 127) / 128, 128>>>(kFfChunks, w.S, w.ffpart.p, opt.tol, w.tol2.p, w.ff.p);
+      g_stats.kernel_launches += 7;
       if (d_u_guess && d_u_guess[k]) {
         UFEM_CUDA_TRY(cudaMemcpyAsync(w.x64.p, d_u_guess[k], n * sizeof(double), cudaMemcpyDeviceToDevice));
       } else {
