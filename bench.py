@@ -391,13 +391,15 @@ def ours(a):
         plain = plain_n / plain_t
         peak, peak_kind = measured_peaks()
         achieved = pcg_bytes / (pcg_ms / 1000.0) / 1e9 if pcg_ms > 0 else 0.0
+        # DRAM traffic per launch: the ncu-measured traffic / algorithmic
+        # ratio of this kernel (profiles/, a smaller case of the same kernel)
+        # times this run's algorithmic bytes per launch
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "batch_pcg_traffic.json")
-        if os.path.exists(tf):
-            try:
-                traffic = json.load(open(tf)).get("traffic_bytes_per_launch")
-            except Exception:
-                traffic = None
+        tf = os.path.join(ROOT, "profiles", "k_batch_pcg_60x15x15_128samples.md")
+        if os.path.exists(tf) and pcg_launches > 0:
+            for line in open(tf):
+                if line.startswith("traffic_over_algorithmic:"):
+                    traffic = float(line.split(":")[1]) * pcg_bytes / pcg_launches
         # ---- CPU baseline: the reference on a bounded sample ------------------
         cpu = None
         if os.path.exists(REF_LIB) and not a.no_cpu:

@@ -275,6 +275,74 @@ int  ufem_mlp_train_step(ufem_mlp *p, long nbatch, const float *d_x, const float
  * at most 256. */
 int  ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, float *d_C);
 
+/* ---- learned warm start of the batched Monte Carlo solve (no counterpart in
+ * the reference; its only hook is the disabled warm start of
+ * monte_linear_solver, fem/fem_mont.c:493-504) ------------------------------
+ * Training: the batched solver solves ntrain samples from zero; a POD basis
+ * of n_modes modes is built from the first n_snapshots solutions (FP64,
+ * randomised subspace iteration + Rayleigh-Ritz); the MLP above learns the
+ * map from the chosen inputs to the solutions' POD coefficients (divided by
+ * the sample's value in scale_col: the solution is linear in the load).
+ * Solving: u0 = scale * Phi * MLP(inputs) is the initial guess of the
+ * batched PCG, which still iterates to the same tolerance; its iteration cap
+ * is the largest cold iteration count seen in training, and a sample that
+ * does not converge within it is solved again from zero (UFEM_ST_FALLBACK).
+ * d_ifld: device, nsamp*ilen (the model's Monte Carlo inputs). */
+typedef struct ufem_warm_options {
+  int n_modes;               /* POD modes: a multiple of 16, at most 80 */
+  int n_hidden;              /* MLP width: a multiple of 16, at most 256 */
+  int n_feat;                /* network inputs, 1..32 */
+  long feat_cols[32];        /* ifld column of each input */
+  int feat_log[32];          /* nonzero: the input enters as log|value| */
+  long scale_col;            /* ifld column the solution is proportional to, or -1 */
+  long n_snapshots;          /* solutions the basis is built from (>= n_modes + 16) */
+  int power_iters;           /* subspace iterations of the POD */
+  int epochs, batch;         /* MLP training: passes over the set, minibatch size */
+  float lr;                  /* Adam learning rate (cosine decay to 2 %) */
+  unsigned long long seed;
+} ufem_warm_options;
+
+typedef struct ufem_warm_train_stats {
+  long cold_iters_max;       /* largest PCG iteration count of the cold solves */
+  double cold_iters_mean;
+  double ms_solve, ms_basis, ms_train;
+  double sigma2[80];         /* energy (squared singular value) of each POD mode */
+  float loss_first, loss_last;  /* mean training loss of the first / last epoch */
+  int epochs;
+  long steps;
+} ufem_warm_train_stats;
+
+typedef struct ufem_warm_stats {
+  long nsamp, fallbacks;     /* samples solved; of them solved again from zero */
+  double guess_err_mean, guess_err_max;  /* |u0 - u| / |u| against the converged u */
+  double iters_mean;
+  long iters_max;
+  long cold_cap;             /* the iteration cap of the warm-started run */
+  double ms_guess, ms_solve, ms_fallback, ms_total;
+} ufem_warm_stats;
+
+typedef struct ufem_warm ufem_warm;
+void ufem_warm_default_options(ufem_warm_options *o);
+int  ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out);
+void ufem_warm_free(ufem_warm *w);
+int  ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_mc_options *opt,
+                     ufem_warm_train_stats *st);
+/* the guesses alone, d_u0: device, nsamp*nDOFAct (sample-major) */
+int  ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u0);
+/* warm-started batched solve; d_ofld nsamp*olen, d_status, d_iters nsamp (device; may be NULL) */
+int  ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
+                     const ufem_mc_options *opt, ufem_warm_stats *st);
+/* multiplies every guess by factor (1 by default): a diagnostic that makes the
+ * guesses bad on purpose, to exercise the fallback */
+int  ufem_warm_set_guess_scale(ufem_warm *w, double factor);
+/* the basis [nDOFAct][n_modes] and the mode energies (host; either may be NULL) */
+int  ufem_warm_get_basis(const ufem_warm *w, double *h_phi, double *h_sigma2);
+/* the warm start's FP64 kernels, exposed for their tests: C [M x N] = A [M x K]
+ * B [K x N] (row-major, device); symmetric eigen-decomposition of A [l x l]
+ * (l even, <= 96; host arrays; V columns = eigenvectors, unsorted) */
+int  ufem_dgemm_f64(int M, int N, long K, const double *d_A, const double *d_B, double *d_C);
+int  ufem_sym_eig(int l, const double *h_A, double *h_V, double *h_lam, int *sweeps);
+
 /* ---- device / diagnostics ------------------------------------------------ */
 int ufem_device_info(int *sm_count, int *cc_major, int *cc_minor, long *mem_bytes);
 const char *ufem_last_error(void);

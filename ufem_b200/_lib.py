@@ -36,6 +36,26 @@ class McOptions(C.Structure):
                 ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int)]
 
 
+class WarmOptions(C.Structure):
+    _fields_ = [("n_modes", C.c_int), ("n_hidden", C.c_int), ("n_feat", C.c_int), ("feat_cols", C.c_long * 32),
+                ("feat_log", C.c_int * 32), ("scale_col", C.c_long), ("n_snapshots", C.c_long),
+                ("power_iters", C.c_int), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
+                ("seed", C.c_ulonglong)]
+
+
+class WarmTrainStats(C.Structure):
+    _fields_ = [("cold_iters_max", C.c_long), ("cold_iters_mean", C.c_double), ("ms_solve", C.c_double),
+                ("ms_basis", C.c_double), ("ms_train", C.c_double), ("sigma2", C.c_double * 80),
+                ("loss_first", C.c_float), ("loss_last", C.c_float), ("epochs", C.c_int), ("steps", C.c_long)]
+
+
+class WarmStats(C.Structure):
+    _fields_ = [("nsamp", C.c_long), ("fallbacks", C.c_long), ("guess_err_mean", C.c_double),
+                ("guess_err_max", C.c_double), ("iters_mean", C.c_double), ("iters_max", C.c_long),
+                ("cold_cap", C.c_long), ("ms_guess", C.c_double), ("ms_solve", C.c_double),
+                ("ms_fallback", C.c_double), ("ms_total", C.c_double)]
+
+
 class McStats(C.Structure):
     _fields_ = [("ms_assemble", C.c_double), ("ms_pcg", C.c_double), ("ms_refine", C.c_double),
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
@@ -102,6 +122,18 @@ _SIGS = {
     "ufem_mlp_train_step": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_float,
                                       C.POINTER(C.c_float)]),
     "ufem_tc_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ufem_warm_default_options": (None, [C.POINTER(WarmOptions)]),
+    "ufem_warm_create": (C.c_int, [C.c_void_p, C.POINTER(WarmOptions), C.POINTER(C.c_void_p)]),
+    "ufem_warm_free": (None, [C.c_void_p]),
+    "ufem_warm_train": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.POINTER(McOptions),
+                                  C.POINTER(WarmTrainStats)]),
+    "ufem_warm_guess": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p]),
+    "ufem_warm_solve": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(McOptions), C.POINTER(WarmStats)]),
+    "ufem_warm_set_guess_scale": (C.c_int, [C.c_void_p, C.c_double]),
+    "ufem_warm_get_basis": (C.c_int, [C.c_void_p, _d, _d]),
+    "ufem_dgemm_f64": (C.c_int, [C.c_int, C.c_int, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ufem_sym_eig": (C.c_int, [C.c_int, _d, _d, _d, _i]),
 }
 
 # every symbol include/ufem_gpu.h declares (checked by the CPU test suite)

@@ -1,0 +1,924 @@
+// Learned warm start for the batched Monte Carlo solve.  No counterpart in
+// the reference: its only hook is the disabled warm start of
+// monte_linear_solver (fem/fem_mont.c:493-504, the femVecClone of the
+// previous solution into u before femEqsCGwSSOR).
+//
+// Pipeline, every step on the GPU:
+//   1. the batched solver (batch.cu) solves ntrain samples from zero; their
+//      solutions U [ndof][ntrain] stay on the device;
+//   2. POD basis Phi [ndof][r] of the first nsnap solutions: randomised
+//      subspace iteration (Halko, Martinsson & Tropp, SIAM Review 53, 2011,
+//      algorithm 4.4) with l = r + 16 columns, every product orthonormalised
+//      through the eigen-decomposition of its Gram matrix (twice), then a
+//      Rayleigh-Ritz step that orders the modes by energy; when the
+//      snapshots span fewer than r directions above 1e-12 of the largest
+//      singular value, the missing modes are zero columns;
+//   3. targets: the coefficients Phi^T u of every training solution divided
+//      by the sample's load scale (the solution is linear in the load),
+//      standardised per mode; inputs: the chosen ifld columns, log|.| where
+//      asked, standardised;
+//   4. the MLP (mlp.cu: tcgen05 BF16 GEMMs, FP32 accumulation, Adam) is
+//      trained on them for a number of epochs with a cosine learning rate;
+//   5. a warm-started solve runs the MLP on the new samples' inputs, forms
+//      u0 = scale * Phi c in FP64 and hands it to the batched PCG as the
+//      initial guess, with the iteration cap set to the largest count the
+//      cold training solves needed.  A sample that does not converge within
+//      it (the guess made the iterations regress) is solved again from zero
+//      by the same batched solver and reported UFEM_ST_FALLBACK.
+//
+// Dense FP64 products run in one generic tiled kernel (k_gemm_f64) with a
+// split K dimension whose partial sums are added in a fixed order, so every
+// result is identical run to run.  The l x l symmetric eigenproblems run in
+// one thread block (k_jacobi_eig): cyclic Jacobi with the round-robin
+// ordering, l/2 disjoint rotations per round.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <vector>
+
+#include "ufem_internal.h"
+
+namespace ufem {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// C(m, n) = alpha * sum_k A(m, k) B(k, n), any element strides
+// ---------------------------------------------------------------------------
+constexpr int kGT = 64;   // output tile (kGT x kGT), 4 x 4 per thread
+constexpr int kGK = 16;   // K chunk staged in shared memory
+constexpr int kMaxSplits = 64;
+
+struct G64 {
+  int M, N;
+  long K;
+  const double *A;
+  long sam, sak;
+  const double *B;
+  long sbk, sbn;
+  double *C;
+  long scm, scn;
+  double alpha;
+  int splits;
+  double *part;  // [splits][M][N] when splits > 1
+};
+
+__global__ void __launch_bounds__(256) k_gemm_f64(G64 g) {
+  __shared__ double As[kGK][kGT + 1];
+  __shared__ double Bs[kGK][kGT + 1];
+  const int m0 = blockIdx.x * kGT, n0 = blockIdx.y * kGT;
+  const long per = (g.K + g.splits - 1) / g.splits;
+  const long kbeg = (long)blockIdx.z * per, kend = min(g.K, kbeg + per);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const bool a_kfast = (g.sak == 1), b_kfast = (g.sbk == 1);
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  for (long kb = kbeg; kb < kend; kb += kGK) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q;
+      int mm, kk;
+      if (a_kfast) { kk = e % kGK; mm = e / kGK; }
+      else { mm = e % kGT; kk = e / kGT; }
+      const long gk = kb + kk;
+      const int gm = m0 + mm;
+      As[kk][mm] = (gm < g.M && gk < kend) ? g.A[(size_t)gm * g.sam + (size_t)gk * g.sak] : 0.0;
+      int nn;
+      if (b_kfast) { kk = e % kGK; nn = e / kGK; }
+      else { nn = e % kGT; kk = e / kGT; }
+      const long gk2 = kb + kk;
+      const int gn = n0 + nn;
+      Bs[kk][nn] = (gn < g.N && gk2 < kend) ? g.B[(size_t)gk2 * g.sbk + (size_t)gn * g.sbn] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; kk++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int gm = m0 + ty + 16 * i, gn = n0 + tx + 16 * j;
+      if (gm >= g.M || gn >= g.N) continue;
+      if (g.splits == 1) g.C[(size_t)gm * g.scm + (size_t)gn * g.scn] = g.alpha * acc[i][j];
+      else g.part[((size_t)blockIdx.z * g.M + gm) * g.N + gn] = acc[i][j];
+    }
+}
+
+__global__ void k_split_sum(int M, int N, int splits, const double *__restrict__ part, double alpha,
+                            double *__restrict__ C, long scm, long scn) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long)M * N) return;
+  const int m = (int)(e / N), n = (int)(e % N);
+  double t = 0.0;
+  for (int s = 0; s < splits; s++) t += part[(size_t)s * M * N + e];
+  C[(size_t)m * scm + (size_t)n * scn] = alpha * t;
+}
+
+// Launches k_gemm_f64; splits the K range when the output has few tiles.
+int gemm_f64(int M, int N, long K, const double *A, long sam, long sak, const double *B, long sbk, long sbn,
+             double *C, long scm, long scn, DBuf<double> &part, double alpha = 1.0) {
+  if (M <= 0 || N <= 0) return UFEM_AF_OK;
+  G64 g;
+  g.M = M; g.N = N; g.K = K; g.A = A; g.sam = sam; g.sak = sak; g.B = B; g.sbk = sbk; g.sbn = sbn;
+  g.C = C; g.scm = scm; g.scn = scn; g.alpha = alpha; g.splits = 1; g.part = nullptr;
+  const long tiles = (long)((M + kGT - 1) / kGT) * ((N + kGT - 1) / kGT);
+  if (tiles < 296 && K > 512) {
+    long s = (296 + tiles - 1) / tiles;
+    s = std::min<long>(s, K / 256);
+    s = std::min<long>(s, kMaxSplits);
+    g.splits = (int)std::max<long>(1, s);
+  }
+  if (g.splits > 1) {
+    int rv = part.ensure((size_t)g.splits * M * N);
+    if (rv != UFEM_AF_OK) return rv;
+    g.part = part.p;
+  }
+  dim3 grid((unsigned)((M + kGT - 1) / kGT), (unsigned)((N + kGT - 1) / kGT), (unsigned)g.splits);
+  k_gemm_f64<<<grid, 256>>>(g);
+  if (g.splits > 1) {
+    const long tot = (long)M * N;
+    k_split_sum<<<(unsigned)((tot + 255) / 256), 256>>>(M, N, g.splits, part.p, alpha, C, scm, scn);
+  }
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// symmetric eigen-decomposition of an l x l matrix (l even, <= kMaxL) in one
+// block: cyclic Jacobi, round-robin ordering (l - 1 rounds of l/2 disjoint
+// rotations per sweep), rotation of Numerical Recipes (Press et al., 11.1):
+// theta = (a_qq - a_pp) / (2 a_pq), t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)),
+// c = 1 / sqrt(t^2 + 1), s = t c; A <- P^T A P, V <- V P.
+// ---------------------------------------------------------------------------
+constexpr int kMaxL = 96;
+constexpr int kJacThreads = 512;
+
+__global__ void __launch_bounds__(kJacThreads) k_jacobi_eig(int l, const double *__restrict__ Ain,
+                                                            double *__restrict__ Vout, double *__restrict__ lam,
+                                                            int max_sweeps, int *__restrict__ sweeps_out) {
+  extern __shared__ double sm[];
+  const int ld = l + 1;
+  double *A = sm;             // [l][ld]
+  double *V = sm + l * ld;    // [l][ld]
+  double *cs = V + l * ld;    // [l/2][2]
+  int *pq = (int *)(cs + l);  // [l/2][2]
+  __shared__ double red[kJacThreads];
+  __shared__ int s_done;
+  const int half = l / 2;
+  for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+    const int i = e / l, j = e % l;
+    A[i * ld + j] = 0.5 * (Ain[i * l + j] + Ain[j * l + i]);
+    V[i * ld + j] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < max_sweeps; sweep++) {
+    // convergence test: off-diagonal mass against the diagonal
+    double off = 0.0, dia = 0.0;
+    for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+      const int i = e / l, j = e % l;
+      const double v = A[i * ld + j];
+      if (i == j) dia += v * v;
+      else off += v * v;
+    }
+    red[threadIdx.x] = off;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    const double off_t = red[0];
+    __syncthreads();
+    red[threadIdx.x] = dia;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    const double dia_t = red[0];
+    if (threadIdx.x == 0) s_done = (off_t <= 1e-30 * dia_t) || !(off_t > 0.0);
+    __syncthreads();
+    if (s_done) break;
+    for (int round = 0; round < l - 1; round++) {
+      if (threadIdx.x < half) {
+        const int k = threadIdx.x;
+        int p, q;
+        if (k == 0) { p = round; q = l - 1; }
+        else { p = (round + k) % (l - 1); q = (round - k + (l - 1)) % (l - 1); }
+        if (p > q) { const int t = p; p = q; q = t; }
+        const double apq = A[p * ld + q], app = A[p * ld + p], aqq = A[q * ld + q];
+        double c = 1.0, s = 0.0;
+        if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * sqrt(fabs(app * aqq))) {
+          const double theta = (aqq - app) / (2.0 * apq);
+          double t;
+          if (fabs(theta) > 1e150) t = 0.5 / theta;
+          else t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          c = 1.0 / sqrt(t * t + 1.0);
+          s = t * c;
+        }
+        pq[2 * k] = p; pq[2 * k + 1] = q;
+        cs[2 * k] = c; cs[2 * k + 1] = s;
+      }
+      __syncthreads();
+      // rows p, q of A
+      for (int e = threadIdx.x; e < half * l; e += blockDim.x) {
+        const int k = e / l, j = e % l;
+        const int p = pq[2 * k], q = pq[2 * k + 1];
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        const double a = A[p * ld + j], b = A[q * ld + j];
+        A[p * ld + j] = c * a - s * b;
+        A[q * ld + j] = s * a + c * b;
+      }
+      __syncthreads();
+      // columns p, q of A and of V
+      for (int e = threadIdx.x; e < half * l; e += blockDim.x) {
+        const int k = e / l, i = e % l;
+        const int p = pq[2 * k], q = pq[2 * k + 1];
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        double a = A[i * ld + p], b = A[i * ld + q];
+        A[i * ld + p] = c * a - s * b;
+        A[i * ld + q] = s * a + c * b;
+        a = V[i * ld + p];
+        b = V[i * ld + q];
+        V[i * ld + p] = c * a - s * b;
+        V[i * ld + q] = s * a + c * b;
+      }
+      __syncthreads();
+    }
+  }
+  for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+    const int i = e / l, j = e % l;
+    Vout[i * l + j] = V[i * ld + j];
+  }
+  for (int j = threadIdx.x; j < l; j += blockDim.x) lam[j] = A[j * ld + j];
+  if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweep;
+}
+
+size_t jacobi_smem(int l) { return (size_t)(2 * l * (l + 1) + l) * sizeof(double) + (size_t)l * sizeof(int); }
+
+// T[i][c] = V[i][perm[c]] * scale[c]   (l rows, rc columns)
+__global__ void k_cols_perm_scale(int l, int rc, const double *__restrict__ V, const int *__restrict__ perm,
+                                  const double *__restrict__ scale, double *__restrict__ T) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= l * rc) return;
+  const int i = e / rc, c = e % rc;
+  T[e] = V[i * l + perm[c]] * scale[c];
+}
+
+// ---------------------------------------------------------------------------
+// features, targets, statistics
+// ---------------------------------------------------------------------------
+// raw[s][f] = ifld[s][col[f]] (log|.| where asked)
+__global__ void k_feat_raw(long nsamp, int nf, long ilen, const double *__restrict__ ifld, const long *__restrict__ col,
+                           const int *__restrict__ lg, double *__restrict__ raw) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * nf) return;
+  const long s = e / nf;
+  const int f = (int)(e % nf);
+  double v = ifld[s * ilen + col[f]];
+  if (lg[f]) v = log(fabs(v));
+  raw[e] = v;
+}
+
+// per-column mean and standard deviation (each column summed in row order)
+__global__ void k_col_stats(long nrow, int ncol, const double *__restrict__ X, double *__restrict__ mean,
+                            double *__restrict__ sd) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  double s = 0.0;
+  for (long r = 0; r < nrow; r++) s += X[r * ncol + c];
+  const double mu = s / (double)nrow;
+  double v = 0.0;
+  for (long r = 0; r < nrow; r++) {
+    const double d = X[r * ncol + c] - mu;
+    v += d * d;
+  }
+  v /= (double)nrow;
+  mean[c] = mu;
+  sd[c] = v > 0.0 ? sqrt(v) : 1.0;
+}
+
+// network input rows: standardised features, zero-padded to ldx columns (FP32)
+__global__ void k_standardise(long nsamp, int nf, int ldx, const double *__restrict__ raw,
+                              const double *__restrict__ mean, const double *__restrict__ sd, float *__restrict__ X) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * ldx) return;
+  const long s = e / ldx;
+  const int f = (int)(e % ldx);
+  X[e] = f < nf ? (float)((raw[s * nf + f] - mean[f]) / sd[f]) : 0.0f;
+}
+
+// per-sample load scale (1 when no scale column)
+__global__ void k_scale(long nsamp, long ilen, long col, const double *__restrict__ ifld, double *__restrict__ sc) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsamp) return;
+  sc[s] = col >= 0 ? ifld[s * ilen + col] : 1.0;
+}
+
+// c[s][k] /= sc[s]
+__global__ void k_div_scale(long nsamp, int r, const double *__restrict__ sc, double *__restrict__ c) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * r) return;
+  const double d = sc[e / r];
+  c[e] = d != 0.0 ? c[e] / d : 0.0;
+}
+
+// FP32 targets t = (c - mean) / sd
+__global__ void k_targets(long nsamp, int r, const double *__restrict__ c, const double *__restrict__ mean,
+                          const double *__restrict__ sd, float *__restrict__ t) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * r) return;
+  const int k = (int)(e % r);
+  t[e] = (float)((c[e] - mean[k]) / sd[k]);
+}
+
+// network outputs -> coefficients: c[s][k] = (y * sd + mean) * sc[s]
+__global__ void k_coeffs(long nsamp, int r, const float *__restrict__ y, const double *__restrict__ mean,
+                         const double *__restrict__ sd, const double *__restrict__ sc, double gscale,
+                         double *__restrict__ c) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * r) return;
+  const int k = (int)(e % r);
+  c[e] = ((double)y[e] * sd[k] + mean[k]) * sc[e / r] * gscale;
+}
+
+// rows of a row-major matrix picked by idx (minibatches)
+template <typename T>
+__global__ void k_gather_rows(long nrow, int ncol, const long *__restrict__ idx, const T *__restrict__ src,
+                              T *__restrict__ dst) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nrow * ncol) return;
+  const long r = e / ncol;
+  dst[e] = src[idx[r] * ncol + (e % ncol)];
+}
+
+// |u0_s - u_s| / |u_s| per sample, both [n][S] (rows summed in order)
+__global__ void k_rel_err(long n, int S, int nsamp, const double *__restrict__ u0, const double *__restrict__ u,
+                          double *__restrict__ err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsamp) return;
+  double a = 0.0, b = 0.0;
+  for (long i = 0; i < n; i++) {
+    const double x = u[i * S + s], d = u0[i * S + s] - x;
+    a += d * d;
+    b += x * x;
+  }
+  err[s] = b > 0.0 ? sqrt(a / b) : sqrt(a);
+}
+
+// [n][S] (first nsamp columns) -> [nsamp][n]
+__global__ void k_to_sample_major(long n, int S, long nsamp, const double *__restrict__ src, double *__restrict__ dst) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nsamp) return;
+  const long i = e / nsamp, s = e % nsamp;
+  dst[s * n + i] = src[i * S + s];
+}
+
+int grid1(long n, int b = 256) { return (int)((n + b - 1) / b); }
+
+}  // namespace
+
+}  // namespace ufem
+
+using namespace ufem;
+
+struct ufem_warm {
+  ufem_model *m = nullptr;
+  ufem_warm_options o;
+  int r = 0, l = 0;
+  long n = 0;
+  ufem_mlp *mlp = nullptr;
+  bool trained = false;
+  long cold_cap = 0;
+  double guess_scale = 1.0;
+  // basis and normalisation
+  DBuf<double> phi;                       // [n][r]
+  DBuf<double> fmean, fsd, cmean, csd;    // feature / coefficient statistics
+  DBuf<long> fcol;
+  DBuf<int> flog;
+  std::vector<double> sigma2;             // Rayleigh-Ritz energies of the modes
+  // scratch
+  DBuf<double> U, Y, Q, Z, G, V, lam, T, scale, part, raw, sc, c;
+  DBuf<int> perm, sweeps;
+  DBuf<float> X, Tt, Xb, Tb, Yo;
+  DBuf<long> bidx;
+  DBuf<double> ifsub, u0, uf, err;
+  DBuf<double> ofsub;
+  DBuf<int> stsub;
+  DBuf<long> itsub;
+  DBuf<int> st;
+  DBuf<long> it;
+};
+
+namespace ufem {
+
+int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *d_ifld,
+                    double *const *d_ofld, int *const *d_status, long *const *d_iters,
+                    const double *const *d_u_guess, double *const *d_u_out, const ufem_mc_options *opt_in);
+
+namespace {
+
+// eigen-decomposition of the l x l matrix w->G; columns of w->V sorted by
+// descending eigenvalue through w->perm, eigenvalues (sorted) into lam_sorted
+int sym_eig_sorted(ufem_warm *w, int l, std::vector<double> &lam_sorted, std::vector<int> &order) {
+  static int configured_for = 0;
+  const size_t smem = jacobi_smem(l);
+  if (configured_for < (int)smem) {
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured_for = (int)smem;
+  }
+  k_jacobi_eig<<<1, kJacThreads, smem>>>(l, w->G.p, w->V.p, w->lam.p, 60, w->sweeps.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  std::vector<double> lam(l);
+  UFEM_CUDA_TRY(cudaMemcpy(lam.data(), w->lam.p, l * sizeof(double), cudaMemcpyDeviceToHost));
+  order.resize(l);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lam[a] > lam[b]; });
+  lam_sorted.resize(l);
+  for (int j = 0; j < l; j++) lam_sorted[j] = lam[order[j]];
+  return UFEM_AF_OK;
+}
+
+// Yin [rows][l] -> out [rows][l] with orthonormal columns spanning Yin:
+// T = V Lambda^-1/2 from the eigen-decomposition of the Gram matrix Yin^T Yin
+// (directions whose eigenvalue is below 1e-24 of the largest, i.e. singular
+// values below 1e-12 of the largest, become zero columns), out = Yin T; done
+// twice so the columns are orthonormal to working precision.  tmp: rows*l.
+int orthonormalise(ufem_warm *w, long rows, int l, const double *Yin, double *out, double *tmp) {
+  int rv;
+  const double *src = Yin;
+  for (int pass = 0; pass < 2; pass++) {
+    if ((rv = gemm_f64(l, l, rows, src, 1, l, src, l, 1, w->G.p, l, 1, w->part))) return rv;
+    std::vector<double> lam;
+    std::vector<int> order;
+    if ((rv = sym_eig_sorted(w, l, lam, order))) return rv;
+    std::vector<double> scale(l, 0.0);
+    const double lmax = std::max(lam[0], 0.0);
+    for (int j = 0; j < l; j++) scale[j] = (lmax > 0.0 && lam[j] > 1e-24 * lmax) ? 1.0 / std::sqrt(lam[j]) : 0.0;
+    if ((rv = w->perm.upload(order.data(), l)) || (rv = w->scale.upload(scale.data(), l))) return rv;
+    k_cols_perm_scale<<<grid1((long)l * l), 256>>>(l, l, w->V.p, w->perm.p, w->scale.p, w->T.p);
+    double *dst = (pass == 0) ? tmp : out;
+    if ((rv = gemm_f64((int)rows, l, l, src, l, 1, w->T.p, l, 1, dst, l, 1, w->part))) return rv;
+    src = dst;
+  }
+  return UFEM_AF_OK;
+}
+
+// POD basis of the first nsnap columns of U [n][S]: randomised range finder
+// with power iterations, every product followed by an orthonormalisation
+// (Halko, Martinsson & Tropp 2011, algorithm 4.4), then Rayleigh-Ritz.
+int fit_basis(ufem_warm *w, int S, long nsnap) {
+  int rv;
+  const long n = w->n;
+  const int l = w->l, r = w->r;
+  const long big = std::max<long>(nsnap, n);
+  if ((rv = w->Y.ensure((size_t)big * l)) || (rv = w->Q.ensure((size_t)n * l)) ||
+      (rv = w->Z.ensure((size_t)big * l)) || (rv = w->G.ensure((size_t)l * l)) ||
+      (rv = w->V.ensure((size_t)l * l)) || (rv = w->lam.ensure(l)) || (rv = w->T.ensure((size_t)l * l)) ||
+      (rv = w->scale.ensure(l)) || (rv = w->perm.ensure(l)) || (rv = w->sweeps.ensure(1)) ||
+      (rv = w->phi.ensure((size_t)n * r)))
+    return rv;
+  // Omega [nsnap][l], seeded standard normal
+  std::mt19937_64 rng(w->o.seed ^ 0x5eed0f0dULL);
+  std::normal_distribution<double> nd(0.0, 1.0);
+  std::vector<double> om((size_t)nsnap * l);
+  for (auto &v : om) v = nd(rng);
+  DBuf<double> d_om, zq;
+  if ((rv = d_om.upload(om.data(), om.size())) || (rv = zq.ensure((size_t)nsnap * l))) return rv;
+  // Q = orth(U Omega)
+  if ((rv = gemm_f64((int)n, l, nsnap, w->U.p, S, 1, d_om.p, l, 1, w->Y.p, l, 1, w->part))) return rv;
+  if ((rv = orthonormalise(w, n, l, w->Y.p, w->Q.p, w->Z.p))) return rv;
+  for (int it = 0; it < w->o.power_iters; it++) {
+    // Zq = orth(U^T Q) [nsnap][l]; Q = orth(U Zq)
+    if ((rv = gemm_f64((int)nsnap, l, n, w->U.p, 1, S, w->Q.p, l, 1, w->Y.p, l, 1, w->part))) return rv;
+    if ((rv = orthonormalise(w, nsnap, l, w->Y.p, zq.p, w->Z.p))) return rv;
+    if ((rv = gemm_f64((int)n, l, nsnap, w->U.p, S, 1, zq.p, l, 1, w->Y.p, l, 1, w->part))) return rv;
+    if ((rv = orthonormalise(w, n, l, w->Y.p, w->Q.p, w->Z.p))) return rv;
+  }
+  // Rayleigh-Ritz: Z = U^T Q, H = Z^T Z, H = W mu W^T, Phi = Q W[:, :r]
+  if ((rv = gemm_f64((int)nsnap, l, n, w->U.p, 1, S, w->Q.p, l, 1, w->Z.p, l, 1, w->part))) return rv;
+  if ((rv = gemm_f64(l, l, nsnap, w->Z.p, 1, l, w->Z.p, l, 1, w->G.p, l, 1, w->part))) return rv;
+  std::vector<double> mu;
+  std::vector<int> order;
+  if ((rv = sym_eig_sorted(w, l, mu, order))) return rv;
+  std::vector<double> one(r, 1.0);
+  if ((rv = w->perm.upload(order.data(), l)) || (rv = w->scale.upload(one.data(), r))) return rv;
+  k_cols_perm_scale<<<grid1((long)l * r), 256>>>(l, r, w->V.p, w->perm.p, w->scale.p, w->T.p);
+  if ((rv = gemm_f64((int)n, r, l, w->Q.p, l, 1, w->T.p, r, 1, w->phi.p, r, 1, w->part))) return rv;
+  w->sigma2.assign(mu.begin(), mu.begin() + r);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+// standardised network inputs of nsamp samples into w->X (FP32 [nsamp][n_feat]);
+// with fit = true the feature statistics are (re)computed from these samples
+int make_inputs(ufem_warm *w, long nsamp, const double *d_ifld, bool fit) {
+  int rv;
+  const int nf = w->o.n_feat;
+  if ((rv = w->raw.ensure((size_t)nsamp * nf)) || (rv = w->X.ensure((size_t)nsamp * nf)) ||
+      (rv = w->sc.ensure(nsamp)))
+    return rv;
+  k_feat_raw<<<grid1(nsamp * nf), 256>>>(nsamp, nf, w->m->mc_ilen, d_ifld, w->fcol.p, w->flog.p, w->raw.p);
+  if (fit) k_col_stats<<<1, 32>>>(nsamp, nf, w->raw.p, w->fmean.p, w->fsd.p);
+  k_standardise<<<grid1(nsamp * nf), 256>>>(nsamp, nf, nf, w->raw.p, w->fmean.p, w->fsd.p, w->X.p);
+  k_scale<<<grid1(nsamp), 256>>>(nsamp, w->m->mc_ilen, w->o.scale_col, d_ifld, w->sc.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
+int padded_S(long nsamp) { return (int)std::max<long>(128, (nsamp + 127) / 128 * 128); }
+
+// u0 [n][S] = Phi c^T for the nsamp samples whose inputs are in w->X / w->sc
+int make_guess(ufem_warm *w, long nsamp, int S) {
+  int rv;
+  const int r = w->r;
+  if ((rv = w->Yo.ensure((size_t)nsamp * r)) || (rv = w->c.ensure((size_t)nsamp * r)) ||
+      (rv = w->u0.ensure((size_t)w->n * S)))
+    return rv;
+  if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) return rv;
+  k_coeffs<<<grid1(nsamp * r), 256>>>(nsamp, r, w->Yo.p, w->cmean.p, w->csd.p, w->sc.p, w->guess_scale, w->c.p);
+  if (S > nsamp) UFEM_CUDA_TRY(cudaMemsetAsync(w->u0.p, 0, (size_t)w->n * S * sizeof(double)));
+  // u0(i, s) = sum_k Phi[i][k] c[s][k]
+  return gemm_f64((int)w->n, (int)nsamp, r, w->phi.p, r, 1, w->c.p, 1, r, w->u0.p, S, 1, w->part);
+}
+
+}  // namespace
+}  // namespace ufem
+
+extern "C" {
+
+void ufem_warm_default_options(ufem_warm_options *o) {
+  std::memset(o, 0, sizeof(*o));
+  o->n_modes = 64;
+  o->n_hidden = 256;
+  o->n_feat = 0;
+  o->scale_col = -1;
+  o->n_snapshots = 512;
+  o->power_iters = 2;
+  o->epochs = 400;
+  o->batch = 256;
+  o->lr = 2e-3f;
+  o->seed = 20261203ULL;
+}
+
+int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out) {
+  if (!m || !o || !out) return UFEM_AF_ERR_EMP;
+  if (m->mc_ilen <= 0) {
+    set_error("ufem_warm_create: the model has no Monte Carlo variable table");
+    return UFEM_AF_ERR_EMP;
+  }
+  if (o->n_modes < 16 || o->n_modes % 16 || o->n_modes + 16 > kMaxL || o->n_feat < 1 || o->n_feat > 32 ||
+      o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 || o->n_snapshots < o->n_modes + 16) {
+    set_error("ufem_warm_create: n_modes a multiple of 16 up to 80, 1..32 inputs, n_hidden a multiple of 16 up to "
+              "256, n_snapshots >= n_modes + 16");
+    return UFEM_AF_ERR_SIZ;
+  }
+  for (int f = 0; f < o->n_feat; f++)
+    if (o->feat_cols[f] < 0 || o->feat_cols[f] >= m->mc_ilen) {
+      set_error("ufem_warm_create: input column out of range");
+      return UFEM_AF_ERR_SIZ;
+    }
+  if (o->scale_col >= m->mc_ilen) {
+    set_error("ufem_warm_create: scale column out of range");
+    return UFEM_AF_ERR_SIZ;
+  }
+  ufem_warm *w = new ufem_warm();
+  w->m = m;
+  w->o = *o;
+  w->r = o->n_modes;
+  w->l = o->n_modes + 16;
+  w->n = m->nDOFAct;
+  int rv;
+  std::vector<int> lg(o->n_feat);
+  for (int f = 0; f < o->n_feat; f++) lg[f] = o->feat_log[f] ? 1 : 0;
+  if ((rv = w->fcol.upload(o->feat_cols, o->n_feat)) || (rv = w->flog.upload(lg.data(), o->n_feat)) ||
+      (rv = w->fmean.ensure(32)) || (rv = w->fsd.ensure(32)) || (rv = w->cmean.ensure(w->r)) ||
+      (rv = w->csd.ensure(w->r)) ||
+      (rv = ufem_mlp_create(o->n_feat, o->n_hidden, w->r, o->seed, &w->mlp))) {
+    delete w;
+    return rv;
+  }
+  *out = w;
+  return UFEM_AF_OK;
+}
+
+void ufem_warm_free(ufem_warm *w) {
+  if (!w) return;
+  if (w->mlp) ufem_mlp_free(w->mlp);
+  delete w;
+}
+
+int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_mc_options *opt,
+                    ufem_warm_train_stats *ts) {
+  if (!w || !d_ifld) return UFEM_AF_ERR_EMP;
+  if (ntrain < w->o.n_snapshots || ntrain < w->o.batch) {
+    set_error("ufem_warm_train: need at least n_snapshots and batch training samples");
+    return UFEM_AF_ERR_SIZ;
+  }
+  int rv;
+  ufem_warm_train_stats st;
+  std::memset(&st, 0, sizeof(st));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto ms_since = [&](cudaEvent_t a) {
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, e1);
+    return (double)ms;
+  };
+  const long n = w->n;
+  const int r = w->r;
+  ufem_model *m = w->m;
+  // 1. cold batched solves of every training sample -> U [n][ntrain]
+  cudaEventRecord(e0);
+  if ((rv = w->U.ensure((size_t)n * ntrain)) || (rv = w->st.ensure(ntrain)) || (rv = w->it.ensure(ntrain))) return rv;
+  {
+    DBuf<double> uchunk;
+    const long chunk = 4096;
+    for (long c0 = 0; c0 < ntrain; c0 += chunk) {
+      const long cn = std::min(chunk, ntrain - c0);
+      const int S = padded_S(cn);
+      if ((rv = uchunk.ensure((size_t)n * S))) return rv;
+      const double *pin = d_ifld + c0 * m->mc_ilen;
+      double *pu = uchunk.p;
+      int *ps = w->st.p + c0;
+      long *pi = w->it.p + c0;
+      if ((rv = mc_solve_device(1, &m, &cn, &pin, nullptr, &ps, &pi, nullptr, &pu, opt))) return rv;
+      UFEM_CUDA_TRY(cudaMemcpy2DAsync(w->U.p + c0, ntrain * sizeof(double), uchunk.p, S * sizeof(double),
+                                      cn * sizeof(double), n, cudaMemcpyDeviceToDevice));
+    }
+  }
+  {
+    std::vector<int> hs(ntrain);
+    std::vector<long> hi(ntrain);
+    UFEM_CUDA_TRY(cudaMemcpy(hs.data(), w->st.p, ntrain * sizeof(int), cudaMemcpyDeviceToHost));
+    UFEM_CUDA_TRY(cudaMemcpy(hi.data(), w->it.p, ntrain * sizeof(long), cudaMemcpyDeviceToHost));
+    long mx = 0;
+    double sum = 0;
+    for (long s = 0; s < ntrain; s++) {
+      if (hs[s] != UFEM_ST_CONVERGED) {
+        set_error("ufem_warm_train: a training sample did not converge");
+        return UFEM_AF_ERR;
+      }
+      mx = std::max(mx, hi[s]);
+      sum += (double)hi[s];
+    }
+    w->cold_cap = mx;
+    st.cold_iters_max = mx;
+    st.cold_iters_mean = sum / (double)ntrain;
+  }
+  st.ms_solve = ms_since(e0);
+  // 2. POD basis from the first n_snapshots solutions
+  cudaEventRecord(e0);
+  if ((rv = fit_basis(w, (int)ntrain, w->o.n_snapshots))) return rv;
+  st.ms_basis = ms_since(e0);
+  for (int k = 0; k < r && k < 80; k++) st.sigma2[k] = w->sigma2[k];
+  // 3. inputs and targets
+  cudaEventRecord(e0);
+  if ((rv = make_inputs(w, ntrain, d_ifld, true))) return rv;
+  if ((rv = w->c.ensure((size_t)ntrain * r)) || (rv = w->Tt.ensure((size_t)ntrain * r))) return rv;
+  // c[s][k] = sum_i U[i][s] Phi[i][k]
+  if ((rv = gemm_f64((int)ntrain, r, n, w->U.p, 1, ntrain, w->phi.p, r, 1, w->c.p, r, 1, w->part))) return rv;
+  k_div_scale<<<grid1(ntrain * r), 256>>>(ntrain, r, w->sc.p, w->c.p);
+  k_col_stats<<<1, 128>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p);
+  k_targets<<<grid1(ntrain * r), 256>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p, w->Tt.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  // 4. training: shuffled minibatches, cosine learning rate
+  const int bs = w->o.batch;
+  const long nb = ntrain / bs;
+  const int nf = w->o.n_feat;
+  if ((rv = w->Xb.ensure((size_t)bs * nf)) || (rv = w->Tb.ensure((size_t)bs * r)) || (rv = w->bidx.ensure(ntrain)))
+    return rv;
+  std::mt19937_64 rng(w->o.seed ^ 0x7a11ULL);
+  std::vector<long> idx(ntrain);
+  std::iota(idx.begin(), idx.end(), 0L);
+  const long total = (long)w->o.epochs * nb;
+  long step = 0;
+  float loss = 0.0f;
+  for (int ep = 0; ep < w->o.epochs; ep++) {
+    std::shuffle(idx.begin(), idx.end(), rng);
+    if ((rv = w->bidx.upload(idx.data(), ntrain))) return rv;
+    double ep_loss = 0.0;
+    for (long b = 0; b < nb; b++, step++) {
+      k_gather_rows<float><<<grid1((long)bs * nf), 256>>>(bs, nf, w->bidx.p + b * bs, w->X.p, w->Xb.p);
+      k_gather_rows<float><<<grid1((long)bs * r), 256>>>(bs, r, w->bidx.p + b * bs, w->Tt.p, w->Tb.p);
+      const double frac = (double)step / (double)std::max<long>(1, total);
+      const float lr = (float)(w->o.lr * (0.02 + 0.98 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
+      if ((rv = ufem_mlp_train_step(w->mlp, bs, w->Xb.p, w->Tb.p, lr, &loss))) return rv;
+      ep_loss += loss;
+    }
+    ep_loss /= (double)nb;
+    if (ep == 0) st.loss_first = (float)ep_loss;
+    st.loss_last = (float)ep_loss;
+  }
+  st.ms_train = ms_since(e0);
+  st.epochs = w->o.epochs;
+  st.steps = step;
+  w->trained = true;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ts) *ts = st;
+  return UFEM_AF_OK;
+}
+
+int ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u0) {
+  if (!w || !d_ifld || !d_u0) return UFEM_AF_ERR_EMP;
+  if (!w->trained) {
+    set_error("ufem_warm_guess: the warm start is not trained");
+    return UFEM_AF_ERR;
+  }
+  int rv;
+  const int S = padded_S(nsamp);
+  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S))) return rv;
+  k_to_sample_major<<<grid1(w->n * nsamp), 256>>>(w->n, S, nsamp, w->u0.p, d_u0);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  return UFEM_AF_OK;
+}
+
+int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
+                    const ufem_mc_options *opt_in, ufem_warm_stats *ws) {
+  if (!w || !d_ifld) return UFEM_AF_ERR_EMP;
+  if (!w->trained) {
+    set_error("ufem_warm_solve: the warm start is not trained");
+    return UFEM_AF_ERR;
+  }
+  int rv;
+  ufem_mc_options opt;
+  if (opt_in) opt = *opt_in;
+  else ufem_mc_default_options(&opt);
+  ufem_warm_stats st;
+  std::memset(&st, 0, sizeof(st));
+  st.nsamp = nsamp;
+  cudaEvent_t e0, e1, e2, e3;
+  cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
+  ufem_model *m = w->m;
+  const long n = w->n;
+  const int S = padded_S(nsamp);
+  if ((rv = w->uf.ensure((size_t)n * S)) || (rv = w->st.ensure(nsamp)) || (rv = w->it.ensure(nsamp)) ||
+      (rv = w->err.ensure(nsamp)))
+    return rv;
+  int *pst = d_status ? d_status : w->st.p;
+  long *pit = d_iters ? d_iters : w->it.p;
+  cudaEventRecord(e0);
+  // guess
+  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S))) return rv;
+  cudaEventRecord(e1);
+  // warm-started batched solve, capped at the cold iteration count
+  ufem_mc_options wopt = opt;
+  if (w->cold_cap > 0) wopt.max_iters = std::min(opt.max_iters, w->cold_cap);
+  {
+    const double *pg = w->u0.p;
+    double *pu = w->uf.p;
+    if ((rv = mc_solve_device(1, &m, &nsamp, &d_ifld, &d_ofld, &pst, &pit, &pg, &pu, &wopt))) return rv;
+  }
+  cudaEventRecord(e2);
+  // fallback: samples that did not converge from the guess, again from zero
+  std::vector<int> hs(nsamp);
+  UFEM_CUDA_TRY(cudaMemcpy(hs.data(), pst, nsamp * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<long> fb;
+  for (long s = 0; s < nsamp; s++)
+    if (hs[s] != UFEM_ST_CONVERGED) fb.push_back(s);
+  st.fallbacks = (long)fb.size();
+  if (!fb.empty()) {
+    const long nf = (long)fb.size();
+    const long ilen = m->mc_ilen, olen = std::max<long>(1, m->mc_olen);
+    DBuf<long> d_idx;
+    if ((rv = d_idx.upload(fb.data(), nf)) || (rv = w->ifsub.ensure((size_t)nf * ilen)) ||
+        (rv = w->ofsub.ensure((size_t)nf * olen)) || (rv = w->stsub.ensure(nf)) || (rv = w->itsub.ensure(nf)))
+      return rv;
+    k_gather_rows<double><<<grid1(nf * ilen), 256>>>(nf, (int)ilen, d_idx.p, d_ifld, w->ifsub.p);
+    const double *pin = w->ifsub.p;
+    double *pof = w->ofsub.p;
+    int *ps = w->stsub.p;
+    long *pi = w->itsub.p;
+    DBuf<double> ufb;
+    const int Sf = padded_S(nf);
+    if ((rv = ufb.ensure((size_t)n * Sf))) return rv;
+    double *pu = ufb.p;
+    if ((rv = mc_solve_device(1, &m, &nf, &pin, d_ofld ? &pof : nullptr, &ps, &pi, nullptr, &pu, &opt))) return rv;
+    std::vector<int> fst(nf);
+    std::vector<long> fit(nf), wit(nsamp);
+    std::vector<double> fof((size_t)nf * olen);
+    UFEM_CUDA_TRY(cudaMemcpy(fst.data(), ps, nf * sizeof(int), cudaMemcpyDeviceToHost));
+    UFEM_CUDA_TRY(cudaMemcpy(fit.data(), pi, nf * sizeof(long), cudaMemcpyDeviceToHost));
+    UFEM_CUDA_TRY(cudaMemcpy(wit.data(), pit, nsamp * sizeof(long), cudaMemcpyDeviceToHost));
+    if (d_ofld && m->mc_olen > 0)
+      UFEM_CUDA_TRY(cudaMemcpy(fof.data(), pof, (size_t)nf * olen * sizeof(double), cudaMemcpyDeviceToHost));
+    for (long j = 0; j < nf; j++) {
+      const long s = fb[j];
+      hs[s] = fst[j] == UFEM_ST_CONVERGED ? UFEM_ST_FALLBACK : fst[j];
+      wit[s] += fit[j];  // iterations spent on this sample: the capped warm run + the cold one
+      if (d_ofld && m->mc_olen > 0)
+        UFEM_CUDA_TRY(cudaMemcpy(d_ofld + s * m->mc_olen, fof.data() + j * olen, m->mc_olen * sizeof(double),
+                                 cudaMemcpyHostToDevice));
+      UFEM_CUDA_TRY(cudaMemcpy2DAsync(w->uf.p + s, S * sizeof(double), ufb.p + j, Sf * sizeof(double),
+                                      sizeof(double), n, cudaMemcpyDeviceToDevice));
+    }
+    UFEM_CUDA_TRY(cudaMemcpy(pst, hs.data(), nsamp * sizeof(int), cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemcpy(pit, wit.data(), nsamp * sizeof(long), cudaMemcpyHostToDevice));
+  }
+  cudaEventRecord(e3);
+  // guess error against the converged solution
+  k_rel_err<<<grid1(nsamp, 128), 128>>>(n, S, (int)nsamp, w->u0.p, w->uf.p, w->err.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  std::vector<double> he(nsamp);
+  std::vector<long> hi(nsamp);
+  UFEM_CUDA_TRY(cudaMemcpy(he.data(), w->err.p, nsamp * sizeof(double), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(hi.data(), pit, nsamp * sizeof(long), cudaMemcpyDeviceToHost));
+  double se = 0, si = 0;
+  for (long s = 0; s < nsamp; s++) {
+    se += he[s];
+    st.guess_err_max = std::max(st.guess_err_max, he[s]);
+    si += (double)hi[s];
+    st.iters_max = std::max(st.iters_max, hi[s]);
+  }
+  st.guess_err_mean = nsamp ? se / (double)nsamp : 0.0;
+  st.iters_mean = nsamp ? si / (double)nsamp : 0.0;
+  st.cold_cap = w->cold_cap;
+  float a = 0, b = 0, c = 0;
+  cudaEventElapsedTime(&a, e0, e1);
+  cudaEventElapsedTime(&b, e1, e2);
+  cudaEventElapsedTime(&c, e2, e3);
+  st.ms_guess = a;
+  st.ms_solve = b;
+  st.ms_fallback = c;
+  st.ms_total = (double)a + b + c;
+  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
+  if (ws) *ws = st;
+  return UFEM_AF_OK;
+}
+
+int ufem_warm_set_guess_scale(ufem_warm *w, double factor) {
+  if (!w) return UFEM_AF_ERR_EMP;
+  w->guess_scale = factor;
+  return UFEM_AF_OK;
+}
+
+int ufem_warm_get_basis(const ufem_warm *w, double *h_phi, double *h_sigma2) {
+  if (!w) return UFEM_AF_ERR_EMP;
+  if (!w->trained) {
+    set_error("ufem_warm_get_basis: the warm start is not trained");
+    return UFEM_AF_ERR;
+  }
+  if (h_phi) UFEM_CUDA_TRY(cudaMemcpy(h_phi, w->phi.p, (size_t)w->n * w->r * sizeof(double), cudaMemcpyDeviceToHost));
+  if (h_sigma2) std::memcpy(h_sigma2, w->sigma2.data(), w->r * sizeof(double));
+  return UFEM_AF_OK;
+}
+
+// FP64 dense product through the warm start's GEMM kernel, for its tests:
+// C [M x N] = A [M x K] . B [K x N], all row-major device arrays.
+int ufem_dgemm_f64(int M, int N, long K, const double *d_A, const double *d_B, double *d_C) {
+  DBuf<double> part;
+  int rv = gemm_f64(M, N, K, d_A, K, 1, d_B, N, 1, d_C, N, 1, part);
+  if (rv) return rv;
+  UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  return UFEM_AF_OK;
+}
+
+// Symmetric eigen-decomposition through the warm start's one-block Jacobi
+// kernel, for its tests: A [l x l] (l even, <= 96) -> V [l x l] (columns =
+// eigenvectors, unsorted), lam [l].  Host arrays.
+int ufem_sym_eig(int l, const double *h_A, double *h_V, double *h_lam, int *sweeps) {
+  if (l < 2 || l % 2 || l > kMaxL) {
+    set_error("ufem_sym_eig: l even, 2..96");
+    return UFEM_AF_ERR_SIZ;
+  }
+  DBuf<double> A, V, lam;
+  DBuf<int> sw;
+  int rv;
+  if ((rv = A.upload(h_A, (size_t)l * l)) || (rv = V.ensure((size_t)l * l)) || (rv = lam.ensure(l)) ||
+      (rv = sw.ensure(1)))
+    return rv;
+  const size_t smem = jacobi_smem(l);
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_jacobi_eig<<<1, kJacThreads, smem>>>(l, A.p, V.p, lam.p, 60, sw.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  UFEM_CUDA_TRY(cudaMemcpy(h_V, V.p, (size_t)l * l * sizeof(double), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(h_lam, lam.p, l * sizeof(double), cudaMemcpyDeviceToHost));
+  if (sweeps) UFEM_CUDA_TRY(cudaMemcpy(sweeps, sw.p, sizeof(int), cudaMemcpyDeviceToHost));
+  return UFEM_AF_OK;
+}
+
+}  // extern "C"

@@ -356,3 +356,26 @@ def mc_samples(model: Model, mesh_id: int, nsamp: int, first_sample: int = 0,
         ifld[s, :nmat] = E0 * np.exp(sigma * z + shift)
         ifld[s, nmat:] = base * lf
     return ifld
+
+
+def warm_beam(nx=40, ny=10, nz=10, zones=16, lx=8.0, ly=2.0, lz=2.0, n_out_nodes=4) -> Model:
+    """The learned-warm-start beam: ``zones`` equal-length materials along x,
+    with the Monte Carlo table of ``mc_attach_vars`` (E of every zone, then the
+    value of every tip force)."""
+    m = beam_brick(nx, ny, nz, lx, ly, lz, zones=zones)
+    return mc_attach_vars(m, n_out_nodes=n_out_nodes)
+
+
+def warm_features(model: Model):
+    """Network inputs of the warm start: the zone E values and the first tip
+    force (all tip forces share one random load factor), both as log|.|, and
+    the solution's scale column (the first tip force: u is linear in it)."""
+    nmat = len(model.mp_vals)
+    cols = list(range(nmat)) + [nmat]
+    return cols, [1] * len(cols), nmat
+
+
+def warm_samples(model: Model, nsamp: int, first_sample: int = 0, mesh_id: int = 5) -> np.ndarray:
+    """Warm-start inputs: zone E = 30 GPa * exp(0.15 z) (median 30 GPa), load
+    factor U(0.8, 1.2).  Training and evaluation draw disjoint sample ids."""
+    return mc_samples(model, mesh_id=mesh_id, nsamp=nsamp, first_sample=first_sample, mean_one=False)
