@@ -319,6 +319,9 @@ typedef struct ufem_warm_stats {
   long iters_max;
   long cold_cap;             /* the iteration cap of the warm-started run */
   double ms_guess, ms_solve, ms_fallback, ms_total;
+  long kernel_launches;      /* kernels launched by the call */
+  double pcg_ms, pcg_bytes;  /* persistent PCG kernel time and algorithmic bytes (warm run) */
+  long pcg_launches;
 } ufem_warm_stats;
 
 typedef struct ufem_warm ufem_warm;

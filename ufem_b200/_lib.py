@@ -53,7 +53,8 @@ class WarmStats(C.Structure):
     _fields_ = [("nsamp", C.c_long), ("fallbacks", C.c_long), ("guess_err_mean", C.c_double),
                 ("guess_err_max", C.c_double), ("iters_mean", C.c_double), ("iters_max", C.c_long),
                 ("cold_cap", C.c_long), ("ms_guess", C.c_double), ("ms_solve", C.c_double),
-                ("ms_fallback", C.c_double), ("ms_total", C.c_double)]
+                ("ms_fallback", C.c_double), ("ms_total", C.c_double), ("kernel_launches", C.c_long),
+                ("pcg_ms", C.c_double), ("pcg_bytes", C.c_double), ("pcg_launches", C.c_long)]
 
 
 class McStats(C.Structure):

@@ -792,7 +792,14 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
     const double *pg = w->u0.p;
     double *pu = w->uf.p;
     if ((rv = mc_solve_device(1, &m, &nsamp, &d_ifld, &d_ofld, &pst, &pit, &pg, &pu, &wopt))) return rv;
+    ufem_mc_stats ms;
+    ufem_mc_get_stats(&ms);
+    st.kernel_launches += ms.kernel_launches;
+    st.pcg_ms = ms.ms_pcg;
+    st.pcg_bytes = ms.pcg_bytes;
+    st.pcg_launches = ms.pcg_launches;
   }
+  st.kernel_launches += 4 + 3 + 1 + 1;  // inputs (3), MLP forward (4), coefficients, u0 = Phi c
   cudaEventRecord(e2);
   // fallback: samples that did not converge from the guess, again from zero
   std::vector<int> hs(nsamp);
@@ -818,6 +825,9 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
     if ((rv = ufb.ensure((size_t)n * Sf))) return rv;
     double *pu = ufb.p;
     if ((rv = mc_solve_device(1, &m, &nf, &pin, d_ofld ? &pof : nullptr, &ps, &pi, nullptr, &pu, &opt))) return rv;
+    ufem_mc_stats ms;
+    ufem_mc_get_stats(&ms);
+    st.kernel_launches += ms.kernel_launches + 1;  // + the input gather
     std::vector<int> fst(nf);
     std::vector<long> fit(nf), wit(nsamp);
     std::vector<double> fof((size_t)nf * olen);
@@ -842,6 +852,7 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   cudaEventRecord(e3);
   // guess error against the converged solution
   k_rel_err<<<grid1(nsamp, 128), 128>>>(n, S, (int)nsamp, w->u0.p, w->uf.p, w->err.p);
+  st.kernel_launches += 1;
   UFEM_CUDA_TRY(cudaGetLastError());
   std::vector<double> he(nsamp);
   std::vector<long> hi(nsamp);
