@@ -52,6 +52,8 @@ METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 P
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
             "warm-started (POD 64 modes from 512 solves, MLP 17-256-256-64 trained on 4096 solves)")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
+KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
+          2: "k_batch_pcg<double,3,implicit>"}
 
 
 def parse():
@@ -66,6 +68,10 @@ def parse():
     p.add_argument("--epochs", type=int, default=400, help="MLP training epochs")
     p.add_argument("--plain-samples", type=int, default=16, help="samples timed by the plain method")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
+    p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
+    p.add_argument("--precision", type=int, default=2,
+                   help="2: FP64 PCG, blocks formed in the kernel (default); 1: FP32 PCG on explicit FP32 "
+                        "matrices with FP64 solution and true-residual replacement; 0: FP64 explicit")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
     p.add_argument("--profile-case", action="store_true",
@@ -73,20 +79,30 @@ def parse():
     return p.parse_args()
 
 
-def profile_case():
-    """A bounded case of the same kernels for profiler captures: the 60x15x15
-    mesh, 128 samples (values 1.76 GB FP32 > L2), the inner PCG capped at 40
-    iterations and one refinement step, run twice (warm + captured)."""
+PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
+           2: ("k_batch_pcg_implicit_40x10x10_1024samples.md", "40x10x10 16 E zones x 1024 samples, 40 iterations")}
+
+
+def profile_case(a):
+    """A bounded case of the same kernels for profiler captures, run twice
+    (warm + captured), the inner PCG capped at 40 iterations.  Precision 1:
+    the 60x15x15 per-element-E beam, 128 samples (FP32 values 1.76 GB > L2);
+    precision 2: the 40x10x10 zone beam, 1,024 samples (every FP64 vector
+    122 MB, eight of them > L2)."""
     from ufem_b200.api import GpuModel
     from ufem_b200.mc import mc_solve
     from ufem_b200 import meshgen as mg
-    m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
-    mg.mc_attach_vars(m)
-    f = mg.mc_samples(m, mesh_id=2, nsamp=128)
+    if a.precision == 2:
+        m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
+        f = mg.warm_samples(m, 1024)
+    else:
+        m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
+        mg.mc_attach_vars(m)
+        f = mg.mc_samples(m, mesh_id=2, nsamp=128)
     g = GpuModel(m)
     for _ in range(2):
-        res, st = mc_solve([g], [f], max_iters=40)
-    print(json.dumps({"profile_case": "60x15x15 x 128 samples, 40 iterations", "pcg_ms": st.ms_pcg,
+        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40)
+    print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
                       "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))
 
@@ -368,12 +384,12 @@ def ours(a):
     ws = WarmStart(g, cols, logs, scale_col, n_modes=64, n_hidden=256, n_snapshots=512, epochs=a.epochs,
                    batch=256, lr=2e-3)
     t0 = time.perf_counter()
-    tstats = ws.train(train)
+    tstats = ws.train(train, precision=a.precision)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
 
     opt = default_options()
-    opt.precision = 1
+    opt.precision = a.precision
     opt.tol = 1e-8
     n = ev.shape[0]
     olen = m.mc_olen
@@ -458,6 +474,37 @@ def ours(a):
             "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
     del d_out2, d_st2, d_it2
 
+    # ---- the warm start at the other precisions (one warm-up, one timed step)
+    PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
+            1: "FP32 PCG on explicit FP32 matrices, FP64 solution and true-residual replacement",
+            2: "FP64 PCG, blocks formed in the kernel from shared unit-E element blocks"}
+    other = {}
+    if not a.no_other:
+        for p_alt in (1, 0):
+            if p_alt == a.precision:
+                continue
+            opt_alt = default_options()
+            opt_alt.precision = p_alt
+            opt_alt.tol = 1e-8
+            wst2 = _lib.WarmStats()
+            args2 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt_alt),
+                     C.byref(wst2))
+            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args2))
+            torch.cuda.synchronize()
+            e0.record()
+            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args2))
+            e1.record()
+            torch.cuda.synchronize()
+            ms2 = e0.elapsed_time(e1)
+            other[str(p_alt)] = {"method": PREC[p_alt], "value": n / (ms2 / 1000.0), "unit": "solves/s",
+                                 "iters_mean": wst2.iters_mean, "iters_max": wst2.iters_max,
+                                 "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
+                                 "pcg_GBs": wst2.pcg_bytes / (wst2.pcg_ms / 1000.0) / 1e9 if wst2.pcg_ms else None,
+                                 "outputs_max_rel_diff": float(np.abs(d_out.cpu().numpy() - out_warm).max()
+                                                               / np.abs(out_warm).max())}
+            if p_alt == 0:
+                break  # FP64 explicit needs the most memory: last
+
     result = None
     if rank == 0:
         # ---- the plain method on a subset of the same samples ----------------
@@ -476,7 +523,7 @@ def ours(a):
         # ratio of this kernel (profiles/, a smaller case of the same kernel)
         # times this run's algorithmic bytes per launch
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "k_batch_pcg_60x15x15_128samples.md")
+        tf = os.path.join(ROOT, "profiles", PROFILE.get(a.precision, ("none", ""))[0])
         if os.path.exists(tf) and pcg_launches > 0:
             for line in open(tf):
                 if line.startswith("traffic_over_algorithmic:"):
@@ -494,10 +541,12 @@ def ours(a):
         result = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32 inner / fp64 refinement", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if a.precision != 1 else "fp32 inner / fp64 refinement",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
-                       "precision": "FP32 Jacobi PCG, FP64 solution and true-residual replacement",
-                       "l2_flush": "not needed: per-sample FP32 values 34 GB per iteration >> 126 MB L2",
+                       "precision": PREC[a.precision],
+                       "l2_flush": "not needed: every per-sample vector is 0.98 GB (FP64, 8192 samples) and the "
+                                   "explicit FP32 values 34 GB per iteration, >> 126 MB L2",
                        "parallelism": f"samples sharded over {world} GPU(s), no collective"},
             "all_converged": bool(np.isin(status, [0, 4]).all()),
             "warm_start": {"iters_mean": float(iters.mean()), "iters_max": int(iters.max()),
@@ -514,11 +563,12 @@ def ours(a):
                                      "loss_first": tstats["loss_first"], "loss_last": tstats["loss_last"],
                                      "pod_energy_mode64_over_mode1": (s2[63] / s2[0]) if s2[0] else None}},
             "batched_without_warm_start": cold,
+            "warm_start_other_precisions": other,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},
             "speedup_vs_plain": value / plain,
-            "roofline": {"bound": "hbm", "kernel": "k_batch_pcg<float,3>", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": KERNEL[a.precision], "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "pcg_ms_per_step": pcg_ms / a.steps,
                          "pcg_launches_per_step": pcg_launches / a.steps},
@@ -540,7 +590,7 @@ def main():
         ref_worker(a.ref_worker)
         return
     if a.profile_case:
-        profile_case()
+        profile_case(a)
         return
     if a.impl == "reference":
         reference_arm(a)

@@ -199,10 +199,14 @@ int   monte_solution(char *param, double *ifld, double *ofld, long if_type); /* 
 int monte_solution_batch(char *param, long nsamp, const double *ifld, double *ofld,
                          long if_type, int *status);
 
-/* Options of the batched solve.  precision 0: FP64 PCG; 1: FP32 PCG (FP32
- * matrix and work vectors) with the solution kept in FP64 and the residual
- * replaced by the true FP64 residual f - K u from time to time.  A sample
- * converges when its true relative residual |f - K u| / |f| <= tol. */
+/* Options of the batched solve.  precision 0: FP64 PCG on an explicit FP64
+ * matrix per sample; 1: FP32 PCG (FP32 matrix and work vectors) with the
+ * solution kept in FP64 and the residual replaced by the true FP64 residual
+ * f - K u from time to time; 2: FP64 PCG with no per-sample matrix -- every
+ * block is formed inside the PCG kernel from the mesh's unit-E element blocks
+ * (summed per random E variable) times the sample's E values, which holds
+ * because K_e is linear in E for the isotropic material.  A sample converges
+ * when its true relative residual |f - K u| / |f| <= tol. */
 typedef struct ufem_mc_options {
   int precision;
   double tol;
@@ -285,8 +289,9 @@ int  ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, fl
  * the sample's value in scale_col: the solution is linear in the load).
  * Solving: u0 = scale * Phi * MLP(inputs) is the initial guess of the
  * batched PCG, which still iterates to the same tolerance; its iteration cap
- * is the largest cold iteration count seen in training, and a sample that
- * does not converge within it is solved again from zero (UFEM_ST_FALLBACK).
+ * is the largest cold iteration count seen in training (when solving at the
+ * training's precision), and a sample that does not converge within it is
+ * solved again from zero (UFEM_ST_FALLBACK).
  * d_ifld: device, nsamp*ilen (the model's Monte Carlo inputs). */
 typedef struct ufem_warm_options {
   int n_modes;               /* POD modes: a multiple of 16, at most 80 */

@@ -74,7 +74,7 @@ def test_batch_matches_single_samples(mc_fixture):
         lib.close()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_uneven_meshes_one_launch(precision):
     """Three meshes of uneven size and sample counts (not multiples of the
     sample group) in one launch, against per-sample FP64 oracle solves."""
@@ -181,3 +181,83 @@ def test_iteration_cap_reports_maxit():
     f = mg.mc_samples(m, 3, 5)
     res, _ = mc_solve([GpuModel(m)], [f], max_iters=3)
     assert (res[0][1] == ST_MAXIT).all()
+
+
+def _solve_u(g, ifld, precision):
+    """Batched solve through ufem_mc_solve_device: (u [nsamp][ndof], status, iters)."""
+    import ctypes as C
+    import torch
+    from ufem_b200 import _lib
+    from ufem_b200.mc import default_options
+    L = _lib.load()
+    n = ifld.shape[0]
+    S = max(128, (n + 127) // 128 * 128)
+    d_in = torch.from_numpy(np.ascontiguousarray(ifld)).cuda()
+    d_out = torch.zeros((n, max(1, g.model.mc_olen)), dtype=torch.float64, device="cuda")
+    d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_it = torch.zeros(n, dtype=torch.int64, device="cuda")
+    d_u = torch.zeros((g.ndof, S), dtype=torch.float64, device="cuda")
+    vp = lambda t: (C.c_void_p * 1)(t.data_ptr())
+    opt = default_options()
+    opt.precision = precision
+    rv = L.ufem_mc_solve_device(1, (C.c_void_p * 1)(g.h.value), np.array([n], np.int64).ctypes.data_as(
+        C.POINTER(C.c_long)), vp(d_in), vp(d_out), vp(d_st), vp(d_it), (C.c_void_p * 1)(), vp(d_u), C.byref(opt))
+    _lib.check("ufem_mc_solve_device", rv)
+    return d_u[:, :n].T.cpu().numpy(), d_st.cpu().numpy(), d_it.cpu().numpy(), d_out.cpu().numpy()
+
+
+def _drop_first_input(m, ifld):
+    """The model with its first Monte Carlo input (material 0's E) made
+    non-random, and the inputs without that column."""
+    rows = [r.copy() for r in m.mc_vars]
+    ins = rows[1:m.mc_ilen]
+    outs = rows[m.mc_ilen:]
+    for j, r in enumerate(ins):
+        r[0] = j
+    m.mc_vars = np.array(ins + outs, dtype=np.int64)
+    m.mc_ilen -= 1
+    return ifld[:, 1:].copy()
+
+
+def _implicit_cases():
+    from ufem_b200 import meshgen as mg
+    zones = mg.warm_beam(12, 3, 3, zones=4)
+    f_zones = mg.warm_samples(zones, 100)
+    part = mg.mc_attach_vars(mg.beam_brick(6, 2, 2, 3.0, 1.0, 1.0, zones=3))
+    f_part = _drop_first_input(part, mg.mc_samples(part, mesh_id=4, nsamp=70))
+    quad = mg.mc_attach_vars(mg.plate_quad(16, 4, 4.0, 1.0, distort=0.2, seed=3))
+    f_quad = mg.mc_samples(quad, mesh_id=6, nsamp=50)
+    elem = mg.mc_attach_vars(mg.beam_brick(5, 2, 2, 2.5, 1.0, 1.0, per_element_material=True))
+    f_elem = mg.mc_samples(elem, mesh_id=7, nsamp=40)
+    return [("zones", zones, f_zones), ("constant_part", part, f_part), ("quad", quad, f_quad),
+            ("per_element", elem, f_elem)]
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_implicit_form_matches_explicit_fp64(case):
+    """precision 2 (each block formed inside the PCG kernel from the shared
+    unit-E element blocks summed per random multiplier) against precision 0
+    (an explicit FP64 matrix per sample): E zones (several elements per
+    multiplier), a non-random material (the constant part), quads (B = 2)
+    and per-element E.  Both are FP64 PCGs to the true relative residual
+    1e-8: solutions within 1e-6 relative, iteration counts within 3 %."""
+    from ufem_b200.api import GpuModel
+    name, m, f = _implicit_cases()[case]
+    g = GpuModel(m)
+    u0, st0, it0, o0 = _solve_u(g, f, 0)
+    u2, st2, it2, o2 = _solve_u(g, f, 2)
+    assert (st0 == 0).all() and (st2 == 0).all(), name
+    assert np.abs(u2 - u0).max() <= 1e-6 * np.abs(u0).max(), name
+    assert np.abs(o2 - o0).max() <= 1e-6 * max(np.abs(o0).max(), 1e-300), name
+    assert (np.abs(it2 - it0) <= 0.03 * it0 + 2).all(), (name, it0, it2)
+
+
+def test_implicit_run_twice_identical():
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    m = mg.warm_beam(8, 2, 2, zones=4)
+    f = mg.warm_samples(m, 150)
+    g = GpuModel(m)
+    a = _solve_u(g, f, 2)
+    b = _solve_u(g, f, 2)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])

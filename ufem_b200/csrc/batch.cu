@@ -71,6 +71,18 @@ struct McPlan {
   DBuf<int> d_out_type, d_out_pos, d_out_row, d_out_elem, d_out_ip, d_out_comp;
   DBuf<int> reac_rows;             // DOF rows of the reaction list
   long ilen = 0, olen = 0;
+  // host copies for the implicit form
+  std::vector<int> h_gptr, h_gel, h_gpair, h_elem_var;
+  // implicit (matrix-free) form, precision 2: per block, the unit-E element
+  // blocks summed per multiplier -- multiplier 0 is the constant 1 (elements
+  // whose E is not random, pre-scaled by their E), multiplier j >= 1 is the
+  // ifld column mult_col[j] -- with supported rows/columns zeroed
+  bool imp_built = false;
+  int nmult = 0, cstride = 0;
+  std::vector<int> mult_col;
+  DBuf<int> d_mult_col, cptr;
+  DBuf<double> cval;               // [nc][cstride]: B*B values, then the multiplier index
+  long nc = 0;
 };
 
 static std::vector<std::unique_ptr<McPlan>> g_plans;
@@ -119,6 +131,9 @@ static int build_plan(ufem_model *m, McPlan *P) {
       gpair[fill[k]] = p;
       fill[k]++;
     }
+  P->h_gptr = cnt;
+  P->h_gel = gel;
+  P->h_gpair = gpair;
   if ((rv = P->gptr.upload(cnt.data(), cnt.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->gel.upload(gel.data(), gel.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->gpair.upload(gpair.data(), gpair.size())) != UFEM_AF_OK) return rv;
@@ -155,6 +170,7 @@ static int build_plan(ufem_model *m, McPlan *P) {
   }
   std::vector<int> ev(m->eLen);
   for (long e = 0; e < m->eLen; e++) ev[e] = mat_var[m->eMat[e]];
+  P->h_elem_var = ev;
   if ((rv = P->elem_var.upload(ev.data(), ev.size())) != UFEM_AF_OK) return rv;
   std::vector<double> F0(m->nDOFAct, 0.0);
   P->ovr_row.clear();
@@ -228,6 +244,82 @@ static int build_plan(ufem_model *m, McPlan *P) {
   if ((rv = P->d_out_ip.upload(oip.data(), oip.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->d_out_comp.upload(ocomp.data(), ocomp.size())) != UFEM_AF_OK) return rv;
   P->built = true;
+  return UFEM_AF_OK;
+}
+
+// The implicit form of K_s = sum_e E_{s,e} K_e: for every block, the
+// element contributions (element order) summed per multiplier.  Rows and
+// columns of supported DOFs are zeroed; the PCG kernel gives those rows the
+// identity (fem/fem_loads.c:158-166).
+static int build_implicit(ufem_model *m, McPlan *P) {
+  int rv;
+  const int B = m->b, nn = m->nn, se = P->s, BB = B * B;
+  const int stride = (BB + 2) & ~1;  // values + index, a multiple of 16 bytes
+  std::vector<double> Kh((size_t)m->eLen * se * se);
+  UFEM_CUDA_TRY(cudaMemcpy(Kh.data(), P->Khat.p, Kh.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<int> col2mult(std::max<long>(1, m->mc_ilen), -1), emult(m->eLen);
+  P->mult_col.assign(1, -1);
+  for (long e = 0; e < m->eLen; e++) {
+    const int v = P->h_elem_var[e];
+    if (v < 0) {
+      emult[e] = 0;
+      continue;
+    }
+    if (col2mult[v] < 0) {
+      col2mult[v] = (int)P->mult_col.size();
+      P->mult_col.push_back(v);
+    }
+    emult[e] = col2mult[v];
+  }
+  std::vector<int> blkrow(m->nnzb);
+  for (int r = 0; r < m->nbr; r++)
+    for (int k = m->rowptr[r]; k < m->rowptr[r + 1]; k++) blkrow[k] = r;
+  std::vector<int> cptr(m->nnzb + 1, 0);
+  std::vector<double> cval;
+  cval.reserve((size_t)m->nnzb * stride * 2);
+  std::vector<int> slot_mult;
+  std::vector<double> W;
+  for (long k = 0; k < m->nnzb; k++) {
+    slot_mult.clear();
+    W.clear();
+    for (int c = P->h_gptr[k]; c < P->h_gptr[k + 1]; c++) {
+      const int e = P->h_gel[c], p = P->h_gpair[c], la = p / nn, lb = p % nn, mi = emult[e];
+      const double scale = (mi == 0) ? m->eE[e] : 1.0;
+      size_t sl = 0;
+      while (sl < slot_mult.size() && slot_mult[sl] != mi) sl++;
+      if (sl == slot_mult.size()) {
+        slot_mult.push_back(mi);
+        W.resize(W.size() + BB, 0.0);
+      }
+      const double *kh = Kh.data() + (size_t)e * se * se + (size_t)(la * B) * se + lb * B;
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) W[sl * BB + i * B + j] += scale * kh[i * se + j];
+    }
+    const int I = blkrow[k], J = m->colind[k];
+    for (size_t sl = 0; sl < slot_mult.size(); sl++) {
+      bool any = false;
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) {
+          double &w = W[sl * BB + i * B + j];
+          if (m->fixedMask[I * B + i] || m->fixedMask[J * B + j]) w = 0.0;
+          any = any || (w != 0.0);
+        }
+      if (!any) continue;
+      for (int t = 0; t < BB; t++) cval.push_back(W[sl * BB + t]);
+      cval.push_back((double)slot_mult[sl]);
+      for (int t = BB + 1; t < stride; t++) cval.push_back(0.0);
+      cptr[k + 1]++;
+    }
+  }
+  for (long k = 0; k < m->nnzb; k++) cptr[k + 1] += cptr[k];
+  P->nmult = (int)P->mult_col.size();
+  P->cstride = stride;
+  P->nc = cptr[m->nnzb];
+  if (cval.empty()) cval.assign(stride, 0.0);
+  if ((rv = P->cptr.upload(cptr.data(), cptr.size())) || (rv = P->cval.upload(cval.data(), cval.size())) ||
+      (rv = P->d_mult_col.upload(P->mult_col.data(), P->mult_col.size())))
+    return rv;
+  P->imp_built = true;
   return UFEM_AF_OK;
 }
 
@@ -404,6 +496,37 @@ __global__ void __launch_bounds__(128) k_assemble_batch(int S, int s_el, const i
     }
 }
 
+// per-sample multipliers of the implicit form: mult[j][s] = 1 (j = 0) or the
+// sample's ifld value of column mult_col[j]
+__global__ void k_make_mult(int nmult, int S, int nsamp, long ilen, const double *__restrict__ ifld,
+                            const int *__restrict__ mult_col, double *__restrict__ mult) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)nmult * S) return;
+  const int j = (int)(t / S), s = (int)(t % S);
+  mult[t] = (j == 0 || s >= nsamp) ? 1.0 : ifld[(size_t)s * ilen + mult_col[j]];
+}
+
+// Jacobi diagonal of the implicit K_s (supported rows: 1)
+template <int B>
+__global__ void k_diag_implicit(int nbr, int S, const int *__restrict__ diagblk, const int *__restrict__ cptr,
+                                const double *__restrict__ cval, int cstride, const double *__restrict__ mult,
+                                const unsigned char *__restrict__ fixed, double *__restrict__ M) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)nbr * S) return;
+  const int I = (int)(t / S), s = (int)(t % S);
+  const int k = diagblk[I];
+#pragma unroll
+  for (int a = 0; a < B; a++) {
+    double d = 0.0;
+    for (int c = cptr[k]; c < cptr[k + 1]; c++) {
+      const double *w = cval + (size_t)c * cstride;
+      d += mult[(size_t)(int)w[B * B] * S + s] * w[a * B + a];
+    }
+    const int row = I * B + a;
+    M[(size_t)row * S + s] = fixed[row] ? 1.0 : d;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // the persistent masked PCG over all meshes, with residual replacement
@@ -430,6 +553,13 @@ struct BMesh {
   int *gtrue;           // [ngroups] the group's latest rr partials are true residuals
   int *gneed;           // [ngroups] a replacement is due after this iteration
   int *glast;           // [ngroups] iteration of the last replacement
+  // implicit form (precision 2): block k = sum over c in [cptr[k], cptr[k+1])
+  // of mult[idx_c][s] * W_c, W_c and idx_c in cval[c*cstride ...]
+  const int *cptr;
+  const double *cval;
+  const double *mult;
+  const unsigned char *fixed;
+  int cstride;
 };
 
 template <typename T>
@@ -446,11 +576,55 @@ struct BArgs {
   long *iter_out;
 };
 
+// One contribution of the implicit form: its B x B unit block and its
+// multiplier index (read-only for the whole kernel: non-coherent loads).
+template <int B>
+__device__ __forceinline__ int ld_contrib(const double *w, double (&W)[B * B]) {
+  constexpr int CS = (B * B + 2) & ~1;
+  double t[CS];
+#pragma unroll
+  for (int h = 0; h < CS / 2; h++) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
+    t[2 * h] = v.x;
+    t[2 * h + 1] = v.y;
+  }
+#pragma unroll
+  for (int e = 0; e < B * B; e++) W[e] = t[e];
+  return (int)t[B * B];
+}
+
+// acc[a] += mult_s * (W x)[a] over the contributions [c0, c1) of one block
+template <int B, int VN>
+__device__ __forceinline__ void implicit_block(const double *cval, int cstride, const double *mult, int S, int sb,
+                                               int c0, int c1, const double (&xv)[B][VN], double (&acc)[B][VN]) {
+  for (int c = c0; c < c1; c++) {
+    double W[B * B];
+    const int mi = ld_contrib<B>(cval + (size_t)c * cstride, W);
+    double av[VN];
+#pragma unroll
+    for (int h = 0; h < VN / 2; h++) {
+      const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)mi * S + sb) + h);
+      av[2 * h] = v.x;
+      av[2 * h + 1] = v.y;
+    }
+#pragma unroll
+    for (int a = 0; a < B; a++)
+#pragma unroll
+      for (int v = 0; v < VN; v++) {
+        double t = 0.0;
+#pragma unroll
+        for (int b = 0; b < B; b++) t = fma(W[a * B + b], xv[b][v], t);
+        acc[a][v] = fma(av[v], t, acc[a][v]);
+      }
+  }
+}
+
 // y = A (z + beta p_old) on the block rows of one tile for GS samples;
 // pnew = z + beta p_old on the own rows; partial p.q per sample.
-template <typename T, int B>
+template <typename T, int B, bool IMP>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VecOf<T>::N]) {
+  static_assert(!IMP || sizeof(T) == 8, "the implicit form runs in FP64");
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -474,12 +648,21 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       // the row's column indices, one per lane, then broadcast by shuffle:
       // the neighbour gathers no longer wait on a dependent index load
       const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+      int myC0 = 0, myC1 = 0;
+      if constexpr (IMP) {
+        if (kb + lane < k1) {
+          myC0 = __ldg(M.cptr + kb + lane);
+          myC1 = __ldg(M.cptr + kb + lane + 1);
+        }
+      }
       const int cnt = min(32, k1 - kb);
       for (int j = 0; j < cnt; j++) {
         const int k = kb + j;
-        T vv[B * B][VN];
+        T vv[IMP ? 1 : B * B][VN];
+        if constexpr (!IMP) {
 #pragma unroll
-        for (int e = 0; e < B * B; e++) ldv_stream<T>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
+          for (int e = 0; e < B * B; e++) ldv_stream<T>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
+        }
         const int J = __shfl_sync(0xffffffffu, myJ, j);
         T xv[B][VN];
 #pragma unroll
@@ -492,12 +675,17 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
             for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
           }
         }
+        if constexpr (IMP) {
+          const int c0 = __shfl_sync(0xffffffffu, myC0, j), c1 = __shfl_sync(0xffffffffu, myC1, j);
+          implicit_block<B, VN>(M.cval, M.cstride, M.mult, S, sb, c0, c1, xv, acc);
+        } else {
 #pragma unroll
-        for (int a = 0; a < B; a++)
+          for (int a = 0; a < B; a++)
 #pragma unroll
-          for (int c = 0; c < B; c++)
+            for (int c = 0; c < B; c++)
 #pragma unroll
-            for (int v = 0; v < VN; v++) acc[a][v] += vv[a * B + c][v] * xv[c][v];
+              for (int v = 0; v < VN; v++) acc[a][v] += vv[a * B + c][v] * xv[c][v];
+        }
       }
     }
 #pragma unroll
@@ -513,6 +701,12 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       } else {
 #pragma unroll
         for (int v = 0; v < VN; v++) pi[v] = zi[v];
+      }
+      if constexpr (IMP) {
+        if (M.fixed[I * B + a]) {  // supported DOF: identity row
+#pragma unroll
+          for (int v = 0; v < VN; v++) acc[a][v] = pi[v];
+        }
       }
       stv<T>(pnew + o, pi);
       stv<T>(M.q + o, acc[a]);
@@ -603,7 +797,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
 
 // Residual replacement: r = F - K x in FP64 from the FP64 values, then
 // r (inner precision), z = r / M and the partials of the true residual.
-template <typename T, int B>
+template <typename T, int B, bool IMP>
 __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
                                                    double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
@@ -624,6 +818,13 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
     const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
     for (int kb = k0; kb < k1; kb += 32) {
       const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+      int myC0 = 0, myC1 = 0;
+      if constexpr (IMP) {
+        if (kb + lane < k1) {
+          myC0 = __ldg(M.cptr + kb + lane);
+          myC1 = __ldg(M.cptr + kb + lane + 1);
+        }
+      }
       const int cnt = min(32, k1 - kb);
       for (int j = 0; j < cnt; j++) {
         const int k = kb + j;
@@ -631,15 +832,20 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
         double xv[B][VN];
 #pragma unroll
         for (int c = 0; c < B; c++) ldv_d<VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
+        if constexpr (IMP) {
+          const int c0 = __shfl_sync(0xffffffffu, myC0, j), c1 = __shfl_sync(0xffffffffu, myC1, j);
+          implicit_block<B, VN>(M.cval, M.cstride, M.mult, S, sb, c0, c1, xv, acc);
+        } else {
 #pragma unroll
-        for (int a = 0; a < B; a++)
+          for (int a = 0; a < B; a++)
 #pragma unroll
-          for (int c = 0; c < B; c++) {
-            double vv[VN];
-            ldv_d_stream<VN>(M.V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+            for (int c = 0; c < B; c++) {
+              double vv[VN];
+              ldv_d_stream<VN>(M.V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
 #pragma unroll
-            for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
-          }
+              for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
+            }
+        }
       }
     }
 #pragma unroll
@@ -649,6 +855,14 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
       T ri[VN], mi[VN], zi[VN];
       ldv_d<VN>(M.F + o, f);
       ldv<T>(M.M + o, mi);
+      if constexpr (IMP) {
+        if (M.fixed[I * B + a]) {  // supported DOF: identity row
+          double xo[VN];
+          ldv_d<VN>(M.x + o, xo);
+#pragma unroll
+          for (int v = 0; v < VN; v++) acc[a][v] = xo[v];
+        }
+      }
 #pragma unroll
       for (int v = 0; v < VN; v++) {
         const double r64 = f[v] - acc[a][v];
@@ -670,7 +884,7 @@ __device__ __forceinline__ double group_total(const double *part, int g, int ntp
   return t;
 }
 
-template <typename T, int B>
+template <typename T, int B, bool IMP>
 __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
@@ -690,7 +904,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
     if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
     any = __syncthreads_or(any);
     if (any) {
-      tile_true_residual<T, B>(M, ti.y, ti.z, 0, s_red, s_red2);
+      tile_true_residual<T, B, IMP>(M, ti.y, ti.z, 0, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) {
         M.gtrue[ti.y] = 1;
         M.glast[ti.y] = 0;
@@ -758,7 +972,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       }
       const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+      tile_spmv<T, B, IMP>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
     // The group counter changes only in phase S: read between the barriers,
@@ -817,7 +1031,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
           __syncthreads();  // thread 0 rewrites s_m / s_flag for the next tile
           continue;
         }
-        tile_true_residual<T, B>(M, ti.y, ti.z, par, s_red, s_red2);
+        tile_true_residual<T, B, IMP>(M, ti.y, ti.z, par, s_red, s_red2);
         if (ti.z == 0 && threadIdx.x == 0) {
           M.gtrue[ti.y] = 1;
           M.glast[ti.y] = (int)k;
@@ -992,6 +1206,7 @@ struct McWork {
   int S = 0, nsamp = 0;
   DBuf<double> E, F, Fraw, V64, M64, x64, tol2, ff, ffpart;
   DBuf<float> V32, M32;
+  DBuf<double> mult;     // implicit form: per-sample multipliers [nmult][S]
   // inner vectors, FP32 or FP64
   DBuf<float> fr, fz, fp0, fp1, fq;
   DBuf<double> dr, dz, dp0, dp1, dq, pq, prr, prz, rho, rrlast;
@@ -1056,9 +1271,9 @@ struct EvTimer {
   }
 };
 
-template <typename T>
-int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, const ufem_mc_options &opt,
-            long *iters_run) {
+template <typename T, bool IMP>
+int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, const std::vector<McPlan *> &plans,
+            const ufem_mc_options &opt, long *iters_run) {
   constexpr int VN = VecOf<T>::N, GS = 32 * VN;
   int rv;
   std::vector<BMesh<T>> hm(nmesh);
@@ -1067,7 +1282,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int B = models[0]->b;
-  void (*kern)(BArgs<T>) = (B == 3) ? k_batch_pcg<T, 3> : k_batch_pcg<T, 2>;
+  void (*kern)(BArgs<T>) = (B == 3) ? k_batch_pcg<T, 3, IMP> : k_batch_pcg<T, 2, IMP>;
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     set_error("batched PCG kernel does not fit on an SM");
@@ -1096,6 +1311,11 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     b.F = w.F.p;
     b.x = w.x64.p;
     b.tol2 = w.tol2.p;
+    b.cptr = plans[k]->cptr.p;
+    b.cval = plans[k]->cval.p;
+    b.mult = w.mult.p;
+    b.fixed = m->d_fixed.p;
+    b.cstride = plans[k]->cstride;
     const size_t n = (size_t)m->nDOFAct * w.S;
     const size_t np = (size_t)b.ngroups * b.ntpg * GS;
     if constexpr (sizeof(T) == 4) {
@@ -1106,7 +1326,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
         return rv;
       b.r = w.fr.p; b.z = w.fz.p; b.p0 = w.fp0.p; b.p1 = w.fp1.p; b.q = w.fq.p;
     } else {
-      b.V = w.V64.p;
+      b.V = IMP ? nullptr : w.V64.p;
       b.M = w.M64.p;
       if ((rv = w.dr.ensure(n)) || (rv = w.dz.ensure(n)) || (rv = w.dp0.ensure(n)) || (rv = w.dp1.ensure(n)) ||
           (rv = w.dq.ensure(n)))
@@ -1217,13 +1437,17 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
         gi = std::max(gi, si);
       }
       mesh_its = std::max(mesh_its, gi);
-      const double vals = m->nnzb * bb * sizeof(T) * GS, vec = n * GS * sizeof(T);
+      // explicit: every sample's values; implicit: every sample's multipliers
+      const double vals = IMP ? (double)plans[k]->nmult * sizeof(double) * GS : m->nnzb * bb * sizeof(T) * GS;
+      const double vec = n * GS * sizeof(T);
       g_stats.spmv_bytes += (vals + 2.0 * vec) * gi;
       // S phase: values, 2 gathered and 2 own vectors in, 2 out; U phase:
       // M, r, p, q in, r, z out, x (FP64) in and out
       g_stats.pcg_bytes += (vals + 11.0 * vec + 2.0 * n * GS * sizeof(double)) * gi;
     }
-    const double idx = m->nnzb * 4.0 + 4.0 * (m->nbr + 1);
+    double idx = m->nnzb * 4.0 + 4.0 * (m->nbr + 1);
+    // implicit: the shared contribution table, once per mesh-iteration
+    if (IMP) idx += 4.0 * (m->nnzb + 1) + 8.0 * plans[k]->nc * plans[k]->cstride;
     g_stats.spmv_bytes += idx * mesh_its;
     g_stats.pcg_bytes += idx * mesh_its;
   }
@@ -1257,6 +1481,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       ufem_model *m = models[k];
       McPlan *P = get_plan(m);
       if (!P->built && (rv = build_plan(m, P)) != UFEM_AF_OK) return rv;
+      const bool imp = (opt.precision == 2);
+      if (imp && !P->imp_built && (rv = build_implicit(m, P)) != UFEM_AF_OK) return rv;
       plans[k] = P;
       W[k] = get_work(m);
       McWork &w = *W[k];
@@ -1264,11 +1490,19 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       w.S = std::max(128, (int)((nsamp[k] + 127) / 128 * 128));
       const size_t n = (size_t)m->nDOFAct * w.S, nv = (size_t)m->nnzb * B * B * w.S;
       if ((rv = w.E.ensure((size_t)m->eLen * w.S)) || (rv = w.F.ensure(n)) || (rv = w.Fraw.ensure(n)) ||
-          (rv = w.V64.ensure(nv)) || (rv = w.M64.ensure(n)) || (rv = w.x64.ensure(n)) || (rv = w.state.ensure(w.S)) ||
+          (rv = w.M64.ensure(n)) || (rv = w.x64.ensure(n)) || (rv = w.state.ensure(w.S)) ||
           (rv = w.iters.ensure(w.S)) || (rv = w.tol2.ensure(w.S)) || (rv = w.ff.ensure(w.S)) ||
           (rv = w.ffpart.ensure((size_t)kFfChunks * w.S)))
         return rv;
-      if (opt.precision != 0) {
+      if (imp) {
+        // no per-sample matrix: the values are formed inside the PCG kernel
+        w.V64.release();
+        w.V32.release();
+        if ((rv = w.mult.ensure((size_t)P->nmult * w.S))) return rv;
+      } else if ((rv = w.V64.ensure(nv))) {
+        return rv;
+      }
+      if (opt.precision == 1) {
         if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n))) return rv;
       }
       const long ne = (long)m->eLen * w.S;
@@ -1279,15 +1513,30 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
                                                      w.Fraw.p);
       UFEM_CUDA_TRY(cudaMemcpyAsync(w.F.p, w.Fraw.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
       k_fix_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, m->d_fixed.p, w.F.p);
-      dim3 ga((unsigned)m->nnzb, (unsigned)(w.S / 128));
-      float *v32 = opt.precision != 0 ? w.V32.p : nullptr;
-      float *m32 = opt.precision != 0 ? w.M32.p : nullptr;
-      if (B == 3)
-        k_assemble_batch<3><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
-                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
-      else
-        k_assemble_batch<2><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
-                                         P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
+      if (imp) {
+        const long nm = (long)P->nmult * w.S, nd = (long)m->nbr * w.S;
+        k_make_mult<<<(unsigned)((nm + 255) / 256), 256>>>(P->nmult, w.S, w.nsamp, P->ilen, d_ifld[k],
+                                                           P->d_mult_col.p, w.mult.p);
+        if (B == 3)
+          k_diag_implicit<3><<<(unsigned)((nd + 255) / 256), 256>>>(m->nbr, w.S, m->d_diagblk.p, P->cptr.p,
+                                                                    P->cval.p, P->cstride, w.mult.p,
+                                                                    m->d_fixed.p, w.M64.p);
+        else
+          k_diag_implicit<2><<<(unsigned)((nd + 255) / 256), 256>>>(m->nbr, w.S, m->d_diagblk.p, P->cptr.p,
+                                                                    P->cval.p, P->cstride, w.mult.p,
+                                                                    m->d_fixed.p, w.M64.p);
+        g_stats.kernel_launches += 1;  // two kernels here in place of the assembly
+      } else {
+        dim3 ga((unsigned)m->nnzb, (unsigned)(w.S / 128));
+        float *v32 = opt.precision == 1 ? w.V32.p : nullptr;
+        float *m32 = opt.precision == 1 ? w.M32.p : nullptr;
+        if (B == 3)
+          k_assemble_batch<3><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
+                                           P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
+        else
+          k_assemble_batch<2><<<ga, 128>>>(w.S, P->s, m->d_blkrow.p, m->d_colind.p, P->gptr.p, P->gel.p,
+                                           P->gpair.p, P->Khat.p, w.E.p, m->d_fixed.p, w.V64.p, v32, w.M64.p, m32);
+      }
       k_ff_part<<<dim3((unsigned)(w.S / 32), kFfChunks), 256>>>((long)m->nDOFAct, w.S, w.F.p, w.ffpart.p);
       k_tol2<<<(w.S + 127) / 128, 128>>>(kFfChunks, w.S, w.ffpart.p, opt.tol, w.tol2.p, w.ff.p);
       g_stats.kernel_launches += 7;
@@ -1308,8 +1557,9 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   }
   // ---- one persistent launch over every mesh -----------------------------
   long its = 0;
-  if (opt.precision != 0) rv = run_pcg<float>(nmesh, models, W, opt, &its);
-  else rv = run_pcg<double>(nmesh, models, W, opt, &its);
+  if (opt.precision == 1) rv = run_pcg<float, false>(nmesh, models, W, plans, opt, &its);
+  else if (opt.precision == 2) rv = run_pcg<double, true>(nmesh, models, W, plans, opt, &its);
+  else rv = run_pcg<double, false>(nmesh, models, W, plans, opt, &its);
   if (rv != UFEM_AF_OK) return rv;
   g_stats.pcg_iterations = its;
   // ---- outputs -------------------------------------------------------------

@@ -409,6 +409,7 @@ struct ufem_warm {
   ufem_mlp *mlp = nullptr;
   bool trained = false;
   long cold_cap = 0;
+  int train_precision = -1;  // the cap holds for solves at this precision
   double guess_scale = 1.0;
   // basis and normalisation
   DBuf<double> phi;                       // [n][r]
@@ -685,6 +686,7 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
       sum += (double)hi[s];
     }
     w->cold_cap = mx;
+    w->train_precision = opt ? opt->precision : 1;
     st.cold_iters_max = mx;
     st.cold_iters_mean = sum / (double)ntrain;
   }
@@ -785,9 +787,11 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   // guess
   if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S))) return rv;
   cudaEventRecord(e1);
-  // warm-started batched solve, capped at the cold iteration count
+  // warm-started batched solve, capped at the cold iteration count seen in
+  // training at the same precision (other precisions: the caller's cap)
   ufem_mc_options wopt = opt;
-  if (w->cold_cap > 0) wopt.max_iters = std::min(opt.max_iters, w->cold_cap);
+  const bool capped = w->cold_cap > 0 && opt.precision == w->train_precision;
+  if (capped) wopt.max_iters = std::min(opt.max_iters, w->cold_cap);
   {
     const double *pg = w->u0.p;
     double *pu = w->uf.p;
@@ -867,7 +871,7 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   }
   st.guess_err_mean = nsamp ? se / (double)nsamp : 0.0;
   st.iters_mean = nsamp ? si / (double)nsamp : 0.0;
-  st.cold_cap = w->cold_cap;
+  st.cold_cap = capped ? w->cold_cap : opt.max_iters;
   float a = 0, b = 0, c = 0;
   cudaEventElapsedTime(&a, e0, e1);
   cudaEventElapsedTime(&b, e1, e2);
