@@ -80,8 +80,8 @@ struct McPlan {
   bool imp_built = false;
   int nmult = 0, cstride = 0;
   std::vector<int> mult_col;
-  DBuf<int> d_mult_col, cptr;
-  DBuf<double> cval;               // [nc][cstride]: B*B values, then the multiplier index
+  DBuf<int> d_mult_col, cptr, crow;  // contributions of block k / of block row I
+  DBuf<double> cval;               // [nc][cstride]: B*B values, then (multiplier << 32 | J)
   long nc = 0;
 };
 
@@ -306,17 +306,21 @@ static int build_implicit(ufem_model *m, McPlan *P) {
         }
       if (!any) continue;
       for (int t = 0; t < BB; t++) cval.push_back(W[sl * BB + t]);
-      cval.push_back((double)slot_mult[sl]);
+      // the multiplier and the block column in one exactly representable integer
+      cval.push_back((double)(((long long)slot_mult[sl] << 32) | (long long)J));
       for (int t = BB + 1; t < stride; t++) cval.push_back(0.0);
       cptr[k + 1]++;
     }
   }
   for (long k = 0; k < m->nnzb; k++) cptr[k + 1] += cptr[k];
+  std::vector<int> crow(m->nbr + 1);
+  for (int r = 0; r <= m->nbr; r++) crow[r] = cptr[m->rowptr[r]];
   P->nmult = (int)P->mult_col.size();
   P->cstride = stride;
   P->nc = cptr[m->nnzb];
   if (cval.empty()) cval.assign(stride, 0.0);
   if ((rv = P->cptr.upload(cptr.data(), cptr.size())) || (rv = P->cval.upload(cval.data(), cval.size())) ||
+      (rv = P->crow.upload(crow.data(), crow.size())) ||
       (rv = P->d_mult_col.upload(P->mult_col.data(), P->mult_col.size())))
     return rv;
   P->imp_built = true;
@@ -520,7 +524,7 @@ __global__ void k_diag_implicit(int nbr, int S, const int *__restrict__ diagblk,
     double d = 0.0;
     for (int c = cptr[k]; c < cptr[k + 1]; c++) {
       const double *w = cval + (size_t)c * cstride;
-      d += mult[(size_t)(int)w[B * B] * S + s] * w[a * B + a];
+      d += mult[(size_t)((long long)w[B * B] >> 32) * S + s] * w[a * B + a];
     }
     const int row = I * B + a;
     M[(size_t)row * S + s] = fixed[row] ? 1.0 : d;
@@ -531,7 +535,9 @@ __global__ void k_diag_implicit(int nbr, int S, const int *__restrict__ diagblk,
 // ---------------------------------------------------------------------------
 // the persistent masked PCG over all meshes, with residual replacement
 // ---------------------------------------------------------------------------
-enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4 };
+// ST_CAND: the recursive residual is below tol; the sample is frozen until
+// the group's next true-residual pass decides (converged, or resumed)
+enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4, ST_CAND = 5 };
 
 template <typename T>
 struct BMesh {
@@ -556,6 +562,7 @@ struct BMesh {
   // implicit form (precision 2): block k = sum over c in [cptr[k], cptr[k+1])
   // of mult[idx_c][s] * W_c, W_c and idx_c in cval[c*cstride ...]
   const int *cptr;
+  const int *crow;      // contributions of block row I: [crow[I], crow[I+1])
   const double *cval;
   const double *mult;
   const unsigned char *fixed;
@@ -576,51 +583,66 @@ struct BArgs {
   long *iter_out;
 };
 
-// One contribution of the implicit form: its B x B unit block and its
-// multiplier index (read-only for the whole kernel: non-coherent loads).
-template <int B>
-__device__ __forceinline__ int ld_contrib(const double *w, double (&W)[B * B]) {
-  constexpr int CS = (B * B + 2) & ~1;
-  double t[CS];
+// acc[a][v] += mult[var_c][s] * (W_c X_{J_c})[a] over the contributions
+// [c0, c1) of one block row of the implicit form.  The row's contribution
+// keys (multiplier << 32 | J) are fetched 32 at a time, one per lane, and
+// broadcast; the gathers of U contributions are issued together so that U
+// neighbour loads are in flight per warp.  W and the multipliers are
+// read-only for the whole kernel (non-coherent loads); X is written by
+// other blocks during the kernel (L2 loads).
+template <int B, int VN, int U>
+__device__ __forceinline__ void implicit_row(const double *__restrict__ cval, int cstride,
+                                             const double *__restrict__ mult, const double *X, int S, int sb,
+                                             int c0, int c1, double (&acc)[B][VN]) {
+  const int lane = threadIdx.x & 31;
+  for (int cb = c0; cb < c1; cb += 32) {
+    const long long mykey = (cb + lane < c1) ? (long long)__ldg(cval + (size_t)(cb + lane) * cstride + B * B) : 0;
+    const int cnt = min(32, c1 - cb);
+    for (int j = 0; j < cnt; j += U) {
+      double xv[U][B][VN], av[U][VN];
 #pragma unroll
-  for (int h = 0; h < CS / 2; h++) {
-    const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
-    t[2 * h] = v.x;
-    t[2 * h + 1] = v.y;
-  }
+      for (int u = 0; u < U; u++) {
+        const long long key = __shfl_sync(0xffffffffu, mykey, min(j + u, cnt - 1));
+        const int J = (int)(key & 0xffffffffLL), var = (int)(key >> 32);
 #pragma unroll
-  for (int e = 0; e < B * B; e++) W[e] = t[e];
-  return (int)t[B * B];
-}
-
-// acc[a] += mult_s * (W x)[a] over the contributions [c0, c1) of one block
-template <int B, int VN>
-__device__ __forceinline__ void implicit_block(const double *cval, int cstride, const double *mult, int S, int sb,
-                                               int c0, int c1, const double (&xv)[B][VN], double (&acc)[B][VN]) {
-  for (int c = c0; c < c1; c++) {
-    double W[B * B];
-    const int mi = ld_contrib<B>(cval + (size_t)c * cstride, W);
-    double av[VN];
+        for (int b = 0; b < B; b++) ldv_d<VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
 #pragma unroll
-    for (int h = 0; h < VN / 2; h++) {
-      const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)mi * S + sb) + h);
-      av[2 * h] = v.x;
-      av[2 * h + 1] = v.y;
-    }
-#pragma unroll
-    for (int a = 0; a < B; a++)
-#pragma unroll
-      for (int v = 0; v < VN; v++) {
-        double t = 0.0;
-#pragma unroll
-        for (int b = 0; b < B; b++) t = fma(W[a * B + b], xv[b][v], t);
-        acc[a][v] = fma(av[v], t, acc[a][v]);
+        for (int h = 0; h < VN / 2; h++) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)var * S + sb) + h);
+          av[u][2 * h] = v.x;
+          av[u][2 * h + 1] = v.y;
+        }
       }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (j + u >= cnt) break;
+        const double *w = cval + (size_t)(cb + j + u) * cstride;
+        double W[B * B];
+#pragma unroll
+        for (int h = 0; h < (B * B) / 2; h++) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
+          W[2 * h] = v.x;
+          W[2 * h + 1] = v.y;
+        }
+        if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
+#pragma unroll
+        for (int a = 0; a < B; a++)
+#pragma unroll
+          for (int v = 0; v < VN; v++) {
+            double t = 0.0;
+#pragma unroll
+            for (int b = 0; b < B; b++) t = fma(W[a * B + b], xv[u][b][v], t);
+            acc[a][v] = fma(av[u][v], t, acc[a][v]);
+          }
+      }
+    }
   }
 }
 
-// y = A (z + beta p_old) on the block rows of one tile for GS samples;
-// pnew = z + beta p_old on the own rows; partial p.q per sample.
+// q = A p with p = z + beta p_old on the block rows of one tile for GS
+// samples; pnew = p on the own rows; partial p.q per sample.  Explicit form:
+// p is formed at every gathered neighbour.  Implicit form: q = A z + beta
+// q_old (A p_old is the previous q), so only z is gathered.
 template <typename T, int B, bool IMP>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VecOf<T>::N]) {
@@ -643,42 +665,32 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
     for (int a = 0; a < B; a++)
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
-    const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
-    for (int kb = k0; kb < k1; kb += 32) {
-      // the row's column indices, one per lane, then broadcast by shuffle:
-      // the neighbour gathers no longer wait on a dependent index load
-      const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
-      int myC0 = 0, myC1 = 0;
-      if constexpr (IMP) {
-        if (kb + lane < k1) {
-          myC0 = __ldg(M.cptr + kb + lane);
-          myC1 = __ldg(M.cptr + kb + lane + 1);
-        }
-      }
-      const int cnt = min(32, k1 - kb);
-      for (int j = 0; j < cnt; j++) {
-        const int k = kb + j;
-        T vv[IMP ? 1 : B * B][VN];
-        if constexpr (!IMP) {
+    if constexpr (IMP) {
+      implicit_row<B, VN, 4>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+    } else {
+      const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
+      for (int kb = k0; kb < k1; kb += 32) {
+        // the row's column indices, one per lane, then broadcast by shuffle:
+        // the neighbour gathers no longer wait on a dependent index load
+        const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+        const int cnt = min(32, k1 - kb);
+        for (int j = 0; j < cnt; j++) {
+          const int k = kb + j;
+          T vv[B * B][VN];
 #pragma unroll
           for (int e = 0; e < B * B; e++) ldv_stream<T>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
-        }
-        const int J = __shfl_sync(0xffffffffu, myJ, j);
-        T xv[B][VN];
+          const int J = __shfl_sync(0xffffffffu, myJ, j);
+          T xv[B][VN];
 #pragma unroll
-        for (int c = 0; c < B; c++) {
-          ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
-          if (!first) {
-            T pv[VN];
-            ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
+          for (int c = 0; c < B; c++) {
+            ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
+            if (!first) {
+              T pv[VN];
+              ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
 #pragma unroll
-            for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
+              for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
+            }
           }
-        }
-        if constexpr (IMP) {
-          const int c0 = __shfl_sync(0xffffffffu, myC0, j), c1 = __shfl_sync(0xffffffffu, myC1, j);
-          implicit_block<B, VN>(M.cval, M.cstride, M.mult, S, sb, c0, c1, xv, acc);
-        } else {
 #pragma unroll
           for (int a = 0; a < B; a++)
 #pragma unroll
@@ -703,6 +715,12 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
         for (int v = 0; v < VN; v++) pi[v] = zi[v];
       }
       if constexpr (IMP) {
+        if (!first) {
+          T qo[VN];
+          ldv<T>(M.q + o, qo);
+#pragma unroll
+          for (int v = 0; v < VN; v++) acc[a][v] = fma(beta[v], qo[v], acc[a][v]);
+        }
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
 #pragma unroll
           for (int v = 0; v < VN; v++) acc[a][v] = pi[v];
@@ -815,27 +833,19 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
     for (int a = 0; a < B; a++)
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
-    const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
-    for (int kb = k0; kb < k1; kb += 32) {
-      const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
-      int myC0 = 0, myC1 = 0;
-      if constexpr (IMP) {
-        if (kb + lane < k1) {
-          myC0 = __ldg(M.cptr + kb + lane);
-          myC1 = __ldg(M.cptr + kb + lane + 1);
-        }
-      }
-      const int cnt = min(32, k1 - kb);
-      for (int j = 0; j < cnt; j++) {
-        const int k = kb + j;
-        const int J = __shfl_sync(0xffffffffu, myJ, j);
-        double xv[B][VN];
+    if constexpr (IMP) {
+      implicit_row<B, VN, 4>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+    } else {
+      const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
+      for (int kb = k0; kb < k1; kb += 32) {
+        const int myJ = (kb + lane < k1) ? __ldg(M.colind + kb + lane) : 0;
+        const int cnt = min(32, k1 - kb);
+        for (int j = 0; j < cnt; j++) {
+          const int k = kb + j;
+          const int J = __shfl_sync(0xffffffffu, myJ, j);
+          double xv[B][VN];
 #pragma unroll
-        for (int c = 0; c < B; c++) ldv_d<VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
-        if constexpr (IMP) {
-          const int c0 = __shfl_sync(0xffffffffu, myC0, j), c1 = __shfl_sync(0xffffffffu, myC1, j);
-          implicit_block<B, VN>(M.cval, M.cstride, M.mult, S, sb, c0, c1, xv, acc);
-        } else {
+          for (int c = 0; c < B; c++) ldv_d<VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
 #pragma unroll
           for (int a = 0; a < B; a++)
 #pragma unroll
@@ -928,7 +938,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       const BMesh<T> &M = s_m;
       const int g = ti.y;
       const bool is_true = s_flag != 0;
-      int upd = 0, near = 0;
+      int upd = 0, near = 0, wait = 0;
       if (threadIdx.x < GS) {
         const int sl = threadIdx.x, s = g * GS + sl;
         const size_t half = (size_t)M.ngroups * M.ntpg * GS;
@@ -937,21 +947,32 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
         const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
         const double tol2 = M.tol2[s];
         const int st = __ldcg(M.state + s);
+        // FP64 inner iterations: the recursive residual tracks the true one,
+        // so a sample whose recursive residual reaches tol is frozen until
+        // the group's next true-residual pass.  FP32: the recursive residual
+        // drifts, so such a sample keeps iterating and asks for a true
+        // residual every iteration until one confirms convergence.
+        constexpr bool kFreeze = sizeof(T) == 8;
         int nst = st;
-        if (st == ST_ACTIVE) {
+        if (st == ST_ACTIVE || st == ST_CAND) {
           if (!(rr == rr) || isinf(rr)) nst = ST_BREAK;
           else if (is_true && (double)rr <= tol2) nst = ST_CONV;
           else if (k > A.maxit) nst = ST_MAXIT;
+          else if (is_true) nst = ST_ACTIVE;  // a candidate that failed its check resumes
+          else if (kFreeze && rr <= 0.25 * tol2) nst = ST_CAND;
         }
         upd = (nst == ST_ACTIVE);
+        wait = (nst == ST_CAND);
         // replace once the recursive residual has dropped by the factor
-        // near since the last replacement, and to verify convergence
-        near = upd && !is_true && (rr <= A.near2 * __ldcg(M.rrlast + s) || rr <= 0.25 * tol2);
+        // near since the last replacement (FP32: also to verify convergence)
+        near = upd && !is_true &&
+               (rr <= A.near2 * __ldcg(M.rrlast + s) || (!kFreeze && rr <= 0.25 * tol2));
         s_sc[sl] = upd ? (first ? T(0) : (T)(rzn / rzo)) : T(0);
         if (ti.z == 0) {  // the group's first tile records per-sample results
           if (nst != st) {
             M.state[s] = nst;
-            M.iters[s] = (int)(k - 1);
+            // a verified candidate keeps the count of the iterate it froze at
+            if (!(st == ST_CAND && nst == ST_CONV)) M.iters[s] = (int)(k - 1);
           }
           M.rho[(size_t)par * M.S + s] = rzn;
           if (is_true) M.rrlast[s] = rr;
@@ -959,12 +980,19 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       }
       upd = __syncthreads_or(upd);
       near = __syncthreads_or(near);
+      wait = __syncthreads_or(wait);
       if (ti.z == 0 && threadIdx.x == 0) {
-        if (!upd && M.gactive[g]) {
+        if (!upd && !wait && M.gactive[g]) {
           M.gactive[g] = 0;
           atomicSub(A.active_count, 1);
         }
-        M.gneed[g] = upd && (near || (k - M.glast[g] >= A.rr_every));
+        // a true-residual pass.  FP32: on the residual drop and every
+        // rr_every iterations.  FP64 (no drift to correct): only to verify
+        // candidates, once no sample of the group still iterates or rr_every
+        // iterations after the last pass.
+        const bool due = (k - M.glast[g] >= A.rr_every);
+        if (sizeof(T) == 8) M.gneed[g] = wait && (!upd || due);
+        else M.gneed[g] = upd && (near || due);
       }
       if (!upd) {
         __syncthreads();
@@ -1007,13 +1035,13 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       int live = 0;
       if (threadIdx.x < GS) live = (__ldcg(M.state + g * GS + threadIdx.x) == ST_ACTIVE);
       live = __syncthreads_or(live) | upd;
+      // groups due for a true-residual pass are counted whether or not they
+      // update (a group of frozen candidates only waits for that pass)
+      if (ti.z == 0 && threadIdx.x == 0 && __ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
       if (!live) continue;
       const T *pnew = (k & 1) ? M.p1 : M.p0;
       tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
-      if (ti.z == 0 && threadIdx.x == 0) {
-        M.gtrue[g] = 0;
-        if (__ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
-      }
+      if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
     }
     if (!grid_barrier(A.bar)) return;
     // ---- phase R (when a group asked): replace the recursive residual -------
@@ -1312,6 +1340,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     b.x = w.x64.p;
     b.tol2 = w.tol2.p;
     b.cptr = plans[k]->cptr.p;
+    b.crow = plans[k]->crow.p;
     b.cval = plans[k]->cval.p;
     b.mult = w.mult.p;
     b.fixed = m->d_fixed.p;
