@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--plain-samples", type=int, default=16, help="samples timed by the plain method")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
+    p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--precision", type=int, default=2,
                    help="2: FP64 PCG, blocks formed in the kernel (default); 1: FP32 PCG on explicit FP32 "
                         "matrices with FP64 solution and true-residual replacement; 0: FP64 explicit")
@@ -101,7 +102,7 @@ def profile_case(a):
         f = mg.mc_samples(m, mesh_id=2, nsamp=128)
     g = GpuModel(m)
     for _ in range(2):
-        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40)
+        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block)
     print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
                       "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))

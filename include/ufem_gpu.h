@@ -215,6 +215,8 @@ typedef struct ufem_mc_options {
   double replace_near;       /* also replace once the recursive residual has dropped by this factor
                                 since the last replacement, and when it reaches tol */
   int use_graphs;            /* reserved */
+  int tiles_per_block;       /* work tiles per persistent block and phase (0: the autotuned or default choice) */
+  int unroll;                /* precision 2: neighbour gathers issued together, 2, 4 or 8 (0: tuned or 4) */
 } ufem_mc_options;
 void ufem_mc_default_options(ufem_mc_options *o);
 

@@ -33,7 +33,8 @@ class Tables(C.Structure):
 
 class McOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iters", C.c_long),
-                ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int)]
+                ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int),
+                ("tiles_per_block", C.c_int), ("unroll", C.c_int)]
 
 
 class WarmOptions(C.Structure):

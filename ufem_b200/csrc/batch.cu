@@ -551,6 +551,9 @@ struct BMesh {
   T *r, *z, *p0, *p1, *q;
   double *part_pq;      // [ngroups*ntpg*GS] (dot products accumulate in FP64)
   double *part_rr, *part_rz;  // [2][ngroups*ntpg*GS] by iteration parity
+  double *tot_pq;       // [S] group totals of the partials, written by the
+  double *tot_rr, *tot_rz;  // [2][S] last tile of the group to finish
+  int *gcnt;            // [ngroups][2] tiles finished (p.q; r.r and r.z)
   double *rho;          // [2][S]
   double *rrlast;       // [S] true |r|^2 at the last replacement
   const double *tol2;   // [S] (tol |F_s|)^2
@@ -572,6 +575,7 @@ struct BMesh {
 template <typename T>
 struct BArgs {
   const BMesh<T> *meshes;
+  int nmesh;                // at most kMaxMeshes
   const int4 *tiles;  // (mesh, group, chunk, -)
   int ntiles;
   GridBar *bar;
@@ -639,11 +643,39 @@ __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, in
   }
 }
 
+// Called by every tile of group g after it wrote its partials: the last
+// tile of the group to arrive adds the group's partials in tile order (the
+// same order every run) into the per-sample totals, so no other tile has to.
+template <int GS>
+__device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const double *part, double *tot,
+                                            const double *part2, double *tot2) {
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(cnt, 1) == ntpg - 1);
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    if (threadIdx.x < GS) {
+      double t = 0.0, t2 = 0.0;
+      for (int c = 0; c < ntpg; c++) {
+        const size_t o = ((size_t)g * ntpg + c) * GS + threadIdx.x;
+        t += __ldcg(part + o);
+        if (part2) t2 += __ldcg(part2 + o);
+      }
+      tot[(size_t)g * GS + threadIdx.x] = t;
+      if (tot2) tot2[(size_t)g * GS + threadIdx.x] = t2;
+    }
+    if (threadIdx.x == 0) atomicExch(cnt, 0);  // next used after a grid barrier
+  }
+  __syncthreads();
+}
+
 // q = A p with p = z + beta p_old on the block rows of one tile for GS
 // samples; pnew = p on the own rows; partial p.q per sample.  Explicit form:
 // p is formed at every gathered neighbour.  Implicit form: q = A z + beta
 // q_old (A p_old is the previous q), so only z is gathered.
-template <typename T, int B, bool IMP>
+template <typename T, int B, bool IMP, int UN>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VecOf<T>::N]) {
   static_assert(!IMP || sizeof(T) == 8, "the implicit form runs in FP64");
@@ -666,7 +698,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     if constexpr (IMP) {
-      implicit_row<B, VN, 4>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+      implicit_row<B, VN, UN>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -740,7 +772,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
     for (int w = 0; w < kWarps; w++) t += s_red[w][threadIdx.x];
     M.part_pq[((size_t)g * M.ntpg + chunk) * GS + threadIdx.x] = t;
   }
-  __syncthreads();
+  group_close<GS>(M.gcnt + 2 * g, M.ntpg, g, M.part_pq, M.tot_pq, nullptr, nullptr);
 }
 
 // Writes the tile's r.r and r.z partials of parity slot `par`.
@@ -767,7 +799,9 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
     M.part_rr[slot] = a;
     M.part_rz[slot] = b;
   }
-  __syncthreads();
+  const size_t half = (size_t)M.ngroups * M.ntpg * GS;
+  group_close<GS>(M.gcnt + 2 * g + 1, M.ntpg, g, M.part_rr + par * half, M.tot_rr + (size_t)par * M.S,
+                  M.part_rz + par * half, M.tot_rz + (size_t)par * M.S);
 }
 
 // x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z.
@@ -815,7 +849,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
 
 // Residual replacement: r = F - K x in FP64 from the FP64 values, then
 // r (inner precision), z = r / M and the partials of the true residual.
-template <typename T, int B, bool IMP>
+template <typename T, int B, bool IMP, int UN>
 __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
                                                    double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
   constexpr int VN = VecOf<T>::N;
@@ -834,7 +868,7 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
     if constexpr (IMP) {
-      implicit_row<B, VN, 4>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+      implicit_row<B, VN, UN>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -888,33 +922,35 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
-__device__ __forceinline__ double group_total(const double *part, int g, int ntpg, int GS, int sl) {
-  double t = 0;
-  for (int c = 0; c < ntpg; c++) t += __ldcg(part + ((size_t)g * ntpg + c) * GS + sl);
-  return t;
-}
+constexpr int kMaxMeshes = 8;
 
-template <typename T, int B, bool IMP>
-__global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
+#ifndef UFEM_PCG_MIN_BLOCKS
+#define UFEM_PCG_MIN_BLOCKS 2
+#endif
+// UN: contributions whose gathers are issued together (implicit form)
+template <typename T, int B, bool IMP, int UN>
+__global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_batch_pcg(BArgs<T> A) {
   constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   __shared__ double s_red[kWarps][GS];
   __shared__ double s_red2[kWarps][GS];
   __shared__ T s_sc[GS];
-  __shared__ BMesh<T> s_m;
+  __shared__ BMesh<T> s_meshes[kMaxMeshes];
   __shared__ int s_flag;
   const int G = gridDim.x;
+  // the mesh descriptors, once per launch
+  for (int i = threadIdx.x; i < A.nmesh * (int)(sizeof(BMesh<T>) / sizeof(int)); i += blockDim.x)
+    reinterpret_cast<int *>(s_meshes)[i] = reinterpret_cast<const int *>(A.meshes)[i];
+  __syncthreads();
   // phase 0: the true residual of the initial guess (parity slot 0)
   for (int t = blockIdx.x; t < A.ntiles; t += G) {
     const int4 ti = A.tiles[t];
-    if (threadIdx.x == 0) s_m = A.meshes[ti.x];
-    __syncthreads();
-    const BMesh<T> &M = s_m;
+    const BMesh<T> &M = s_meshes[ti.x];
     int any = 0;
     if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
     any = __syncthreads_or(any);
     if (any) {
-      tile_true_residual<T, B, IMP>(M, ti.y, ti.z, 0, s_red, s_red2);
+      tile_true_residual<T, B, IMP, UN>(M, ti.y, ti.z, 0, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) {
         M.gtrue[ti.y] = 1;
         M.glast[ti.y] = 0;
@@ -930,20 +966,16 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
     // ---- phase S: convergence on true residuals, beta, q = A p -------------
     for (int t = blockIdx.x; t < A.ntiles; t += G) {
       const int4 ti = A.tiles[t];
-      if (threadIdx.x == 0) {
-        s_m = A.meshes[ti.x];
-        s_flag = __ldcg(A.meshes[ti.x].gtrue + ti.y);
-      }
+      const BMesh<T> &M = s_meshes[ti.x];
+      if (threadIdx.x == 0) s_flag = __ldcg(M.gtrue + ti.y);
       __syncthreads();
-      const BMesh<T> &M = s_m;
       const int g = ti.y;
       const bool is_true = s_flag != 0;
       int upd = 0, near = 0, wait = 0;
       if (threadIdx.x < GS) {
         const int sl = threadIdx.x, s = g * GS + sl;
-        const size_t half = (size_t)M.ngroups * M.ntpg * GS;
-        const double rr = group_total(M.part_rr + (size_t)parm1 * half, g, M.ntpg, GS, sl);
-        const double rzn = group_total(M.part_rz + (size_t)parm1 * half, g, M.ntpg, GS, sl);
+        const double rr = __ldcg(M.tot_rr + (size_t)parm1 * M.S + s);
+        const double rzn = __ldcg(M.tot_rz + (size_t)parm1 * M.S + s);
         const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
         const double tol2 = M.tol2[s];
         const int st = __ldcg(M.state + s);
@@ -1000,7 +1032,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
       }
       const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B, IMP>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+      tile_spmv<T, B, IMP, UN>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
     // The group counter changes only in phase S: read between the barriers,
@@ -1009,9 +1041,8 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
     // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
     for (int t = blockIdx.x; t < A.ntiles; t += G) {
       const int4 ti = A.tiles[t];
-      if (threadIdx.x == 0) s_m = A.meshes[ti.x];
+      const BMesh<T> &M = s_meshes[ti.x];
       __syncthreads();
-      const BMesh<T> &M = s_m;
       const int g = ti.y;
       int upd = 0;
       if (threadIdx.x < GS) {
@@ -1019,7 +1050,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
         const int st = __ldcg(M.state + s);
         T alpha = 0;
         if (st == ST_ACTIVE) {
-          const double pq = group_total(M.part_pq, g, M.ntpg, GS, sl);
+          const double pq = __ldcg(M.tot_pq + s);
           const double rho = __ldcg(M.rho + (size_t)par * M.S + s);
           if (pq > 0.0 && isfinite(pq)) {
             alpha = (T)(rho / pq);
@@ -1049,17 +1080,14 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(BArgs<T> A) {
     if (nrep > 0) {
       for (int t = blockIdx.x; t < A.ntiles; t += G) {
         const int4 ti = A.tiles[t];
-        if (threadIdx.x == 0) {
-          s_m = A.meshes[ti.x];
-          s_flag = __ldcg(A.meshes[ti.x].gneed + ti.y);
-        }
+        const BMesh<T> &M = s_meshes[ti.x];
+        if (threadIdx.x == 0) s_flag = __ldcg(M.gneed + ti.y);
         __syncthreads();
-        const BMesh<T> &M = s_m;
         if (!s_flag) {
-          __syncthreads();  // thread 0 rewrites s_m / s_flag for the next tile
+          __syncthreads();  // thread 0 rewrites s_flag for the next tile
           continue;
         }
-        tile_true_residual<T, B, IMP>(M, ti.y, ti.z, par, s_red, s_red2);
+        tile_true_residual<T, B, IMP, UN>(M, ti.y, ti.z, par, s_red, s_red2);
         if (ti.z == 0 && threadIdx.x == 0) {
           M.gtrue[ti.y] = 1;
           M.glast[ti.y] = (int)k;
@@ -1238,7 +1266,8 @@ struct McWork {
   // inner vectors, FP32 or FP64
   DBuf<float> fr, fz, fp0, fp1, fq;
   DBuf<double> dr, dz, dp0, dp1, dq, pq, prr, prz, rho, rrlast;
-  DBuf<int> state, iters, gactive, gtrue, gneed, glast;
+  DBuf<int> state, iters, gactive, gtrue, gneed, glast, gcnt;
+  DBuf<double> tpq, trr, trz;  // group totals of the PCG partials
   std::vector<double> h_ff;
 };
 
@@ -1270,6 +1299,8 @@ extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->replace_every = 50;
   o->replace_near = 1e-2;
   o->use_graphs = 0;
+  o->tiles_per_block = 0;
+  o->unroll = 0;
 }
 
 extern "C" int ufem_mc_get_stats(ufem_mc_stats *s) {
@@ -1310,17 +1341,26 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int B = models[0]->b;
-  void (*kern)(BArgs<T>) = (B == 3) ? k_batch_pcg<T, 3, IMP> : k_batch_pcg<T, 2, IMP>;
+  void (*kern)(BArgs<T>) = nullptr;
+  if constexpr (!IMP) {
+    kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 1> : k_batch_pcg<T, 2, IMP, 1>;
+  } else {
+    const int un = opt.unroll > 0 ? opt.unroll : 4;
+    if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2> : k_batch_pcg<T, 2, IMP, 2>;
+    else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4> : k_batch_pcg<T, 2, IMP, 4>;
+    else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8> : k_batch_pcg<T, 2, IMP, 8>;
+  }
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     set_error("batched PCG kernel does not fit on an SM");
     return UFEM_AF_ERR;
   }
   const int G = nsm * occ;
-  // rows per tile: about three tiles per block over the whole batch
+  // rows per tile: about tiles_per_block tiles per block over the whole batch
   long total_rows = 0;
   for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
-  int rpt = (int)std::max<long>(kWarps, (total_rows + 3L * G - 1) / (3L * G));
+  const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : 12;  // measured best on B200 for both forms
+  int rpt = (int)std::max<long>(kWarps, (total_rows + tpb * G - 1) / (tpb * G));
   rpt = (rpt + kWarps - 1) / kWarps * kWarps;
   int active_groups = 0;
   for (int k = 0; k < nmesh; k++) {
@@ -1366,6 +1406,11 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
         (rv = w.rho.ensure(2 * w.S)) || (rv = w.rrlast.ensure(w.S)))
       return rv;
     b.part_pq = w.pq.p; b.part_rr = w.prr.p; b.part_rz = w.prz.p; b.rho = w.rho.p; b.rrlast = w.rrlast.p;
+    if ((rv = w.tpq.ensure(w.S)) || (rv = w.trr.ensure(2 * (size_t)w.S)) || (rv = w.trz.ensure(2 * (size_t)w.S)) ||
+        (rv = w.gcnt.ensure(2 * (size_t)b.ngroups)))
+      return rv;
+    UFEM_CUDA_TRY(cudaMemsetAsync(w.gcnt.p, 0, 2 * b.ngroups * sizeof(int)));
+    b.tot_pq = w.tpq.p; b.tot_rr = w.trr.p; b.tot_rz = w.trz.p; b.gcnt = w.gcnt.p;
     UFEM_CUDA_TRY(cudaMemsetAsync(b.p0, 0, n * sizeof(T)));
     UFEM_CUDA_TRY(cudaMemsetAsync(b.p1, 0, n * sizeof(T)));
     if ((rv = w.gactive.ensure(b.ngroups)) || (rv = w.gtrue.ensure(b.ngroups)) || (rv = w.gneed.ensure(b.ngroups)) ||
@@ -1413,6 +1458,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
   BArgs<T> a;
   a.meshes = d_meshes.p;
+  a.nmesh = nmesh;
   a.tiles = d_tiles.p;
   a.ntiles = (int)tiles.size();
   a.bar = bar.p;
@@ -1493,7 +1539,10 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   else ufem_mc_default_options(&opt);
   std::memset(&g_stats, 0, sizeof(g_stats));
   int rv;
-  if (nmesh < 1) return UFEM_AF_ERR_SIZ;
+  if (nmesh < 1 || nmesh > kMaxMeshes) {
+    set_error("batched Monte Carlo: 1 to 8 meshes per launch");
+    return UFEM_AF_ERR_SIZ;
+  }
   const int B = models[0]->b;
   for (int k = 0; k < nmesh; k++)
     if (models[k]->b != B) {
