@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--plain-samples", type=int, default=16, help="samples timed by the plain method")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
+    p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--precision", type=int, default=2,
                    help="2: FP64 PCG, blocks formed in the kernel (default); 1: FP32 PCG on explicit FP32 "
@@ -346,6 +347,63 @@ def uneven_section(a, rank, dev):
     return out
 
 
+def static_section(a, peak):
+    """Configs 2 and 3 of the single-system path: the 80x20x20 brick
+    cantilever (107,163 DOFs) and the 128x128x64 block (3,244,995 DOFs), each
+    solved to true relative residual 1e-8 by the plain FP64 Jacobi PCG and by
+    the FP32-inner / FP64-refinement PCG, with the error of each against a
+    FP64 solve to 1e-12.  Bytes are algorithmic (SURVEY formula): one FP64
+    PCG iteration reads nb*(72+4) + 4*(nbr+1) + 13*n*8 bytes, one FP32 inner
+    iteration nb*(36+4) + 4*(nbr+1) + 13*n*4, one FP64 residual nb*(72+4) +
+    4*(nbr+1) + 3*n*8."""
+    import ctypes as C
+    import numpy as np
+    from ufem_b200 import api, meshgen as mg
+    from ufem_b200.api import GpuModel
+    out = {}
+    for name, m in (("beam_80x20x20", mg.beam_brick(80, 20, 20, 8.0, 2.0, 2.0)),
+                    ("block_128x128x64", mg.block_brick(128, 128, 64))):
+        t0 = time.perf_counter()
+        g = GpuModel(m)
+        g.fill_K(0)
+        g.add_loads()
+        g.add_disps()
+        setup_s = time.perf_counter() - t0
+        b, nbr, nnzb = g.bsr_shape()
+        n = g.ndof
+        fill_ms = C.c_double(); bc_ms = C.c_double(); sol_ms = C.c_double(); res_ms = C.c_double()
+        L = g.L if hasattr(g, "L") else None
+        from ufem_b200 import _lib
+        L = _lib.load()
+        res = {"ndof": n, "blocks": nnzb, "setup_s": setup_s}
+        g.set_u(np.zeros(n))
+        g.solve(api.SOLVER_CGWJ, api.STOP_RELRES, 1e-12, 0)
+        uref = g.u()
+        for label, solver in (("fp64", api.SOLVER_CGWJ), ("fp32_fp64_refinement", api.SOLVER_CGWJ_MIXED)):
+            g.set_u(np.zeros(n))
+            g.solve(solver, api.STOP_RELRES, 1e-8, 0)  # warm-up
+            best = None
+            for _ in range(2):
+                g.set_u(np.zeros(n))
+                rv, its = g.solve(solver, api.STOP_RELRES, 1e-8, 0)
+                L.ufem_get_phase_ms(g.h, C.byref(fill_ms), C.byref(bc_ms), C.byref(sol_ms), C.byref(res_ms))
+                if best is None or sol_ms.value < best[0]:
+                    best = (sol_ms.value, its, rv)
+            ms, its, rv = best
+            u = g.u()
+            if solver == api.SOLVER_CGWJ:
+                by = its * (nnzb * 76.0 + 4.0 * (nbr + 1) + 13.0 * n * 8)
+            else:
+                by = its * (nnzb * 40.0 + 4.0 * (nbr + 1) + 13.0 * n * 4)
+            res[label] = {"converged": rv == 0, "iterations": its, "ms": ms,
+                          "DOF_iterations_per_s": n * its / (ms / 1000.0),
+                          "achieved_GBs": by / (ms / 1000.0) / 1e9, "frac_of_measured_hbm": by / (ms / 1000.0) / 1e9 / peak,
+                          "u_rel_err_vs_fp64_1e-12": float(np.abs(u - uref).max() / np.abs(uref).max())}
+        out[name] = res
+        del g
+    return out
+
+
 def ours(a):
     import ctypes as C
     import numpy as np
@@ -520,6 +578,7 @@ def ours(a):
         plain_diff = float(np.abs(o_plain - out_warm[:sub.shape[0]]).max() / np.abs(o_plain).max())
         uneven = None if a.no_uneven else uneven_section(a, rank, dev)
         peak, peak_kind = measured_peaks()
+        static = None if a.no_static else static_section(a, peak)
         achieved = pcg_bytes / (pcg_ms / 1000.0) / 1e9 if pcg_ms > 0 else 0.0
         # DRAM traffic per launch: the ncu-measured traffic / algorithmic
         # ratio of this kernel (profiles/, a smaller case of the same kernel)
@@ -578,6 +637,7 @@ def ours(a):
                     "d2h_bytes_per_step": d2h, "matches_device_run": e2e_ok},
             "gpu_launches": launches, "clocks": clk.summary(local),
             "uneven_batch": uneven,
+            "static_configs": static,
             "cpu_baseline": cpu,
         }
         print(json.dumps(result))

@@ -240,3 +240,40 @@ def test_beam_80x20x20_true_residual():
     assert np.linalg.norm(f - K @ u) / np.linalg.norm(f) <= 1e-10
     # cantilever sanity: tip deflection is downward and of the beam-theory size
     assert u.min() < 0
+
+
+def _assembled_csr(g):
+    from scipy.sparse import csr_matrix
+    b, nbr, nnzb = g.bsr_shape()
+    rp, ci = g.bsr_pattern()
+    vals = g.K_values()
+    rows = np.repeat(np.arange(nbr), np.diff(rp))
+    r_idx = (rows[:, None, None] * b + np.arange(b)[None, :, None]) + 0 * np.arange(b)[None, None, :]
+    c_idx = (ci[:, None, None] * b + np.arange(b)[None, None, :]) + 0 * np.arange(b)[None, :, None]
+    return csr_matrix((vals.ravel(), (r_idx.ravel(), c_idx.ravel())), shape=(g.ndof, g.ndof))
+
+
+@pytest.mark.parametrize("shape", [(20, 5, 5), (80, 20, 20)])
+def test_mixed_precision_pcg(shape):
+    """FP32 inner PCG in FP64 iterative refinement (UFEM_SOLVER_CGWJ_MIXED) to
+    true relative residual 1e-8, checked in numpy with the GPU's FP64 K, and
+    against the plain FP64 PCG solution to 1e-10 (displacements within 1e-6
+    relative: the residual-to-solution amplification of the cantilever)."""
+    from ufem_b200 import api, meshgen as mg
+    m = mg.beam_brick(*shape, 8.0, 2.0, 2.0)
+    ref = gpu_model(m)
+    ref.fill_K(0)
+    ref.add_loads()
+    ref.add_disps()
+    ref.solve(api.SOLVER_CGWJ, api.STOP_RELRES, 1e-10, 0)
+    u64 = ref.u()
+    g = gpu_model(m)
+    g.fill_K(0)
+    g.add_loads()
+    g.add_disps()
+    rv, it = g.solve(api.SOLVER_CGWJ_MIXED, api.STOP_RELRES, 1e-8, 0)
+    assert rv == 0 and it > 0
+    K = _assembled_csr(g)
+    f, u = g.F(), g.u()
+    assert np.linalg.norm(f - K @ u) / np.linalg.norm(f) <= 1e-8
+    assert np.abs(u - u64).max() <= 1e-6 * np.abs(u64).max()

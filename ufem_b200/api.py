@@ -14,7 +14,7 @@ import numpy as np
 from . import _lib
 from .meshgen import Model
 
-SOLVER_CGWJ, SOLVER_SSOR, SOLVER_BICG = 0, 1, 2
+SOLVER_CGWJ, SOLVER_SSOR, SOLVER_BICG, SOLVER_CGWJ_MIXED = 0, 1, 2, 3
 STOP_REFERENCE, STOP_RELRES = 0, 1
 EPS_REF = 1e-17 / 10000.0   # FEM_ZERO/10000, fem/fem.h:59, fem/fem_sol.c:1722
 

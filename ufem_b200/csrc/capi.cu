@@ -146,7 +146,10 @@ int ufem_solve(ufem_model *m, int solver, int stop_rule, double eps, long maxIt,
   float ms = 0;
   long it = 0;
   int rv;
-  if (solver == UFEM_SOLVER_BICG) {
+  if (solver == UFEM_SOLVER_CGWJ_MIXED) {
+    int outer = 0;
+    rv = cg_jacobi_mixed(A, m->d_F.p, m->d_u.p, eps, maxIt, 1e-4, 4000, &it, &outer, &ms);
+  } else if (solver == UFEM_SOLVER_BICG) {
     rv = bicgstab_jacobi_fp64(A, m->d_F.p, m->d_u.p, eps, maxIt, stop_rule, &it, &ms);
   } else if (solver == UFEM_SOLVER_SSOR) {
     rv = cg_ssor_fp64(A, m->d_F.p, m->d_u.p, eps, maxIt, stop_rule, &it, &ms);

@@ -45,14 +45,19 @@ struct CgResult {
   double normRes, normX;
 };
 
-struct CgArgs {
+// TV: the type of the matrix values and of every vector (double, or float
+// for the inner solves of the mixed-precision PCG); products and dot
+// products accumulate in double either way.
+template <typename TV>
+struct CgArgsT {
   int nbr;
+  long nnzb;
   const int *rowptr, *colind;
-  const double *val;
-  const double *b;
-  double *x;
-  const double *M;
-  double *r, *z, *p0, *p1, *q;
+  const TV *val;  // [nnzb][B][B]
+  const TV *b;
+  TV *x;
+  const TV *M;
+  TV *r, *z, *p0, *p1, *q;
   double *part;  // [grid][4]: slots 0..2 = r.r, x.x, r.z ; slot 3 = p.q
   GridBar *bar;
   CgResult *res;
@@ -60,13 +65,14 @@ struct CgArgs {
   long maxIt;
   int stop_rule;
 };
+using CgArgs = CgArgsT<double>;
 
 // One block row of y = A (z + beta p) (use_p) or y = A z: the B row sums come
 // back on lanes < B.
-template <int B>
+template <int B, typename TV>
 __device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ rowptr,
-                                                const int *__restrict__ colind, const double *__restrict__ val,
-                                                const double *z, const double *p, double beta, bool use_p,
+                                                const int *__restrict__ colind, const TV *__restrict__ val,
+                                                const TV *z, const TV *p, double beta, bool use_p,
                                                 double *s_acc) {
   constexpr int L = 32 - (32 % B);
   const int lane = threadIdx.x & 31;
@@ -78,12 +84,12 @@ __device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ r
     for (int t = lane; t < nitems; t += L) {
       const int k = k0 + t / B;
       const int J = __ldg(colind + k);
-      const double *v = val + (size_t)k * B * B + a * B;
+      const TV *v = val + (size_t)k * B * B + a * B;
 #pragma unroll
       for (int c = 0; c < B; c++) {
-        double xj = __ldcg(z + (size_t)J * B + c);
-        if (use_p) xj = xj + beta * __ldcg(p + (size_t)J * B + c);
-        acc += __ldg(v + c) * xj;
+        double xj = (double)__ldcg(z + (size_t)J * B + c);
+        if (use_p) xj = xj + beta * (double)__ldcg(p + (size_t)J * B + c);
+        acc += (double)__ldg(v + c) * xj;
       }
     }
   }
@@ -120,8 +126,8 @@ __device__ __forceinline__ double part_total(const double *part, int G, int off)
   return v;
 }
 
-template <int B>
-__global__ void __launch_bounds__(kThreads) k_cg_fp64(CgArgs A) {
+template <typename TV, int B>
+__global__ void __launch_bounds__(kThreads) k_cg(CgArgsT<TV> A) {
   __shared__ double s_acc[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
@@ -133,16 +139,16 @@ __global__ void __launch_bounds__(kThreads) k_cg_fp64(CgArgs A) {
   {
     double rr = 0.0, xx = 0.0, rz = 0.0;
     for (int I = I0; I < I1; I++) {
-      double y = warp_row_spmv<B>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
+      double y = warp_row_spmv<B, TV>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
       if (lane < B) {
         size_t i = (size_t)I * B + lane;
-        double ri = A.b[i] - y;
-        double zi = ri / A.M[i];
+        const TV ri = (TV)((double)A.b[i] - y);
+        const TV zi = (TV)((double)ri / (double)A.M[i]);
         A.r[i] = ri;
         A.z[i] = zi;
-        rr += ri * ri;
-        xx += A.x[i] * A.x[i];
-        rz += ri * zi;
+        rr += (double)ri * (double)ri;
+        xx += (double)A.x[i] * (double)A.x[i];
+        rz += (double)ri * (double)zi;
       }
     }
     double v[3] = {rr, xx, rz};
@@ -156,20 +162,21 @@ __global__ void __launch_bounds__(kThreads) k_cg_fp64(CgArgs A) {
   for (it = 1; it <= A.maxIt; it++) {
     const bool first = (it == 1);
     const double beta = first ? 0.0 : rho / rhoold;  // fem/fem_eqs.c:172
-    const double *pold = (it & 1) ? A.p0 : A.p1;
-    double *pnew = (it & 1) ? A.p1 : A.p0;
+    const TV *pold = (it & 1) ? A.p0 : A.p1;
+    TV *pnew = (it & 1) ? A.p1 : A.p0;
     // phase S: q = A p, p = z + beta p_old (fem/fem_eqs.c:168-186), partial p.q
     {
       double pq = 0.0;
       for (int I = I0; I < I1; I++) {
-        double y = warp_row_spmv<B>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
+        double y = warp_row_spmv<B, TV>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
         if (lane < B) {
           size_t i = (size_t)I * B + lane;
-          double zi = A.z[i];
-          double pi = first ? zi : (zi + (beta * pold[i]));
+          const double zi = (double)A.z[i];
+          const TV pi = (TV)(first ? zi : (zi + (beta * (double)pold[i])));
+          const TV qi = (TV)y;
           pnew[i] = pi;
-          A.q[i] = y;
-          pq += pi * y;
+          A.q[i] = qi;
+          pq += (double)pi * (double)qi;
         }
       }
       double v[1] = {pq};
@@ -188,15 +195,15 @@ __global__ void __launch_bounds__(kThreads) k_cg_fp64(CgArgs A) {
       double rr = 0.0, xx = 0.0, rz = 0.0;
       const size_t i0 = (size_t)I0 * B, i1 = (size_t)I1 * B;
       for (size_t i = i0 + lane; i < i1; i += 32) {
-        double xi = A.x[i] + (alpha * pnew[i]);
-        double ri = A.r[i] - (alpha * A.q[i]);
-        double zi = ri / A.M[i];
+        const TV xi = (TV)((double)A.x[i] + (alpha * (double)pnew[i]));
+        const TV ri = (TV)((double)A.r[i] - (alpha * (double)A.q[i]));
+        const TV zi = (TV)((double)ri / (double)A.M[i]);
         A.x[i] = xi;
         A.r[i] = ri;
         A.z[i] = zi;
-        rr += ri * ri;
-        xx += xi * xi;
-        rz += ri * zi;
+        rr += (double)ri * (double)ri;
+        xx += (double)xi * (double)xi;
+        rz += (double)ri * (double)zi;
       }
       double v[3] = {rr, xx, rz};
       block_partials<3>(v, mypart);
@@ -239,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv(int nbr, const int *__restric
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * kWarps + warp;
   if (I >= nbr) return;
-  double v = warp_row_spmv<B>(I, rowptr, colind, val, x, nullptr, 0.0, false, s_acc[warp]);
+  double v = warp_row_spmv<B, double>(I, rowptr, colind, val, x, nullptr, 0.0, false, s_acc[warp]);
   if (lane < B) y[(size_t)I * B + lane] = v;
 }
 
@@ -383,7 +390,7 @@ int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double ep
   int dev = 0, nsm = 0, occ = 0;
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  void (*kern)(CgArgs) = A.B == 1 ? k_cg_fp64<1> : (A.B == 2 ? k_cg_fp64<2> : k_cg_fp64<3>);
+  void (*kern)(CgArgs) = A.B == 1 ? k_cg<double, 1> : (A.B == 2 ? k_cg<double, 2> : k_cg<double, 3>);
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     set_error("persistent CG kernel does not fit on an SM");
@@ -398,7 +405,7 @@ int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double ep
   UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
   UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
   CgArgs a;
-  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
+  a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
   a.M = M.p; a.r = r.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
   a.bar = bar.p; a.res = res.p; a.eps = eps; a.normA = normA; a.normB = normB;
   a.maxIt = maxIt; a.stop_rule = stop_rule;
@@ -765,6 +772,121 @@ double true_relres(const DevMatrix &A, const double *d_b, const double *d_x) {
 }
 
 // ---------------------------------------------------------------------------
+// Mixed precision: FP32 inner Jacobi PCG inside FP64 iterative refinement.
+// Every outer step forms the true residual r = b - A x with the FP64 matrix,
+// solves A d = r with an FP32 copy of the matrix and FP32 vectors (the same
+// persistent kernel, products and dots accumulated in FP64) to inner_tol
+// relative, and adds d to x in FP64.  Converged when |b - A x| / |b| <= eps,
+// always judged on the FP64 true residual.
+namespace {
+__global__ void k_to_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_add_f32(long n, const float *__restrict__ d, double *__restrict__ x) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += (double)d[i];
+}
+}  // namespace
+
+int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
+                    long inner_cap, long *iters, int *outer_steps, float *ms) {
+  const long n = (long)A.nbr * A.B, nv = A.nnzb * A.B * A.B;
+  int rv;
+  if (iters) *iters = 0;
+  if (outer_steps) *outer_steps = 0;
+  double normA = 0.0;
+  int zero_row = 0;
+  DBuf<double> M;
+  if ((rv = setup_common(A, M, &normA, &zero_row)) != UFEM_AF_OK) return rv;
+  const double normB = host_norm(n, d_b);
+  if (!(normB > 0.0)) {
+    UFEM_CUDA_TRY(cudaMemset(d_x, 0, n * sizeof(double)));
+    return UFEM_AF_OK;
+  }
+  if (zero_row != 0x7fffffff) {
+    set_error("matrix member on the diagonal has zero size");  // fem/fem_eqs.c:134-145
+    return UFEM_AF_ERR_ZER;
+  }
+  DBuf<float> V32, M32, r32, d32, ri, z, p0, p1, q;
+  DBuf<double> r64, part;
+  DBuf<GridBar> bar;
+  DBuf<CgResult> res;
+  if ((rv = V32.alloc(nv)) || (rv = M32.alloc(n)) || (rv = r32.alloc(n)) || (rv = d32.alloc(n)) ||
+      (rv = ri.alloc(n)) || (rv = z.alloc(n)) || (rv = p0.alloc(n)) || (rv = p1.alloc(n)) || (rv = q.alloc(n)) ||
+      (rv = r64.alloc(n)))
+    return rv;
+  const unsigned gv = (unsigned)((nv + 255) / 256), gn = (unsigned)((n + 255) / 256);
+  k_to_f32<<<gv, 256>>>(nv, A.val, V32.p);
+  k_to_f32<<<gn, 256>>>(n, M.p, M32.p);
+  int dev = 0, nsm = 0, occ = 0;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  void (*kern)(CgArgsT<float>) = A.B == 1 ? k_cg<float, 1> : (A.B == 2 ? k_cg<float, 2> : k_cg<float, 3>);
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  if (occ < 1) {
+    set_error("persistent CG kernel does not fit on an SM");
+    return UFEM_AF_ERR;
+  }
+  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  G = std::max(G, 1);
+  if ((rv = part.alloc((size_t)G * 4)) || (rv = bar.alloc(1)) || (rv = res.alloc(1))) return rv;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  long total = 0;
+  int outer = 0, status = UFEM_AF_ERR;
+  for (; outer < 40 && total < maxIt; outer++) {
+    // r = b - A x (FP64)
+    spmv_launch(A, d_x, r64.p);
+    k_sub<<<gn, 256>>>(n, d_b, r64.p, r64.p);
+    const double normR = host_norm(n, r64.p);
+    if (!std::isfinite(normR)) break;
+    if (normR <= eps * normB) {
+      status = UFEM_AF_OK;
+      break;
+    }
+    k_to_f32<<<gn, 256>>>(n, r64.p, r32.p);
+    UFEM_CUDA_TRY(cudaMemsetAsync(d32.p, 0, n * sizeof(float)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(p0.p, 0, n * sizeof(float)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(p1.p, 0, n * sizeof(float)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(bar.p, 0, sizeof(GridBar)));
+    UFEM_CUDA_TRY(cudaMemsetAsync(res.p, 0, sizeof(CgResult)));
+    CgArgsT<float> a;
+    a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = V32.p; a.b = r32.p;
+    a.x = d32.p;
+    a.M = M32.p; a.r = ri.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
+    a.bar = bar.p; a.res = res.p; a.eps = inner_tol; a.normA = normA; a.normB = normR;
+    a.maxIt = std::min(inner_cap, maxIt - total); a.stop_rule = UFEM_STOP_RELRES;
+    void *args[] = {&a};
+    UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
+    GridBar hb;
+    CgResult hr;
+    UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+    UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
+    if (hb.err) {
+      set_error("persistent CG: grid barrier timed out");
+      return UFEM_AF_ERR;
+    }
+    total += hr.iters < 0 ? -hr.iters : hr.iters;
+    // the correction, even from an inner solve that stopped at its cap
+    k_add_f32<<<gn, 256>>>(n, d32.p, d_x);
+  }
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (iters) *iters = total;
+  if (outer_steps) *outer_steps = outer;
+  if (status != UFEM_AF_OK) set_error("unconverged solution");
+  return status;
+}
+
+// ---------------------------------------------------------------------------
 // Jacobi PCG without any allocation (ufem_eqs_cgwj_noalloc)
 //
 // Some callers cannot allocate device memory at solve time: code running
@@ -877,7 +999,7 @@ int cg_jacobi_fp64_noalloc(const DevMatrix &A, const double *d_b, double *d_x, d
     return UFEM_AF_ERR_ZER;
   }
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  void (*kern)(CgArgs) = A.B == 1 ? k_cg_fp64<1> : (A.B == 2 ? k_cg_fp64<2> : k_cg_fp64<3>);
+  void (*kern)(CgArgs) = A.B == 1 ? k_cg<double, 1> : (A.B == 2 ? k_cg<double, 2> : k_cg<double, 3>);
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     set_error("persistent CG kernel does not fit on an SM");

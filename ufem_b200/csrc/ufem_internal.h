@@ -172,5 +172,7 @@ int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, dou
                          int stop_rule, long *iters, float *ms);
 int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
                  int stop_rule, long *iters, float *ms);
+int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
+                    long inner_cap, long *iters, int *outer_steps, float *ms);
 
 }  // namespace ufem
