@@ -247,6 +247,18 @@ int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp
                          long *const *d_iters, const double *const *d_u_guess,
                          double *const *d_u_out, const ufem_mc_options *opt);
 
+/* Autotuner of the batched solve's launch shape (no reference counterpart):
+ * times bounded runs (30 PCG iterations) of every candidate -- work tiles per
+ * persistent block 3..48 and, for precision 2, 2/4/8 neighbour gathers in
+ * flight per warp -- on the given batch (device inputs as for
+ * ufem_mc_solve_device), keeps the fastest for batches of this shape (device,
+ * precision, element family, block rows and padded sample count of every
+ * mesh) in memory and in the text file cache_path (NULL: $UFEM_TUNE_CACHE,
+ * else ~/.cache/ufem_b200_tune.txt), and returns it in *best.  Later solves
+ * whose options leave tiles_per_block / unroll at 0 use the cached choice. */
+int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *d_ifld,
+                     const ufem_mc_options *opt, const char *cache_path, ufem_mc_options *best);
+
 /* Statistics of the last ufem_mc_solve*: kernel milliseconds of the inner
  * PCG, FP64 refinement, assembly and outputs, the number of inner PCG
  * iterations run, the algorithmic bytes moved by the PCG kernels, and the
@@ -259,6 +271,7 @@ typedef struct ufem_mc_stats {
   long kernel_launches;
   long pcg_launches;         /* persistent PCG launches (one per refinement step) */
   double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
+  int tiles_per_block, unroll;  /* the launch shape used */
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 

@@ -261,3 +261,29 @@ def test_implicit_run_twice_identical():
     a = _solve_u(g, f, 2)
     b = _solve_u(g, f, 2)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+
+
+def test_autotune_writes_cache_and_is_used(tmp_path):
+    """The autotuner times every candidate launch shape on the batch, writes
+    its choice to the cache file and later solves that leave the shape at 0
+    use it; the solution agrees across shapes within the batched tolerance."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import autotune, mc_solve
+    m = mg.warm_beam(8, 2, 2, zones=4)
+    f = mg.warm_samples(m, 200)
+    g = GpuModel(m)
+    cache = tmp_path / "tune.txt"
+    best = autotune([g], [f], precision=2, cache_path=str(cache))
+    assert best.tiles_per_block in (3, 6, 12, 24, 48) and best.unroll in (2, 4, 8)
+    line = cache.read_text().split()
+    assert len(line) == 4 and line[0].endswith(f"/p2/b3/{g.bsr_shape()[1]}x256")
+    assert int(line[1]) == best.tiles_per_block and int(line[2]) == best.unroll
+    res, st = mc_solve([g], [f], precision=2)
+    o_t, s_t, _ = res[0]
+    assert st.tiles_per_block == best.tiles_per_block and st.unroll == best.unroll
+    res, _ = mc_solve([g], [f], precision=2, tiles_per_block=3, unroll=2)
+    o_f, s_f, _ = res[0]
+    assert (s_t == 0).all() and (s_f == 0).all()
+    # the tile count changes the grouping of the dot products, not the answer
+    assert np.abs(o_t - o_f).max() <= 1e-6 * np.abs(o_f).max()

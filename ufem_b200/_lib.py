@@ -62,7 +62,8 @@ class McStats(C.Structure):
     _fields_ = [("ms_assemble", C.c_double), ("ms_pcg", C.c_double), ("ms_refine", C.c_double),
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
                 ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long),
-                ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16)]
+                ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16), ("tiles_per_block", C.c_int),
+                ("unroll", C.c_int)]
 
 
 _SIGS = {
@@ -112,6 +113,8 @@ _SIGS = {
                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(McOptions)]),
     "ufem_mc_get_stats": (C.c_int, [C.POINTER(McStats)]),
+    "ufem_mc_autotune": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), _l, C.POINTER(C.c_void_p), C.POINTER(McOptions),
+                                   C.c_char_p, C.POINTER(McOptions)]),
     "ufem_mc_solve_serial": (C.c_int, [C.c_void_p, C.c_long, _d, _d, _i, _l, C.c_double]),
     "ufem_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
     "ufem_mlp_free": (None, [C.c_void_p]),

@@ -38,7 +38,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
+#include <sys/stat.h>
 #include <memory>
 #include <vector>
 
@@ -1273,6 +1277,86 @@ struct McWork {
 
 static ufem_mc_stats g_stats;
 
+// ---------------------------------------------------------------------------
+// autotuned launch shapes: (tiles per block, gather unroll) per batch shape,
+// kept in memory and in a text cache file (one "key tpb unroll ms" per line)
+// ---------------------------------------------------------------------------
+struct TuneEntry {
+  std::string key;
+  int tpb, unroll;
+  double ms;
+};
+static std::vector<TuneEntry> g_tune;
+static bool g_tune_loaded = false;
+
+static std::string tune_cache_path(const char *path) {
+  if (path && *path) return path;
+  const char *e = getenv("UFEM_TUNE_CACHE");
+  if (e && *e) return e;
+  const char *h = getenv("HOME");
+  return std::string(h ? h : "/tmp") + "/.cache/ufem_b200_tune.txt";
+}
+
+static void tune_load(const std::string &path) {
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return;
+  char key[512];
+  int tpb, un;
+  double ms;
+  while (fscanf(f, "%511s %d %d %lf", key, &tpb, &un, &ms) == 4) {
+    bool found = false;
+    for (auto &t : g_tune)
+      if (t.key == key) {
+        t.tpb = tpb; t.unroll = un; t.ms = ms;
+        found = true;
+      }
+    if (!found) g_tune.push_back({key, tpb, un, ms});
+  }
+  fclose(f);
+}
+
+static void tune_save(const std::string &path) {
+  const size_t slash = path.find_last_of('/');
+  if (slash != std::string::npos) {
+    std::string dir = path.substr(0, slash);
+    for (size_t i = 1; i <= dir.size(); i++)  // mkdir -p
+      if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+  }
+  FILE *f = fopen(path.c_str(), "w");
+  if (!f) return;
+  for (auto &t : g_tune) fprintf(f, "%s %d %d %.4f\n", t.key.c_str(), t.tpb, t.unroll, t.ms);
+  fclose(f);
+}
+
+// the batch shape a tuned choice is valid for: device, precision, element
+// family, and per mesh its block rows and padded sample count
+static std::string tune_key(int nmesh, ufem_model *const *models, const long *nsamp, int precision) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  std::string name = prop.name;
+  for (auto &c : name)
+    if (c == ' ') c = '_';
+  std::string k = name + "/sm" + std::to_string(nsm) + "/p" + std::to_string(precision) + "/b" +
+                  std::to_string(models[0]->b);
+  for (int i = 0; i < nmesh; i++)
+    k += "/" + std::to_string(models[i]->nbr) + "x" +
+         std::to_string(std::max<long>(128, (nsamp[i] + 127) / 128 * 128));
+  return k;
+}
+
+static const TuneEntry *tune_find(const std::string &key) {
+  if (!g_tune_loaded) {
+    tune_load(tune_cache_path(nullptr));
+    g_tune_loaded = true;
+  }
+  for (auto &t : g_tune)
+    if (t.key == key) return &t;
+  return nullptr;
+}
+
 // Workspaces are kept per model between calls, so repeated batches reuse
 // their device buffers instead of allocating gigabytes each time.
 static std::vector<std::pair<const ufem_model *, std::unique_ptr<McWork>>> g_work;
@@ -1360,6 +1444,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   long total_rows = 0;
   for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
   const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : 12;  // measured best on B200 for both forms
+  g_stats.tiles_per_block = (int)tpb;
+  g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 4) : 0;
   int rpt = (int)std::max<long>(kWarps, (total_rows + tpb * G - 1) / (tpb * G));
   rpt = (rpt + kWarps - 1) / kWarps * kWarps;
   int active_groups = 0;
@@ -1633,6 +1719,14 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
     UFEM_CUDA_TRY(cudaGetLastError());
     g_stats.ms_assemble = t.stop();
   }
+  // ---- launch shape: the caller's, else the autotuned one for this batch --
+  if (opt.tiles_per_block <= 0 || (opt.precision == 2 && opt.unroll <= 0)) {
+    const TuneEntry *t = tune_find(tune_key(nmesh, models, nsamp, opt.precision));
+    if (t) {
+      if (opt.tiles_per_block <= 0) opt.tiles_per_block = t->tpb;
+      if (opt.unroll <= 0) opt.unroll = t->unroll;
+    }
+  }
   // ---- one persistent launch over every mesh -----------------------------
   long its = 0;
   if (opt.precision == 1) rv = run_pcg<float, false>(nmesh, models, W, plans, opt, &its);
@@ -1695,6 +1789,61 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
 }  // namespace ufem
 
 using namespace ufem;
+
+// Times bounded runs (30 PCG iterations) of every candidate launch shape on
+// the caller's batch and keeps the fastest for batches of this shape.
+extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long *nsamp,
+                                const double *const *d_ifld, const ufem_mc_options *opt_in, const char *cache_path,
+                                ufem_mc_options *best) {
+  if (nmesh < 1 || !models || !nsamp || !d_ifld) return UFEM_AF_ERR_EMP;
+  ufem_mc_options base;
+  if (opt_in) base = *opt_in;
+  else ufem_mc_default_options(&base);
+  const std::string path = tune_cache_path(cache_path);
+  if (!g_tune_loaded) {
+    tune_load(path);
+    g_tune_loaded = true;
+  }
+  const int tpbs[] = {3, 6, 12, 24, 48};
+  std::vector<int> unrolls;
+  if (base.precision == 2) unrolls = {2, 4, 8};
+  else unrolls = {4};
+  double best_ms = 1e300;
+  int best_tpb = 12, best_un = unrolls[0];
+  for (int tpb : tpbs)
+    for (int un : unrolls) {
+      ufem_mc_options o = base;
+      o.tiles_per_block = tpb;
+      o.unroll = un;
+      o.max_iters = 30;
+      double per_it = 0.0;
+      for (int rep = 0; rep < 2; rep++) {  // the first run also builds the workspace
+        int rv = mc_solve_device(nmesh, models, nsamp, d_ifld, nullptr, nullptr, nullptr, nullptr, nullptr, &o);
+        if (rv != UFEM_AF_OK) return rv;
+        per_it = g_stats.ms_pcg / (double)std::max<long>(1, g_stats.pcg_iterations);
+      }
+      if (per_it < best_ms) {
+        best_ms = per_it;
+        best_tpb = tpb;
+        best_un = un;
+      }
+    }
+  const std::string key = tune_key(nmesh, models, nsamp, base.precision);
+  bool found = false;
+  for (auto &t : g_tune)
+    if (t.key == key) {
+      t.tpb = best_tpb; t.unroll = best_un; t.ms = best_ms;
+      found = true;
+    }
+  if (!found) g_tune.push_back({key, best_tpb, best_un, best_ms});
+  tune_save(path);
+  if (best) {
+    *best = base;
+    best->tiles_per_block = best_tpb;
+    best->unroll = best_un;
+  }
+  return UFEM_AF_OK;
+}
 
 extern "C" int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp,
                                     const double *const *d_ifld, double *const *d_ofld, int *const *d_status,

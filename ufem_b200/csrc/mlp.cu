@@ -23,6 +23,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -39,6 +40,10 @@ constexpr int kMaxN = 256;    // UMMA N per CTA (TMEM columns)
 constexpr int kKC = 64;       // K chunk staged per round
 constexpr int kGemmThreads = 128;
 constexpr long kSpinLimit = 1L << 26;
+
+// the stream every launch of this file goes to: 0 for the public calls, the
+// capture stream while a training step is being recorded as a CUDA graph
+static cudaStream_t g_stream = 0;
 
 struct GemmArgs {
   int M, N, K;
@@ -282,6 +287,42 @@ __global__ void k_sum(long n, const float *__restrict__ x, float *__restrict__ o
   if (threadIdx.x == 0) *out = sh[0];
 }
 
+// Adam with the learning rate taken from a per-step schedule and the bias
+// corrections from the device step counter, so that one captured training
+// step can be replayed (CUDA graph) without host arguments.
+__global__ void k_adam_sched(long n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                             float *__restrict__ m2, const float *__restrict__ sched, const long *__restrict__ step,
+                             float b1, float b2, float eps, const unsigned char *__restrict__ frozen) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n || (frozen && frozen[i])) return;
+  const long s = *step;
+  const float lr = sched[s];
+  const float c1 = 1.0f - powf(b1, (float)(s + 1)), c2 = 1.0f - powf(b2, (float)(s + 1));
+  const float gi = g[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+// end of a replayed step: add its loss to the running sum, advance the step
+__global__ void k_step_tail(const float *__restrict__ loss, float *__restrict__ acc, long *__restrict__ step) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    *acc += *loss;
+    *step += 1;
+  }
+}
+
+// minibatch rows of a replayed step: rows perm[b * B + r], b = step mod (steps per epoch)
+__global__ void k_gather_step(long B, int ncol, const long *__restrict__ perm, const long *__restrict__ step,
+                              long steps_per_epoch, const float *__restrict__ src, float *__restrict__ dst) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= B * ncol) return;
+  const long r = t / ncol, b = (*step) % steps_per_epoch;
+  dst[t] = src[perm[b * B + r] * ncol + (t % ncol)];
+}
+
 __global__ void k_adam(long n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
                        float *__restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2,
                        const unsigned char *__restrict__ frozen) {
@@ -319,18 +360,24 @@ struct ufem_mlp {
 
 namespace {
 
-int launch_gemm(const GemmArgs &a) {
-  if (a.N > kMaxN || a.N % 16 != 0) {
-    set_error("tensor-core GEMM: N must be a multiple of 16 up to 256");
-    return UFEM_AF_ERR_SIZ;
-  }
+int gemm_configure() {
   static bool configured = false;
   if (!configured) {
     UFEM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
     configured = true;
   }
+  return UFEM_AF_OK;
+}
+
+int launch_gemm(const GemmArgs &a) {
+  if (a.N > kMaxN || a.N % 16 != 0) {
+    set_error("tensor-core GEMM: N must be a multiple of 16 up to 256");
+    return UFEM_AF_ERR_SIZ;
+  }
+  int rv = gemm_configure();
+  if (rv != UFEM_AF_OK) return rv;
   dim3 grid((unsigned)((a.M + kTileM - 1) / kTileM));
-  k_gemm_tc<<<grid, kGemmThreads, kGemmSmem>>>(a);
+  k_gemm_tc<<<grid, kGemmThreads, kGemmSmem, g_stream>>>(a);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_AF_OK;
 }
@@ -351,9 +398,9 @@ int ensure_batch(ufem_mlp *p, long B) {
 
 int refresh_bf16(ufem_mlp *p) {
   const long n1 = (long)p->H * p->n_inp, n2 = (long)p->H * p->H, n3 = (long)p->n_out * p->H;
-  k_f32_to_bf16<<<(unsigned)((n1 + 255) / 256), 256>>>(n1, p->w.p + p->oW1, p->wb.p);
-  k_f32_to_bf16<<<(unsigned)((n2 + 255) / 256), 256>>>(n2, p->w.p + p->oW2, p->wb.p + n1);
-  k_f32_to_bf16<<<(unsigned)((n3 + 255) / 256), 256>>>(n3, p->w.p + p->oW3, p->wb.p + n1 + n2);
+  k_f32_to_bf16<<<(unsigned)((n1 + 255) / 256), 256, 0, g_stream>>>(n1, p->w.p + p->oW1, p->wb.p);
+  k_f32_to_bf16<<<(unsigned)((n2 + 255) / 256), 256, 0, g_stream>>>(n2, p->w.p + p->oW2, p->wb.p + n1);
+  k_f32_to_bf16<<<(unsigned)((n3 + 255) / 256), 256, 0, g_stream>>>(n3, p->w.p + p->oW3, p->wb.p + n1 + n2);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_AF_OK;
 }
@@ -371,7 +418,7 @@ int forward(ufem_mlp *p, long B, const float *d_x) {
   int rv;
   const int H = p->H;
   const __nv_bfloat16 *W1 = p->wb.p, *W2 = W1 + (long)H * p->n_inp, *W3 = W2 + (long)H * H;
-  k_to_bf16_pad<<<(unsigned)((B * p->n_inp + 255) / 256), 256>>>(B, p->n_in, p->n_inp, d_x, p->X.p);
+  k_to_bf16_pad<<<(unsigned)((B * p->n_inp + 255) / 256), 256, 0, g_stream>>>(B, p->n_in, p->n_inp, d_x, p->X.p);
   // Z1 = X W1^T + b1, H1 = gelu(Z1)
   if ((rv = launch_gemm(gemm((int)B, H, p->n_inp, p->X.p, p->n_inp, 1, W1, p->n_inp, 1, 1, nullptr, H,
                              p->w.p + p->ob1, p->Z1.p, p->H1.p, H, p->err.p))))
@@ -390,15 +437,15 @@ int backward(ufem_mlp *p, long B, const float *d_t) {
   int rv;
   const int H = p->H, O = p->n_out;
   const __nv_bfloat16 *W2 = p->wb.p + (long)H * p->n_inp, *W3 = W2 + (long)H * H;
-  k_loss_grad<<<(unsigned)((B + 127) / 128), 128>>>(B, O, p->Y.p, d_t, p->dY.p, p->dYb.p, p->rowloss.p);
-  k_sum<<<1, 256>>>(B, p->rowloss.p, p->scal.p);
+  k_loss_grad<<<(unsigned)((B + 127) / 128), 128, 0, g_stream>>>(B, O, p->Y.p, d_t, p->dY.p, p->dYb.p, p->rowloss.p);
+  k_sum<<<1, 256, 0, g_stream>>>(B, p->rowloss.p, p->scal.p);
   float *gW1 = p->grad.p + p->oW1, *gb1 = p->grad.p + p->ob1, *gW2 = p->grad.p + p->oW2;
   float *gb2 = p->grad.p + p->ob2, *gW3 = p->grad.p + p->oW3, *gb3 = p->grad.p + p->ob3;
   // dW3 = dY^T H2 (O x H, K = B); db3 = colsum(dY)
   if ((rv = launch_gemm(gemm(O, H, (int)B, p->dYb.p, 1, O, p->H2.p, 1, H, 0, gW3, H, nullptr, nullptr, nullptr, 0,
                              p->err.p))))
     return rv;
-  k_colsum<<<(O + 127) / 128, 128>>>(B, O, p->dY.p, gb3);
+  k_colsum<<<(O + 127) / 128, 128, 0, g_stream>>>(B, O, p->dY.p, gb3);
   // dZ2 = (dY W3) * gelu'(Z2)   (B x H, K = O)
   if ((rv = launch_gemm(gemm((int)B, H, O, p->dYb.p, O, 1, W3, 1, H, 3, p->dZ2.p, H, nullptr, p->Z2.p, p->dZ2b.p,
                              H, p->err.p))))
@@ -407,7 +454,7 @@ int backward(ufem_mlp *p, long B, const float *d_t) {
   if ((rv = launch_gemm(gemm(H, H, (int)B, p->dZ2b.p, 1, H, p->H1.p, 1, H, 0, gW2, H, nullptr, nullptr, nullptr, 0,
                              p->err.p))))
     return rv;
-  k_colsum<<<(H + 127) / 128, 128>>>(B, H, p->dZ2.p, gb2);
+  k_colsum<<<(H + 127) / 128, 128, 0, g_stream>>>(B, H, p->dZ2.p, gb2);
   // dZ1 = (dZ2 W2) * gelu'(Z1)   (B x H, K = H)
   if ((rv = launch_gemm(gemm((int)B, H, H, p->dZ2b.p, H, 1, W2, 1, H, 3, p->dZ1.p, H, nullptr, p->Z1.p, p->dZ1b.p,
                              H, p->err.p))))
@@ -416,7 +463,7 @@ int backward(ufem_mlp *p, long B, const float *d_t) {
   if ((rv = launch_gemm(gemm(H, p->n_inp, (int)B, p->dZ1b.p, 1, H, p->X.p, 1, p->n_inp, 0, gW1, p->n_inp, nullptr,
                              nullptr, nullptr, 0, p->err.p))))
     return rv;
-  k_colsum<<<(H + 127) / 128, 128>>>(B, H, p->dZ1.p, gb1);
+  k_colsum<<<(H + 127) / 128, 128, 0, g_stream>>>(B, H, p->dZ1.p, gb1);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_AF_OK;
 }
@@ -432,6 +479,91 @@ int check_mlp_err(ufem_mlp *p) {
 }
 
 }  // namespace
+
+namespace ufem {
+
+// Trains the network for `epochs` passes over (X [ntrain][n_in], T
+// [ntrain][n_out]) in minibatches of bs rows, reshuffled every epoch (seeded),
+// with the per-step learning rates `sched` (epochs * ntrain / bs values).  One
+// training step -- minibatch gather, forward, backward, Adam, BF16 refresh --
+// is recorded once as a CUDA graph on its own stream and replayed for every
+// step; the host only uploads each epoch's permutation and reads each
+// epoch's summed loss.  loss_first / loss_last: mean squared error of the
+// first and last epoch (per output, as ufem_mlp_train_step reports it).
+int mlp_train_graph(ufem_mlp *p, long ntrain, int bs, const float *d_X, const float *d_T,
+                    const std::vector<float> &sched, int epochs, unsigned long long seed, float *loss_first,
+                    float *loss_last, long *steps) {
+  int rv;
+  const long nb = ntrain / bs;
+  const long total = (long)epochs * nb;
+  if (nb < 1 || (long)sched.size() < total) {
+    set_error("mlp_train_graph: need at least one minibatch and a learning rate per step");
+    return UFEM_AF_ERR_SIZ;
+  }
+  DBuf<long> perm, step;
+  DBuf<float> d_sched, acc, Xb, Tb;
+  if ((rv = ensure_batch(p, bs)) || (rv = perm.alloc(ntrain)) || (rv = step.alloc(1)) ||
+      (rv = d_sched.upload(sched.data(), total)) || (rv = acc.alloc(1)) ||
+      (rv = Xb.alloc((size_t)bs * p->n_in)) || (rv = Tb.alloc((size_t)bs * p->n_out)) || (rv = gemm_configure()))
+    return rv;
+  UFEM_CUDA_TRY(cudaMemset(step.p, 0, sizeof(long)));
+  cudaStream_t st;
+  UFEM_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int fail = UFEM_AF_OK;
+  // ---- record one step ------------------------------------------------------
+  g_stream = st;
+  cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    const long nx = (long)bs * p->n_in, nt = (long)bs * p->n_out;
+    k_gather_step<<<(unsigned)((nx + 255) / 256), 256, 0, st>>>(bs, p->n_in, perm.p, step.p, nb, d_X, Xb.p);
+    k_gather_step<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(bs, p->n_out, perm.p, step.p, nb, d_T, Tb.p);
+    if ((fail = forward(p, bs, Xb.p)) == UFEM_AF_OK && (fail = backward(p, bs, Tb.p)) == UFEM_AF_OK) {
+      k_adam_sched<<<(unsigned)((p->nparam + 255) / 256), 256, 0, st>>>(p->nparam, p->w.p, p->grad.p, p->m1.p,
+                                                                         p->m2.p, d_sched.p, step.p, 0.9f, 0.999f,
+                                                                         1e-8f, p->frozen.p);
+      if ((fail = refresh_bf16(p)) == UFEM_AF_OK) k_step_tail<<<1, 32, 0, st>>>(p->scal.p, acc.p, step.p);
+    }
+    ce = cudaStreamEndCapture(st, &graph);
+  }
+  g_stream = 0;
+  if (fail == UFEM_AF_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+  if (fail != UFEM_AF_OK || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(st);
+    if (fail == UFEM_AF_OK) set_error(std::string("MLP training graph: ") + cudaGetErrorString(ce));
+    return fail != UFEM_AF_OK ? fail : UFEM_AF_ERR;
+  }
+  // ---- replay ----------------------------------------------------------------
+  std::mt19937_64 rng(seed);
+  std::vector<long> idx(ntrain);
+  for (long i = 0; i < ntrain; i++) idx[i] = i;
+  const float norm = 1.0f / ((float)nb * (float)bs * (float)p->n_out);
+  for (int ep = 0; ep < epochs && ce == cudaSuccess; ep++) {
+    std::shuffle(idx.begin(), idx.end(), rng);
+    ce = cudaMemcpyAsync(perm.p, idx.data(), ntrain * sizeof(long), cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(acc.p, 0, sizeof(float), st);
+    for (long b = 0; b < nb && ce == cudaSuccess; b++) ce = cudaGraphLaunch(exec, st);
+    float h = 0.0f;
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h, acc.p, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ep == 0 && loss_first) *loss_first = h * norm;
+    if (loss_last) *loss_last = h * norm;
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  cudaStreamDestroy(st);
+  if (ce != cudaSuccess) {
+    set_error(std::string("MLP training replay: ") + cudaGetErrorString(ce));
+    return UFEM_AF_ERR;
+  }
+  p->step += total;
+  if (steps) *steps = total;
+  return check_mlp_err(p);
+}
+
+}  // namespace ufem
 
 extern "C" {
 
@@ -528,7 +660,7 @@ int ufem_mlp_train_step(ufem_mlp *p, long nbatch, const float *d_x, const float 
   p->step++;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - std::pow(b1, (float)p->step), c2 = 1.0f - std::pow(b2, (float)p->step);
-  k_adam<<<(unsigned)((p->nparam + 255) / 256), 256>>>(p->nparam, p->w.p, p->grad.p, p->m1.p, p->m2.p, lr, b1, b2,
+  k_adam<<<(unsigned)((p->nparam + 255) / 256), 256, 0, g_stream>>>(p->nparam, p->w.p, p->grad.p, p->m1.p, p->m2.p, lr, b1, b2,
                                                        1e-8f, c1, c2, p->frozen.p);
   if ((rv = refresh_bf16(p)) != UFEM_AF_OK) return rv;
   if (loss) {

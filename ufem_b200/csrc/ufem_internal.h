@@ -172,6 +172,10 @@ int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, dou
                          int stop_rule, long *iters, float *ms);
 int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
                  int stop_rule, long *iters, float *ms);
+// MLP training with one step recorded as a CUDA graph (mlp.cu)
+int mlp_train_graph(ufem_mlp *p, long ntrain, int bs, const float *d_X, const float *d_T,
+                    const std::vector<float> &sched, int epochs, unsigned long long seed, float *loss_first,
+                    float *loss_last, long *steps);
 int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
                     long inner_cap, long *iters, int *outer_steps, float *ms);
 

@@ -420,8 +420,7 @@ struct ufem_warm {
   // scratch
   DBuf<double> U, Y, Q, Z, G, V, lam, T, scale, part, raw, sc, c;
   DBuf<int> perm, sweeps;
-  DBuf<float> X, Tt, Xb, Tb, Yo;
-  DBuf<long> bidx;
+  DBuf<float> X, Tt, Yo;
   DBuf<double> ifsub, u0, uf, err;
   DBuf<double> ofsub;
   DBuf<int> stsub;
@@ -706,37 +705,21 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   k_col_stats<<<1, 128>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p);
   k_targets<<<grid1(ntrain * r), 256>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p, w->Tt.p);
   UFEM_CUDA_TRY(cudaGetLastError());
-  // 4. training: shuffled minibatches, cosine learning rate
+  // 4. training: shuffled minibatches, cosine learning rate; every step is
+  // the replay of one recorded CUDA graph
   const int bs = w->o.batch;
   const long nb = ntrain / bs;
-  const int nf = w->o.n_feat;
-  if ((rv = w->Xb.ensure((size_t)bs * nf)) || (rv = w->Tb.ensure((size_t)bs * r)) || (rv = w->bidx.ensure(ntrain)))
-    return rv;
-  std::mt19937_64 rng(w->o.seed ^ 0x7a11ULL);
-  std::vector<long> idx(ntrain);
-  std::iota(idx.begin(), idx.end(), 0L);
   const long total = (long)w->o.epochs * nb;
-  long step = 0;
-  float loss = 0.0f;
-  for (int ep = 0; ep < w->o.epochs; ep++) {
-    std::shuffle(idx.begin(), idx.end(), rng);
-    if ((rv = w->bidx.upload(idx.data(), ntrain))) return rv;
-    double ep_loss = 0.0;
-    for (long b = 0; b < nb; b++, step++) {
-      k_gather_rows<float><<<grid1((long)bs * nf), 256>>>(bs, nf, w->bidx.p + b * bs, w->X.p, w->Xb.p);
-      k_gather_rows<float><<<grid1((long)bs * r), 256>>>(bs, r, w->bidx.p + b * bs, w->Tt.p, w->Tb.p);
-      const double frac = (double)step / (double)std::max<long>(1, total);
-      const float lr = (float)(w->o.lr * (0.02 + 0.98 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
-      if ((rv = ufem_mlp_train_step(w->mlp, bs, w->Xb.p, w->Tb.p, lr, &loss))) return rv;
-      ep_loss += loss;
-    }
-    ep_loss /= (double)nb;
-    if (ep == 0) st.loss_first = (float)ep_loss;
-    st.loss_last = (float)ep_loss;
+  std::vector<float> sched(std::max<long>(1, total));
+  for (long step = 0; step < total; step++) {
+    const double frac = (double)step / (double)std::max<long>(1, total);
+    sched[step] = (float)(w->o.lr * (0.02 + 0.98 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
   }
+  if ((rv = mlp_train_graph(w->mlp, ntrain, bs, w->X.p, w->Tt.p, sched, w->o.epochs, w->o.seed ^ 0x7a11ULL,
+                            &st.loss_first, &st.loss_last, &st.steps)))
+    return rv;
   st.ms_train = ms_since(e0);
   st.epochs = w->o.epochs;
-  st.steps = step;
   w->trained = true;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

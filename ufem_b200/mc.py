@@ -131,3 +131,24 @@ def mc_solve_serial(model: GpuModel, ifld: np.ndarray, tol: float = 1e-8):
     it = np.zeros(n, np.int64)
     _lib.check("ufem_mc_solve_serial", L.ufem_mc_solve_serial(model.h, n, _dp(f), _dp(o), _ip(st), _lp(it), tol))
     return o[:, :olen], st, it
+
+
+def autotune(models: list[GpuModel], iflds, precision: int = 2, tol: float = 1e-8, cache_path: str | None = None):
+    """Pick the batched solve's launch shape for this batch (``ufem_mc_autotune``)
+    and return the tuned options; later solves of batches of the same shape
+    pick it up from the cache by themselves."""
+    import torch
+    L = _lib.load()
+    nm = len(models)
+    d = [f if isinstance(f, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(f, np.float64)).cuda()
+         for f in iflds]
+    ns = np.array([t.shape[0] for t in d], np.int64)
+    opt = default_options()
+    opt.precision = precision
+    opt.tol = tol
+    best = _lib.McOptions()
+    rv = L.ufem_mc_autotune(nm, (C.c_void_p * nm)(*[m.h.value for m in models]), _lp(ns),
+                            (C.c_void_p * nm)(*[t.data_ptr() for t in d]), C.byref(opt),
+                            cache_path.encode() if cache_path else None, C.byref(best))
+    _lib.check("ufem_mc_autotune", rv)
+    return best
