@@ -533,6 +533,31 @@ def ours(a):
             "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
     del d_out2, d_st2, d_it2
 
+    # ---- the POD-Galerkin guess (guess mode 1), same precision -------------
+    galerkin = None
+    if not a.no_other:
+        L.ufem_warm_set_guess_mode(ws.h, 1)
+        wst3 = _lib.WarmStats()
+        args3 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt),
+                 C.byref(wst3))
+        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args3))
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args3))
+        e1.record()
+        torch.cuda.synchronize()
+        ms3 = e0.elapsed_time(e1) / a.steps
+        galerkin = {"method": "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the "
+                              "per-zone reduced operators) as the guess", "value": n / (ms3 / 1000.0),
+                    "unit": "solves/s", "iters_mean": wst3.iters_mean, "iters_max": wst3.iters_max,
+                    "guess_rel_err_mean": wst3.guess_err_mean, "guess_rel_err_max": wst3.guess_err_max,
+                    "fallbacks": wst3.fallbacks, "ms_guess": wst3.ms_guess,
+                    "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
+                    "outputs_max_rel_diff_vs_mlp": float(np.abs(d_out.cpu().numpy() - out_warm).max()
+                                                         / np.abs(out_warm).max())}
+        L.ufem_warm_set_guess_mode(ws.h, 0)
+
     # ---- the warm start at the other precisions (one warm-up, one timed step)
     PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
             1: "FP32 PCG on explicit FP32 matrices, FP64 solution and true-residual replacement",
@@ -625,6 +650,7 @@ def ours(a):
                                      "pod_energy_mode64_over_mode1": (s2[63] / s2[0]) if s2[0] else None}},
             "batched_without_warm_start": cold,
             "warm_start_other_precisions": other,
+            "galerkin_guess": galerkin,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},

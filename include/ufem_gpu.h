@@ -323,6 +323,10 @@ typedef struct ufem_warm_options {
   int epochs, batch;         /* MLP training: passes over the set, minibatch size */
   float lr;                  /* Adam learning rate (cosine decay to 2 %) */
   unsigned long long seed;
+  int guess_mode;            /* 0: the MLP's coefficients; 1: each sample's POD-Galerkin
+                                coefficients (Phi^T K Phi c = Phi^T f, assembled from the
+                                per-variable operators Phi^T K_v Phi; models with at most
+                                64 E variables, else the MLP's) */
 } ufem_warm_options;
 
 typedef struct ufem_warm_train_stats {
@@ -358,6 +362,8 @@ int  ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u
 /* warm-started batched solve; d_ofld nsamp*olen, d_status, d_iters nsamp (device; may be NULL) */
 int  ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
                      const ufem_mc_options *opt, ufem_warm_stats *st);
+/* switches the guess between the MLP (0) and the POD-Galerkin system (1) */
+int  ufem_warm_set_guess_mode(ufem_warm *w, int mode);
 /* multiplies every guess by factor (1 by default): a diagnostic that makes the
  * guesses bad on purpose, to exercise the fallback */
 int  ufem_warm_set_guess_scale(ufem_warm *w, double factor);

@@ -165,3 +165,59 @@ def test_guess_deterministic(warm_small):
     b = ws.guess(ev)
     assert np.array_equal(a, b)
     assert a.shape == (40, g.ndof)
+
+
+def test_galerkin_guess_beats_the_mlp(warm_small):
+    """Guess mode 1 (each sample's POD-Galerkin coefficients from the
+    per-variable reduced operators Phi^T K_v Phi): a far smaller guess error
+    than the MLP's, fewer PCG iterations, the same outputs as a cold solve."""
+    from ufem_b200 import meshgen as mg
+    m, g, ws, train, st = warm_small
+    ev = mg.warm_samples(m, 128, first_sample=1 << 23)
+    of_m, st_m, it_m, ws_m = ws.solve(ev)
+    ws.set_guess_mode(1)
+    try:
+        of_g, st_g, it_g, ws_g = ws.solve(ev)
+    finally:
+        ws.set_guess_mode(0)
+    _, of_cold, it_cold = _cold_solutions(g, ev)
+    assert np.isin(st_g, [ST_CONVERGED, ST_FALLBACK]).all()
+    assert ws_g["guess_err_mean"] < 1e-2 * ws_m["guess_err_mean"]
+    assert it_g.mean() < it_m.mean() < it_cold.mean()
+    assert _rel(of_g, of_cold) < 1e-6
+
+
+def test_galerkin_guess_equals_dense_projection(warm_small):
+    """The reduced system built from the per-variable operators equals the
+    Galerkin projection with the sample's assembled stiffness: the guess is
+    Phi (Phi^T K Phi)^-1 Phi^T f, checked in numpy on the GPU's own K."""
+    import scipy.sparse.linalg as spl
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from test_mc_gpu import model_from_sample
+    m, g, ws, train, st = warm_small
+    ev = mg.warm_samples(m, 3, first_sample=1 << 24)
+    ws.set_guess_mode(1)
+    try:
+        u0 = ws.guess(ev)
+    finally:
+        ws.set_guess_mode(0)
+    phi, _ = ws.basis()
+    for s in range(3):
+        gs = GpuModel(model_from_sample(m, ev[s]))
+        gs.fill_K(0)
+        gs.add_loads()
+        gs.add_disps()
+        b, nbr, nnzb = gs.bsr_shape()
+        rp, ci = gs.bsr_pattern()
+        vals = gs.K_values()
+        from scipy.sparse import csr_matrix
+        rows = np.repeat(np.arange(nbr), np.diff(rp))
+        r_idx = (rows[:, None, None] * b + np.arange(b)[None, :, None]) + 0 * np.arange(b)[None, None, :]
+        c_idx = (ci[:, None, None] * b + np.arange(b)[None, None, :]) + 0 * np.arange(b)[None, :, None]
+        K = csr_matrix((vals.ravel(), (r_idx.ravel(), c_idx.ravel())), shape=(gs.ndof, gs.ndof))
+        live = np.abs(phi).max(axis=0) > 0
+        P = phi[:, live]
+        c = np.linalg.solve(P.T @ (K @ P), P.T @ gs.F())
+        ref = P @ c
+        assert np.abs(u0[s] - ref).max() <= 1e-8 * np.abs(ref).max()

@@ -41,7 +41,7 @@ class WarmOptions(C.Structure):
     _fields_ = [("n_modes", C.c_int), ("n_hidden", C.c_int), ("n_feat", C.c_int), ("feat_cols", C.c_long * 32),
                 ("feat_log", C.c_int * 32), ("scale_col", C.c_long), ("n_snapshots", C.c_long),
                 ("power_iters", C.c_int), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
-                ("seed", C.c_ulonglong)]
+                ("seed", C.c_ulonglong), ("guess_mode", C.c_int)]
 
 
 class WarmTrainStats(C.Structure):
@@ -135,6 +135,7 @@ _SIGS = {
     "ufem_warm_guess": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p]),
     "ufem_warm_solve": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(McOptions), C.POINTER(WarmStats)]),
+    "ufem_warm_set_guess_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "ufem_warm_set_guess_scale": (C.c_int, [C.c_void_p, C.c_double]),
     "ufem_warm_get_basis": (C.c_int, [C.c_void_p, _d, _d]),
     "ufem_dgemm_f64": (C.c_int, [C.c_int, C.c_int, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -364,19 +364,6 @@ __device__ __forceinline__ void ldv<double>(const double *p, double (&o)[2]) {
   double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
   o[0] = v.x; o[1] = v.y;
 }
-// read-only for the whole kernel (matrix values): non-coherent path
-template <typename T>
-__device__ __forceinline__ void ldv_ro(const T *p, T (&o)[VecOf<T>::N]);
-template <>
-__device__ __forceinline__ void ldv_ro<float>(const float *p, float (&o)[4]) {
-  float4 v = __ldg(reinterpret_cast<const float4 *>(p));
-  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-}
-template <>
-__device__ __forceinline__ void ldv_ro<double>(const double *p, double (&o)[2]) {
-  double2 v = __ldg(reinterpret_cast<const double2 *>(p));
-  o[0] = v.x; o[1] = v.y;
-}
 template <typename T>
 __device__ __forceinline__ void stv(T *p, const T (&o)[VecOf<T>::N]);
 template <>
@@ -1616,6 +1603,26 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
 }
 
 }  // namespace
+
+// The implicit form and the load tables of a model's Monte Carlo plan, for
+// the warm start's reduced (Galerkin) operators; builds them when needed.
+int mc_implicit_view(ufem_model *m, McImplicitView *v) {
+  int rv;
+  McPlan *P = get_plan(m);
+  if (!P->built && (rv = build_plan(m, P)) != UFEM_AF_OK) return rv;
+  if (!P->imp_built && (rv = build_implicit(m, P)) != UFEM_AF_OK) return rv;
+  v->B = m->b;
+  v->nbr = m->nbr;
+  v->nmult = P->nmult;
+  v->cstride = P->cstride;
+  v->crow = P->crow.p;
+  v->cval = P->cval.p;
+  v->mult_col = P->mult_col;
+  v->F0 = P->F0.p;
+  v->ovr_row = P->ovr_row;
+  v->ovr_var = P->ovr_var;
+  return UFEM_AF_OK;
+}
 
 int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *d_ifld,
                     double *const *d_ofld, int *const *d_status, long *const *d_iters,

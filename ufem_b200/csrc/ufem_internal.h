@@ -172,6 +172,21 @@ int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, dou
                          int stop_rule, long *iters, float *ms);
 int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt,
                  int stop_rule, long *iters, float *ms);
+// the implicit form of a model's Monte Carlo plan (batch.cu): block row I has
+// the contributions [crow[I], crow[I+1]) of cval ([cstride] each: B*B unit
+// values, then (multiplier << 32 | block column)); multiplier 0 is the
+// constant 1, j >= 1 the ifld column mult_col[j].  F0: loads that no input
+// overrides; row ovr_row[j] adds ifld column ovr_var[j].
+struct McImplicitView {
+  int B = 0, nbr = 0, nmult = 0, cstride = 0;
+  const int *crow = nullptr;
+  const double *cval = nullptr;
+  std::vector<int> mult_col;
+  const double *F0 = nullptr;
+  std::vector<int> ovr_row, ovr_var;
+};
+int mc_implicit_view(ufem_model *m, McImplicitView *v);
+
 // MLP training with one step recorded as a CUDA graph (mlp.cu)
 int mlp_train_graph(ufem_mlp *p, long ntrain, int bs, const float *d_X, const float *d_T,
                     const std::vector<float> &sched, int epochs, unsigned long long seed, float *loss_first,

@@ -342,6 +342,11 @@ __global__ void k_div_scale(long nsamp, int r, const double *__restrict__ sc, do
   c[e] = d != 0.0 ? c[e] / d : 0.0;
 }
 
+__global__ void k_mul(long n, double f, double *__restrict__ c) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) c[e] *= f;
+}
+
 // FP32 targets t = (c - mean) / sd
 __global__ void k_targets(long nsamp, int r, const double *__restrict__ c, const double *__restrict__ mean,
                           const double *__restrict__ sd, float *__restrict__ t) {
@@ -393,6 +398,115 @@ __global__ void k_to_sample_major(long n, int S, long nsamp, const double *__res
   dst[s * n + i] = src[i * S + s];
 }
 
+// Y [n][r] = K_v Phi: the part of the implicit stiffness that multiplier v
+// scales (supported rows and columns are zero in the unit blocks; Phi is zero
+// on supported DOFs, so the identity rows add nothing to Phi^T K Phi).
+// thread per (block row I, column k)
+template <int B>
+__global__ void k_zone_apply(int nbr, int r, const int *__restrict__ crow, const double *__restrict__ cval,
+                             int cstride, int v, const double *__restrict__ Phi, double *__restrict__ Y) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)nbr * r) return;
+  const int I = (int)(t / r), k = (int)(t % r);
+  double y[B];
+#pragma unroll
+  for (int a = 0; a < B; a++) y[a] = 0.0;
+  for (int c = crow[I]; c < crow[I + 1]; c++) {
+    const double *w = cval + (size_t)c * cstride;
+    const long long key = (long long)w[B * B];
+    if ((int)(key >> 32) != v) continue;
+    const int J = (int)(key & 0xffffffffLL);
+#pragma unroll
+    for (int a = 0; a < B; a++)
+#pragma unroll
+      for (int b = 0; b < B; b++) y[a] += w[a * B + b] * Phi[(size_t)(J * B + b) * r + k];
+  }
+#pragma unroll
+  for (int a = 0; a < B; a++) Y[(size_t)(I * B + a) * r + k] = y[a];
+}
+
+// Prow[j][k] = Phi[row_j][k]: the basis rows of the randomised loads
+__global__ void k_phi_rows(int nrow, int r, const int *__restrict__ rows, const double *__restrict__ Phi,
+                           double *__restrict__ Prow) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrow * r) return;
+  Prow[t] = Phi[(size_t)rows[t / r] * r + (t % r)];
+}
+
+// The POD-Galerkin coefficients of one sample per block: A = sum_v a_v G_v
+// (a_0 = 1, a_v = the sample's E of variable v), b = Phi^T F0 + sum_j
+// f_j Phi[row_j], A c = b by Cholesky in shared memory.  Directions with a
+// pivot below 1e-13 of the largest diagonal (zero basis columns) get c = 0.
+constexpr int kMaxR = 80;
+__global__ void __launch_bounds__(128) k_reduced_solve(long nsamp, int r, int nmult, long ilen,
+                                                       const double *__restrict__ ifld, const int *__restrict__ mcol,
+                                                       const double *__restrict__ G, const double *__restrict__ PF0,
+                                                       int novr, const int *__restrict__ ovar,
+                                                       const double *__restrict__ Prow, double *__restrict__ c_out) {
+  extern __shared__ double s_A[];  // r x (r + 1)
+  const int ld = r + 1;
+  __shared__ double bb[kMaxR];
+  __shared__ double av[64];
+  __shared__ int skip[kMaxR];
+  __shared__ double s_dmax;
+  const long s = blockIdx.x;
+  const int tid = threadIdx.x;
+  const double *row = ifld + s * ilen;
+  for (int v = tid; v < nmult; v += blockDim.x) av[v] = (v == 0) ? 1.0 : row[mcol[v]];
+  __syncthreads();
+  for (int e = tid; e < r * r; e += blockDim.x) {
+    double t = 0.0;
+    for (int v = 0; v < nmult; v++) t += av[v] * G[(size_t)v * r * r + e];
+    s_A[(e / r) * ld + (e % r)] = t;
+  }
+  for (int i = tid; i < r; i += blockDim.x) {
+    double t = PF0[i];
+    for (int j = 0; j < novr; j++) t += row[ovar[j]] * Prow[(size_t)j * r + i];
+    bb[i] = t;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double m = 0.0;
+    for (int i = 0; i < r; i++) m = fmax(m, fabs(s_A[(i) * ld + (i)]));
+    s_dmax = m;
+  }
+  __syncthreads();
+  // right-looking Cholesky, L in the lower triangle
+  for (int j = 0; j < r; j++) {
+    if (tid == 0) {
+      const double d = s_A[(j) * ld + (j)];
+      skip[j] = !(d > 1e-13 * s_dmax);
+      s_A[(j) * ld + (j)] = skip[j] ? 1.0 : sqrt(d);
+    }
+    __syncthreads();
+    for (int i = j + 1 + tid; i < r; i += blockDim.x) s_A[(i) * ld + (j)] = skip[j] ? 0.0 : s_A[(i) * ld + (j)] / s_A[(j) * ld + (j)];
+    __syncthreads();
+    const int m = r - j - 1;
+    for (int e = tid; e < m * m; e += blockDim.x) {
+      const int i = j + 1 + e / m, k = j + 1 + e % m;
+      if (k <= i) s_A[(i) * ld + (k)] -= s_A[(i) * ld + (j)] * s_A[(k) * ld + (j)];
+    }
+    __syncthreads();
+  }
+  // L y = b, L^T c = y (one thread: r <= 80)
+  if (tid == 0) {
+    for (int i = 0; i < r; i++) {
+      double t = skip[i] ? 0.0 : bb[i];
+      if (!skip[i])
+        for (int k = 0; k < i; k++) t -= s_A[(i) * ld + (k)] * bb[k];
+      bb[i] = skip[i] ? 0.0 : t / s_A[(i) * ld + (i)];
+    }
+    for (int i = r - 1; i >= 0; i--) {
+      double t = bb[i];
+      if (!skip[i])
+        for (int k = i + 1; k < r; k++) t -= s_A[(k) * ld + (i)] * bb[k];
+      bb[i] = skip[i] ? 0.0 : t / s_A[(i) * ld + (i)];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < r; i += blockDim.x) c_out[s * r + i] = bb[i];
+}
+
 int grid1(long n, int b = 256) { return (int)((n + b - 1) / b); }
 
 }  // namespace
@@ -410,6 +524,12 @@ struct ufem_warm {
   bool trained = false;
   long cold_cap = 0;
   int train_precision = -1;  // the cap holds for solves at this precision
+  // POD-Galerkin operators (when the model has at most 64 E variables)
+  bool galerkin = false;
+  int nmult = 0;
+  DBuf<double> Gv, PF0, Prow;
+  DBuf<int> d_mcol, d_ovar;
+  int novr = 0;
   double guess_scale = 1.0;
   // basis and normalisation
   DBuf<double> phi;                       // [n][r]
@@ -529,6 +649,45 @@ int fit_basis(ufem_warm *w, int S, long nsnap) {
   return UFEM_AF_OK;
 }
 
+// The POD-Galerkin operators of the model's affine stiffness K = sum_v a_v K_v:
+// G_v = Phi^T K_v Phi for every multiplier v, Phi^T F0 and the basis rows of
+// the randomised loads.  Only for models with at most 64 E variables (the
+// per-sample reduced system then costs nmult r^2 to assemble).
+int build_galerkin(ufem_warm *w) {
+  int rv;
+  McImplicitView v;
+  if ((rv = mc_implicit_view(w->m, &v))) return rv;
+  w->galerkin = false;
+  if (v.nmult > 64) return UFEM_AF_OK;
+  const int r = w->r;
+  const long n = w->n;
+  DBuf<double> Y;
+  if ((rv = Y.ensure((size_t)n * r)) || (rv = w->Gv.ensure((size_t)v.nmult * r * r)) || (rv = w->PF0.ensure(r)))
+    return rv;
+  for (int m = 0; m < v.nmult; m++) {
+    if (v.B == 3)
+      k_zone_apply<3><<<grid1((long)v.nbr * r), 256>>>(v.nbr, r, v.crow, v.cval, v.cstride, m, w->phi.p, Y.p);
+    else
+      k_zone_apply<2><<<grid1((long)v.nbr * r), 256>>>(v.nbr, r, v.crow, v.cval, v.cstride, m, w->phi.p, Y.p);
+    if ((rv = gemm_f64(r, r, n, w->phi.p, 1, r, Y.p, r, 1, w->Gv.p + (size_t)m * r * r, r, 1, w->part))) return rv;
+  }
+  if ((rv = gemm_f64(r, 1, n, w->phi.p, 1, r, v.F0, 1, 1, w->PF0.p, 1, 1, w->part))) return rv;
+  w->novr = (int)v.ovr_row.size();
+  if (w->novr > 0) {
+    DBuf<int> rows;
+    if ((rv = rows.upload(v.ovr_row.data(), w->novr)) || (rv = w->d_ovar.upload(v.ovr_var.data(), w->novr)) ||
+        (rv = w->Prow.ensure((size_t)w->novr * r)))
+      return rv;
+    k_phi_rows<<<grid1((long)w->novr * r), 256>>>(w->novr, r, rows.p, w->phi.p, w->Prow.p);
+    UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  }
+  if ((rv = w->d_mcol.upload(v.mult_col.data(), v.mult_col.size()))) return rv;
+  w->nmult = v.nmult;
+  w->galerkin = true;
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
 // standardised network inputs of nsamp samples into w->X (FP32 [nsamp][n_feat]);
 // with fit = true the feature statistics are (re)computed from these samples
 int make_inputs(ufem_warm *w, long nsamp, const double *d_ifld, bool fit) {
@@ -547,15 +706,28 @@ int make_inputs(ufem_warm *w, long nsamp, const double *d_ifld, bool fit) {
 
 int padded_S(long nsamp) { return (int)std::max<long>(128, (nsamp + 127) / 128 * 128); }
 
-// u0 [n][S] = Phi c^T for the nsamp samples whose inputs are in w->X / w->sc
-int make_guess(ufem_warm *w, long nsamp, int S) {
+// u0 [n][S] = Phi c^T for nsamp samples: c from the MLP (inputs in w->X /
+// w->sc), or from the POD-Galerkin system of each sample (guess mode 1)
+int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
   int rv;
   const int r = w->r;
   if ((rv = w->Yo.ensure((size_t)nsamp * r)) || (rv = w->c.ensure((size_t)nsamp * r)) ||
       (rv = w->u0.ensure((size_t)w->n * S)))
     return rv;
-  if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) return rv;
-  k_coeffs<<<grid1(nsamp * r), 256>>>(nsamp, r, w->Yo.p, w->cmean.p, w->csd.p, w->sc.p, w->guess_scale, w->c.p);
+  if (w->o.guess_mode == 1 && w->galerkin) {
+    const size_t smem = (size_t)r * (r + 1) * sizeof(double);
+    static size_t configured = 0;
+    if (configured < smem) {
+      UFEM_CUDA_TRY(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured = smem;
+    }
+    k_reduced_solve<<<(unsigned)nsamp, 128, smem>>>(nsamp, r, w->nmult, w->m->mc_ilen, d_ifld, w->d_mcol.p, w->Gv.p,
+                                                     w->PF0.p, w->novr, w->d_ovar.p, w->Prow.p, w->c.p);
+    if (w->guess_scale != 1.0) k_mul<<<grid1(nsamp * r), 256>>>(nsamp * r, w->guess_scale, w->c.p);
+  } else {
+    if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) return rv;
+    k_coeffs<<<grid1(nsamp * r), 256>>>(nsamp, r, w->Yo.p, w->cmean.p, w->csd.p, w->sc.p, w->guess_scale, w->c.p);
+  }
   if (S > nsamp) UFEM_CUDA_TRY(cudaMemsetAsync(w->u0.p, 0, (size_t)w->n * S * sizeof(double)));
   // u0(i, s) = sum_k Phi[i][k] c[s][k]
   return gemm_f64((int)w->n, (int)nsamp, r, w->phi.p, r, 1, w->c.p, 1, r, w->u0.p, S, 1, w->part);
@@ -578,6 +750,7 @@ void ufem_warm_default_options(ufem_warm_options *o) {
   o->batch = 256;
   o->lr = 2e-3f;
   o->seed = 20261203ULL;
+  o->guess_mode = 0;
 }
 
 int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out) {
@@ -692,7 +865,7 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   st.ms_solve = ms_since(e0);
   // 2. POD basis from the first n_snapshots solutions
   cudaEventRecord(e0);
-  if ((rv = fit_basis(w, (int)ntrain, w->o.n_snapshots))) return rv;
+  if ((rv = fit_basis(w, (int)ntrain, w->o.n_snapshots)) || (rv = build_galerkin(w))) return rv;
   st.ms_basis = ms_since(e0);
   for (int k = 0; k < r && k < 80; k++) st.sigma2[k] = w->sigma2[k];
   // 3. inputs and targets
@@ -735,7 +908,7 @@ int ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u0
   }
   int rv;
   const int S = padded_S(nsamp);
-  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S))) return rv;
+  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S, d_ifld))) return rv;
   k_to_sample_major<<<grid1(w->n * nsamp), 256>>>(w->n, S, nsamp, w->u0.p, d_u0);
   UFEM_CUDA_TRY(cudaGetLastError());
   UFEM_CUDA_TRY(cudaDeviceSynchronize());
@@ -768,7 +941,7 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   long *pit = d_iters ? d_iters : w->it.p;
   cudaEventRecord(e0);
   // guess
-  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S))) return rv;
+  if ((rv = make_inputs(w, nsamp, d_ifld, false)) || (rv = make_guess(w, nsamp, S, d_ifld))) return rv;
   cudaEventRecord(e1);
   // warm-started batched solve, capped at the cold iteration count seen in
   // training at the same precision (other precisions: the caller's cap)
@@ -865,6 +1038,16 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   st.ms_total = (double)a + b + c;
   cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   if (ws) *ws = st;
+  return UFEM_AF_OK;
+}
+
+int ufem_warm_set_guess_mode(ufem_warm *w, int mode) {
+  if (!w) return UFEM_AF_ERR_EMP;
+  if (mode != 0 && mode != 1) {
+    set_error("ufem_warm_set_guess_mode: 0 (MLP) or 1 (POD-Galerkin)");
+    return UFEM_AF_ERR_VAL;
+  }
+  w->o.guess_mode = mode;
   return UFEM_AF_OK;
 }
 

@@ -88,6 +88,10 @@ class WarmStart:
         _lib.check("ufem_warm_guess", self.L.ufem_warm_guess(self.h, d.shape[0], d.data_ptr(), out.data_ptr()))
         return out.cpu().numpy()
 
+    def set_guess_mode(self, mode: int) -> None:
+        """0: the MLP's coefficients; 1: each sample's POD-Galerkin coefficients."""
+        _lib.check("ufem_warm_set_guess_mode", self.L.ufem_warm_set_guess_mode(self.h, int(mode)))
+
     def set_guess_scale(self, factor: float) -> None:
         _lib.check("ufem_warm_set_guess_scale", self.L.ufem_warm_set_guess_scale(self.h, float(factor)))
 
