@@ -219,7 +219,9 @@ typedef struct ufem_mc_options {
                                 since the last replacement, and when it reaches tol */
   int use_graphs;            /* reserved */
   int tiles_per_block;       /* work tiles per persistent block and phase (0: the autotuned or default choice) */
-  int unroll;                /* precision 2: neighbour gathers issued together, 2, 4 or 8 (0: tuned or 4) */
+  int unroll;                /* precision 2: neighbour gathers issued together, 2, 4 or 8 (0: tuned or 2) */
+  int lane_samples;          /* precision 2: samples per lane, 2 or 4 (a sample group is 32x that;
+                                0: tuned or 4) */
 } ufem_mc_options;
 void ufem_mc_default_options(ufem_mc_options *o);
 
@@ -250,12 +252,13 @@ int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp
 /* Autotuner of the batched solve's launch shape (no reference counterpart):
  * times bounded runs (30 PCG iterations) of every candidate -- work tiles per
  * persistent block 3..48 and, for precision 2, 2/4/8 neighbour gathers in
- * flight per warp -- on the given batch (device inputs as for
+ * flight per warp and 2/4 samples per lane -- on the given batch (device inputs as for
  * ufem_mc_solve_device), keeps the fastest for batches of this shape (device,
  * precision, element family, block rows and padded sample count of every
  * mesh) in memory and in the text file cache_path (NULL: $UFEM_TUNE_CACHE,
  * else ~/.cache/ufem_b200_tune.txt), and returns it in *best.  Later solves
- * whose options leave tiles_per_block / unroll at 0 use the cached choice. */
+ * whose options leave tiles_per_block / unroll / lane_samples at 0 use the
+ * cached choice. */
 int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long *nsamp, const double *const *d_ifld,
                      const ufem_mc_options *opt, const char *cache_path, ufem_mc_options *best);
 
@@ -271,7 +274,7 @@ typedef struct ufem_mc_stats {
   long kernel_launches;
   long pcg_launches;         /* persistent PCG launches (one per refinement step) */
   double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
-  int tiles_per_block, unroll;  /* the launch shape used */
+  int tiles_per_block, unroll, lane_samples;  /* the launch shape used */
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 

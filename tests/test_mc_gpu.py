@@ -277,11 +277,13 @@ def test_autotune_writes_cache_and_is_used(tmp_path):
     best = autotune([g], [f], precision=2, cache_path=str(cache))
     assert best.tiles_per_block in (3, 6, 12, 24, 48) and best.unroll in (2, 4, 8)
     line = cache.read_text().split()
-    assert len(line) == 4 and line[0].endswith(f"/p2/b3/{g.bsr_shape()[1]}x256")
+    assert len(line) == 5 and line[0].endswith(f"/p2/b3/{g.bsr_shape()[1]}x256")
     assert int(line[1]) == best.tiles_per_block and int(line[2]) == best.unroll
+    assert int(line[3]) == best.lane_samples in (2, 4)
     res, st = mc_solve([g], [f], precision=2)
     o_t, s_t, _ = res[0]
     assert st.tiles_per_block == best.tiles_per_block and st.unroll == best.unroll
+    assert st.lane_samples == best.lane_samples
     res, _ = mc_solve([g], [f], precision=2, tiles_per_block=3, unroll=2)
     o_f, s_f, _ = res[0]
     assert (s_t == 0).all() and (s_f == 0).all()

@@ -34,7 +34,7 @@ class Tables(C.Structure):
 class McOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iters", C.c_long),
                 ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int),
-                ("tiles_per_block", C.c_int), ("unroll", C.c_int)]
+                ("tiles_per_block", C.c_int), ("unroll", C.c_int), ("lane_samples", C.c_int)]
 
 
 class WarmOptions(C.Structure):
@@ -63,7 +63,7 @@ class McStats(C.Structure):
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
                 ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long),
                 ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16), ("tiles_per_block", C.c_int),
-                ("unroll", C.c_int)]
+                ("unroll", C.c_int), ("lane_samples", C.c_int)]
 
 
 _SIGS = {

@@ -352,42 +352,60 @@ struct VecOf<double> {
   using V = double2;
 };
 
-template <typename T>
-__device__ __forceinline__ void ldv(const T *p, T (&o)[VecOf<T>::N]);
-template <>
-__device__ __forceinline__ void ldv<float>(const float *p, float (&o)[4]) {
-  float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
-  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+// VN values of type T at a 16-byte aligned address (double: VN = 2 or 4,
+// float: VN = 4), read through L2 (other blocks write them during the kernel)
+template <typename T, int VN>
+__device__ __forceinline__ void ldn(const T *p, T (&o)[VN]) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < VN / 2; h++) {
+      const double2 v = __ldcg(reinterpret_cast<const double2 *>(p) + h);
+      o[2 * h] = v.x;
+      o[2 * h + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < VN / 4; h++) {
+      const float4 v = __ldcg(reinterpret_cast<const float4 *>(p) + h);
+      o[4 * h] = v.x;
+      o[4 * h + 1] = v.y;
+      o[4 * h + 2] = v.z;
+      o[4 * h + 3] = v.w;
+    }
+  }
 }
-template <>
-__device__ __forceinline__ void ldv<double>(const double *p, double (&o)[2]) {
-  double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
-  o[0] = v.x; o[1] = v.y;
+template <typename T, int VN>
+__device__ __forceinline__ void stn(T *p, const T (&o)[VN]) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < VN / 2; h++) reinterpret_cast<double2 *>(p)[h] = make_double2(o[2 * h], o[2 * h + 1]);
+  } else {
+#pragma unroll
+    for (int h = 0; h < VN / 4; h++)
+      reinterpret_cast<float4 *>(p)[h] = make_float4(o[4 * h], o[4 * h + 1], o[4 * h + 2], o[4 * h + 3]);
+  }
 }
-template <typename T>
-__device__ __forceinline__ void stv(T *p, const T (&o)[VecOf<T>::N]);
-template <>
-__device__ __forceinline__ void stv<float>(float *p, const float (&o)[4]) {
-  *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
-}
-template <>
-__device__ __forceinline__ void stv<double>(double *p, const double (&o)[2]) {
-  *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
-}
-
 // streaming (evict-first) loads for data read once per iteration: the
 // matrix values, so that L2 keeps the gathered vectors instead
-template <typename T>
-__device__ __forceinline__ void ldv_stream(const T *p, T (&o)[VecOf<T>::N]);
-template <>
-__device__ __forceinline__ void ldv_stream<float>(const float *p, float (&o)[4]) {
-  float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
-  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-}
-template <>
-__device__ __forceinline__ void ldv_stream<double>(const double *p, double (&o)[2]) {
-  double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
-  o[0] = v.x; o[1] = v.y;
+template <typename T, int VN>
+__device__ __forceinline__ void ldn_stream(const T *p, T (&o)[VN]) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < VN / 2; h++) {
+      const double2 v = __ldcs(reinterpret_cast<const double2 *>(p) + h);
+      o[2 * h] = v.x;
+      o[2 * h + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < VN / 4; h++) {
+      const float4 v = __ldcs(reinterpret_cast<const float4 *>(p) + h);
+      o[4 * h] = v.x;
+      o[4 * h + 1] = v.y;
+      o[4 * h + 2] = v.z;
+      o[4 * h + 3] = v.w;
+    }
+  }
 }
 // VN doubles (VN = 2 or 4) at a 16-byte aligned address
 template <int VN>
@@ -666,11 +684,10 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 // samples; pnew = p on the own rows; partial p.q per sample.  Explicit form:
 // p is formed at every gathered neighbour.  Implicit form: q = A z + beta
 // q_old (A p_old is the previous q), so only z is gathered.
-template <typename T, int B, bool IMP, int UN>
+template <typename T, int B, bool IMP, int UN, int VN>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
-                                          const T *pold, T *pnew, double (*s_red)[32 * VecOf<T>::N]) {
+                                          const T *pold, T *pnew, double (*s_red)[32 * VN]) {
   static_assert(!IMP || sizeof(T) == 8, "the implicit form runs in FP64");
-  constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -701,15 +718,15 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           const int k = kb + j;
           T vv[B * B][VN];
 #pragma unroll
-          for (int e = 0; e < B * B; e++) ldv_stream<T>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
+          for (int e = 0; e < B * B; e++) ldn_stream<T, VN>(M.V + ((size_t)k * B * B + e) * S + sb, vv[e]);
           const int J = __shfl_sync(0xffffffffu, myJ, j);
           T xv[B][VN];
 #pragma unroll
           for (int c = 0; c < B; c++) {
-            ldv<T>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
+            ldn<T, VN>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
             if (!first) {
               T pv[VN];
-              ldv<T>(pold + (size_t)(J * B + c) * S + sb, pv);
+              ldn<T, VN>(pold + (size_t)(J * B + c) * S + sb, pv);
 #pragma unroll
               for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
             }
@@ -727,10 +744,10 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
     for (int a = 0; a < B; a++) {
       const size_t o = (size_t)(I * B + a) * S + sb;
       T zi[VN], pi[VN];
-      ldv<T>(M.z + o, zi);
+      ldn<T, VN>(M.z + o, zi);
       if (!first) {
         T po[VN];
-        ldv<T>(pold + o, po);
+        ldn<T, VN>(pold + o, po);
 #pragma unroll
         for (int v = 0; v < VN; v++) pi[v] = zi[v] + beta[v] * po[v];
       } else {
@@ -740,7 +757,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       if constexpr (IMP) {
         if (!first) {
           T qo[VN];
-          ldv<T>(M.q + o, qo);
+          ldn<T, VN>(M.q + o, qo);
 #pragma unroll
           for (int v = 0; v < VN; v++) acc[a][v] = fma(beta[v], qo[v], acc[a][v]);
         }
@@ -749,8 +766,8 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           for (int v = 0; v < VN; v++) acc[a][v] = pi[v];
         }
       }
-      stv<T>(pnew + o, pi);
-      stv<T>(M.q + o, acc[a]);
+      stn<T, VN>(pnew + o, pi);
+      stn<T, VN>(M.q + o, acc[a]);
 #pragma unroll
       for (int v = 0; v < VN; v++) pq[v] += (double)pi[v] * (double)acc[a][v];
     }
@@ -767,11 +784,10 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
 }
 
 // Writes the tile's r.r and r.z partials of parity slot `par`.
-template <typename T>
-__device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const double (&rr)[VecOf<T>::N],
-                                              const double (&rz)[VecOf<T>::N], double (*s_red)[32 * VecOf<T>::N],
-                                              double (*s_red2)[32 * VecOf<T>::N]) {
-  constexpr int VN = VecOf<T>::N;
+template <typename T, int VN>
+__device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const double (&rr)[VN],
+                                              const double (&rz)[VN], double (*s_red)[32 * VN],
+                                              double (*s_red2)[32 * VN]) {
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -796,10 +812,9 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
 }
 
 // x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z.
-template <typename T, int B>
+template <typename T, int B, int VN>
 __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, const T *pnew,
-                                            int par, double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
-  constexpr int VN = VecOf<T>::N;
+                                            int par, double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -817,10 +832,10 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
       const size_t o = (size_t)(I * B + a) * S + sb;
       T ri[VN], mi[VN], pi[VN], qi[VN], zi[VN];
       double xi[VN];
-      ldv<T>(M.M + o, mi);
-      ldv<T>(M.r + o, ri);
-      ldv<T>(pnew + o, pi);
-      ldv<T>(M.q + o, qi);
+      ldn<T, VN>(M.M + o, mi);
+      ldn<T, VN>(M.r + o, ri);
+      ldn<T, VN>(pnew + o, pi);
+      ldn<T, VN>(M.q + o, qi);
       ldv_d<VN>(M.x + o, xi);
 #pragma unroll
       for (int v = 0; v < VN; v++) {
@@ -831,19 +846,18 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
         rz[v] += (double)ri[v] * (double)zi[v];
       }
       stv_d<VN>(M.x + o, xi);
-      stv<T>(M.r + o, ri);
-      stv<T>(M.z + o, zi);
+      stn<T, VN>(M.r + o, ri);
+      stn<T, VN>(M.z + o, zi);
     }
   }
-  tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
+  tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
 // Residual replacement: r = F - K x in FP64 from the FP64 values, then
 // r (inner precision), z = r / M and the partials of the true residual.
-template <typename T, int B, bool IMP, int UN>
+template <typename T, int B, bool IMP, int UN, int VN>
 __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
-                                                   double (*s_red)[32 * VecOf<T>::N], double (*s_red2)[32 * VecOf<T>::N]) {
-  constexpr int VN = VecOf<T>::N;
+                                                   double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -889,7 +903,7 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
       double f[VN];
       T ri[VN], mi[VN], zi[VN];
       ldv_d<VN>(M.F + o, f);
-      ldv<T>(M.M + o, mi);
+      ldn<T, VN>(M.M + o, mi);
       if constexpr (IMP) {
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
           double xo[VN];
@@ -906,11 +920,11 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
         rr[v] += r64 * r64;
         rz[v] += (double)ri[v] * (double)zi[v];
       }
-      stv<T>(M.r + o, ri);
-      stv<T>(M.z + o, zi);
+      stn<T, VN>(M.r + o, ri);
+      stn<T, VN>(M.z + o, zi);
     }
   }
-  tile_partials<T>(M, g, chunk, par, rr, rz, s_red, s_red2);
+  tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
 constexpr int kMaxMeshes = 8;
@@ -918,10 +932,10 @@ constexpr int kMaxMeshes = 8;
 #ifndef UFEM_PCG_MIN_BLOCKS
 #define UFEM_PCG_MIN_BLOCKS 2
 #endif
-// UN: contributions whose gathers are issued together (implicit form)
-template <typename T, int B, bool IMP, int UN>
+// UN: contributions whose gathers are issued together (implicit form);
+// VN: samples per lane (a sample group is 32 VN samples)
+template <typename T, int B, bool IMP, int UN, int VN>
 __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_batch_pcg(BArgs<T> A) {
-  constexpr int VN = VecOf<T>::N;
   constexpr int GS = 32 * VN;
   __shared__ double s_red[kWarps][GS];
   __shared__ double s_red2[kWarps][GS];
@@ -941,7 +955,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
     if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
     any = __syncthreads_or(any);
     if (any) {
-      tile_true_residual<T, B, IMP, UN>(M, ti.y, ti.z, 0, s_red, s_red2);
+      tile_true_residual<T, B, IMP, UN, VN>(M, ti.y, ti.z, 0, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) {
         M.gtrue[ti.y] = 1;
         M.glast[ti.y] = 0;
@@ -1023,7 +1037,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
       }
       const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B, IMP, UN>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+      tile_spmv<T, B, IMP, UN, VN>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
     // The group counter changes only in phase S: read between the barriers,
@@ -1062,7 +1076,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
       if (ti.z == 0 && threadIdx.x == 0 && __ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
       if (!live) continue;
       const T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_update<T, B>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
+      tile_update<T, B, VN>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
     }
     if (!grid_barrier(A.bar)) return;
@@ -1078,7 +1092,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
           __syncthreads();  // thread 0 rewrites s_flag for the next tile
           continue;
         }
-        tile_true_residual<T, B, IMP, UN>(M, ti.y, ti.z, par, s_red, s_red2);
+        tile_true_residual<T, B, IMP, UN, VN>(M, ti.y, ti.z, par, s_red, s_red2);
         if (ti.z == 0 && threadIdx.x == 0) {
           M.gtrue[ti.y] = 1;
           M.glast[ti.y] = (int)k;
@@ -1270,7 +1284,7 @@ static ufem_mc_stats g_stats;
 // ---------------------------------------------------------------------------
 struct TuneEntry {
   std::string key;
-  int tpb, unroll;
+  int tpb, unroll, lanes;
   double ms;
 };
 static std::vector<TuneEntry> g_tune;
@@ -1288,16 +1302,16 @@ static void tune_load(const std::string &path) {
   FILE *f = fopen(path.c_str(), "r");
   if (!f) return;
   char key[512];
-  int tpb, un;
+  int tpb, un, ln;
   double ms;
-  while (fscanf(f, "%511s %d %d %lf", key, &tpb, &un, &ms) == 4) {
+  while (fscanf(f, "%511s %d %d %d %lf", key, &tpb, &un, &ln, &ms) == 5) {
     bool found = false;
     for (auto &t : g_tune)
       if (t.key == key) {
-        t.tpb = tpb; t.unroll = un; t.ms = ms;
+        t.tpb = tpb; t.unroll = un; t.lanes = ln; t.ms = ms;
         found = true;
       }
-    if (!found) g_tune.push_back({key, tpb, un, ms});
+    if (!found) g_tune.push_back({key, tpb, un, ln, ms});
   }
   fclose(f);
 }
@@ -1311,7 +1325,7 @@ static void tune_save(const std::string &path) {
   }
   FILE *f = fopen(path.c_str(), "w");
   if (!f) return;
-  for (auto &t : g_tune) fprintf(f, "%s %d %d %.4f\n", t.key.c_str(), t.tpb, t.unroll, t.ms);
+  for (auto &t : g_tune) fprintf(f, "%s %d %d %d %.4f\n", t.key.c_str(), t.tpb, t.unroll, t.lanes, t.ms);
   fclose(f);
 }
 
@@ -1372,6 +1386,7 @@ extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->use_graphs = 0;
   o->tiles_per_block = 0;
   o->unroll = 0;
+  o->lane_samples = 0;
 }
 
 extern "C" int ufem_mc_get_stats(ufem_mc_stats *s) {
@@ -1401,10 +1416,10 @@ struct EvTimer {
   }
 };
 
-template <typename T, bool IMP>
+template <typename T, bool IMP, int VN>
 int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, const std::vector<McPlan *> &plans,
             const ufem_mc_options &opt, long *iters_run) {
-  constexpr int VN = VecOf<T>::N, GS = 32 * VN;
+  constexpr int GS = 32 * VN;
   int rv;
   std::vector<BMesh<T>> hm(nmesh);
   std::vector<int4> tiles;
@@ -1414,12 +1429,12 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   const int B = models[0]->b;
   void (*kern)(BArgs<T>) = nullptr;
   if constexpr (!IMP) {
-    kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 1> : k_batch_pcg<T, 2, IMP, 1>;
+    kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 1, VN> : k_batch_pcg<T, 2, IMP, 1, VN>;
   } else {
-    const int un = opt.unroll > 0 ? opt.unroll : 4;
-    if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2> : k_batch_pcg<T, 2, IMP, 2>;
-    else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4> : k_batch_pcg<T, 2, IMP, 4>;
-    else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8> : k_batch_pcg<T, 2, IMP, 8>;
+    const int un = opt.unroll > 0 ? opt.unroll : 2;
+    if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN> : k_batch_pcg<T, 2, IMP, 2, VN>;
+    else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN> : k_batch_pcg<T, 2, IMP, 4, VN>;
+    else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8, VN> : k_batch_pcg<T, 2, IMP, 8, VN>;
   }
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
@@ -1432,7 +1447,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
   const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : 12;  // measured best on B200 for both forms
   g_stats.tiles_per_block = (int)tpb;
-  g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 4) : 0;
+  g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 2) : 0;
+  g_stats.lane_samples = VN;
   int rpt = (int)std::max<long>(kWarps, (total_rows + tpb * G - 1) / (tpb * G));
   rpt = (rpt + kWarps - 1) / kWarps * kWarps;
   int active_groups = 0;
@@ -1727,18 +1743,21 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
     g_stats.ms_assemble = t.stop();
   }
   // ---- launch shape: the caller's, else the autotuned one for this batch --
-  if (opt.tiles_per_block <= 0 || (opt.precision == 2 && opt.unroll <= 0)) {
+  if (opt.tiles_per_block <= 0 || (opt.precision == 2 && (opt.unroll <= 0 || opt.lane_samples <= 0))) {
     const TuneEntry *t = tune_find(tune_key(nmesh, models, nsamp, opt.precision));
     if (t) {
       if (opt.tiles_per_block <= 0) opt.tiles_per_block = t->tpb;
       if (opt.unroll <= 0) opt.unroll = t->unroll;
+      if (opt.lane_samples <= 0) opt.lane_samples = t->lanes;
     }
   }
   // ---- one persistent launch over every mesh -----------------------------
   long its = 0;
-  if (opt.precision == 1) rv = run_pcg<float, false>(nmesh, models, W, plans, opt, &its);
-  else if (opt.precision == 2) rv = run_pcg<double, true>(nmesh, models, W, plans, opt, &its);
-  else rv = run_pcg<double, false>(nmesh, models, W, plans, opt, &its);
+  if (opt.precision == 1) rv = run_pcg<float, false, 4>(nmesh, models, W, plans, opt, &its);
+  // implicit form: 4 samples per lane unless 2 is asked for (measured best on B200)
+  else if (opt.precision == 2 && opt.lane_samples != 2) rv = run_pcg<double, true, 4>(nmesh, models, W, plans, opt, &its);
+  else if (opt.precision == 2) rv = run_pcg<double, true, 2>(nmesh, models, W, plans, opt, &its);
+  else rv = run_pcg<double, false, 2>(nmesh, models, W, plans, opt, &its);
   if (rv != UFEM_AF_OK) return rv;
   g_stats.pcg_iterations = its;
   // ---- outputs -------------------------------------------------------------
@@ -1812,16 +1831,23 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
     g_tune_loaded = true;
   }
   const int tpbs[] = {3, 6, 12, 24, 48};
-  std::vector<int> unrolls;
-  if (base.precision == 2) unrolls = {2, 4, 8};
-  else unrolls = {4};
+  std::vector<int> unrolls, lanes;
+  if (base.precision == 2) {
+    unrolls = {2, 4, 8};
+    lanes = {2, 4};
+  } else {
+    unrolls = {4};
+    lanes = {0};
+  }
   double best_ms = 1e300;
-  int best_tpb = 12, best_un = unrolls[0];
+  int best_tpb = 12, best_un = unrolls[0], best_ln = lanes[0];
+  for (int ln : lanes)
   for (int tpb : tpbs)
     for (int un : unrolls) {
       ufem_mc_options o = base;
       o.tiles_per_block = tpb;
       o.unroll = un;
+      o.lane_samples = ln;
       o.max_iters = 30;
       double per_it = 0.0;
       for (int rep = 0; rep < 2; rep++) {  // the first run also builds the workspace
@@ -1833,21 +1859,23 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
         best_ms = per_it;
         best_tpb = tpb;
         best_un = un;
+        best_ln = ln;
       }
     }
   const std::string key = tune_key(nmesh, models, nsamp, base.precision);
   bool found = false;
   for (auto &t : g_tune)
     if (t.key == key) {
-      t.tpb = best_tpb; t.unroll = best_un; t.ms = best_ms;
+      t.tpb = best_tpb; t.unroll = best_un; t.lanes = best_ln; t.ms = best_ms;
       found = true;
     }
-  if (!found) g_tune.push_back({key, best_tpb, best_un, best_ms});
+  if (!found) g_tune.push_back({key, best_tpb, best_un, best_ln, best_ms});
   tune_save(path);
   if (best) {
     *best = base;
     best->tiles_per_block = best_tpb;
     best->unroll = best_un;
+    best->lane_samples = best_ln;
   }
   return UFEM_AF_OK;
 }

@@ -66,7 +66,7 @@ def default_options():
 def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1, tol: float = 1e-8,
              max_iters: int | None = None, replace_every: int | None = None, replace_near: float | None = None,
              u_guess: list[np.ndarray | None] | None = None, olens: list[int] | None = None,
-             tiles_per_block: int = 0, unroll: int = 0):
+             tiles_per_block: int = 0, unroll: int = 0, lane_samples: int = 0):
     """Batched solve of every sample of every mesh in one launch.
 
     Returns per mesh (ofld[nsamp, olen], status[nsamp], iters[nsamp]) and the
@@ -84,6 +84,7 @@ def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1
         opt.replace_near = replace_near
     opt.tiles_per_block = tiles_per_block
     opt.unroll = unroll
+    opt.lane_samples = lane_samples
     keep = []
     hs = (C.c_void_p * nm)(*[m.h.value for m in models])
     ns = np.array([f.shape[0] for f in iflds], np.int64)
