@@ -1,24 +1,34 @@
 #!/usr/bin/env python
 """Benchmark: Monte Carlo brick-beam solves/s at relative residual 1e-8,
-learned warm start + FP32/FP64 batched PCG against plain FP64 PCG, 1 B200.
+learned warm start + batched PCG against plain FP64 PCG, 1 B200.
 
 Workload (one step): 8,192 fresh samples of the 40x10x10 brick cantilever
 beam (8 x 2 x 2 m, 14,883 DOFs) with 16 equal-length E zones along x
 (E = 30 GPa * exp(0.15 z), z iid N(0,1), median 30 GPa) and one load factor
 U(0.8, 1.2) on the 1 MPa end-face traction (17 random inputs), x = 0 face
-fixed, seeded Philox streams per sample, synthetic data.  Set-up (not
-timed): 4,096 training samples solved by the batched solver, a 64-mode POD
-basis from the first 512 solutions, a 17-256-256-64 GELU MLP trained on the
-tensor cores.  Timed step: MLP inference -> POD guess -> batched FP32 Jacobi
-PCG with FP64 solution and true-residual replacement to |f - K u| / |f| <=
-1e-8 for every sample, cold fallback for samples whose iterations regress,
-outputs (tip displacements, reactions) on the GPU.
+fixed, seeded Philox streams per sample, synthetic data.
 
-Reported beside it: the plain method (FP64 assembly + FP64 Jacobi PCG, one
-sample at a time, on a subset of the same samples), the same batch solved
-without the warm start, the uneven batch (20x5x5 + 40x10x10 + 60x15x15
-beams, per-element lognormal E, 512 samples each, one launch), and the
-reference's own Monte Carlo library on the host cores.
+Set-up (not timed): 4,096 training samples solved by the batched solver, a
+64-mode POD basis from the first 512 solutions, the per-zone reduced
+operators Phi^T K_z Phi, and a 17-256-256-64 GELU MLP trained on the tensor
+cores (CUDA-graph-replayed steps).
+
+Timed step (ufem_warm_solve): the guess -- by default each sample's
+POD-Galerkin coefficients on the learned basis (--guess 1), or the MLP's
+coefficients (--guess 0) -- then the batched Jacobi PCG to |f - K u| / |f|
+<= 1e-8 for every sample, by default in FP64 with every 3x3 block formed in
+the kernel from the shared unit-E element blocks (--precision 2; 1 = FP32
+PCG on explicit FP32 matrices with FP64 solution and true-residual
+replacement, 0 = explicit FP64), cold fallback for samples whose iterations
+regress, outputs (tip displacements, reactions) on the GPU.
+
+Reported beside it: the other guess, the other precisions, the same batch
+without a warm start, the plain method (FP64 assembly + FP64 Jacobi PCG, one
+sample at a time, on a subset of the same samples), the uneven batch
+(20x5x5 + 40x10x10 + 60x15x15 beams, per-element lognormal E, 512 samples
+each, one launch), the single-system configs (80x20x20 beam, 128x128x64
+block; FP64 and FP32-inner/FP64-refinement PCG) and the reference's own
+Monte Carlo library on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]     # this implementation
   python bench.py --impl reference [...]                  # the reference, host cores
@@ -50,7 +60,7 @@ WARM_EVAL = 8192
 EVAL_FIRST = 1 << 20     # evaluation sample ids: disjoint from training
 METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 PCG, 1 B200"
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
-            "warm-started (POD 64 modes from 512 solves, MLP 17-256-256-64 trained on 4096 solves)")
+            "warm-started (POD 64 modes from 512 solves; MLP 17-256-256-64 trained on 4096 solves)")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
           2: "k_batch_pcg<double,3,implicit>"}
@@ -71,6 +81,9 @@ def parse():
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
     p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
+    p.add_argument("--guess", type=int, default=1,
+                   help="warm-start guess: 1 = each sample's POD-Galerkin coefficients on the learned basis "
+                        "(default), 0 = the MLP's coefficients")
     p.add_argument("--precision", type=int, default=2,
                    help="2: FP64 PCG, blocks formed in the kernel (default); 1: FP32 PCG on explicit FP32 "
                         "matrices with FP64 solution and true-residual replacement; 0: FP64 explicit")
@@ -446,6 +459,7 @@ def ours(a):
     tstats = ws.train(train, precision=a.precision)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    ws.set_guess_mode(a.guess)
 
     opt = default_options()
     opt.precision = a.precision
@@ -533,10 +547,13 @@ def ours(a):
             "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
     del d_out2, d_st2, d_it2
 
-    # ---- the POD-Galerkin guess (guess mode 1), same precision -------------
+    # ---- the other guess (MLP <-> POD-Galerkin), same precision ------------
+    GUESS = {0: "the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> 64 coefficients)",
+             1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the per-zone reduced "
+                "operators) on the learned POD basis"}
     galerkin = None
     if not a.no_other:
-        L.ufem_warm_set_guess_mode(ws.h, 1)
+        L.ufem_warm_set_guess_mode(ws.h, 1 - a.guess)
         wst3 = _lib.WarmStats()
         args3 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt),
                  C.byref(wst3))
@@ -548,15 +565,14 @@ def ours(a):
         e1.record()
         torch.cuda.synchronize()
         ms3 = e0.elapsed_time(e1) / a.steps
-        galerkin = {"method": "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the "
-                              "per-zone reduced operators) as the guess", "value": n / (ms3 / 1000.0),
+        galerkin = {"guess": GUESS[1 - a.guess], "value": n / (ms3 / 1000.0),
                     "unit": "solves/s", "iters_mean": wst3.iters_mean, "iters_max": wst3.iters_max,
                     "guess_rel_err_mean": wst3.guess_err_mean, "guess_rel_err_max": wst3.guess_err_max,
                     "fallbacks": wst3.fallbacks, "ms_guess": wst3.ms_guess,
                     "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
-                    "outputs_max_rel_diff_vs_mlp": float(np.abs(d_out.cpu().numpy() - out_warm).max()
-                                                         / np.abs(out_warm).max())}
-        L.ufem_warm_set_guess_mode(ws.h, 0)
+                    "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
+                                                              / np.abs(out_warm).max())}
+        L.ufem_warm_set_guess_mode(ws.h, a.guess)
 
     # ---- the warm start at the other precisions (one warm-up, one timed step)
     PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
@@ -635,7 +651,7 @@ def ours(a):
                                    "explicit FP32 values 34 GB per iteration, >> 126 MB L2",
                        "parallelism": f"samples sharded over {world} GPU(s), no collective"},
             "all_converged": bool(np.isin(status, [0, 4]).all()),
-            "warm_start": {"iters_mean": float(iters.mean()), "iters_max": int(iters.max()),
+            "warm_start": {"guess": GUESS[a.guess], "iters_mean": float(iters.mean()), "iters_max": int(iters.max()),
                            "cold_iters_mean": cold["iters_mean"],
                            "iterations_saved_frac": 1.0 - float(iters.mean()) / cold["iters_mean"],
                            "guess_rel_err_mean": warm_info["guess_err_mean"],
@@ -650,7 +666,7 @@ def ours(a):
                                      "pod_energy_mode64_over_mode1": (s2[63] / s2[0]) if s2[0] else None}},
             "batched_without_warm_start": cold,
             "warm_start_other_precisions": other,
-            "galerkin_guess": galerkin,
+            "warm_start_other_guess": galerkin,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},

@@ -71,6 +71,7 @@ struct McPlan {
   DBuf<double> F0;                 // loads that no input variable overrides
   std::vector<int> ovr_row, ovr_var;
   DBuf<int> d_ovr_row, d_ovr_var;
+  DBuf<int> d_ovr_ptr, d_ovr_rvar;  // the overrides by DOF row (input order within a row)
   std::vector<McOut> outs;
   DBuf<int> d_out_type, d_out_pos, d_out_row, d_out_elem, d_out_ip, d_out_comp;
   DBuf<int> reac_rows;             // DOF rows of the reaction list
@@ -198,6 +199,15 @@ static int build_plan(ufem_model *m, McPlan *P) {
   if ((rv = P->F0.upload(F0.data(), F0.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->d_ovr_row.upload(P->ovr_row.data(), P->ovr_row.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->d_ovr_var.upload(P->ovr_var.data(), P->ovr_var.size())) != UFEM_AF_OK) return rv;
+  {
+    std::vector<int> ptr(m->nDOFAct + 1, 0), rvar(P->ovr_row.size()), fill;
+    for (int r : P->ovr_row) ptr[r + 1]++;
+    for (long i = 0; i < m->nDOFAct; i++) ptr[i + 1] += ptr[i];
+    fill.assign(ptr.begin(), ptr.end() - 1);
+    for (size_t j = 0; j < P->ovr_row.size(); j++) rvar[fill[P->ovr_row[j]]++] = P->ovr_var[j];
+    if ((rv = P->d_ovr_ptr.upload(ptr.data(), ptr.size())) != UFEM_AF_OK) return rv;
+    if ((rv = P->d_ovr_rvar.upload(rvar.data(), rvar.size())) != UFEM_AF_OK) return rv;
+  }
   // outputs (fem/fem_mont.c:514-686)
   P->outs.clear();
   std::vector<int> ot, op, orow, oel, oip, ocomp;
@@ -445,15 +455,15 @@ __global__ void k_make_E(int eLen, int S, int nsamp, long ilen, const double *__
 // F for every sample (fem_add_loads order: fixed part, then the overridden
 // lines in input order); F at fixed DOFs is kept in Fval and zeroed.
 __global__ void k_make_F(int n, int S, int nsamp, long ilen, const double *__restrict__ ifld,
-                         const double *__restrict__ F0, int novr, const int *__restrict__ ovr_row,
+                         const double *__restrict__ F0, const int *__restrict__ ovr_ptr,
                          const int *__restrict__ ovr_var, double *__restrict__ F) {
   long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= (long)n * S) return;
   int i = (int)(t / S), s = (int)(t % S);
-  F[t] = (s < nsamp) ? F0[i] : 0.0;
+  double f = (s < nsamp) ? F0[i] : 0.0;
   if (s < nsamp)
-    for (int j = 0; j < novr; j++)
-      if (ovr_row[j] == i) F[t] += ifld[(size_t)s * ilen + ovr_var[j]];
+    for (int j = ovr_ptr[i]; j < ovr_ptr[i + 1]; j++) f += ifld[(size_t)s * ilen + ovr_var[j]];
+  F[t] = f;
 }
 
 __global__ void k_fix_F(int n, int S, const unsigned char *__restrict__ fixed, double *__restrict__ F) {
@@ -1696,7 +1706,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       k_make_E<<<(unsigned)((ne + 255) / 256), 256>>>((int)m->eLen, w.S, w.nsamp, P->ilen, d_ifld[k],
                                                       P->elem_var.p, m->d_eE.p, w.E.p);
       k_make_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, w.nsamp, P->ilen, d_ifld[k], P->F0.p,
-                                                     (int)P->ovr_row.size(), P->d_ovr_row.p, P->d_ovr_var.p,
+                                                     P->d_ovr_ptr.p, P->d_ovr_rvar.p,
                                                      w.Fraw.p);
       UFEM_CUDA_TRY(cudaMemcpyAsync(w.F.p, w.Fraw.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
       k_fix_F<<<(unsigned)((n + 255) / 256), 256>>>((int)m->nDOFAct, w.S, m->d_fixed.p, w.F.p);

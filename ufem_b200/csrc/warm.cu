@@ -376,16 +376,43 @@ __global__ void k_gather_rows(long nrow, int ncol, const long *__restrict__ idx,
   dst[e] = src[idx[r] * ncol + (e % ncol)];
 }
 
-// |u0_s - u_s| / |u_s| per sample, both [n][S] (rows summed in order)
-__global__ void k_rel_err(long n, int S, int nsamp, const double *__restrict__ u0, const double *__restrict__ u,
-                          double *__restrict__ err) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsamp) return;
+// |u0_s - u_s| / |u_s| per sample, both [n][S], in two passes with a fixed
+// order: k_rel_err_part sums a chunk of rows for 32 samples per block (8
+// warps stride the chunk, combined in warp order), k_rel_err adds the chunks.
+constexpr int kErrChunks = 64;
+__global__ void __launch_bounds__(256) k_rel_err_part(long n, int S, const double *__restrict__ u0,
+                                                      const double *__restrict__ u, double *__restrict__ part) {
+  __shared__ double sa[8][32], sb[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int s = blockIdx.x * 32 + lane;  // S is a multiple of 128
+  const long per = (n + gridDim.y - 1) / gridDim.y;
+  const long i0 = (long)blockIdx.y * per, i1 = min(n, i0 + per);
   double a = 0.0, b = 0.0;
-  for (long i = 0; i < n; i++) {
+  for (long i = i0 + w; i < i1; i += 8) {
     const double x = u[i * S + s], d = u0[i * S + s] - x;
     a += d * d;
     b += x * x;
+  }
+  sa[w][lane] = a;
+  sb[w][lane] = b;
+  __syncthreads();
+  if (w == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int k = 0; k < 8; k++) {
+      ta += sa[k][lane];
+      tb += sb[k][lane];
+    }
+    part[((size_t)blockIdx.y * S + s) * 2] = ta;
+    part[((size_t)blockIdx.y * S + s) * 2 + 1] = tb;
+  }
+}
+__global__ void k_rel_err(int nch, int S, int nsamp, const double *__restrict__ part, double *__restrict__ err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsamp) return;
+  double a = 0.0, b = 0.0;
+  for (int c = 0; c < nch; c++) {
+    a += part[((size_t)c * S + s) * 2];
+    b += part[((size_t)c * S + s) * 2 + 1];
   }
   err[s] = b > 0.0 ? sqrt(a / b) : sqrt(a);
 }
@@ -541,7 +568,7 @@ struct ufem_warm {
   DBuf<double> U, Y, Q, Z, G, V, lam, T, scale, part, raw, sc, c;
   DBuf<int> perm, sweeps;
   DBuf<float> X, Tt, Yo;
-  DBuf<double> ifsub, u0, uf, err;
+  DBuf<double> ifsub, u0, uf, err, errpart;
   DBuf<double> ofsub;
   DBuf<int> stsub;
   DBuf<long> itsub;
@@ -1011,8 +1038,10 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   }
   cudaEventRecord(e3);
   // guess error against the converged solution
-  k_rel_err<<<grid1(nsamp, 128), 128>>>(n, S, (int)nsamp, w->u0.p, w->uf.p, w->err.p);
-  st.kernel_launches += 1;
+  if ((rv = w->errpart.ensure((size_t)kErrChunks * S * 2))) return rv;
+  k_rel_err_part<<<dim3((unsigned)(S / 32), kErrChunks), 256>>>(n, S, w->u0.p, w->uf.p, w->errpart.p);
+  k_rel_err<<<grid1(nsamp, 128), 128>>>(kErrChunks, S, (int)nsamp, w->errpart.p, w->err.p);
+  st.kernel_launches += 2;
   UFEM_CUDA_TRY(cudaGetLastError());
   std::vector<double> he(nsamp);
   std::vector<long> hi(nsamp);
