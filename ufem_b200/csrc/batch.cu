@@ -362,6 +362,46 @@ struct VecOf<double> {
   using V = double2;
 };
 
+// Which samples a lane holds.  FP32 kernels: 4 adjacent samples (one 16-byte
+// load).  FP64 kernels: pairs of adjacent samples, one pair in every 64-sample
+// half of the group (lane l: 2l, 2l+1 [, 64 + 2l, 64 + 2l + 1]), so that every
+// 16-byte-per-lane load reads 512 contiguous bytes -- with 4 adjacent doubles
+// per lane, the two loads would each fetch half of every sector from L2.
+template <typename T, int VN>
+__device__ __forceinline__ int lane_base(int lane) {
+  return sizeof(T) == 8 ? lane * 2 : lane * VN;
+}
+template <typename T, int VN>
+__device__ __forceinline__ int lane_sample(int lane, int v) {
+  return sizeof(T) == 8 ? (v >> 1) * 64 + lane * 2 + (v & 1) : lane * VN + v;
+}
+// VN doubles of this lane's samples (p = row + group start + lane_base):
+// FP64 kernels read pairs 64 samples apart, FP32 kernels VN adjacent ones
+template <typename T, int VN>
+__device__ __forceinline__ void ld64(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2)));
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
+template <typename T, int VN>
+__device__ __forceinline__ void ld64_stream(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    const double2 v = __ldcs(reinterpret_cast<const double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2)));
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
+template <typename T, int VN>
+__device__ __forceinline__ void st64(double *p, const double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++)
+    *reinterpret_cast<double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2)) = make_double2(o[2 * h], o[2 * h + 1]);
+}
+
 // VN values of type T at a 16-byte aligned address (double: VN = 2 or 4,
 // float: VN = 4), read through L2 (other blocks write them during the kernel)
 template <typename T, int VN>
@@ -369,7 +409,7 @@ __device__ __forceinline__ void ldn(const T *p, T (&o)[VN]) {
   if constexpr (sizeof(T) == 8) {
 #pragma unroll
     for (int h = 0; h < VN / 2; h++) {
-      const double2 v = __ldcg(reinterpret_cast<const double2 *>(p) + h);
+      const double2 v = __ldcg(reinterpret_cast<const double2 *>(p + h * 64));
       o[2 * h] = v.x;
       o[2 * h + 1] = v.y;
     }
@@ -388,7 +428,7 @@ template <typename T, int VN>
 __device__ __forceinline__ void stn(T *p, const T (&o)[VN]) {
   if constexpr (sizeof(T) == 8) {
 #pragma unroll
-    for (int h = 0; h < VN / 2; h++) reinterpret_cast<double2 *>(p)[h] = make_double2(o[2 * h], o[2 * h + 1]);
+    for (int h = 0; h < VN / 2; h++) *reinterpret_cast<double2 *>(p + h * 64) = make_double2(o[2 * h], o[2 * h + 1]);
   } else {
 #pragma unroll
     for (int h = 0; h < VN / 4; h++)
@@ -402,7 +442,7 @@ __device__ __forceinline__ void ldn_stream(const T *p, T (&o)[VN]) {
   if constexpr (sizeof(T) == 8) {
 #pragma unroll
     for (int h = 0; h < VN / 2; h++) {
-      const double2 v = __ldcs(reinterpret_cast<const double2 *>(p) + h);
+      const double2 v = __ldcs(reinterpret_cast<const double2 *>(p + h * 64));
       o[2 * h] = v.x;
       o[2 * h + 1] = v.y;
     }
@@ -417,31 +457,6 @@ __device__ __forceinline__ void ldn_stream(const T *p, T (&o)[VN]) {
     }
   }
 }
-// VN doubles (VN = 2 or 4) at a 16-byte aligned address
-template <int VN>
-__device__ __forceinline__ void ldv_d(const double *p, double (&o)[VN]) {
-#pragma unroll
-  for (int h = 0; h < VN / 2; h++) {
-    double2 v = __ldcg(reinterpret_cast<const double2 *>(p) + h);
-    o[2 * h] = v.x;
-    o[2 * h + 1] = v.y;
-  }
-}
-template <int VN>
-__device__ __forceinline__ void ldv_d_stream(const double *p, double (&o)[VN]) {
-#pragma unroll
-  for (int h = 0; h < VN / 2; h++) {
-    double2 v = __ldcs(reinterpret_cast<const double2 *>(p) + h);
-    o[2 * h] = v.x;
-    o[2 * h + 1] = v.y;
-  }
-}
-template <int VN>
-__device__ __forceinline__ void stv_d(double *p, const double (&o)[VN]) {
-#pragma unroll
-  for (int h = 0; h < VN / 2; h++) reinterpret_cast<double2 *>(p)[h] = make_double2(o[2 * h], o[2 * h + 1]);
-}
-
 // E of every element for every sample: E[e*S + s]
 __global__ void k_make_E(int eLen, int S, int nsamp, long ilen, const double *__restrict__ ifld,
                          const int *__restrict__ elem_var, const double *__restrict__ eE, double *__restrict__ E) {
@@ -628,10 +643,10 @@ __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, in
         const long long key = __shfl_sync(0xffffffffu, mykey, min(j + u, cnt - 1));
         const int J = (int)(key & 0xffffffffLL), var = (int)(key >> 32);
 #pragma unroll
-        for (int b = 0; b < B; b++) ldv_d<VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
+        for (int b = 0; b < B; b++) ld64<double, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
 #pragma unroll
         for (int h = 0; h < VN / 2; h++) {
-          const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)var * S + sb) + h);
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)var * S + sb + h * 64));
           av[u][2 * h] = v.x;
           av[u][2 * h + 1] = v.y;
         }
@@ -701,11 +716,11 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
-  const int sb = g * GS + lane * VN;
+  const int sb = g * GS + lane_base<T, VN>(lane);
   const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
   T beta[VN];
 #pragma unroll
-  for (int v = 0; v < VN; v++) beta[v] = s_beta[lane * VN + v];
+  for (int v = 0; v < VN; v++) beta[v] = s_beta[lane_sample<T, VN>(lane, v)];
   double pq[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) pq[v] = 0;
@@ -783,7 +798,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
     }
   }
 #pragma unroll
-  for (int v = 0; v < VN; v++) s_red[warp][lane * VN + v] = pq[v];
+  for (int v = 0; v < VN; v++) s_red[warp][lane_sample<T, VN>(lane, v)] = pq[v];
   __syncthreads();
   if (threadIdx.x < GS) {
     double t = 0;
@@ -802,8 +817,8 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
   for (int v = 0; v < VN; v++) {
-    s_red[warp][lane * VN + v] = rr[v];
-    s_red2[warp][lane * VN + v] = rz[v];
+    s_red[warp][lane_sample<T, VN>(lane, v)] = rr[v];
+    s_red2[warp][lane_sample<T, VN>(lane, v)] = rz[v];
   }
   __syncthreads();
   if (threadIdx.x < GS) {
@@ -828,11 +843,11 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
-  const int sb = g * GS + lane * VN;
+  const int sb = g * GS + lane_base<T, VN>(lane);
   const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
   T alpha[VN];
 #pragma unroll
-  for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane * VN + v];
+  for (int v = 0; v < VN; v++) alpha[v] = s_alpha[lane_sample<T, VN>(lane, v)];
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
@@ -846,7 +861,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
       ldn<T, VN>(M.r + o, ri);
       ldn<T, VN>(pnew + o, pi);
       ldn<T, VN>(M.q + o, qi);
-      ldv_d<VN>(M.x + o, xi);
+      ld64<T, VN>(M.x + o, xi);
 #pragma unroll
       for (int v = 0; v < VN; v++) {
         xi[v] += (double)alpha[v] * (double)pi[v];
@@ -855,7 +870,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
         rr[v] += (double)ri[v] * (double)ri[v];
         rz[v] += (double)ri[v] * (double)zi[v];
       }
-      stv_d<VN>(M.x + o, xi);
+      st64<T, VN>(M.x + o, xi);
       stn<T, VN>(M.r + o, ri);
       stn<T, VN>(M.z + o, zi);
     }
@@ -871,7 +886,7 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
-  const int sb = g * GS + lane * VN;
+  const int sb = g * GS + lane_base<T, VN>(lane);
   const int row0 = chunk * M.rows_per_tile, row1 = min(M.nbr, row0 + M.rows_per_tile);
   double rr[VN], rz[VN];
 #pragma unroll
@@ -894,13 +909,13 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
           const int J = __shfl_sync(0xffffffffu, myJ, j);
           double xv[B][VN];
 #pragma unroll
-          for (int c = 0; c < B; c++) ldv_d<VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
+          for (int c = 0; c < B; c++) ld64<T, VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
 #pragma unroll
           for (int a = 0; a < B; a++)
 #pragma unroll
             for (int c = 0; c < B; c++) {
               double vv[VN];
-              ldv_d_stream<VN>(M.V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
+              ld64_stream<T, VN>(M.V64 + ((size_t)k * B * B + a * B + c) * S + sb, vv);
 #pragma unroll
               for (int v = 0; v < VN; v++) acc[a][v] += vv[v] * xv[c][v];
             }
@@ -912,12 +927,12 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
       const size_t o = (size_t)(I * B + a) * S + sb;
       double f[VN];
       T ri[VN], mi[VN], zi[VN];
-      ldv_d<VN>(M.F + o, f);
+      ld64<T, VN>(M.F + o, f);
       ldn<T, VN>(M.M + o, mi);
       if constexpr (IMP) {
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
           double xo[VN];
-          ldv_d<VN>(M.x + o, xo);
+          ld64<T, VN>(M.x + o, xo);
 #pragma unroll
           for (int v = 0; v < VN; v++) acc[a][v] = xo[v];
         }
