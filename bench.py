@@ -268,9 +268,11 @@ def host_cores():
 def warm_setup(a, rank=0):
     """The warm-start model, its training samples and this rank's evaluation samples."""
     from ufem_b200 import meshgen as mg
+    from ufem_b200.shard import rank_samples
     m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
     train = mg.warm_samples(m, a.train)
-    ev = mg.warm_samples(m, a.eval, first_sample=EVAL_FIRST + rank * a.eval)
+    first, count = rank_samples(rank, a.eval, EVAL_FIRST)
+    ev = mg.warm_samples(m, count, first_sample=first)
     return m, train, ev
 
 
@@ -319,7 +321,8 @@ def _vp(ts):
 
 def uneven_section(a, rank, dev):
     """The uneven batch: three meshes, a.nsamp samples each, one launch; one
-    warm-up and one timed step, cold starts, FP32/FP64 refinement."""
+    warm-up and one timed step, cold starts, for the FP32-inner / FP64
+    refinement form (explicit FP32 matrices) and the FP64 implicit form."""
     import ctypes as C
     import numpy as np
     import torch
@@ -330,9 +333,6 @@ def uneven_section(a, rank, dev):
     models, iflds = build_meshes(a.nsamp, rank)
     gms = [GpuModel(m) for m in models]
     nm = len(gms)
-    opt = default_options()
-    opt.precision = 1
-    opt.tol = 1e-8
     d_in = [torch.from_numpy(f).to(dev) for f in iflds]
     d_out = [torch.zeros((f.shape[0], m.mc_olen), dtype=torch.float64, device=dev) for f, m in zip(iflds, models)]
     d_st = [torch.zeros(f.shape[0], dtype=torch.int32, device=dev) for f in iflds]
@@ -340,22 +340,27 @@ def uneven_section(a, rank, dev):
     hs = (C.c_void_p * nm)(*[g.h.value for g in gms])
     ns = np.array([f.shape[0] for f in iflds], np.int64)
     null = (C.c_void_p * nm)()
-    args = (nm, hs, ns.ctypes.data_as(C.POINTER(C.c_long)), _vp(d_in), _vp(d_out), _vp(d_st), _vp(d_it), null, null,
-            C.byref(opt))
-    _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*args))
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*args))
-    e1.record()
-    torch.cuda.synchronize()
-    st = _lib.McStats()
-    L.ufem_mc_get_stats(C.byref(st))
-    ms = e0.elapsed_time(e1)
-    out = {"workload": UNEVEN, "value": int(ns.sum()) / (ms / 1000.0), "unit": "solves/s", "ms_per_step": ms,
-           "all_converged": all(bool((x == 0).all()) for x in d_st),
-           "max_iters_per_mesh": [int(x.max().item()) for x in d_it],
-           "pcg_GBs": st.pcg_bytes / (st.ms_pcg / 1000.0) / 1e9 if st.ms_pcg else None}
+    out = {"workload": UNEVEN}
+    for prec, label in ((1, "fp32_explicit_fp64_refinement"), (2, "fp64_implicit")):
+        opt = default_options()
+        opt.precision = prec
+        opt.tol = 1e-8
+        args = (nm, hs, ns.ctypes.data_as(C.POINTER(C.c_long)), _vp(d_in), _vp(d_out), _vp(d_st), _vp(d_it), null,
+                null, C.byref(opt))
+        _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*args))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*args))
+        e1.record()
+        torch.cuda.synchronize()
+        st = _lib.McStats()
+        L.ufem_mc_get_stats(C.byref(st))
+        ms = e0.elapsed_time(e1)
+        out[label] = {"value": int(ns.sum()) / (ms / 1000.0), "unit": "solves/s", "ms_per_step": ms,
+                      "all_converged": all(bool((x == 0).all()) for x in d_st),
+                      "max_iters_per_mesh": [int(x.max().item()) for x in d_it],
+                      "pcg_GBs": st.pcg_bytes / (st.ms_pcg / 1000.0) / 1e9 if st.ms_pcg else None}
     del gms
     return out
 
@@ -427,6 +432,7 @@ def ours(a):
     from ufem_b200.mc import default_options, mc_solve_serial
     from ufem_b200 import meshgen as mg
     from ufem_b200.warm import WarmStart
+    from ufem_b200 import shard
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -443,11 +449,7 @@ def ours(a):
             dist.barrier()
 
     def max_over_ranks(v):
-        if world > 1:
-            t = torch.tensor([v], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return v
+        return shard.max_over_ranks(v, device=dev)
 
     # ---- set-up (not timed): train the warm start -----------------------------
     m, train, ev = warm_setup(a, rank)
