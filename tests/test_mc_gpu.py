@@ -289,3 +289,39 @@ def test_autotune_writes_cache_and_is_used(tmp_path):
     assert (s_t == 0).all() and (s_f == 0).all()
     # the tile count changes the grouping of the dot products, not the answer
     assert np.abs(o_t - o_f).max() <= 1e-6 * np.abs(o_f).max()
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_non_finite_samples_report_nan_and_leave_others_alone(precision):
+    """A sample with a NaN E value or a NaN load is reported UFEM_ST_NAN (not
+    converged, not a breakdown); the other samples of its group converge to
+    the same outputs as without it."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import ST_NAN, mc_solve
+    m = mg.warm_beam(6, 2, 2, zones=3)
+    f = mg.warm_samples(m, 20)
+    g = GpuModel(m)
+    (o_ok, s_ok, _), = mc_solve([g], [f], precision=precision)[0]
+    bad = f.copy()
+    bad[3, 0] = np.nan                  # E of zone 0
+    bad[7, len(m.mp_vals)] = np.nan     # one tip force
+    (o_b, s_b, _), = mc_solve([g], [bad], precision=precision)[0]
+    assert s_b[3] == ST_NAN and s_b[7] == ST_NAN
+    keep = np.setdiff1d(np.arange(20), [3, 7])
+    assert (s_b[keep] == 0).all() and (s_ok == 0).all()
+    assert np.abs(o_b[keep] - o_ok[keep]).max() <= 1e-12 * np.abs(o_ok).max()
+
+
+def test_mesh_without_samples_in_a_multi_mesh_launch():
+    """One mesh of a launch has no samples: the others solve as usual."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    a = mg.warm_beam(6, 2, 2, zones=3)
+    b = mg.warm_beam(4, 2, 2, zones=2)
+    fa = mg.warm_samples(a, 30)
+    fb = mg.warm_samples(b, 0)
+    for prec in (1, 2):
+        res, _ = mc_solve([GpuModel(a), GpuModel(b)], [fa, fb], precision=prec)
+        assert (res[0][1] == 0).all() and res[1][1].shape == (0,)

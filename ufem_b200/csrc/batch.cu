@@ -571,7 +571,8 @@ __global__ void k_diag_implicit(int nbr, int S, const int *__restrict__ diagblk,
 // ---------------------------------------------------------------------------
 // ST_CAND: the recursive residual is below tol; the sample is frozen until
 // the group's next true-residual pass decides (converged, or resumed)
-enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4, ST_CAND = 5 };
+// ST_NAN: a non-finite residual or p.q (NaN or infinite inputs); the sample is frozen
+enum { ST_ACTIVE = 0, ST_CONV = 1, ST_MAXIT = 2, ST_BREAK = 3, ST_SKIP = 4, ST_CAND = 5, ST_NAN = 6 };
 
 template <typename T>
 struct BMesh {
@@ -1017,7 +1018,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
         constexpr bool kFreeze = sizeof(T) == 8;
         int nst = st;
         if (st == ST_ACTIVE || st == ST_CAND) {
-          if (!(rr == rr) || isinf(rr)) nst = ST_BREAK;
+          if (!(rr == rr) || isinf(rr)) nst = ST_NAN;
           else if (is_true && (double)rr <= tol2) nst = ST_CONV;
           else if (k > A.maxit) nst = ST_MAXIT;
           else if (is_true) nst = ST_ACTIVE;  // a candidate that failed its check resumes
@@ -1086,7 +1087,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
             alpha = (T)(rho / pq);
             upd = 1;
           } else if (ti.z == 0) {
-            M.state[s] = ST_BREAK;  // p.q <= 0: breakdown, the sample is frozen
+            M.state[s] = isfinite(pq) ? ST_BREAK : ST_NAN;  // p.q <= 0 or not finite: the sample is frozen
             M.iters[s] = (int)k;
           }
         }
@@ -1543,6 +1544,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     std::vector<int> st(w.S), ga(b.ngroups, 0);
     for (int s = 0; s < w.S; s++) {
       if (s >= w.nsamp) st[s] = ST_SKIP;
+      else if (!std::isfinite(w.h_ff[s])) st[s] = ST_NAN;  // NaN or infinite loads
       else if (!(w.h_ff[s] > 0.0)) st[s] = ST_CONV;  // zero load: u = 0 at once
       else st[s] = ST_ACTIVE;
       if (st[s] == ST_ACTIVE) ga[s / GS] = 1;
@@ -1761,7 +1763,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       UFEM_CUDA_TRY(cudaMemcpy(w.h_ff.data(), w.ff.p, w.S * sizeof(double), cudaMemcpyDeviceToHost));
       // a sample without load has u = 0, whatever its guess (fem/fem_eqs.c:108-116)
       for (int s = 0; s < w.nsamp; s++)
-        if (!(w.h_ff[s] > 0.0))
+        if (std::isfinite(w.h_ff[s]) && !(w.h_ff[s] > 0.0))
           UFEM_CUDA_TRY(cudaMemset2DAsync(w.x64.p + s, w.S * sizeof(double), 0, sizeof(double), m->nDOFAct));
     }
     UFEM_CUDA_TRY(cudaGetLastError());
@@ -1821,6 +1823,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
         switch (st[s]) {
           case ST_CONV: hs[s] = UFEM_ST_CONVERGED; break;
           case ST_BREAK: hs[s] = UFEM_ST_BREAKDOWN; break;
+          case ST_NAN: hs[s] = UFEM_ST_NAN; break;
           default: hs[s] = UFEM_ST_MAXIT; break;
         }
         hi[s] = (st[s] == ST_ACTIVE || st[s] == ST_MAXIT) ? its : itv[s];
