@@ -158,6 +158,17 @@ class ClockSampler:
                                           "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # nvidia-smi's start-up (NVML initialisation) must not fall into the
+        # timed region: wait for its first sample
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 5.0:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
@@ -370,7 +381,7 @@ def static_section(a, peak):
     cantilever (107,163 DOFs) and the 128x128x64 block (3,244,995 DOFs), each
     solved to true relative residual 1e-8 by the plain FP64 Jacobi PCG and by
     the FP32-inner / FP64-refinement PCG, with the error of each against a
-    FP64 solve to 1e-12.  Bytes are algorithmic (SURVEY formula): one FP64
+    FP64 solve to 1e-12.  Bytes are algorithmic (the block-sparse PCG count): one FP64
     PCG iteration reads nb*(72+4) + 4*(nbr+1) + 13*n*8 bytes, one FP32 inner
     iteration nb*(36+4) + 4*(nbr+1) + 13*n*4, one FP64 residual nb*(72+4) +
     4*(nbr+1) + 3*n*8."""

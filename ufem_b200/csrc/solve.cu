@@ -777,7 +777,7 @@ double true_relres(const DevMatrix &A, const double *d_b, const double *d_x) {
 // solves A d = r with an FP32 copy of the matrix and FP32 vectors (the same
 // persistent kernel, products and dots accumulated in FP64) to inner_tol
 // relative, and adds d to x in FP64.  Converged when |b - A x| / |b| <= eps,
-// always judged on the FP64 true residual.
+// always decided on the FP64 true residual.
 namespace {
 __global__ void k_to_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
