@@ -222,6 +222,8 @@ typedef struct ufem_mc_options {
   int unroll;                /* precision 2: neighbour gathers issued together, 2, 4 or 8 (0: tuned or 2) */
   int lane_samples;          /* precision 2: samples per lane, 2 or 4 (a sample group is 32x that;
                                 0: tuned or 4) */
+  int coarse;                /* precision 2: apply the model's coarse space (ufem_mc_set_coarse)
+                                when it has one (default 1); forces 4 samples per lane */
 } ufem_mc_options;
 void ufem_mc_default_options(ufem_mc_options *o);
 
@@ -249,6 +251,17 @@ int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp
                          long *const *d_iters, const double *const *d_u_guess,
                          double *const *d_u_out, const ufem_mc_options *opt);
 
+/* Coarse space of the batched solve's preconditioner (no reference
+ * counterpart): with d_Wc an nDOFAct x nmodes row-major FP64 device array,
+ * precision-2 solves of this model use M^-1 = D^-1 + Wc Wc^T (D the Jacobi
+ * diagonal of each sample) -- an additive two-level preconditioner; with
+ * Wc = Phi L^-T, L L^T = Phi^T K Phi, it corrects the residual on span(Phi).
+ * Both products run on the tensor cores (BF16 operands, FP32 accumulation);
+ * the iterate, residual and stopping test stay FP64.  nmodes: a multiple of
+ * 16, at most 128; 0 removes the coarse space.  Rows of supported DOFs are
+ * ignored.  The warm start sets one from its POD basis after training. */
+int ufem_mc_set_coarse(ufem_model *m, int nmodes, const double *d_Wc);
+
 /* Autotuner of the batched solve's launch shape (no reference counterpart):
  * times bounded runs (30 PCG iterations) of every candidate -- work tiles per
  * persistent block 3..48 and, for precision 2, 2/4/8 neighbour gathers in
@@ -275,6 +288,7 @@ typedef struct ufem_mc_stats {
   long pcg_launches;         /* persistent PCG launches (one per refinement step) */
   double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
   int tiles_per_block, unroll, lane_samples;  /* the launch shape used */
+  int coarse_modes;          /* modes of the coarse correction applied (0: Jacobi alone) */
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 
@@ -330,6 +344,10 @@ typedef struct ufem_warm_options {
                                 coefficients (Phi^T K Phi c = Phi^T f, assembled from the
                                 per-variable operators Phi^T K_v Phi; models with at most
                                 64 E variables, else the MLP's) */
+  int n_coarse;              /* the leading POD modes that become the coarse space of the
+                                PCG preconditioner after training (ufem_mc_set_coarse; at
+                                most n_modes, a multiple of 16; 0: none; default 64; models
+                                with at most 64 E variables) */
 } ufem_warm_options;
 
 typedef struct ufem_warm_train_stats {
@@ -340,6 +358,7 @@ typedef struct ufem_warm_train_stats {
   float loss_first, loss_last;  /* mean training loss of the first / last epoch */
   int epochs;
   long steps;
+  int coarse_modes;          /* modes of the coarse space set on the model (0: none) */
 } ufem_warm_train_stats;
 
 typedef struct ufem_warm_stats {

@@ -34,20 +34,22 @@ class Tables(C.Structure):
 class McOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iters", C.c_long),
                 ("replace_every", C.c_long), ("replace_near", C.c_double), ("use_graphs", C.c_int),
-                ("tiles_per_block", C.c_int), ("unroll", C.c_int), ("lane_samples", C.c_int)]
+                ("tiles_per_block", C.c_int), ("unroll", C.c_int), ("lane_samples", C.c_int),
+                ("coarse", C.c_int)]
 
 
 class WarmOptions(C.Structure):
     _fields_ = [("n_modes", C.c_int), ("n_hidden", C.c_int), ("n_feat", C.c_int), ("feat_cols", C.c_long * 32),
                 ("feat_log", C.c_int * 32), ("scale_col", C.c_long), ("n_snapshots", C.c_long),
                 ("power_iters", C.c_int), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
-                ("seed", C.c_ulonglong), ("guess_mode", C.c_int)]
+                ("seed", C.c_ulonglong), ("guess_mode", C.c_int), ("n_coarse", C.c_int)]
 
 
 class WarmTrainStats(C.Structure):
     _fields_ = [("cold_iters_max", C.c_long), ("cold_iters_mean", C.c_double), ("ms_solve", C.c_double),
                 ("ms_basis", C.c_double), ("ms_train", C.c_double), ("sigma2", C.c_double * 80),
-                ("loss_first", C.c_float), ("loss_last", C.c_float), ("epochs", C.c_int), ("steps", C.c_long)]
+                ("loss_first", C.c_float), ("loss_last", C.c_float), ("epochs", C.c_int), ("steps", C.c_long),
+                ("coarse_modes", C.c_int)]
 
 
 class WarmStats(C.Structure):
@@ -63,7 +65,7 @@ class McStats(C.Structure):
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
                 ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long),
                 ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16), ("tiles_per_block", C.c_int),
-                ("unroll", C.c_int), ("lane_samples", C.c_int)]
+                ("unroll", C.c_int), ("lane_samples", C.c_int), ("coarse_modes", C.c_int)]
 
 
 _SIGS = {
@@ -116,6 +118,7 @@ _SIGS = {
     "ufem_mc_autotune": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), _l, C.POINTER(C.c_void_p), C.POINTER(McOptions),
                                    C.c_char_p, C.POINTER(McOptions)]),
     "ufem_mc_solve_serial": (C.c_int, [C.c_void_p, C.c_long, _d, _d, _i, _l, C.c_double]),
+    "ufem_mc_set_coarse": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "ufem_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
     "ufem_mlp_free": (None, [C.c_void_p]),
     "ufem_mlp_num_params": (C.c_long, [C.c_void_p]),

@@ -34,6 +34,7 @@
 // iteration cap.  Per-sample scalars come from per-tile partials reduced in
 // a fixed order (run-to-run identical); partial buffers are double-buffered
 // by iteration parity so no block overwrites what another still reads.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +48,7 @@
 #include <vector>
 
 #include "device_util.cuh"
+#include "tcgen05.cuh"
 #include "ufem_internal.h"
 
 namespace ufem {
@@ -88,6 +90,10 @@ struct McPlan {
   DBuf<int> d_mult_col, cptr, crow;  // contributions of block k / of block row I
   DBuf<double> cval;               // [nc][cstride]: B*B values, then (multiplier << 32 | J)
   long nc = 0;
+  // coarse space of the preconditioner (ufem_mc_set_coarse): Wc [n][cmodes]
+  // as BF16 tensor-core operand tiles, supported rows zero
+  int cmodes = 0;
+  DBuf<uint8_t> wt1, wt3;
 };
 
 static std::vector<std::unique_ptr<McPlan>> g_plans;
@@ -605,6 +611,17 @@ struct BMesh {
   const double *mult;
   const unsigned char *fixed;
   int cstride;
+  // coarse correction of the preconditioner (precision 2, 128-sample groups):
+  // z = r / M + Wc c with c = Wc^T r, both products on the tensor cores
+  int n;                // scalar rows (nbr * B)
+  int cmodes;           // modes of Wc (0: Jacobi alone), a multiple of 16, at most 128
+  int nsplit, rps;      // c = Wc^T r runs as nsplit row ranges of rps rows (a multiple of 64) per group
+  const uint8_t *wt1;   // Wc^T, BF16 operand tiles of 64 rows: [ceil(n/64)][cmodes x 64]
+  const uint8_t *wt3;   // Wc, BF16 operand tiles of 128 rows: [ceil(n/128)][128 x cmodes]
+  uint8_t *cb;          // c of each group, BF16 operand tile: [ngroups][128 x cmodes]
+  float *cpart;         // partial c of each row range: [ngroups][nsplit][cmodes][128]
+  int *ccnt;            // [ngroups] row ranges finished
+  int *gcz;             // [ngroups] z has to be formed from r this iteration
 };
 
 template <typename T>
@@ -620,6 +637,11 @@ struct BArgs {
   long rr_every;      // at most this many iterations between replacements
   double near2;       // recursive |r|^2 <= near2 * (true |r|^2 at the last replacement) asks for one
   long *iter_out;
+  int coarse;          // some mesh has a coarse space (the launch holds TMEM and shared memory for it)
+  const int4 *c1items;  // (mesh, group, row range) of c = Wc^T r
+  int nc1;
+  const int4 *c3items;  // (mesh, group, 128-row chunk) of z = r / M + Wc c
+  int nc3;
 };
 
 // acc[a][v] += mult[var_c][s] * (W_c X_{J_c})[a] over the contributions
@@ -837,7 +859,8 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
                   M.part_rz + par * half, M.tot_rz + (size_t)par * M.S);
 }
 
-// x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z.
+// x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z (the
+// Jacobi part r.(r / M) when the mesh has a coarse space).
 template <typename T, int B, int VN>
 __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, const T *pnew,
                                             int par, double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
@@ -873,7 +896,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
       }
       st64<T, VN>(M.x + o, xi);
       stn<T, VN>(M.r + o, ri);
-      stn<T, VN>(M.z + o, zi);
+      if (!M.cmodes) stn<T, VN>(M.z + o, zi);  // with a coarse space z is formed after c = Wc^T r
     }
   }
   tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
@@ -947,10 +970,225 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
         rz[v] += (double)ri[v] * (double)zi[v];
       }
       stn<T, VN>(M.r + o, ri);
-      stn<T, VN>(M.z + o, zi);
+      if (!M.cmodes) stn<T, VN>(M.z + o, zi);
     }
   }
   tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
+}
+
+// ---------------------------------------------------------------------------
+// coarse correction of the preconditioner: M^-1 = D^-1 + Wc Wc^T
+// ---------------------------------------------------------------------------
+// Wc = Phi L^-T spans a coarse space (the POD basis of earlier solutions) and
+// is scaled by the Cholesky factor L of a mean reduced operator Phi^T K Phi,
+// so Wc Wc^T = Phi (Phi^T K Phi)^-1 Phi^T: the additive two-level
+// preconditioner (the AD variant of Tang, Nabben, Vuik & Erlangga 2009).
+// It removes the smooth modes that Jacobi PCG resolves last; symmetric
+// positive definite, so plain PCG applies.  Both products run per group of
+// 128 samples on the tensor cores (BF16 operands, FP32 accumulation): the
+// preconditioner need not be exact, and the residual, x and every dot
+// product stay FP64.  Per iteration:
+//   C1  c = Wc^T r   D[128 samples x cmodes] = R^T . Wc over row ranges; the
+//                    group's last range adds the partials in range order,
+//                    writes c (BF16 operand tile) and adds c.c to r.z
+//                    (r.z = r.(r / M) + |Wc^T r|^2 without reading z)
+//   C3  z = r / M + Wc c   D[128 samples x 128 rows] = c^T . Wc^T per chunk
+// TMEM lane = sample of the group, so every epilogue access of a warp covers
+// 32 consecutive samples of one row (256 contiguous bytes).
+constexpr int kCoarseMaxModes = 128;
+constexpr int kCoarseCols = 128;                    // TMEM columns per block
+constexpr int kCoarseStage = 32 * 1024;             // C1: A (128 x 64) + B (<= 128 x 64), BF16
+constexpr size_t kCoarseSmem = 2 * kCoarseStage;    // C1 double-buffered; C3 A + B (2 x 128 x 128 BF16)
+constexpr long kMmaSpinLimit = 1L << 24;
+constexpr int kErrMma = 2;                          // GridBar::err: a tensor-core wait ran out
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Leaves the kernel at the next grid barrier: every block sees the error.
+__device__ __forceinline__ void coarse_fail(GridBar *bar) { atomicExch(&bar->err, kErrMma); }
+
+// c = Wc^T r over row range `range` of group g (GS = 128 samples).
+__device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range, int par, uint32_t tmem,
+                                       uint64_t *bar, uint32_t &phase, uint8_t *sm, GridBar *gb) {
+  __shared__ int s_last;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nmod = M.cmodes, S = M.S;
+  const int r0 = range * M.rps, r1 = min(M.n, r0 + M.rps);
+  const int nch = (r1 - r0 + 63) / 64;
+  const uint32_t idesc = tc::idesc_bf16(128, nmod);
+  const int stage_b = nmod * 64 * 2;
+  const int m = tid & 127;  // sample of the group staged by this thread
+  const double *rcol = M.r + (size_t)g * 128 + m;
+  bool ok = true;
+  for (int ch = 0; ch < nch; ch++) {
+    uint8_t *sA = sm + (ch & 1) * kCoarseStage, *sB = sA + 128 * 64 * 2;
+    // A = R^T (128 samples x 64 rows): 8 rows of one sample per 16-byte store
+    const int rb = r0 + ch * 64;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int kg = (tid >> 7) + 2 * j;
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int row = rb + kg * 8 + e;
+        v[e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : 0.0;
+      }
+      uint4 pk;
+      pk.x = pack_bf16x2((float)v[0], (float)v[1]);
+      pk.y = pack_bf16x2((float)v[2], (float)v[3]);
+      pk.z = pack_bf16x2((float)v[4], (float)v[5]);
+      pk.w = pack_bf16x2((float)v[6], (float)v[7]);
+      *reinterpret_cast<uint4 *>(sA + tc::cm_offset(m, kg * 8, 64)) = pk;
+    }
+    // B = the chunk's Wc^T tile (cmodes x 64), stored in operand order
+    const uint4 *src = reinterpret_cast<const uint4 *>(M.wt1 + (size_t)(r0 / 64 + ch) * stage_b);
+    for (int i = tid; i < stage_b / 16; i += kThreads) reinterpret_cast<uint4 *>(sB)[i] = __ldg(src + i);
+    tc::fence_proxy_async();
+    // the MMAs of the previous chunk read the other buffer; wait for them
+    // before the next staging round overwrites it
+    if (ch > 0) {
+      ok = ok && tc::mbar_wait(bar, phase, kMmaSpinLimit);
+      phase ^= 1u;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < 4; ks++)
+        tc::mma_bf16(tmem, tc::desc_kmajor(tc::smem_u32(sA) + ks * 256, 128, 1024),
+                     tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, 1024), idesc, ch > 0 || ks > 0);
+      tc::commit(bar);
+    }
+  }
+  ok = ok && tc::mbar_wait(bar, phase, kMmaSpinLimit);
+  phase ^= 1u;
+  tc::fence_after_sync();
+  if (!ok) coarse_fail(gb);
+  // partial c -> cpart[g][range][mode][sample]
+  const int half = nmod / 2, k0 = (warp >> 2) * half, ms = (warp & 3) * 32 + lane;
+  float *dst = M.cpart + ((size_t)g * M.nsplit + range) * nmod * 128;
+  for (int kk = 0; kk < half; kk += 8) {
+    uint32_t v[8];
+    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(k0 + kk), v);
+#pragma unroll
+    for (int e = 0; e < 8; e++) __stcg(dst + (size_t)(k0 + kk + e) * 128 + ms, __uint_as_float(v[e]));
+  }
+  tc::fence_before_sync();
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(M.ccnt + g, 1) == M.nsplit - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // the group's last range: c = sum of the partials in range order; BF16
+  // operand tile for C3; c.c into the group's r.z
+  __shared__ double s_cc[kThreads];
+  const int kb = (tid >> 7) * half;
+  double cc = 0.0;
+  for (int kk = 0; kk < half; kk += 8) {
+    float c8[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int k = kb + kk + e;
+      float t = 0.0f;
+      for (int sp = 0; sp < M.nsplit; sp++)
+        t += __ldcg(M.cpart + (((size_t)g * M.nsplit + sp) * nmod + k) * 128 + m);
+      c8[e] = t;
+      cc += (double)t * (double)t;
+    }
+    uint4 pk;
+    pk.x = pack_bf16x2(c8[0], c8[1]);
+    pk.y = pack_bf16x2(c8[2], c8[3]);
+    pk.z = pack_bf16x2(c8[4], c8[5]);
+    pk.w = pack_bf16x2(c8[6], c8[7]);
+    __stcg(reinterpret_cast<uint4 *>(M.cb + (size_t)g * 128 * nmod * 2 + tc::cm_offset(m, kb + kk, nmod)), pk);
+  }
+  s_cc[tid] = cc;
+  __syncthreads();
+  if (tid < 128) {
+    double *rz = M.tot_rz + (size_t)par * S + (size_t)g * 128 + tid;
+    __stcg(rz, __ldcg(rz) + s_cc[tid] + s_cc[tid + 128]);
+  }
+  if (tid == 0) atomicExch(M.ccnt + g, 0);  // next used after a grid barrier
+  __syncthreads();
+}
+
+// z = r / M + Wc c on the 128-row chunk `chunk` of group g.
+__device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk, uint32_t tmem, uint64_t *bar,
+                                       uint32_t &phase, uint8_t *sm, GridBar *gb) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nmod = M.cmodes, S = M.S;
+  const int tbytes = 128 * nmod * 2;
+  uint8_t *sA = sm, *sB = sm + tbytes;
+  // A = c of the group (written in this launch: L2 loads), B = Wc rows of the chunk
+  const uint4 *ca = reinterpret_cast<const uint4 *>(M.cb + (size_t)g * tbytes);
+  const uint4 *wb = reinterpret_cast<const uint4 *>(M.wt3 + (size_t)chunk * tbytes);
+  for (int i = tid; i < tbytes / 16; i += kThreads) {
+    reinterpret_cast<uint4 *>(sA)[i] = __ldcg(ca + i);
+    reinterpret_cast<uint4 *>(sB)[i] = __ldg(wb + i);
+  }
+  tc::fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    tc::fence_after_sync();
+    const uint32_t idesc = tc::idesc_bf16(128, 128), sbo = (uint32_t)(nmod / 8) * 128;
+    for (int ks = 0; ks < nmod / 16; ks++)
+      tc::mma_bf16(tmem, tc::desc_kmajor(tc::smem_u32(sA) + ks * 256, 128, sbo),
+                   tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, sbo), idesc, ks > 0);
+    tc::commit(bar);
+  }
+  const bool ok = tc::mbar_wait(bar, phase, kMmaSpinLimit);
+  phase ^= 1u;
+  tc::fence_after_sync();
+  if (!ok) coarse_fail(gb);
+  // lanes = samples, columns = rows of the chunk; warps 4-7 take rows 64-127
+  const int ms = (warp & 3) * 32 + lane, j0 = (warp >> 2) * 64;
+  const size_t col = (size_t)g * 128 + ms;
+  const int rbase = chunk * 128 + j0;
+  for (int jj = 0; jj < 64; jj += 8) {
+    uint32_t v[8];
+    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + jj), v);
+    double rv[8], mv[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int row = rbase + jj + e;
+      if (row < M.n) {
+        rv[e] = __ldcg(M.r + (size_t)row * S + col);
+        mv[e] = __ldg(M.M + (size_t)row * S + col);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int row = rbase + jj + e;
+      if (row < M.n) M.z[(size_t)row * S + col] = rv[e] / mv[e] + (double)__uint_as_float(v[e]);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();  // the next item restages the operand tiles and reuses the accumulator
+}
+
+// Wc [n][cm] (FP64, row-major) -> the two BF16 operand tilings; supported rows zero
+__global__ void k_coarse_tiles(int n, int cm, const double *__restrict__ Wc, const unsigned char *__restrict__ fixed,
+                               __nv_bfloat16 *__restrict__ wt1, __nv_bfloat16 *__restrict__ wt3, int n64, int n128) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long tot1 = (long)n64 * 64 * cm, tot3 = (long)n128 * 128 * cm;
+  if (t < tot1) {
+    // wt1: tile q holds rows 64q..64q+63 as a cm x 64 operand (mode, row)
+    const int q = (int)(t / (64L * cm)), rem = (int)(t % (64L * cm));
+    const int k = rem / 64, j = rem % 64, row = q * 64 + j;
+    const double v = (row < n && !fixed[row]) ? Wc[(size_t)row * cm + k] : 0.0;
+    wt1[((size_t)q * 64 * cm * 2 + tc::cm_offset(k, j, 64)) / 2] = __float2bfloat16((float)v);
+  } else if (t < tot1 + tot3) {
+    // wt3: tile q holds rows 128q..128q+127 as a 128 x cm operand (row, mode)
+    const long u = t - tot1;
+    const int q = (int)(u / (128L * cm)), rem = (int)(u % (128L * cm));
+    const int j = rem / cm, k = rem % cm, row = q * 128 + j;
+    const double v = (row < n && !fixed[row]) ? Wc[(size_t)row * cm + k] : 0.0;
+    wt3[((size_t)q * 128 * cm * 2 + tc::cm_offset(j, k, cm)) / 2] = __float2bfloat16((float)v);
+  }
 }
 
 constexpr int kMaxMeshes = 8;
@@ -958,11 +1196,43 @@ constexpr int kMaxMeshes = 8;
 #ifndef UFEM_PCG_MIN_BLOCKS
 #define UFEM_PCG_MIN_BLOCKS 2
 #endif
-// UN: contributions whose gathers are issued together (implicit form);
-// VN: samples per lane (a sample group is 32 VN samples)
+// The coarse phases (precision 2 with 128-sample groups): C1 then C3 over the
+// groups whose z has to be formed from r; two grid barriers.
+template <typename T>
+__device__ __forceinline__ bool coarse_phases(const BArgs<T> &A, const BMesh<T> *s_meshes, int par, uint32_t tmem,
+                                              uint64_t *bar, uint32_t &phase, uint8_t *sm) {
+  __shared__ int s_go;
+  const int G = gridDim.x;
+  if constexpr (sizeof(T) == 8) {
+    for (int t = blockIdx.x; t < A.nc1; t += G) {
+      const int4 it = A.c1items[t];
+      const BMesh<T> &M = s_meshes[it.x];
+      if (threadIdx.x == 0) s_go = __ldcg(M.gcz + it.y);
+      __syncthreads();
+      const int go = s_go;
+      __syncthreads();
+      if (go) coarse_c1(M, it.y, it.z, par, tmem, bar, phase, sm, A.bar);
+    }
+    if (!grid_barrier(A.bar)) return false;
+    for (int t = blockIdx.x; t < A.nc3; t += G) {
+      const int4 it = A.c3items[t];
+      const BMesh<T> &M = s_meshes[it.x];
+      if (threadIdx.x == 0) s_go = __ldcg(M.gcz + it.y);
+      __syncthreads();
+      const int go = s_go;
+      __syncthreads();
+      if (go) coarse_c3(M, it.y, it.z, tmem, bar, phase, sm, A.bar);
+    }
+    if (!grid_barrier(A.bar)) return false;
+  }
+  return true;
+}
+
 template <typename T, int B, bool IMP, int UN, int VN>
-__global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_batch_pcg(BArgs<T> A) {
+__device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *mbar, uint8_t *sm) {
   constexpr int GS = 32 * VN;
+  constexpr bool kCoarse = IMP && VN == 4;
+  uint32_t mphase = 0;
   __shared__ double s_red[kWarps][GS];
   __shared__ double s_red2[kWarps][GS];
   __shared__ T s_sc[GS];
@@ -986,10 +1256,14 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
         M.gtrue[ti.y] = 1;
         M.glast[ti.y] = 0;
       }
+      if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
     }
     __syncthreads();
   }
   if (!grid_barrier(A.bar)) return;
+  if constexpr (kCoarse) {
+    if (A.coarse && !coarse_phases<T>(A, s_meshes, 0, tmem, mbar, mphase, sm)) return;
+  }
   long k;
   for (k = 1;; k++) {
     const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
@@ -1032,6 +1306,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
                (rr <= A.near2 * __ldcg(M.rrlast + s) || (!kFreeze && rr <= 0.25 * tol2));
         s_sc[sl] = upd ? (first ? T(0) : (T)(rzn / rzo)) : T(0);
         if (ti.z == 0) {  // the group's first tile records per-sample results
+          if (sl == 0 && M.cmodes) M.gcz[g] = 0;  // z was formed in the last coarse phase
           if (nst != st) {
             M.state[s] = nst;
             // a verified candidate keeps the count of the iterate it froze at
@@ -1104,6 +1379,7 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
       const T *pnew = (k & 1) ? M.p1 : M.p0;
       tile_update<T, B, VN>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
+      if (M.cmodes && threadIdx.x == 0) M.gcz[g] = 1;
     }
     if (!grid_barrier(A.bar)) return;
     // ---- phase R (when a group asked): replace the recursive residual -------
@@ -1123,13 +1399,47 @@ __global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_bat
           M.gtrue[ti.y] = 1;
           M.glast[ti.y] = (int)k;
         }
+        if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
       }
       if (!grid_barrier(A.bar)) return;
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(A.rcount, 0);  // read again only after the next U
     }
     if (remaining <= 0 || k > A.maxit + 1) break;
+    // ---- phases C1, C3 (coarse space): z = r / M + Wc Wc^T r ----------------
+    if constexpr (kCoarse) {
+      if (A.coarse && !coarse_phases<T>(A, s_meshes, par, tmem, mbar, mphase, sm)) return;
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
+}
+
+// UN: contributions whose gathers are issued together (implicit form);
+// VN: samples per lane (a sample group is 32 VN samples).  With a coarse
+// space the block holds kCoarseCols TMEM columns and kCoarseSmem bytes of
+// dynamic shared memory for the whole launch (at most 2 blocks per SM).
+template <typename T, int B, bool IMP, int UN, int VN>
+__global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_batch_pcg(BArgs<T> A) {
+  extern __shared__ __align__(1024) uint8_t s_dyn[];
+  __shared__ __align__(8) uint64_t s_mbar;
+  __shared__ uint32_t s_tmem;
+  constexpr bool kCoarse = IMP && VN == 4;
+  if constexpr (kCoarse) {
+    if (A.coarse) {
+      if (threadIdx.x == 0) tc::mbar_init(&s_mbar, 1);
+      if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s_tmem, kCoarseCols);
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+    }
+  }
+  pcg_body<T, B, IMP, UN, VN>(A, s_tmem, &s_mbar, s_dyn);
+  if constexpr (kCoarse) {
+    if (A.coarse) {
+      tc::fence_before_sync();
+      __syncthreads();
+      if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, kCoarseCols);
+    }
+  }
 }
 
 // outputs: RES_D (u), RES_R (reaction = internal force - F at the support),
@@ -1299,6 +1609,10 @@ struct McWork {
   DBuf<double> dr, dz, dp0, dp1, dq, pq, prr, prz, rho, rrlast;
   DBuf<int> state, iters, gactive, gtrue, gneed, glast, gcnt;
   DBuf<double> tpq, trr, trz;  // group totals of the PCG partials
+  // coarse correction: c per group (BF16 operand tiles), partial c per row range
+  DBuf<uint8_t> cb;
+  DBuf<float> cpart;
+  DBuf<int> ccnt, gcz;
   std::vector<double> h_ff;
 };
 
@@ -1357,7 +1671,15 @@ static void tune_save(const std::string &path) {
 
 // the batch shape a tuned choice is valid for: device, precision, element
 // family, and per mesh its block rows and padded sample count
-static std::string tune_key(int nmesh, ufem_model *const *models, const long *nsamp, int precision) {
+static int coarse_modes(int nmesh, ufem_model *const *models, const ufem_mc_options &opt) {
+  if (opt.precision != 2 || !opt.coarse) return 0;
+  int cm = 0;
+  for (int i = 0; i < nmesh; i++) cm = std::max(cm, get_plan(models[i])->cmodes);
+  return cm;
+}
+
+static std::string tune_key(int nmesh, ufem_model *const *models, const long *nsamp, int precision,
+                            int cmodes = 0) {
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1371,6 +1693,7 @@ static std::string tune_key(int nmesh, ufem_model *const *models, const long *ns
   for (int i = 0; i < nmesh; i++)
     k += "/" + std::to_string(models[i]->nbr) + "x" +
          std::to_string(std::max<long>(128, (nsamp[i] + 127) / 128 * 128));
+  if (cmodes) k += "/c" + std::to_string(cmodes);
   return k;
 }
 
@@ -1413,6 +1736,7 @@ extern "C" void ufem_mc_default_options(ufem_mc_options *o) {
   o->tiles_per_block = 0;
   o->unroll = 0;
   o->lane_samples = 0;
+  o->coarse = 1;
 }
 
 extern "C" int ufem_mc_get_stats(ufem_mc_stats *s) {
@@ -1462,11 +1786,18 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN> : k_batch_pcg<T, 2, IMP, 4, VN>;
     else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8, VN> : k_batch_pcg<T, 2, IMP, 8, VN>;
   }
-  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  // the coarse correction needs 128-sample groups (one UMMA M tile)
+  bool coarse = false;
+  if constexpr (IMP && VN == 4) coarse = coarse_modes(nmesh, models, opt) > 0;
+  const size_t dsmem = coarse ? kCoarseSmem : 0;
+  if (coarse) UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, dsmem));
   if (occ < 1) {
     set_error("batched PCG kernel does not fit on an SM");
     return UFEM_AF_ERR;
   }
+  // every resident block holds kCoarseCols of the SM's 512 TMEM columns
+  if (coarse) occ = std::min(occ, 512 / kCoarseCols);
   const int G = nsm * occ;
   // rows per tile: about tiles_per_block tiles per block over the whole batch
   long total_rows = 0;
@@ -1478,10 +1809,17 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   int rpt = (int)std::max<long>(kWarps, (total_rows + tpb * G - 1) / (tpb * G));
   rpt = (rpt + kWarps - 1) / kWarps * kWarps;
   int active_groups = 0;
+  std::vector<std::vector<int>> act(nmesh);  // active groups of each mesh
   for (int k = 0; k < nmesh; k++) {
     ufem_model *m = models[k];
     McWork &w = *W[k];
     BMesh<T> &b = hm[k];
+    b.n = (int)m->nDOFAct;
+    b.cmodes = b.nsplit = b.rps = 0;
+    b.wt1 = b.wt3 = nullptr;
+    b.cb = nullptr;
+    b.cpart = nullptr;
+    b.ccnt = b.gcz = nullptr;
     b.nbr = m->nbr;
     b.S = w.S;
     b.ngroups = w.S / GS;
@@ -1554,15 +1892,51 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     UFEM_CUDA_TRY(cudaMemsetAsync(w.iters.p, 0, w.S * sizeof(int)));
     UFEM_CUDA_TRY(cudaMemcpyAsync(w.gactive.p, ga.data(), b.ngroups * sizeof(int), cudaMemcpyHostToDevice));
     for (int g = 0; g < b.ngroups; g++)
-      if (ga[g])
+      if (ga[g]) {
+        act[k].push_back(g);
         for (int c = 0; c < b.ntpg; c++) tiles.push_back(make_int4(k, g, c, 0));
+      }
   }
   if (active_groups == 0) {
     *iters_run = 0;
     return UFEM_AF_OK;
   }
+  // coarse phases: about one wave of C1 row ranges over all active groups
+  std::vector<int4> c1items, c3items;
+  int max_cmodes = 0;
+  if (coarse) {
+    for (int k = 0; k < nmesh; k++) {
+      McPlan *P = plans[k];
+      BMesh<T> &b = hm[k];
+      McWork &w = *W[k];
+      if (P->cmodes <= 0) continue;
+      const int n = b.n, n64 = (n + 63) / 64, n128 = (n + 127) / 128;
+      int nsplit = std::max(1, std::min(n64, G / active_groups));
+      b.rps = (n64 + nsplit - 1) / nsplit * 64;
+      b.nsplit = (n + b.rps - 1) / b.rps;
+      b.cmodes = P->cmodes;
+      b.wt1 = P->wt1.p;
+      b.wt3 = P->wt3.p;
+      if ((rv = w.cb.ensure((size_t)b.ngroups * 128 * b.cmodes * 2)) ||
+          (rv = w.cpart.ensure((size_t)b.ngroups * b.nsplit * b.cmodes * 128)) ||
+          (rv = w.ccnt.ensure(b.ngroups)) || (rv = w.gcz.ensure(b.ngroups)))
+        return rv;
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.ccnt.p, 0, b.ngroups * sizeof(int)));
+      UFEM_CUDA_TRY(cudaMemsetAsync(w.gcz.p, 0, b.ngroups * sizeof(int)));
+      b.cb = w.cb.p;
+      b.cpart = w.cpart.p;
+      b.ccnt = w.ccnt.p;
+      b.gcz = w.gcz.p;
+      max_cmodes = std::max(max_cmodes, b.cmodes);
+      for (int g : act[k]) {
+        for (int sp = 0; sp < b.nsplit; sp++) c1items.push_back(make_int4(k, g, sp, 0));
+        for (int c = 0; c < n128; c++) c3items.push_back(make_int4(k, g, c, 0));
+      }
+    }
+  }
+  g_stats.coarse_modes = max_cmodes;
   DBuf<BMesh<T>> d_meshes;
-  DBuf<int4> d_tiles;
+  DBuf<int4> d_tiles, d_c1, d_c3;
   DBuf<GridBar> bar;
   DBuf<int> cnt, rcnt;
   DBuf<long> itout;
@@ -1570,6 +1944,9 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
       (rv = bar.alloc(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
       (rv = itout.alloc(1)))
+    return rv;
+  if (!c1items.empty() && ((rv = d_c1.upload(c1items.data(), c1items.size())) ||
+                           (rv = d_c3.upload(c3items.data(), c3items.size()))))
     return rv;
   UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
   BArgs<T> a;
@@ -1584,13 +1961,18 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   a.rr_every = std::max<long>(1, opt.replace_every);
   a.near2 = opt.replace_near * opt.replace_near;
   a.iter_out = itout.p;
+  a.coarse = !c1items.empty();
+  a.c1items = d_c1.p;
+  a.nc1 = (int)c1items.size();
+  a.c3items = d_c3.p;
+  a.nc3 = (int)c3items.size();
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0);
-  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kThreads), args, 0, 0));
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kThreads), args, a.coarse ? dsmem : 0, 0));
   cudaEventRecord(ev1);
   g_stats.kernel_launches += 1;
   long its = 0;
@@ -1605,7 +1987,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   g_stats.pcg_launch_ms[std::min<long>(g_stats.pcg_launches, 15)] = kms;
   g_stats.pcg_launches += 1;
   if (hb.err) {
-    set_error("batched PCG: grid barrier timed out");
+    set_error(hb.err == kErrMma ? "batched PCG: a tensor-core wait of the coarse correction timed out"
+                                : "batched PCG: grid barrier timed out");
     return UFEM_AF_ERR;
   }
   *iters_run = its;
@@ -1635,12 +2018,18 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       // S phase: values, 2 gathered and 2 own vectors in, 2 out; U phase:
       // M, r, p, q in, r, z out, x (FP64) in and out
       g_stats.pcg_bytes += (vals + 11.0 * vec + 2.0 * n * GS * sizeof(double)) * gi;
+      // coarse phases: C1 reads r, C3 reads r and M and writes z (U no
+      // longer writes z); the partial and BF16 c tiles of the group
+      const int cm = hm[k].cmodes;
+      if (cm) g_stats.pcg_bytes += (3.0 * vec + 2.0 * hm[k].nsplit * cm * 128 * 4.0 + 3.0 * 128 * cm * 2.0) * gi;
     }
     double idx = m->nnzb * 4.0 + 4.0 * (m->nbr + 1);
     // implicit: the shared contribution table, once per mesh-iteration
     if (IMP) idx += 4.0 * (m->nnzb + 1) + 8.0 * plans[k]->nc * plans[k]->cstride;
     g_stats.spmv_bytes += idx * mesh_its;
     g_stats.pcg_bytes += idx * mesh_its;
+    // the Wc tiles, once per mesh-iteration (both tilings)
+    if (hm[k].cmodes) g_stats.pcg_bytes += 2.0 * n * hm[k].cmodes * 2.0 * mesh_its;
   }
   return UFEM_AF_OK;
 }
@@ -1771,7 +2160,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   }
   // ---- launch shape: the caller's, else the autotuned one for this batch --
   if (opt.tiles_per_block <= 0 || (opt.precision == 2 && (opt.unroll <= 0 || opt.lane_samples <= 0))) {
-    const TuneEntry *t = tune_find(tune_key(nmesh, models, nsamp, opt.precision));
+    const TuneEntry *t = tune_find(tune_key(nmesh, models, nsamp, opt.precision, coarse_modes(nmesh, models, opt)));
     if (t) {
       if (opt.tiles_per_block <= 0) opt.tiles_per_block = t->tpb;
       if (opt.unroll <= 0) opt.unroll = t->unroll;
@@ -1782,7 +2171,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   long its = 0;
   if (opt.precision == 1) rv = run_pcg<float, false, 4>(nmesh, models, W, plans, opt, &its);
   // implicit form: 4 samples per lane unless 2 is asked for (measured best on B200)
-  else if (opt.precision == 2 && opt.lane_samples != 2) rv = run_pcg<double, true, 4>(nmesh, models, W, plans, opt, &its);
+  else if (opt.precision == 2 && (opt.lane_samples != 2 || coarse_modes(nmesh, models, opt) > 0))
+    rv = run_pcg<double, true, 4>(nmesh, models, W, plans, opt, &its);
   else if (opt.precision == 2) rv = run_pcg<double, true, 2>(nmesh, models, W, plans, opt, &its);
   else rv = run_pcg<double, false, 2>(nmesh, models, W, plans, opt, &its);
   if (rv != UFEM_AF_OK) return rv;
@@ -1863,6 +2253,7 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
   if (base.precision == 2) {
     unrolls = {2, 4, 8};
     lanes = {2, 4};
+    if (coarse_modes(nmesh, models, base) > 0) lanes = {4};  // the coarse correction needs 128-sample groups
   } else {
     unrolls = {4};
     lanes = {0};
@@ -1890,7 +2281,7 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
         best_ln = ln;
       }
     }
-  const std::string key = tune_key(nmesh, models, nsamp, base.precision);
+  const std::string key = tune_key(nmesh, models, nsamp, base.precision, coarse_modes(nmesh, models, base));
   bool found = false;
   for (auto &t : g_tune)
     if (t.key == key) {
@@ -1905,6 +2296,31 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
     best->unroll = best_un;
     best->lane_samples = best_ln;
   }
+  return UFEM_AF_OK;
+}
+
+extern "C" int ufem_mc_set_coarse(ufem_model *m, int nmodes, const double *d_Wc) {
+  if (!m) return UFEM_AF_ERR_EMP;
+  McPlan *P = get_plan(m);
+  if (nmodes == 0) {
+    P->cmodes = 0;
+    return UFEM_AF_OK;
+  }
+  if (nmodes < 16 || nmodes > kCoarseMaxModes || nmodes % 16 || !d_Wc) {
+    set_error("ufem_mc_set_coarse: nmodes a multiple of 16 up to 128 and a device array of nDOFAct x nmodes");
+    return UFEM_AF_ERR_VAL;
+  }
+  int rv;
+  const int n = (int)m->nDOFAct, n64 = (n + 63) / 64, n128 = (n + 127) / 128;
+  if ((rv = P->wt1.ensure((size_t)n64 * 64 * nmodes * 2)) || (rv = P->wt3.ensure((size_t)n128 * 128 * nmodes * 2)))
+    return rv;
+  const long tot = (long)n64 * 64 * nmodes + (long)n128 * 128 * nmodes;
+  k_coarse_tiles<<<(unsigned)((tot + 255) / 256), 256>>>(n, nmodes, d_Wc, m->d_fixed.p,
+                                                         reinterpret_cast<__nv_bfloat16 *>(P->wt1.p),
+                                                         reinterpret_cast<__nv_bfloat16 *>(P->wt3.p), n64, n128);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  P->cmodes = nmodes;
   return UFEM_AF_OK;
 }
 

@@ -30,6 +30,7 @@
 #include <random>
 #include <vector>
 
+#include "tcgen05.cuh"
 #include "ufem_internal.h"
 
 namespace ufem {
@@ -62,29 +63,10 @@ struct GemmArgs {
   int *err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// canonical K-major, no-swizzle UMMA shared-memory descriptor (version 1)
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-  return d;               // base offset 0, legacy LBO mode, SWIZZLE_NONE
-}
-
-// instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major
-__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
+using tc::smem_u32;
 
 // byte offset of element (r, k) of an R x KC tile in the core-matrix layout
-__device__ __forceinline__ uint32_t cm_offset(int r, int k) {
-  return (uint32_t)(((r >> 3) * (kKC / 8) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
-}
+__device__ __forceinline__ uint32_t cm_offset(int r, int k) { return tc::cm_offset(r, k, kKC); }
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -106,19 +88,14 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
   const int ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
   if (threadIdx.x == 0) {
     s_bad = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;");
+    tc::mbar_init(&mbar, 1);
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;");
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  tc::fence_before_sync();
   __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
+  tc::fence_after_sync();
   const uint32_t tmem = tmem_base;
-  const uint32_t idesc = umma_idesc(kTileM, N);
+  const uint32_t idesc = tc::idesc_bf16(kTileM, N);
   const uint32_t sbo = (kKC / 8) * 128;
   uint32_t phase = 0;
   const int nchunks = (g.K + kKC - 1) / kKC;
@@ -140,58 +117,30 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
       *reinterpret_cast<__nv_bfloat16 *>(sB + cm_offset(r, k)) = v;
     }
     // make the generic-proxy shared stores visible to the tensor core
-    asm volatile("fence.proxy.async.shared::cta;");
+    tc::fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;");
+      tc::fence_after_sync();
       for (int ks = 0; ks < kKC / 16; ks++) {
-        const uint64_t da = umma_desc(smem_u32(sA) + ks * 256, 128, sbo);
-        const uint64_t db = umma_desc(smem_u32(sB) + ks * 256, 128, sbo);
-        const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
-        asm volatile(
-            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        const uint64_t da = tc::desc_kmajor(smem_u32(sA) + ks * 256, 128, sbo);
+        const uint64_t db = tc::desc_kmajor(smem_u32(sB) + ks * 256, 128, sbo);
+        tc::mma_bf16(tmem, da, db, idesc, c > 0 || ks > 0);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(&mbar)));
+      tc::commit(&mbar);
     }
     // wait for the MMAs of this chunk (they also release the staged tiles)
-    {
-      uint32_t done = 0;
-      long spins = 0;
-      while (!done) {
-        asm volatile(
-            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.b32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(smem_u32(&mbar)), "r"(phase));
-        if (!done && ++spins > kSpinLimit) {
-          s_bad = 1;
-          break;
-        }
-      }
-      phase ^= 1u;
-    }
+    if (!tc::mbar_wait(&mbar, phase, kSpinLimit)) s_bad = 1;
+    phase ^= 1u;
     __syncthreads();
     if (s_bad) break;
   }
-  asm volatile("tcgen05.fence::after_thread_sync;");
+  tc::fence_after_sync();
   if (!s_bad) {
     // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows m0+32w+lane
     const int m = m0 + warp * 32 + lane;
     for (int c0 = 0; c0 < N; c0 += 32) {
       uint32_t v[32];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-            "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-            "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;");
+      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       if (m < g.M) {
 #pragma unroll
         for (int j = 0; j < 32; j++) {
@@ -222,9 +171,9 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
       }
     }
   }
-  asm volatile("tcgen05.fence::before_thread_sync;");
+  tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
   if (threadIdx.x == 0 && s_bad) atomicExch(g.err, 1);
 }
 

@@ -558,6 +558,7 @@ struct ufem_warm {
   DBuf<int> d_mcol, d_ovar;
   int novr = 0;
   double guess_scale = 1.0;
+  int coarse_modes = 0;                   // modes of the preconditioner's coarse space
   // basis and normalisation
   DBuf<double> phi;                       // [n][r]
   DBuf<double> fmean, fsd, cmean, csd;    // feature / coefficient statistics
@@ -715,6 +716,79 @@ int build_galerkin(ufem_warm *w) {
   return UFEM_AF_OK;
 }
 
+// Coarse space of the batched PCG's preconditioner from the leading rc POD
+// modes: Wc = Phi_c L^-T with L L^T = Phi_c^T Kbar Phi_c, Kbar the stiffness
+// at the training samples' mean multipliers (sum_v mean(a_v) G_v, the
+// Galerkin operators above), so Wc Wc^T = Phi_c (Phi_c^T Kbar Phi_c)^-1
+// Phi_c^T.  One operator serves every sample: the preconditioner only has to
+// be a fixed symmetric positive definite map.  Pivots below 1e-13 of the
+// largest drop their mode.
+int build_coarse(ufem_warm *w, long ntrain, const double *d_ifld) {
+  const int rc = std::min(w->o.n_coarse, w->r);
+  w->coarse_modes = 0;
+  if (!w->galerkin || rc < 16) return ufem_mc_set_coarse(w->m, 0, nullptr);
+  int rv;
+  const int r = w->r, nmult = w->nmult;
+  const long ilen = w->m->mc_ilen;
+  std::vector<int> mcol(nmult);
+  std::vector<double> ifl((size_t)ntrain * ilen), G((size_t)nmult * r * r);
+  UFEM_CUDA_TRY(cudaMemcpy(mcol.data(), w->d_mcol.p, nmult * sizeof(int), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(ifl.data(), d_ifld, ifl.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(G.data(), w->Gv.p, G.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<double> abar(nmult, 1.0);
+  for (int v = 1; v < nmult; v++) {
+    double t = 0.0;
+    for (long s = 0; s < ntrain; s++) t += ifl[(size_t)s * ilen + mcol[v]];
+    abar[v] = t / (double)ntrain;
+  }
+  // Ebar (rc x rc), then its Cholesky factor in place (lower triangle)
+  std::vector<double> L((size_t)rc * rc, 0.0);
+  for (int i = 0; i < rc; i++)
+    for (int j = 0; j < rc; j++) {
+      double t = 0.0;
+      for (int v = 0; v < nmult; v++) t += abar[v] * G[(size_t)v * r * r + (size_t)i * r + j];
+      L[(size_t)i * rc + j] = t;
+    }
+  double dmax = 0.0;
+  for (int i = 0; i < rc; i++) dmax = std::max(dmax, std::fabs(L[(size_t)i * rc + i]));
+  std::vector<char> skip(rc, 0);
+  for (int j = 0; j < rc; j++) {
+    double d = L[(size_t)j * rc + j];
+    for (int k = 0; k < j; k++) d -= L[(size_t)j * rc + k] * L[(size_t)j * rc + k];
+    skip[j] = !(d > 1e-13 * dmax);
+    const double ljj = skip[j] ? 1.0 : std::sqrt(d);
+    L[(size_t)j * rc + j] = ljj;
+    for (int i = j + 1; i < rc; i++) {
+      double t = L[(size_t)i * rc + j];
+      for (int k = 0; k < j; k++) t -= L[(size_t)i * rc + k] * L[(size_t)j * rc + k];
+      L[(size_t)i * rc + j] = skip[j] ? 0.0 : t / ljj;
+    }
+    for (int k = 0; k < j; k++) L[(size_t)k * rc + j] = 0.0;
+  }
+  // T = L^-T (column j of T = row j of L^-1); a dropped mode is a zero column
+  std::vector<double> T((size_t)rc * rc, 0.0);
+  for (int j = 0; j < rc; j++) {
+    // solve L y = e_j; y = column j of L^-1 = row j of T
+    std::vector<double> y(rc, 0.0);
+    for (int i = j; i < rc; i++) {
+      double t = (i == j) ? 1.0 : 0.0;
+      for (int k = j; k < i; k++) t -= L[(size_t)i * rc + k] * y[k];
+      y[i] = t / L[(size_t)i * rc + i];
+    }
+    for (int i = 0; i < rc; i++) T[(size_t)j * rc + i] = y[i];
+  }
+  for (int j = 0; j < rc; j++)
+    if (skip[j])
+      for (int i = 0; i < rc; i++) T[(size_t)i * rc + j] = 0.0;
+  DBuf<double> dT, Wc;
+  if ((rv = dT.upload(T.data(), T.size())) || (rv = Wc.ensure((size_t)w->n * rc))) return rv;
+  // Wc [n][rc] = Phi[:, :rc] T
+  if ((rv = gemm_f64((int)w->n, rc, rc, w->phi.p, r, 1, dT.p, rc, 1, Wc.p, rc, 1, w->part))) return rv;
+  if ((rv = ufem_mc_set_coarse(w->m, rc, Wc.p))) return rv;
+  w->coarse_modes = rc;
+  return UFEM_AF_OK;
+}
+
 // standardised network inputs of nsamp samples into w->X (FP32 [nsamp][n_feat]);
 // with fit = true the feature statistics are (re)computed from these samples
 int make_inputs(ufem_warm *w, long nsamp, const double *d_ifld, bool fit) {
@@ -778,6 +852,7 @@ void ufem_warm_default_options(ufem_warm_options *o) {
   o->lr = 2e-3f;
   o->seed = 20261203ULL;
   o->guess_mode = 0;
+  o->n_coarse = 64;
 }
 
 int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out) {
@@ -787,9 +862,10 @@ int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out)
     return UFEM_AF_ERR_EMP;
   }
   if (o->n_modes < 16 || o->n_modes % 16 || o->n_modes + 16 > kMaxL || o->n_feat < 1 || o->n_feat > 32 ||
-      o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 || o->n_snapshots < o->n_modes + 16) {
+      o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 || o->n_snapshots < o->n_modes + 16 ||
+      o->n_coarse < 0 || o->n_coarse % 16) {
     set_error("ufem_warm_create: n_modes a multiple of 16 up to 80, 1..32 inputs, n_hidden a multiple of 16 up to "
-              "256, n_snapshots >= n_modes + 16");
+              "256, n_snapshots >= n_modes + 16, n_coarse a multiple of 16");
     return UFEM_AF_ERR_SIZ;
   }
   for (int f = 0; f < o->n_feat; f++)
@@ -850,7 +926,12 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   const long n = w->n;
   const int r = w->r;
   ufem_model *m = w->m;
-  // 1. cold batched solves of every training sample -> U [n][ntrain]
+  // 1. cold batched solves of every training sample -> U [n][ntrain], Jacobi
+  // PCG alone (the cap of the warm runs is the cold iteration count)
+  ufem_mc_options cold;
+  if (opt) cold = *opt;
+  else ufem_mc_default_options(&cold);
+  cold.coarse = 0;
   cudaEventRecord(e0);
   if ((rv = w->U.ensure((size_t)n * ntrain)) || (rv = w->st.ensure(ntrain)) || (rv = w->it.ensure(ntrain))) return rv;
   {
@@ -864,7 +945,7 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
       double *pu = uchunk.p;
       int *ps = w->st.p + c0;
       long *pi = w->it.p + c0;
-      if ((rv = mc_solve_device(1, &m, &cn, &pin, nullptr, &ps, &pi, nullptr, &pu, opt))) return rv;
+      if ((rv = mc_solve_device(1, &m, &cn, &pin, nullptr, &ps, &pi, nullptr, &pu, &cold))) return rv;
       UFEM_CUDA_TRY(cudaMemcpy2DAsync(w->U.p + c0, ntrain * sizeof(double), uchunk.p, S * sizeof(double),
                                       cn * sizeof(double), n, cudaMemcpyDeviceToDevice));
     }
@@ -885,15 +966,18 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
       sum += (double)hi[s];
     }
     w->cold_cap = mx;
-    w->train_precision = opt ? opt->precision : 1;
+    w->train_precision = cold.precision;
     st.cold_iters_max = mx;
     st.cold_iters_mean = sum / (double)ntrain;
   }
   st.ms_solve = ms_since(e0);
   // 2. POD basis from the first n_snapshots solutions
   cudaEventRecord(e0);
-  if ((rv = fit_basis(w, (int)ntrain, w->o.n_snapshots)) || (rv = build_galerkin(w))) return rv;
+  if ((rv = fit_basis(w, (int)ntrain, w->o.n_snapshots)) || (rv = build_galerkin(w)) ||
+      (rv = build_coarse(w, ntrain, d_ifld)))
+    return rv;
   st.ms_basis = ms_since(e0);
+  st.coarse_modes = w->coarse_modes;
   for (int k = 0; k < r && k < 80; k++) st.sigma2[k] = w->sigma2[k];
   // 3. inputs and targets
   cudaEventRecord(e0);

@@ -66,7 +66,7 @@ def default_options():
 def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1, tol: float = 1e-8,
              max_iters: int | None = None, replace_every: int | None = None, replace_near: float | None = None,
              u_guess: list[np.ndarray | None] | None = None, olens: list[int] | None = None,
-             tiles_per_block: int = 0, unroll: int = 0, lane_samples: int = 0):
+             tiles_per_block: int = 0, unroll: int = 0, lane_samples: int = 0, coarse: int = 1):
     """Batched solve of every sample of every mesh in one launch.
 
     Returns per mesh (ofld[nsamp, olen], status[nsamp], iters[nsamp]) and the
@@ -85,6 +85,7 @@ def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1
     opt.tiles_per_block = tiles_per_block
     opt.unroll = unroll
     opt.lane_samples = lane_samples
+    opt.coarse = coarse
     keep = []
     hs = (C.c_void_p * nm)(*[m.h.value for m in models])
     ns = np.array([f.shape[0] for f in iflds], np.int64)
@@ -115,6 +116,20 @@ def mc_solve(models: list[GpuModel], iflds: list[np.ndarray], precision: int = 1
     L.ufem_mc_get_stats(C.byref(stats))
     res = [(o[:, :olen], st, it) for (o, st, it, olen) in outs]
     return res, stats
+
+
+def set_coarse(model: GpuModel, Wc) -> None:
+    """Coarse space of the preconditioner of ``model``'s precision-2 solves,
+    M^-1 = D^-1 + Wc Wc^T (``ufem_mc_set_coarse``); ``Wc`` [nDOFAct x m]
+    (m a multiple of 16, at most 128), or None to remove it."""
+    import torch
+    L = _lib.load()
+    if Wc is None:
+        _lib.check("ufem_mc_set_coarse", L.ufem_mc_set_coarse(model.h, 0, None))
+        return
+    d = torch.as_tensor(np.ascontiguousarray(Wc, np.float64)).cuda()
+    _lib.check("ufem_mc_set_coarse", L.ufem_mc_set_coarse(model.h, int(d.shape[1]), C.c_void_p(d.data_ptr())))
+    torch.cuda.synchronize()
 
 
 def stats_dict(s) -> dict:

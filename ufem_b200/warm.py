@@ -66,10 +66,11 @@ class WarmStart:
             self.h = None
 
     @staticmethod
-    def _mc_opts(precision, tol):
+    def _mc_opts(precision, tol, coarse=True):
         opt = default_options()
         opt.precision = precision
         opt.tol = tol
+        opt.coarse = int(bool(coarse))
         return opt
 
     def train(self, ifld, precision: int = 1, tol: float = 1e-8) -> dict:
@@ -95,8 +96,10 @@ class WarmStart:
     def set_guess_scale(self, factor: float) -> None:
         _lib.check("ufem_warm_set_guess_scale", self.L.ufem_warm_set_guess_scale(self.h, float(factor)))
 
-    def solve(self, ifld, precision: int = 1, tol: float = 1e-8):
-        """Warm-started batched solve: (ofld, status, iters, stats)."""
+    def solve(self, ifld, precision: int = 1, tol: float = 1e-8, coarse: bool = True):
+        """Warm-started batched solve: (ofld, status, iters, stats).  With
+        ``coarse`` (precision 2) the preconditioner adds the coarse correction
+        on the leading POD modes that training set on the model."""
         import torch
         d = _dev(ifld, torch.float64)
         n = d.shape[0]
@@ -105,7 +108,7 @@ class WarmStart:
         st = torch.zeros(n, dtype=torch.int32, device="cuda")
         it = torch.zeros(n, dtype=torch.int64, device="cuda")
         ws = _lib.WarmStats()
-        opt = self._mc_opts(precision, tol)
+        opt = self._mc_opts(precision, tol, coarse)
         _lib.check("ufem_warm_solve", self.L.ufem_warm_solve(self.h, n, d.data_ptr(), of.data_ptr(), st.data_ptr(),
                                                              it.data_ptr(), C.byref(opt), C.byref(ws)))
         return (of.cpu().numpy()[:, :self.model.model.mc_olen], st.cpu().numpy(), it.cpu().numpy(), _fields(ws))
