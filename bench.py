@@ -79,6 +79,10 @@ def parse():
     p.add_argument("--plain-samples", type=int, default=16, help="samples timed by the plain method")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
+    p.add_argument("--no-coarse", action="store_true",
+                   help="headline without the coarse correction of the preconditioner (Jacobi PCG)")
+    p.add_argument("--coarse-modes", type=int, default=80,
+                   help="POD modes of the preconditioner's coarse space (a multiple of 16, at most 80)")
     p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--guess", type=int, default=1,
@@ -466,8 +470,8 @@ def ours(a):
     m, train, ev = warm_setup(a, rank)
     g = GpuModel(m)
     cols, logs, scale_col = mg.warm_features(m)
-    ws = WarmStart(g, cols, logs, scale_col, n_modes=64, n_hidden=256, n_snapshots=512, epochs=a.epochs,
-                   batch=256, lr=2e-3)
+    ws = WarmStart(g, cols, logs, scale_col, n_modes=max(64, a.coarse_modes), n_hidden=256, n_snapshots=512,
+                   epochs=a.epochs, batch=256, lr=2e-3, n_coarse=a.coarse_modes)
     t0 = time.perf_counter()
     tstats = ws.train(train, precision=a.precision)
     torch.cuda.synchronize()
@@ -477,6 +481,7 @@ def ours(a):
     opt = default_options()
     opt.precision = a.precision
     opt.tol = 1e-8
+    opt.coarse = 0 if a.no_coarse else 1
     n = ev.shape[0]
     olen = m.mc_olen
     d_in = torch.from_numpy(ev).to(dev)
@@ -545,20 +550,59 @@ def ours(a):
     d_out2 = torch.zeros_like(d_out)
     d_st2 = torch.zeros_like(d_st)
     d_it2 = torch.zeros_like(d_it)
-    cold_args = (1, (C.c_void_p * 1)(g.h.value), one, _vp([d_in]), _vp([d_out2]), _vp([d_st2]), _vp([d_it2]),
-                 (C.c_void_p * 1)(), (C.c_void_p * 1)(), C.byref(opt))
-    torch.cuda.synchronize()
-    e0.record()
-    _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*cold_args))
-    e1.record()
-    torch.cuda.synchronize()
-    cold_ms = e0.elapsed_time(e1)
-    it_cold = d_it2.cpu().numpy()
-    out_cold = d_out2.cpu().numpy()
-    cold = {"value": n / (cold_ms / 1000.0), "unit": "solves/s", "iters_mean": float(it_cold.mean()),
-            "iters_max": int(it_cold.max()), "all_converged": bool((d_st2.cpu().numpy() == 0).all()),
-            "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
+
+    def cold_run(coarse):
+        o = default_options()
+        o.precision = a.precision
+        o.tol = 1e-8
+        o.coarse = coarse
+        cold_args = (1, (C.c_void_p * 1)(g.h.value), one, _vp([d_in]), _vp([d_out2]), _vp([d_st2]), _vp([d_it2]),
+                     (C.c_void_p * 1)(), (C.c_void_p * 1)(), C.byref(o))
+        torch.cuda.synchronize()
+        e0.record()
+        _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(*cold_args))
+        e1.record()
+        torch.cuda.synchronize()
+        cold_ms = e0.elapsed_time(e1)
+        it_cold = d_it2.cpu().numpy()
+        out_cold = d_out2.cpu().numpy()
+        return {"value": n / (cold_ms / 1000.0), "unit": "solves/s", "iters_mean": float(it_cold.mean()),
+                "iters_max": int(it_cold.max()), "all_converged": bool((d_st2.cpu().numpy() == 0).all()),
+                "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
+
+    # Jacobi PCG from zero: the batched solver alone
+    cold = cold_run(0)
+    cold["method"] = "Jacobi PCG from zero"
+    cold_coarse = None
+    if tstats["coarse_modes"] and opt.coarse:
+        cold_coarse = cold_run(1)
+        cold_coarse["method"] = f"PCG from zero, Jacobi + coarse correction on {tstats['coarse_modes']} POD modes"
     del d_out2, d_st2, d_it2
+
+    # ---- the warm start without the coarse correction -----------------------
+    no_coarse = None
+    if tstats["coarse_modes"] and opt.coarse and not a.no_other:
+        opt_nc = default_options()
+        opt_nc.precision = a.precision
+        opt_nc.tol = 1e-8
+        opt_nc.coarse = 0
+        wst4 = _lib.WarmStats()
+        args4 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt_nc),
+                 C.byref(wst4))
+        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args4))
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args4))
+        e1.record()
+        torch.cuda.synchronize()
+        ms4 = e0.elapsed_time(e1) / a.steps
+        no_coarse = {"method": "same warm start, Jacobi PCG (no coarse correction)", "value": n / (ms4 / 1000.0),
+                     "unit": "solves/s", "iters_mean": wst4.iters_mean, "iters_max": wst4.iters_max,
+                     "pcg_GBs": wst4.pcg_bytes / (wst4.pcg_ms / 1000.0) / 1e9 if wst4.pcg_ms else None,
+                     "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
+                     "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
+                                                               / np.abs(out_warm).max())}
 
     # ---- the other guess (MLP <-> POD-Galerkin), same precision ------------
     GUESS = {0: "the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> 64 coefficients)",
@@ -664,7 +708,8 @@ def ours(a):
                                    "explicit FP32 values 34 GB per iteration, >> 126 MB L2",
                        "parallelism": f"samples sharded over {world} GPU(s), no collective"},
             "all_converged": bool(np.isin(status, [0, 4]).all()),
-            "warm_start": {"guess": GUESS[a.guess], "iters_mean": float(iters.mean()), "iters_max": int(iters.max()),
+            "warm_start": {"guess": GUESS[a.guess], "coarse_modes": tstats["coarse_modes"] if opt.coarse else 0,
+                           "iters_mean": float(iters.mean()), "iters_max": int(iters.max()),
                            "cold_iters_mean": cold["iters_mean"],
                            "iterations_saved_frac": 1.0 - float(iters.mean()) / cold["iters_mean"],
                            "guess_rel_err_mean": warm_info["guess_err_mean"],
@@ -678,6 +723,8 @@ def ours(a):
                                      "loss_first": tstats["loss_first"], "loss_last": tstats["loss_last"],
                                      "pod_energy_mode64_over_mode1": (s2[63] / s2[0]) if s2[0] else None}},
             "batched_without_warm_start": cold,
+            "batched_coarse_without_guess": cold_coarse,
+            "warm_start_without_coarse": no_coarse,
             "warm_start_other_precisions": other,
             "warm_start_other_guess": galerkin,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),

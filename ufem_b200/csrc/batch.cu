@@ -353,7 +353,6 @@ static int build_implicit(ufem_model *m, McPlan *P) {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
 
 template <typename T>
 struct VecOf;
@@ -621,7 +620,7 @@ struct BMesh {
   uint8_t *cb;          // c of each group, BF16 operand tile: [ngroups][128 x cmodes]
   float *cpart;         // partial c of each row range: [ngroups][nsplit][cmodes][128]
   int *ccnt;            // [ngroups] row ranges finished
-  int *gcz;             // [ngroups] z has to be formed from r this iteration
+  int *gcz;             // [ngroups] z = r / M was written this iteration: add Wc c
 };
 
 template <typename T>
@@ -640,7 +639,7 @@ struct BArgs {
   int coarse;          // some mesh has a coarse space (the launch holds TMEM and shared memory for it)
   const int4 *c1items;  // (mesh, group, row range) of c = Wc^T r
   int nc1;
-  const int4 *c3items;  // (mesh, group, 128-row chunk) of z = r / M + Wc c
+  const int4 *c3items;  // (mesh, group, 128-row chunk) of z += Wc c
   int nc3;
 };
 
@@ -732,7 +731,7 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 // samples; pnew = p on the own rows; partial p.q per sample.  Explicit form:
 // p is formed at every gathered neighbour.  Implicit form: q = A z + beta
 // q_old (A p_old is the previous q), so only z is gathered.
-template <typename T, int B, bool IMP, int UN, int VN>
+template <typename T, int B, bool IMP, int UN, int VN, int NW>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VN]) {
   static_assert(!IMP || sizeof(T) == 8, "the implicit form runs in FP64");
@@ -747,7 +746,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   double pq[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) pq[v] = 0;
-  for (int I = row0 + warp; I < row1; I += kWarps) {
+  for (int I = row0 + warp; I < row1; I += NW) {
     T acc[B][VN];
 #pragma unroll
     for (int a = 0; a < B; a++)
@@ -825,14 +824,14 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   __syncthreads();
   if (threadIdx.x < GS) {
     double t = 0;
-    for (int w = 0; w < kWarps; w++) t += s_red[w][threadIdx.x];
+    for (int w = 0; w < NW; w++) t += s_red[w][threadIdx.x];
     M.part_pq[((size_t)g * M.ntpg + chunk) * GS + threadIdx.x] = t;
   }
   group_close<GS>(M.gcnt + 2 * g, M.ntpg, g, M.part_pq, M.tot_pq, nullptr, nullptr);
 }
 
 // Writes the tile's r.r and r.z partials of parity slot `par`.
-template <typename T, int VN>
+template <typename T, int VN, int NW>
 __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chunk, int par, const double (&rr)[VN],
                                               const double (&rz)[VN], double (*s_red)[32 * VN],
                                               double (*s_red2)[32 * VN]) {
@@ -846,7 +845,7 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
   __syncthreads();
   if (threadIdx.x < GS) {
     double a = 0, b = 0;
-    for (int w = 0; w < kWarps; w++) {
+    for (int w = 0; w < NW; w++) {
       a += s_red[w][threadIdx.x];
       b += s_red2[w][threadIdx.x];
     }
@@ -861,7 +860,7 @@ __device__ __forceinline__ void tile_partials(const BMesh<T> &M, int g, int chun
 
 // x += alpha p (FP64), r -= alpha q, z = r / M; partial r.r and r.z (the
 // Jacobi part r.(r / M) when the mesh has a coarse space).
-template <typename T, int B, int VN>
+template <typename T, int B, int VN, int NW>
 __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk, const T *s_alpha, const T *pnew,
                                             int par, double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
   constexpr int GS = 32 * VN;
@@ -875,7 +874,7 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
-  for (int I = row0 + warp; I < row1; I += kWarps) {
+  for (int I = row0 + warp; I < row1; I += NW) {
 #pragma unroll
     for (int a = 0; a < B; a++) {
       const size_t o = (size_t)(I * B + a) * S + sb;
@@ -896,15 +895,15 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
       }
       st64<T, VN>(M.x + o, xi);
       stn<T, VN>(M.r + o, ri);
-      if (!M.cmodes) stn<T, VN>(M.z + o, zi);  // with a coarse space z is formed after c = Wc^T r
+      stn<T, VN>(M.z + o, zi);  // with a coarse space the C3 phase adds Wc c
     }
   }
-  tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
+  tile_partials<T, VN, NW>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
 // Residual replacement: r = F - K x in FP64 from the FP64 values, then
 // r (inner precision), z = r / M and the partials of the true residual.
-template <typename T, int B, bool IMP, int UN, int VN>
+template <typename T, int B, bool IMP, int UN, int VN, int NW>
 __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int chunk, int par,
                                                    double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
   constexpr int GS = 32 * VN;
@@ -915,7 +914,7 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
-  for (int I = row0 + warp; I < row1; I += kWarps) {
+  for (int I = row0 + warp; I < row1; I += NW) {
     double acc[B][VN];
 #pragma unroll
     for (int a = 0; a < B; a++)
@@ -970,10 +969,10 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
         rz[v] += (double)ri[v] * (double)zi[v];
       }
       stn<T, VN>(M.r + o, ri);
-      if (!M.cmodes) stn<T, VN>(M.z + o, zi);
+      stn<T, VN>(M.z + o, zi);
     }
   }
-  tile_partials<T, VN>(M, g, chunk, par, rr, rz, s_red, s_red2);
+  tile_partials<T, VN, NW>(M, g, chunk, par, rr, rz, s_red, s_red2);
 }
 
 // ---------------------------------------------------------------------------
@@ -992,10 +991,15 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
 //                    group's last range adds the partials in range order,
 //                    writes c (BF16 operand tile) and adds c.c to r.z
 //                    (r.z = r.(r / M) + |Wc^T r|^2 without reading z)
-//   C3  z = r / M + Wc c   D[128 samples x 128 rows] = c^T . Wc^T per chunk
+//   C3  z += Wc c    D[128 samples x 128 rows] = c^T . Wc^T per chunk, added
+//                    to z = r / M as the U phase (or a true-residual pass)
+//                    wrote it.  Only a group with no iterating sample left can
+//                    see some of its tiles skip U; its z is not used again
+//                    before a true-residual pass rewrites every row.
 // TMEM lane = sample of the group, so every epilogue access of a warp covers
 // 32 consecutive samples of one row (256 contiguous bytes).
 constexpr int kCoarseMaxModes = 128;
+constexpr int kCoarseThreads = 512;                 // threads per block of the coarse instance (1 block per SM)
 constexpr int kCoarseCols = 128;                    // TMEM columns per block
 constexpr int kCoarseStage = 32 * 1024;             // C1: A (128 x 64) + B (<= 128 x 64), BF16
 constexpr size_t kCoarseSmem = 2 * kCoarseStage;    // C1 double-buffered; C3 A + B (2 x 128 x 128 BF16)
@@ -1007,45 +1011,67 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<const uint32_t *>(&h);
 }
 
+// Per-block state of the coarse phases, in shared memory so that none of it
+// stays live in registers through the PCG phases: the TMEM accumulator, the
+// MMA completion barrier, the operand staging area (dynamic shared memory).
+__shared__ uint32_t s_coarse_tmem;
+__shared__ uint32_t s_coarse_phase;  // parity of the MMA barrier's next completion
+__shared__ __align__(8) uint64_t s_coarse_mbar;
+extern __shared__ __align__(1024) uint8_t s_coarse_smem[];
+
 // Leaves the kernel at the next grid barrier: every block sees the error.
 __device__ __forceinline__ void coarse_fail(GridBar *bar) { atomicExch(&bar->err, kErrMma); }
 
-// c = Wc^T r over row range `range` of group g (GS = 128 samples).
-__device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range, int par, uint32_t tmem,
-                                       uint64_t *bar, uint32_t &phase, uint8_t *sm, GridBar *gb) {
+// c = Wc^T r over row range `range` of group g (GS = 128 samples), by the
+// kCoarseThreads threads of the block.
+__device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range, int par, uint32_t &phase,
+                                       GridBar *gb) {
+  constexpr int kQ = kCoarseThreads / 128;  // threads per sample
+  static_assert(8 % kQ == 0, "the 8 row groups of a chunk split evenly over the threads of a sample");
   __shared__ int s_last;
+  __shared__ double s_cc[kCoarseThreads];
+  const uint32_t tmem = s_coarse_tmem;
+  uint64_t *bar = &s_coarse_mbar;
+  uint8_t *sm = s_coarse_smem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = M.cmodes, S = M.S;
   const int r0 = range * M.rps, r1 = min(M.n, r0 + M.rps);
   const int nch = (r1 - r0 + 63) / 64;
   const uint32_t idesc = tc::idesc_bf16(128, nmod);
   const int stage_b = nmod * 64 * 2;
-  const int m = tid & 127;  // sample of the group staged by this thread
+  const int m = tid & 127, q = tid >> 7;  // sample of the group staged by this thread, and its share
   const double *rcol = M.r + (size_t)g * 128 + m;
+  // this thread stages row groups kg = q + kQ j (8 rows each) of sample m
+  auto load_chunk = [&](int ch, double (&v)[8 / kQ][8]) {
+    const int rb = r0 + ch * 64;
+#pragma unroll
+    for (int j = 0; j < 8 / kQ; j++)
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int row = rb + (q + kQ * j) * 8 + e;
+        v[j][e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : 0.0;
+      }
+  };
+  double cur[8 / kQ][8], nxt[8 / kQ][8];
+  load_chunk(0, cur);
   bool ok = true;
   for (int ch = 0; ch < nch; ch++) {
     uint8_t *sA = sm + (ch & 1) * kCoarseStage, *sB = sA + 128 * 64 * 2;
     // A = R^T (128 samples x 64 rows): 8 rows of one sample per 16-byte store
-    const int rb = r0 + ch * 64;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int kg = (tid >> 7) + 2 * j;
-      double v[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int row = rb + kg * 8 + e;
-        v[e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : 0.0;
-      }
+    for (int j = 0; j < 8 / kQ; j++) {
       uint4 pk;
-      pk.x = pack_bf16x2((float)v[0], (float)v[1]);
-      pk.y = pack_bf16x2((float)v[2], (float)v[3]);
-      pk.z = pack_bf16x2((float)v[4], (float)v[5]);
-      pk.w = pack_bf16x2((float)v[6], (float)v[7]);
-      *reinterpret_cast<uint4 *>(sA + tc::cm_offset(m, kg * 8, 64)) = pk;
+      pk.x = pack_bf16x2((float)cur[j][0], (float)cur[j][1]);
+      pk.y = pack_bf16x2((float)cur[j][2], (float)cur[j][3]);
+      pk.z = pack_bf16x2((float)cur[j][4], (float)cur[j][5]);
+      pk.w = pack_bf16x2((float)cur[j][6], (float)cur[j][7]);
+      *reinterpret_cast<uint4 *>(sA + tc::cm_offset(m, (q + kQ * j) * 8, 64)) = pk;
     }
     // B = the chunk's Wc^T tile (cmodes x 64), stored in operand order
     const uint4 *src = reinterpret_cast<const uint4 *>(M.wt1 + (size_t)(r0 / 64 + ch) * stage_b);
-    for (int i = tid; i < stage_b / 16; i += kThreads) reinterpret_cast<uint4 *>(sB)[i] = __ldg(src + i);
+    for (int i = tid; i < stage_b / 16; i += kCoarseThreads) reinterpret_cast<uint4 *>(sB)[i] = __ldg(src + i);
+    // the next chunk's residuals are in flight during the MMAs of this one
+    if (ch + 1 < nch) load_chunk(ch + 1, nxt);
     tc::fence_proxy_async();
     // the MMAs of the previous chunk read the other buffer; wait for them
     // before the next staging round overwrites it
@@ -1062,19 +1088,29 @@ __device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range,
                      tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, 1024), idesc, ch > 0 || ks > 0);
       tc::commit(bar);
     }
+#pragma unroll
+    for (int j = 0; j < 8 / kQ; j++)
+#pragma unroll
+      for (int e = 0; e < 8; e++) cur[j][e] = nxt[j][e];
   }
   ok = ok && tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
   tc::fence_after_sync();
   if (!ok) coarse_fail(gb);
-  // partial c -> cpart[g][range][mode][sample]
-  const int half = nmod / 2, k0 = (warp >> 2) * half, ms = (warp & 3) * 32 + lane;
-  float *dst = M.cpart + ((size_t)g * M.nsplit + range) * nmod * 128;
-  for (int kk = 0; kk < half; kk += 8) {
-    uint32_t v[8];
-    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(k0 + kk), v);
+  // the modes in kQ parts of cw columns (a multiple of 8), the last one short
+  const int cw = ((nmod / kQ) + 7) / 8 * 8;
+  {
+    // partial c -> cpart[g][range][mode][sample]: warp w reads TMEM lanes
+    // 32 (w % 4) .. +31 (its samples), columns of part w / 4
+    const int part = warp >> 2, ms = (warp & 3) * 32 + lane;
+    const int k0 = part * cw, k1 = min(nmod, k0 + cw);
+    float *dst = M.cpart + ((size_t)g * M.nsplit + range) * nmod * 128;
+    for (int kk = k0; kk < k1; kk += 8) {
+      uint32_t v[8];
+      tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)kk, v);
 #pragma unroll
-    for (int e = 0; e < 8; e++) __stcg(dst + (size_t)(k0 + kk + e) * 128 + ms, __uint_as_float(v[e]));
+      for (int e = 0; e < 8; e++) __stcg(dst + (size_t)(kk + e) * 128 + ms, __uint_as_float(v[e]));
+    }
   }
   tc::fence_before_sync();
   __threadfence();
@@ -1085,14 +1121,12 @@ __device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range,
   __threadfence();
   // the group's last range: c = sum of the partials in range order; BF16
   // operand tile for C3; c.c into the group's r.z
-  __shared__ double s_cc[kThreads];
-  const int kb = (tid >> 7) * half;
   double cc = 0.0;
-  for (int kk = 0; kk < half; kk += 8) {
+  for (int kk = q * cw; kk < min(nmod, (q + 1) * cw); kk += 8) {
     float c8[8];
 #pragma unroll
     for (int e = 0; e < 8; e++) {
-      const int k = kb + kk + e;
+      const int k = kk + e;
       float t = 0.0f;
       for (int sp = 0; sp < M.nsplit; sp++)
         t += __ldcg(M.cpart + (((size_t)g * M.nsplit + sp) * nmod + k) * 128 + m);
@@ -1104,21 +1138,26 @@ __device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range,
     pk.y = pack_bf16x2(c8[2], c8[3]);
     pk.z = pack_bf16x2(c8[4], c8[5]);
     pk.w = pack_bf16x2(c8[6], c8[7]);
-    __stcg(reinterpret_cast<uint4 *>(M.cb + (size_t)g * 128 * nmod * 2 + tc::cm_offset(m, kb + kk, nmod)), pk);
+    __stcg(reinterpret_cast<uint4 *>(M.cb + (size_t)g * 128 * nmod * 2 + tc::cm_offset(m, kk, nmod)), pk);
   }
   s_cc[tid] = cc;
   __syncthreads();
   if (tid < 128) {
+    double t = 0.0;
+    for (int j = 0; j < kQ; j++) t += s_cc[tid + 128 * j];
     double *rz = M.tot_rz + (size_t)par * S + (size_t)g * 128 + tid;
-    __stcg(rz, __ldcg(rz) + s_cc[tid] + s_cc[tid + 128]);
+    __stcg(rz, __ldcg(rz) + t);
   }
   if (tid == 0) atomicExch(M.ccnt + g, 0);  // next used after a grid barrier
   __syncthreads();
 }
 
-// z = r / M + Wc c on the 128-row chunk `chunk` of group g.
-__device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk, uint32_t tmem, uint64_t *bar,
-                                       uint32_t &phase, uint8_t *sm, GridBar *gb) {
+// z += Wc c on the 128-row chunk `chunk` of group g.
+__device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk, uint32_t &phase, GridBar *gb) {
+  constexpr int kRows = 128 / (kCoarseThreads / 128);  // rows of the chunk per thread
+  const uint32_t tmem = s_coarse_tmem;
+  uint64_t *bar = &s_coarse_mbar;
+  uint8_t *sm = s_coarse_smem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = M.cmodes, S = M.S;
   const int tbytes = 128 * nmod * 2;
@@ -1126,7 +1165,7 @@ __device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk,
   // A = c of the group (written in this launch: L2 loads), B = Wc rows of the chunk
   const uint4 *ca = reinterpret_cast<const uint4 *>(M.cb + (size_t)g * tbytes);
   const uint4 *wb = reinterpret_cast<const uint4 *>(M.wt3 + (size_t)chunk * tbytes);
-  for (int i = tid; i < tbytes / 16; i += kThreads) {
+  for (int i = tid; i < tbytes / 16; i += kCoarseThreads) {
     reinterpret_cast<uint4 *>(sA)[i] = __ldcg(ca + i);
     reinterpret_cast<uint4 *>(sB)[i] = __ldg(wb + i);
   }
@@ -1140,31 +1179,36 @@ __device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk,
                    tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, sbo), idesc, ks > 0);
     tc::commit(bar);
   }
+  // lanes = samples, columns = rows of the chunk: warp w reads TMEM lanes
+  // 32 (w % 4) .. +31 and rows kRows (w / 4) .. +kRows-1
+  const int ms = (warp & 3) * 32 + lane, j0 = (warp >> 2) * kRows;
+  double *zc = M.z + (size_t)g * 128 + ms;
+  const int rbase = chunk * 128 + j0;
+  const int nrow = min(kRows, M.n - rbase);  // rows of this thread's share in the mesh
+  constexpr int kR = 16;                     // rows per step; the next step's z loads fly during this one
+  double cur[kR], nxt[kR];
+#pragma unroll
+  for (int e = 0; e < kR; e++) cur[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : 0.0;
   const bool ok = tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
   tc::fence_after_sync();
   if (!ok) coarse_fail(gb);
-  // lanes = samples, columns = rows of the chunk; warps 4-7 take rows 64-127
-  const int ms = (warp & 3) * 32 + lane, j0 = (warp >> 2) * 64;
-  const size_t col = (size_t)g * 128 + ms;
-  const int rbase = chunk * 128 + j0;
-  for (int jj = 0; jj < 64; jj += 8) {
-    uint32_t v[8];
+  for (int jj = 0; jj < kRows; jj += kR) {
+    if (jj + kR < kRows) {
+#pragma unroll
+      for (int e = 0; e < kR; e++)
+        nxt[e] = jj + kR + e < nrow ? __ldcg(zc + (size_t)(rbase + jj + kR + e) * S) : 0.0;
+    }
+    uint32_t v[8], w[8];
     tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + jj), v);
-    double rv[8], mv[8];
+    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + jj + 8), w);
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int row = rbase + jj + e;
-      if (row < M.n) {
-        rv[e] = __ldcg(M.r + (size_t)row * S + col);
-        mv[e] = __ldg(M.M + (size_t)row * S + col);
-      }
+    for (int e = 0; e < kR; e++) {
+      const float add = __uint_as_float(e < 8 ? v[e] : w[e - 8]);
+      if (jj + e < nrow) zc[(size_t)(rbase + jj + e) * S] = cur[e] + (double)add;
     }
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int row = rbase + jj + e;
-      if (row < M.n) M.z[(size_t)row * S + col] = rv[e] / mv[e] + (double)__uint_as_float(v[e]);
-    }
+    for (int e = 0; e < kR; e++) cur[e] = nxt[e];
   }
   tc::fence_before_sync();
   __syncthreads();  // the next item restages the operand tiles and reuses the accumulator
@@ -1197,12 +1241,13 @@ constexpr int kMaxMeshes = 8;
 #define UFEM_PCG_MIN_BLOCKS 2
 #endif
 // The coarse phases (precision 2 with 128-sample groups): C1 then C3 over the
-// groups whose z has to be formed from r; two grid barriers.
+// groups whose z has to be formed from r; two grid barriers.  The parity of
+// the MMA barrier is kept in shared memory between calls.
 template <typename T>
-__device__ __forceinline__ bool coarse_phases(const BArgs<T> &A, const BMesh<T> *s_meshes, int par, uint32_t tmem,
-                                              uint64_t *bar, uint32_t &phase, uint8_t *sm) {
+__device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_meshes, int par) {
   __shared__ int s_go;
   const int G = gridDim.x;
+  uint32_t phase = s_coarse_phase;
   if constexpr (sizeof(T) == 8) {
     for (int t = blockIdx.x; t < A.nc1; t += G) {
       const int4 it = A.c1items[t];
@@ -1211,7 +1256,7 @@ __device__ __forceinline__ bool coarse_phases(const BArgs<T> &A, const BMesh<T> 
       __syncthreads();
       const int go = s_go;
       __syncthreads();
-      if (go) coarse_c1(M, it.y, it.z, par, tmem, bar, phase, sm, A.bar);
+      if (go) coarse_c1(M, it.y, it.z, par, phase, A.bar);
     }
     if (!grid_barrier(A.bar)) return false;
     for (int t = blockIdx.x; t < A.nc3; t += G) {
@@ -1221,20 +1266,22 @@ __device__ __forceinline__ bool coarse_phases(const BArgs<T> &A, const BMesh<T> 
       __syncthreads();
       const int go = s_go;
       __syncthreads();
-      if (go) coarse_c3(M, it.y, it.z, tmem, bar, phase, sm, A.bar);
+      if (go) coarse_c3(M, it.y, it.z, phase, A.bar);
     }
     if (!grid_barrier(A.bar)) return false;
   }
+  if (threadIdx.x == 0) s_coarse_phase = phase;  // every thread holds the same parity
+  __syncthreads();
   return true;
 }
 
-template <typename T, int B, bool IMP, int UN, int VN>
-__device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *mbar, uint8_t *sm) {
+template <typename T, int B, bool IMP, int UN, int VN, bool CO, int NW>
+__device__ __forceinline__ void pcg_body(const BArgs<T> A) {
   constexpr int GS = 32 * VN;
-  constexpr bool kCoarse = IMP && VN == 4;
-  uint32_t mphase = 0;
-  __shared__ double s_red[kWarps][GS];
-  __shared__ double s_red2[kWarps][GS];
+  constexpr bool kCoarse = CO;
+  static_assert(!CO || (IMP && VN == 4), "the coarse correction runs with the implicit form and 128-sample groups");
+  __shared__ double s_red[NW][GS];
+  __shared__ double s_red2[NW][GS];
   __shared__ T s_sc[GS];
   __shared__ BMesh<T> s_meshes[kMaxMeshes];
   __shared__ int s_flag;
@@ -1251,7 +1298,7 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
     if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
     any = __syncthreads_or(any);
     if (any) {
-      tile_true_residual<T, B, IMP, UN, VN>(M, ti.y, ti.z, 0, s_red, s_red2);
+      tile_true_residual<T, B, IMP, UN, VN, NW>(M, ti.y, ti.z, 0, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) {
         M.gtrue[ti.y] = 1;
         M.glast[ti.y] = 0;
@@ -1262,7 +1309,7 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
   }
   if (!grid_barrier(A.bar)) return;
   if constexpr (kCoarse) {
-    if (A.coarse && !coarse_phases<T>(A, s_meshes, 0, tmem, mbar, mphase, sm)) return;
+    if (A.coarse && !coarse_phases<T>(A, s_meshes, 0)) return;
   }
   long k;
   for (k = 1;; k++) {
@@ -1338,7 +1385,7 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
       }
       const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B, IMP, UN, VN>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+      tile_spmv<T, B, IMP, UN, VN, NW>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     if (!grid_barrier(A.bar)) return;
     // The group counter changes only in phase S: read between the barriers,
@@ -1377,7 +1424,7 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
       if (ti.z == 0 && threadIdx.x == 0 && __ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
       if (!live) continue;
       const T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_update<T, B, VN>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
+      tile_update<T, B, VN, NW>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
       if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
       if (M.cmodes && threadIdx.x == 0) M.gcz[g] = 1;
     }
@@ -1394,7 +1441,7 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
           __syncthreads();  // thread 0 rewrites s_flag for the next tile
           continue;
         }
-        tile_true_residual<T, B, IMP, UN, VN>(M, ti.y, ti.z, par, s_red, s_red2);
+        tile_true_residual<T, B, IMP, UN, VN, NW>(M, ti.y, ti.z, par, s_red, s_red2);
         if (ti.z == 0 && threadIdx.x == 0) {
           M.gtrue[ti.y] = 1;
           M.glast[ti.y] = (int)k;
@@ -1407,37 +1454,42 @@ __device__ __forceinline__ void pcg_body(BArgs<T> &A, uint32_t tmem, uint64_t *m
     if (remaining <= 0 || k > A.maxit + 1) break;
     // ---- phases C1, C3 (coarse space): z = r / M + Wc Wc^T r ----------------
     if constexpr (kCoarse) {
-      if (A.coarse && !coarse_phases<T>(A, s_meshes, par, tmem, mbar, mphase, sm)) return;
+      if (A.coarse && !coarse_phases<T>(A, s_meshes, par)) return;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
 }
 
 // UN: contributions whose gathers are issued together (implicit form);
-// VN: samples per lane (a sample group is 32 VN samples).  With a coarse
-// space the block holds kCoarseCols TMEM columns and kCoarseSmem bytes of
-// dynamic shared memory for the whole launch (at most 2 blocks per SM).
-template <typename T, int B, bool IMP, int UN, int VN>
-__global__ void __launch_bounds__(kThreads, IMP ? UFEM_PCG_MIN_BLOCKS : 2) k_batch_pcg(BArgs<T> A) {
-  extern __shared__ __align__(1024) uint8_t s_dyn[];
-  __shared__ __align__(8) uint64_t s_mbar;
-  __shared__ uint32_t s_tmem;
-  constexpr bool kCoarse = IMP && VN == 4;
+// VN: samples per lane (a sample group is 32 VN samples); CO: the launch
+// has a coarse space -- a separate instance, so that the Jacobi-only kernel
+// keeps its own register allocation.  A kernel that uses tensor memory runs
+// one block per SM, so the coarse instance has kCoarseThreads threads per
+// block (the Jacobi instance: two blocks of kThreads); the block holds
+// kCoarseCols TMEM columns and kCoarseSmem bytes of dynamic shared memory
+// for the whole launch.
+template <typename T, int B, bool IMP, int UN, int VN, bool CO = false>
+__global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP ? UFEM_PCG_MIN_BLOCKS : 2))
+    k_batch_pcg(BArgs<T> A) {
+  constexpr bool kCoarse = CO;
   if constexpr (kCoarse) {
     if (A.coarse) {
-      if (threadIdx.x == 0) tc::mbar_init(&s_mbar, 1);
-      if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s_tmem, kCoarseCols);
+      if (threadIdx.x == 0) {
+        tc::mbar_init(&s_coarse_mbar, 1);
+        s_coarse_phase = 0;
+      }
+      if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s_coarse_tmem, kCoarseCols);
       tc::fence_before_sync();
       __syncthreads();
       tc::fence_after_sync();
     }
   }
-  pcg_body<T, B, IMP, UN, VN>(A, s_tmem, &s_mbar, s_dyn);
+  pcg_body<T, B, IMP, UN, VN, CO, (CO ? kCoarseThreads : kThreads) / 32>(A);
   if constexpr (kCoarse) {
     if (A.coarse) {
       tc::fence_before_sync();
       __syncthreads();
-      if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, kCoarseCols);
+      if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_coarse_tmem, kCoarseCols);
     }
   }
 }
@@ -1777,6 +1829,9 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int B = models[0]->b;
+  // the coarse correction needs 128-sample groups (one UMMA M tile)
+  bool coarse = false;
+  if constexpr (IMP && VN == 4) coarse = coarse_modes(nmesh, models, opt) > 0;
   void (*kern)(BArgs<T>) = nullptr;
   if constexpr (!IMP) {
     kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 1, VN> : k_batch_pcg<T, 2, IMP, 1, VN>;
@@ -1785,13 +1840,24 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN> : k_batch_pcg<T, 2, IMP, 2, VN>;
     else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN> : k_batch_pcg<T, 2, IMP, 4, VN>;
     else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8, VN> : k_batch_pcg<T, 2, IMP, 8, VN>;
+    if constexpr (VN == 4) {
+      if (coarse) {
+        if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN, true> : k_batch_pcg<T, 2, IMP, 2, VN, true>;
+        else if (un <= 4) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN, true> : k_batch_pcg<T, 2, IMP, 4, VN, true>;
+        else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 8, VN, true> : k_batch_pcg<T, 2, IMP, 8, VN, true>;
+      }
+    }
   }
-  // the coarse correction needs 128-sample groups (one UMMA M tile)
-  bool coarse = false;
-  if constexpr (IMP && VN == 4) coarse = coarse_modes(nmesh, models, opt) > 0;
   const size_t dsmem = coarse ? kCoarseSmem : 0;
-  if (coarse) UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
-  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, dsmem));
+  if (coarse) {
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+    // all of the unified L1 / shared memory as shared memory, so that two
+    // blocks (about 87 KB each) fit on an SM
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+  }
+  const int nthreads = coarse ? kCoarseThreads : kThreads, nwarps = nthreads / 32;
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nthreads, dsmem));
   if (occ < 1) {
     set_error("batched PCG kernel does not fit on an SM");
     return UFEM_AF_ERR;
@@ -1806,8 +1872,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   g_stats.tiles_per_block = (int)tpb;
   g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 2) : 0;
   g_stats.lane_samples = VN;
-  int rpt = (int)std::max<long>(kWarps, (total_rows + tpb * G - 1) / (tpb * G));
-  rpt = (rpt + kWarps - 1) / kWarps * kWarps;
+  int rpt = (int)std::max<long>(nwarps, (total_rows + tpb * G - 1) / (tpb * G));
+  rpt = (rpt + nwarps - 1) / nwarps * nwarps;
   int active_groups = 0;
   std::vector<std::vector<int>> act(nmesh);  // active groups of each mesh
   for (int k = 0; k < nmesh; k++) {
@@ -1972,7 +2038,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0);
-  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kThreads), args, a.coarse ? dsmem : 0, 0));
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, a.coarse ? dsmem : 0, 0));
   cudaEventRecord(ev1);
   g_stats.kernel_launches += 1;
   long its = 0;
@@ -2018,8 +2084,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       // S phase: values, 2 gathered and 2 own vectors in, 2 out; U phase:
       // M, r, p, q in, r, z out, x (FP64) in and out
       g_stats.pcg_bytes += (vals + 11.0 * vec + 2.0 * n * GS * sizeof(double)) * gi;
-      // coarse phases: C1 reads r, C3 reads r and M and writes z (U no
-      // longer writes z); the partial and BF16 c tiles of the group
+      // coarse phases: C1 reads r, C3 reads and writes z; the partial and
+      // BF16 c tiles of the group
       const int cm = hm[k].cmodes;
       if (cm) g_stats.pcg_bytes += (3.0 * vec + 2.0 * hm[k].nsplit * cm * 128 * 4.0 + 3.0 * 128 * cm * 2.0) * gi;
     }
