@@ -60,7 +60,8 @@ WARM_EVAL = 8192
 EVAL_FIRST = 1 << 20     # evaluation sample ids: disjoint from training
 METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 PCG, 1 B200"
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
-            "warm-started (POD 64 modes from 512 solves; MLP 17-256-256-64 trained on 4096 solves)")
+            "warm-started and coarse-corrected (POD 80 modes from 512 solves: Galerkin guess + PCG coarse space; "
+            "MLP 17-256-256-80 trained on 4096 solves)")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
           2: "k_batch_pcg<double,3,implicit>"}
@@ -99,7 +100,8 @@ def parse():
 
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
-           2: ("k_batch_pcg_implicit_40x10x10_1024samples.md", "40x10x10 16 E zones x 1024 samples, 40 iterations")}
+           2: ("k_batch_pcg_coarse_40x10x10_1024samples.md",
+               "40x10x10 16 E zones x 1024 samples, 80-mode coarse space, 40 iterations")}
 
 
 def profile_case(a):
@@ -114,14 +116,25 @@ def profile_case(a):
     if a.precision == 2:
         m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
         f = mg.warm_samples(m, 1024)
+        if not a.no_coarse:
+            # the coarse space from a short warm-start training (sets it on the model)
+            from ufem_b200.warm import WarmStart
+            g = GpuModel(m)
+            cols, logs, scale_col = mg.warm_features(m)
+            ws = WarmStart(g, cols, logs, scale_col, n_modes=a.coarse_modes, n_hidden=64, n_snapshots=512, epochs=2,
+                           batch=256, n_coarse=a.coarse_modes)
+            ws.train(mg.warm_samples(m, 1024, first_sample=EVAL_FIRST), precision=2)
     else:
         m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
         mg.mc_attach_vars(m)
         f = mg.mc_samples(m, mesh_id=2, nsamp=128)
-    g = GpuModel(m)
+    if a.precision != 2 or a.no_coarse:
+        g = GpuModel(m)
     for _ in range(2):
-        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block)
-    print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "pcg_ms": st.ms_pcg,
+        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block,
+                           coarse=0 if a.no_coarse else 1)
+    print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "coarse_modes": st.coarse_modes,
+                      "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
                       "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))
 
@@ -682,7 +695,10 @@ def ours(a):
         # ratio of this kernel (profiles/, a smaller case of the same kernel)
         # times this run's algorithmic bytes per launch
         traffic = None
-        tf = os.path.join(ROOT, "profiles", PROFILE.get(a.precision, ("none", ""))[0])
+        pf = PROFILE.get(a.precision, ("none", ""))[0]
+        if a.precision == 2 and not (tstats["coarse_modes"] and opt.coarse):
+            pf = "k_batch_pcg_implicit_40x10x10_1024samples.md"  # the Jacobi-only instance
+        tf = os.path.join(ROOT, "profiles", pf)
         if os.path.exists(tf) and pcg_launches > 0:
             for line in open(tf):
                 if line.startswith("traffic_over_algorithmic:"):
@@ -731,7 +747,9 @@ def ours(a):
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},
             "speedup_vs_plain": value / plain,
-            "roofline": {"bound": "hbm", "kernel": KERNEL[a.precision], "achieved": achieved,
+            "roofline": {"bound": "hbm",
+                         "kernel": KERNEL[a.precision] + (" + coarse phases (tcgen05)"
+                                                          if tstats["coarse_modes"] and opt.coarse else ""), "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "pcg_ms_per_step": pcg_ms / a.steps,
                          "pcg_launches_per_step": pcg_launches / a.steps},
