@@ -519,8 +519,11 @@ def ours(a):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        step_wall = []
         for _ in range(a.steps):
+            t_step = time.perf_counter()
             step_device()
+            step_wall.append(1000.0 * (time.perf_counter() - t_step))
             launches += wst.kernel_launches
             pcg_ms += wst.pcg_ms
             pcg_bytes += wst.pcg_bytes
@@ -756,6 +759,7 @@ def ours(a):
             "e2e": {"value": solves_step / (e2e_ms / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "matches_device_run": e2e_ok},
             "gpu_launches": launches, "clocks": clk.summary(local),
+            "step_wall_ms": [round(t, 1) for t in step_wall],
             "uneven_batch": uneven,
             "static_configs": static,
             "cpu_baseline": cpu,
