@@ -60,8 +60,8 @@ WARM_EVAL = 8192
 EVAL_FIRST = 1 << 20     # evaluation sample ids: disjoint from training
 METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 PCG, 1 B200"
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
-            "warm-started and coarse-corrected (POD 80 modes from 512 solves: Galerkin guess + PCG coarse space; "
-            "MLP 17-256-256-80 trained on 4096 solves)")
+            "warm-started and coarse-corrected (POD {m} modes from 512 solves: Galerkin guess + PCG coarse space; "
+            "MLP 17-256-256-{m} trained on 4096 solves)")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
           2: "k_batch_pcg<double,3,implicit>"}
@@ -82,8 +82,9 @@ def parse():
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
     p.add_argument("--no-coarse", action="store_true",
                    help="headline without the coarse correction of the preconditioner (Jacobi PCG)")
-    p.add_argument("--coarse-modes", type=int, default=80,
-                   help="POD modes of the preconditioner's coarse space (a multiple of 16, at most 80)")
+    p.add_argument("--coarse-modes", type=int, default=128,
+                   help="POD modes of the basis and of the preconditioner's coarse space (a multiple of 16, "
+                        "at most 128)")
     p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--guess", type=int, default=1,
@@ -330,7 +331,7 @@ def reference_arm(a):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "solver": "reference monte_solution (SSOR PCG, eps 1e-21)",
+            "config": {"workload": WORKLOAD.format(m=max(64, a.coarse_modes)), "solver": "reference monte_solution (SSOR PCG, eps 1e-21)",
                        "processes": procs},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "reference",
                              "sample": f"per step: {procs} processes x 1 evaluation sample of the 40x10x10 "
@@ -621,7 +622,8 @@ def ours(a):
                                                                / np.abs(out_warm).max())}
 
     # ---- the other guess (MLP <-> POD-Galerkin), same precision ------------
-    GUESS = {0: "the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> 64 coefficients)",
+    GUESS = {0: f"the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> {max(64, a.coarse_modes)} "
+                "coefficients)",
              1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the per-zone reduced "
                 "operators) on the learned POD basis"}
     galerkin = None
@@ -721,7 +723,7 @@ def ours(a):
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if a.precision != 1 else "fp32 inner / fp64 refinement",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
+            "config": {"workload": WORKLOAD.format(m=max(64, a.coarse_modes)), "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
                        "precision": PREC[a.precision],
                        "l2_flush": "not needed: every per-sample vector is 0.98 GB (FP64, 8192 samples) and the "
                                    "explicit FP32 values 34 GB per iteration, >> 126 MB L2",

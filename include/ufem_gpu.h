@@ -329,7 +329,7 @@ int  ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, fl
  * solved again from zero (UFEM_ST_FALLBACK).
  * d_ifld: device, nsamp*ilen (the model's Monte Carlo inputs). */
 typedef struct ufem_warm_options {
-  int n_modes;               /* POD modes: a multiple of 16, at most 80 */
+  int n_modes;               /* POD modes: a multiple of 16, at most 128 */
   int n_hidden;              /* MLP width: a multiple of 16, at most 256 */
   int n_feat;                /* network inputs, 1..32 */
   long feat_cols[32];        /* ifld column of each input */
@@ -348,13 +348,15 @@ typedef struct ufem_warm_options {
                                 PCG preconditioner after training (ufem_mc_set_coarse; at
                                 most n_modes, a multiple of 16; 0: none; default 64; models
                                 with at most 64 E variables) */
+  double snap_tol;           /* relative residual of the snapshot solves (the first n_snapshots
+                                training samples; default 1e-11, 0: the training tolerance) */
 } ufem_warm_options;
 
 typedef struct ufem_warm_train_stats {
   long cold_iters_max;       /* largest PCG iteration count of the cold solves */
   double cold_iters_mean;
   double ms_solve, ms_basis, ms_train;
-  double sigma2[80];         /* energy (squared singular value) of each POD mode */
+  double sigma2[80];         /* energy (squared singular value) of each POD mode (the first 80) */
   float loss_first, loss_last;  /* mean training loss of the first / last epoch */
   int epochs;
   long steps;

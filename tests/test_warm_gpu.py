@@ -43,7 +43,7 @@ def test_dgemm_f64_matches_numpy(M, N, K):
     assert (np.abs(dC.cpu().numpy() - ref) / scale).max() < 1e-13
 
 
-@pytest.mark.parametrize("l", [8, 80, 96])
+@pytest.mark.parametrize("l", [8, 80, 96, 98, 144])
 def test_sym_eig_matches_numpy(l):
     from ufem_b200 import _lib
     L = _lib.load()

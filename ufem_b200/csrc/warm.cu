@@ -167,27 +167,34 @@ int gemm_f64(int M, int N, long K, const double *A, long sam, long sak, const do
 // block: cyclic Jacobi, round-robin ordering (l - 1 rounds of l/2 disjoint
 // rotations per sweep), rotation of Numerical Recipes (Press et al., 11.1):
 // theta = (a_qq - a_pp) / (2 a_pq), t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)),
-// c = 1 / sqrt(t^2 + 1), s = t c; A <- P^T A P, V <- V P.
+// c = 1 / sqrt(t^2 + 1), s = t c; A <- P^T A P, V <- V P.  A is kept in
+// shared memory; V too up to kSmemL, beyond that transposed in the global
+// workspace Vg (row p = column p of V, so a rotation reads two contiguous
+// rows; the l x l doubles stay in L2).
 // ---------------------------------------------------------------------------
-constexpr int kMaxL = 96;
+constexpr int kMaxL = 144;
+constexpr int kSmemL = 96;
 constexpr int kJacThreads = 512;
 
+template <bool VG>
 __global__ void __launch_bounds__(kJacThreads) k_jacobi_eig(int l, const double *__restrict__ Ain,
                                                             double *__restrict__ Vout, double *__restrict__ lam,
-                                                            int max_sweeps, int *__restrict__ sweeps_out) {
+                                                            int max_sweeps, int *__restrict__ sweeps_out,
+                                                            double *__restrict__ Vg) {
   extern __shared__ double sm[];
   const int ld = l + 1;
-  double *A = sm;             // [l][ld]
-  double *V = sm + l * ld;    // [l][ld]
-  double *cs = V + l * ld;    // [l/2][2]
-  int *pq = (int *)(cs + l);  // [l/2][2]
+  double *A = sm;                        // [l][ld]
+  double *V = sm + l * ld;               // [l][ld] (shared-memory V only)
+  double *cs = VG ? V : V + l * ld;      // [l/2][2]
+  int *pq = (int *)(cs + l);             // [l/2][2]
   __shared__ double red[kJacThreads];
   __shared__ int s_done;
   const int half = l / 2;
   for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
     const int i = e / l, j = e % l;
     A[i * ld + j] = 0.5 * (Ain[i * l + j] + Ain[j * l + i]);
-    V[i * ld + j] = (i == j) ? 1.0 : 0.0;
+    if (VG) Vg[i * l + j] = (i == j) ? 1.0 : 0.0;
+    else V[i * ld + j] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
   int sweep = 0;
@@ -257,23 +264,47 @@ __global__ void __launch_bounds__(kJacThreads) k_jacobi_eig(int l, const double 
         double a = A[i * ld + p], b = A[i * ld + q];
         A[i * ld + p] = c * a - s * b;
         A[i * ld + q] = s * a + c * b;
-        a = V[i * ld + p];
-        b = V[i * ld + q];
-        V[i * ld + p] = c * a - s * b;
-        V[i * ld + q] = s * a + c * b;
+        if (VG) {
+          a = Vg[p * l + i];
+          b = Vg[q * l + i];
+          Vg[p * l + i] = c * a - s * b;
+          Vg[q * l + i] = s * a + c * b;
+        } else {
+          a = V[i * ld + p];
+          b = V[i * ld + q];
+          V[i * ld + p] = c * a - s * b;
+          V[i * ld + q] = s * a + c * b;
+        }
       }
       __syncthreads();
     }
   }
   for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
     const int i = e / l, j = e % l;
-    Vout[i * l + j] = V[i * ld + j];
+    Vout[i * l + j] = VG ? Vg[j * l + i] : V[i * ld + j];
   }
   for (int j = threadIdx.x; j < l; j += blockDim.x) lam[j] = A[j * ld + j];
   if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sweep;
 }
 
-size_t jacobi_smem(int l) { return (size_t)(2 * l * (l + 1) + l) * sizeof(double) + (size_t)l * sizeof(int); }
+size_t jacobi_smem(int l) {
+  const int nmat = l <= kSmemL ? 2 : 1;
+  return (size_t)(nmat * l * (l + 1) + l) * sizeof(double) + (size_t)l * sizeof(int);
+}
+
+// eigen-decomposition of dA [l x l] -> dV (columns), dlam; dVg: l x l scratch (l > kSmemL)
+int jacobi_eig(int l, const double *dA, double *dV, double *dlam, int *dsweeps, double *dVg) {
+  const size_t smem = jacobi_smem(l);
+  if (l <= kSmemL) {
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_jacobi_eig<false><<<1, kJacThreads, smem>>>(l, dA, dV, dlam, 60, dsweeps, nullptr);
+  } else {
+    UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_jacobi_eig<true><<<1, kJacThreads, smem>>>(l, dA, dV, dlam, 60, dsweeps, dVg);
+  }
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
 
 // T[i][c] = V[i][perm[c]] * scale[c]   (l rows, rc columns)
 __global__ void k_cols_perm_scale(int l, int rc, const double *__restrict__ V, const int *__restrict__ perm,
@@ -464,70 +495,92 @@ __global__ void k_phi_rows(int nrow, int r, const int *__restrict__ rows, const 
 // (a_0 = 1, a_v = the sample's E of variable v), b = Phi^T F0 + sum_j
 // f_j Phi[row_j], A c = b by Cholesky in shared memory.  Directions with a
 // pivot below 1e-13 of the largest diagonal (zero basis columns) get c = 0.
-constexpr int kMaxR = 80;
-__global__ void __launch_bounds__(128) k_reduced_solve(long nsamp, int r, int nmult, long ilen,
-                                                       const double *__restrict__ ifld, const int *__restrict__ mcol,
-                                                       const double *__restrict__ G, const double *__restrict__ PF0,
-                                                       int novr, const int *__restrict__ ovar,
-                                                       const double *__restrict__ Prow, double *__restrict__ c_out) {
-  extern __shared__ double s_A[];  // r x (r + 1)
-  const int ld = r + 1;
+constexpr int kMaxR = 128;
+constexpr int kRedThreads = 256;
+// A is kept as a packed lower triangle, row i at i (i + 1) / 2 (66 KB at
+// r = 128, so three samples share an SM); warps own rows (assembly and the
+// Cholesky updates read and write along a row), one warp does both
+// triangular solves.
+__device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
+
+__global__ void __launch_bounds__(kRedThreads) k_reduced_solve(long nsamp, int r, int nmult, long ilen,
+                                                               const double *__restrict__ ifld,
+                                                               const int *__restrict__ mcol,
+                                                               const double *__restrict__ G,
+                                                               const double *__restrict__ PF0, int novr,
+                                                               const int *__restrict__ ovar,
+                                                               const double *__restrict__ Prow,
+                                                               double *__restrict__ c_out) {
+  extern __shared__ double s_A[];  // packed lower triangle of the r x r system
   __shared__ double bb[kMaxR];
   __shared__ double av[64];
   __shared__ int skip[kMaxR];
   __shared__ double s_dmax;
+  constexpr int kW = kRedThreads / 32;
   const long s = blockIdx.x;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const double *row = ifld + s * ilen;
   for (int v = tid; v < nmult; v += blockDim.x) av[v] = (v == 0) ? 1.0 : row[mcol[v]];
   __syncthreads();
-  for (int e = tid; e < r * r; e += blockDim.x) {
-    double t = 0.0;
-    for (int v = 0; v < nmult; v++) t += av[v] * G[(size_t)v * r * r + e];
-    s_A[(e / r) * ld + (e % r)] = t;
-  }
+  // A[i][k] = sum_v a_v G_v[i][k], k <= i: warp w takes rows w, w + kW, ...
+  for (int i = warp; i < r; i += kW)
+    for (int k = lane; k <= i; k += 32) {
+      const double *g = G + (size_t)i * r + k;
+      double t = 0.0;
+#pragma unroll 4
+      for (int v = 0; v < nmult; v++) t = fma(av[v], __ldg(g + (size_t)v * r * r), t);
+      s_A[tri(i) + k] = t;
+    }
   for (int i = tid; i < r; i += blockDim.x) {
     double t = PF0[i];
     for (int j = 0; j < novr; j++) t += row[ovar[j]] * Prow[(size_t)j * r + i];
     bb[i] = t;
   }
   __syncthreads();
-  if (tid == 0) {
+  if (warp == 0) {
     double m = 0.0;
-    for (int i = 0; i < r; i++) m = fmax(m, fabs(s_A[(i) * ld + (i)]));
-    s_dmax = m;
+    for (int i = lane; i < r; i += 32) m = fmax(m, fabs(s_A[tri(i) + i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) s_dmax = m;
   }
   __syncthreads();
-  // right-looking Cholesky, L in the lower triangle
+  const double dmax = s_dmax;
+  // right-looking Cholesky, L in the packed lower triangle
   for (int j = 0; j < r; j++) {
+    // column j below the diagonal scaled by 1 / L_jj (every thread reads the
+    // pivot; it is rewritten only in the next phase)
+    const double d = s_A[tri(j) + j];
+    const bool sk = !(d > 1e-13 * dmax);
+    const double inv = sk ? 0.0 : 1.0 / sqrt(d);
+    for (int i = j + 1 + tid; i < r; i += blockDim.x) s_A[tri(i) + j] *= inv;
+    __syncthreads();
     if (tid == 0) {
-      const double d = s_A[(j) * ld + (j)];
-      skip[j] = !(d > 1e-13 * s_dmax);
-      s_A[(j) * ld + (j)] = skip[j] ? 1.0 : sqrt(d);
+      s_A[tri(j) + j] = sk ? 1.0 : sqrt(d);
+      skip[j] = sk;
     }
-    __syncthreads();
-    for (int i = j + 1 + tid; i < r; i += blockDim.x) s_A[(i) * ld + (j)] = skip[j] ? 0.0 : s_A[(i) * ld + (j)] / s_A[(j) * ld + (j)];
-    __syncthreads();
-    const int m = r - j - 1;
-    for (int e = tid; e < m * m; e += blockDim.x) {
-      const int i = j + 1 + e / m, k = j + 1 + e % m;
-      if (k <= i) s_A[(i) * ld + (k)] -= s_A[(i) * ld + (j)] * s_A[(k) * ld + (j)];
+    // trailing update A[i][k] -= L[i][j] L[k][j], j < k <= i, along rows
+    for (int i = j + 1 + warp; i < r; i += kW) {
+      const double lij = s_A[tri(i) + j];
+      for (int k = j + 1 + lane; k <= i; k += 32) s_A[tri(i) + k] = fma(-lij, s_A[tri(k) + j], s_A[tri(i) + k]);
     }
     __syncthreads();
   }
-  // L y = b, L^T c = y (one thread: r <= 80)
-  if (tid == 0) {
-    for (int i = 0; i < r; i++) {
-      double t = skip[i] ? 0.0 : bb[i];
-      if (!skip[i])
-        for (int k = 0; k < i; k++) t -= s_A[(i) * ld + (k)] * bb[k];
-      bb[i] = skip[i] ? 0.0 : t / s_A[(i) * ld + (i)];
+  // L y = b, then L^T c = y, by warp 0 (bb holds y, then c)
+  if (warp == 0) {
+    for (int j = 0; j < r; j++) {
+      const double y = skip[j] ? 0.0 : bb[j] / s_A[tri(j) + j];
+      __syncwarp();
+      if (lane == 0) bb[j] = y;
+      for (int i = j + 1 + lane; i < r; i += 32) bb[i] = fma(-s_A[tri(i) + j], y, bb[i]);
+      __syncwarp();
     }
     for (int i = r - 1; i >= 0; i--) {
-      double t = bb[i];
-      if (!skip[i])
-        for (int k = i + 1; k < r; k++) t -= s_A[(k) * ld + (i)] * bb[k];
-      bb[i] = skip[i] ? 0.0 : t / s_A[(i) * ld + (i)];
+      const double c = skip[i] ? 0.0 : bb[i] / s_A[tri(i) + i];
+      __syncwarp();
+      if (lane == 0) bb[i] = c;
+      for (int k = lane; k < i; k += 32) bb[k] = fma(-s_A[tri(i) + k], c, bb[k]);
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -570,6 +623,7 @@ struct ufem_warm {
   DBuf<int> perm, sweeps;
   DBuf<float> X, Tt, Yo;
   DBuf<double> ifsub, u0, uf, err, errpart;
+  DBuf<double> Vg;                        // eigenvector scratch of the larger bases
   DBuf<double> ofsub;
   DBuf<int> stsub;
   DBuf<long> itsub;
@@ -588,14 +642,9 @@ namespace {
 // eigen-decomposition of the l x l matrix w->G; columns of w->V sorted by
 // descending eigenvalue through w->perm, eigenvalues (sorted) into lam_sorted
 int sym_eig_sorted(ufem_warm *w, int l, std::vector<double> &lam_sorted, std::vector<int> &order) {
-  static int configured_for = 0;
-  const size_t smem = jacobi_smem(l);
-  if (configured_for < (int)smem) {
-    UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured_for = (int)smem;
-  }
-  k_jacobi_eig<<<1, kJacThreads, smem>>>(l, w->G.p, w->V.p, w->lam.p, 60, w->sweeps.p);
-  UFEM_CUDA_TRY(cudaGetLastError());
+  int rv;
+  if (l > kSmemL && (rv = w->Vg.ensure((size_t)l * l))) return rv;
+  if ((rv = jacobi_eig(l, w->G.p, w->V.p, w->lam.p, w->sweeps.p, w->Vg.p))) return rv;
   std::vector<double> lam(l);
   UFEM_CUDA_TRY(cudaMemcpy(lam.data(), w->lam.p, l * sizeof(double), cudaMemcpyDeviceToHost));
   order.resize(l);
@@ -816,13 +865,13 @@ int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
       (rv = w->u0.ensure((size_t)w->n * S)))
     return rv;
   if (w->o.guess_mode == 1 && w->galerkin) {
-    const size_t smem = (size_t)r * (r + 1) * sizeof(double);
+    const size_t smem = (size_t)r * (r + 1) / 2 * sizeof(double);
     static size_t configured = 0;
     if (configured < smem) {
       UFEM_CUDA_TRY(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       configured = smem;
     }
-    k_reduced_solve<<<(unsigned)nsamp, 128, smem>>>(nsamp, r, w->nmult, w->m->mc_ilen, d_ifld, w->d_mcol.p, w->Gv.p,
+    k_reduced_solve<<<(unsigned)nsamp, kRedThreads, smem>>>(nsamp, r, w->nmult, w->m->mc_ilen, d_ifld, w->d_mcol.p, w->Gv.p,
                                                      w->PF0.p, w->novr, w->d_ovar.p, w->Prow.p, w->c.p);
     if (w->guess_scale != 1.0) k_mul<<<grid1(nsamp * r), 256>>>(nsamp * r, w->guess_scale, w->c.p);
   } else {
@@ -853,6 +902,7 @@ void ufem_warm_default_options(ufem_warm_options *o) {
   o->seed = 20261203ULL;
   o->guess_mode = 0;
   o->n_coarse = 64;
+  o->snap_tol = 1e-11;
 }
 
 int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out) {
@@ -864,7 +914,7 @@ int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out)
   if (o->n_modes < 16 || o->n_modes % 16 || o->n_modes + 16 > kMaxL || o->n_feat < 1 || o->n_feat > 32 ||
       o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 || o->n_snapshots < o->n_modes + 16 ||
       o->n_coarse < 0 || o->n_coarse % 16) {
-    set_error("ufem_warm_create: n_modes a multiple of 16 up to 80, 1..32 inputs, n_hidden a multiple of 16 up to "
+    set_error("ufem_warm_create: n_modes a multiple of 16 up to 128, 1..32 inputs, n_hidden a multiple of 16 up to "
               "256, n_snapshots >= n_modes + 16, n_coarse a multiple of 16");
     return UFEM_AF_ERR_SIZ;
   }
@@ -934,20 +984,28 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   cold.coarse = 0;
   cudaEventRecord(e0);
   if ((rv = w->U.ensure((size_t)n * ntrain)) || (rv = w->st.ensure(ntrain)) || (rv = w->it.ensure(ntrain))) return rv;
+  // the first n_snapshots samples (the POD snapshots) at snap_tol: the tail
+  // modes of the basis then hold solution content rather than solver error
+  ufem_mc_options snap = cold;
+  if (w->o.snap_tol > 0.0) snap.tol = std::min(cold.tol, w->o.snap_tol);
+  const long nsnap = std::min<long>(w->o.n_snapshots, ntrain);
   {
     DBuf<double> uchunk;
     const long chunk = 4096;
-    for (long c0 = 0; c0 < ntrain; c0 += chunk) {
-      const long cn = std::min(chunk, ntrain - c0);
+    for (long c0 = 0; c0 < ntrain;) {
+      const bool is_snap = c0 < nsnap;
+      const long cn = std::min(chunk, (is_snap ? nsnap : ntrain) - c0);
       const int S = padded_S(cn);
       if ((rv = uchunk.ensure((size_t)n * S))) return rv;
       const double *pin = d_ifld + c0 * m->mc_ilen;
       double *pu = uchunk.p;
       int *ps = w->st.p + c0;
       long *pi = w->it.p + c0;
-      if ((rv = mc_solve_device(1, &m, &cn, &pin, nullptr, &ps, &pi, nullptr, &pu, &cold))) return rv;
+      if ((rv = mc_solve_device(1, &m, &cn, &pin, nullptr, &ps, &pi, nullptr, &pu, is_snap ? &snap : &cold)))
+        return rv;
       UFEM_CUDA_TRY(cudaMemcpy2DAsync(w->U.p + c0, ntrain * sizeof(double), uchunk.p, S * sizeof(double),
                                       cn * sizeof(double), n, cudaMemcpyDeviceToDevice));
+      c0 += cn;
     }
   }
   {
@@ -955,20 +1013,25 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
     std::vector<long> hi(ntrain);
     UFEM_CUDA_TRY(cudaMemcpy(hs.data(), w->st.p, ntrain * sizeof(int), cudaMemcpyDeviceToHost));
     UFEM_CUDA_TRY(cudaMemcpy(hi.data(), w->it.p, ntrain * sizeof(long), cudaMemcpyDeviceToHost));
-    long mx = 0;
+    long mx = 0, cnt = 0;
     double sum = 0;
+    // the cap of the warm runs: the cold iteration counts at the caller's
+    // tolerance (the snapshots' counts when every sample is a snapshot)
+    const bool all_snap = nsnap >= ntrain || snap.tol == cold.tol;
     for (long s = 0; s < ntrain; s++) {
       if (hs[s] != UFEM_ST_CONVERGED) {
         set_error("ufem_warm_train: a training sample did not converge");
         return UFEM_AF_ERR;
       }
+      if (s < nsnap && !all_snap) continue;
       mx = std::max(mx, hi[s]);
       sum += (double)hi[s];
+      cnt++;
     }
     w->cold_cap = mx;
     w->train_precision = cold.precision;
     st.cold_iters_max = mx;
-    st.cold_iters_mean = sum / (double)ntrain;
+    st.cold_iters_mean = sum / (double)std::max<long>(1, cnt);
   }
   st.ms_solve = ms_since(e0);
   // 2. POD basis from the first n_snapshots solutions
@@ -1192,23 +1255,20 @@ int ufem_dgemm_f64(int M, int N, long K, const double *d_A, const double *d_B, d
 }
 
 // Symmetric eigen-decomposition through the warm start's one-block Jacobi
-// kernel, for its tests: A [l x l] (l even, <= 96) -> V [l x l] (columns =
+// kernel, for its tests: A [l x l] (l even, <= 144) -> V [l x l] (columns =
 // eigenvectors, unsorted), lam [l].  Host arrays.
 int ufem_sym_eig(int l, const double *h_A, double *h_V, double *h_lam, int *sweeps) {
   if (l < 2 || l % 2 || l > kMaxL) {
-    set_error("ufem_sym_eig: l even, 2..96");
+    set_error("ufem_sym_eig: l even, 2..144");
     return UFEM_AF_ERR_SIZ;
   }
-  DBuf<double> A, V, lam;
+  DBuf<double> A, V, lam, Vg;
   DBuf<int> sw;
   int rv;
   if ((rv = A.upload(h_A, (size_t)l * l)) || (rv = V.ensure((size_t)l * l)) || (rv = lam.ensure(l)) ||
-      (rv = sw.ensure(1)))
+      (rv = sw.ensure(1)) || (rv = Vg.ensure((size_t)l * l)))
     return rv;
-  const size_t smem = jacobi_smem(l);
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_jacobi_eig<<<1, kJacThreads, smem>>>(l, A.p, V.p, lam.p, 60, sw.p);
-  UFEM_CUDA_TRY(cudaGetLastError());
+  if ((rv = jacobi_eig(l, A.p, V.p, lam.p, sw.p, Vg.p))) return rv;
   UFEM_CUDA_TRY(cudaMemcpy(h_V, V.p, (size_t)l * l * sizeof(double), cudaMemcpyDeviceToHost));
   UFEM_CUDA_TRY(cudaMemcpy(h_lam, lam.p, l * sizeof(double), cudaMemcpyDeviceToHost));
   if (sweeps) UFEM_CUDA_TRY(cudaMemcpy(sweeps, sw.p, sizeof(int), cudaMemcpyDeviceToHost));
