@@ -102,7 +102,7 @@ def parse():
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
            2: ("k_batch_pcg_coarse_40x10x10_1024samples.md",
-               "40x10x10 16 E zones x 1024 samples, 80-mode coarse space, 40 iterations")}
+               "40x10x10 16 E zones x 1024 samples, coarse space of a short warm-start training, 40 iterations")}
 
 
 def profile_case(a):
