@@ -1849,13 +1849,9 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     }
   }
   const size_t dsmem = coarse ? kCoarseSmem : 0;
-  if (coarse) {
-    UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
-    // all of the unified L1 / shared memory as shared memory, so that two
-    // blocks (about 87 KB each) fit on an SM
-    UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared));
-  }
+  // one block per SM either way (tensor memory): the rest of the unified
+  // L1 / shared memory stays L1 for the contribution records
+  if (coarse) UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
   const int nthreads = coarse ? kCoarseThreads : kThreads, nwarps = nthreads / 32;
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nthreads, dsmem));
   if (occ < 1) {
@@ -1868,7 +1864,9 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   // rows per tile: about tiles_per_block tiles per block over the whole batch
   long total_rows = 0;
   for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
-  const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : 12;  // measured best on B200 for both forms
+  // measured best on B200: 12 for both forms (2 x 256-thread blocks per SM),
+  // 24 for the coarse-corrected instance (1 x 512)
+  const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : (coarse ? 24 : 12);
   g_stats.tiles_per_block = (int)tpb;
   g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 2) : 0;
   g_stats.lane_samples = VN;
