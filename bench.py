@@ -516,6 +516,7 @@ def ours(a):
     pcg_launches = 0
     fallbacks = 0
     with ClockSampler(os.path.join(tempfile.gettempdir(), f"ufem_clocks_{rank}.csv")) as clk:
+        step_device()  # one more untimed step once the sampler runs
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

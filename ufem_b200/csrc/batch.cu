@@ -1185,30 +1185,21 @@ __device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk,
   double *zc = M.z + (size_t)g * 128 + ms;
   const int rbase = chunk * 128 + j0;
   const int nrow = min(kRows, M.n - rbase);  // rows of this thread's share in the mesh
-  constexpr int kR = 16;                     // rows per step; the next step's z loads fly during this one
-  double cur[kR], nxt[kR];
+  // all z loads of this thread are in flight during the MMAs
+  double zv[kRows];
 #pragma unroll
-  for (int e = 0; e < kR; e++) cur[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : 0.0;
+  for (int e = 0; e < kRows; e++) zv[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : 0.0;
   const bool ok = tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
   tc::fence_after_sync();
   if (!ok) coarse_fail(gb);
-  for (int jj = 0; jj < kRows; jj += kR) {
-    if (jj + kR < kRows) {
 #pragma unroll
-      for (int e = 0; e < kR; e++)
-        nxt[e] = jj + kR + e < nrow ? __ldcg(zc + (size_t)(rbase + jj + kR + e) * S) : 0.0;
-    }
-    uint32_t v[8], w[8];
-    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + jj), v);
-    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + jj + 8), w);
+  for (int e0 = 0; e0 < kRows; e0 += 8) {
+    uint32_t v[8];
+    tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + e0), v);
 #pragma unroll
-    for (int e = 0; e < kR; e++) {
-      const float add = __uint_as_float(e < 8 ? v[e] : w[e - 8]);
-      if (jj + e < nrow) zc[(size_t)(rbase + jj + e) * S] = cur[e] + (double)add;
-    }
-#pragma unroll
-    for (int e = 0; e < kR; e++) cur[e] = nxt[e];
+    for (int e = 0; e < 8; e++)
+      if (e0 + e < nrow) zc[(size_t)(rbase + e0 + e) * S] = zv[e0 + e] + (double)__uint_as_float(v[e]);
   }
   tc::fence_before_sync();
   __syncthreads();  // the next item restages the operand tiles and reuses the accumulator
@@ -1965,7 +1956,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     *iters_run = 0;
     return UFEM_AF_OK;
   }
-  // coarse phases: about one wave of C1 row ranges over all active groups
+  // coarse phases: C1 row ranges of every active group, C3 128-row chunks
   std::vector<int4> c1items, c3items;
   int max_cmodes = 0;
   if (coarse) {
@@ -1975,6 +1966,8 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       McWork &w = *W[k];
       if (P->cmodes <= 0) continue;
       const int n = b.n, n64 = (n + 63) / 64, n128 = (n + 127) / 128;
+      // at most one wave of row ranges: finer ranges that do not fill whole
+      // waves leave the phase waiting on its last blocks (measured)
       int nsplit = std::max(1, std::min(n64, G / active_groups));
       b.rps = (n64 + nsplit - 1) / nsplit * 64;
       b.nsplit = (n + b.rps - 1) / b.rps;
