@@ -521,11 +521,12 @@ def ours(a):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        step_wall = []
+        step_wall, step_pcg = [], []
         for _ in range(a.steps):
             t_step = time.perf_counter()
             step_device()
             step_wall.append(1000.0 * (time.perf_counter() - t_step))
+            step_pcg.append(wst.pcg_ms)
             launches += wst.kernel_launches
             pcg_ms += wst.pcg_ms
             pcg_bytes += wst.pcg_bytes
@@ -763,6 +764,7 @@ def ours(a):
                     "d2h_bytes_per_step": d2h, "matches_device_run": e2e_ok},
             "gpu_launches": launches, "clocks": clk.summary(local),
             "step_wall_ms": [round(t, 1) for t in step_wall],
+            "step_pcg_ms": [round(t, 1) for t in step_pcg],
             "uneven_batch": uneven,
             "static_configs": static,
             "cpu_baseline": cpu,

@@ -350,6 +350,9 @@ typedef struct ufem_warm_options {
                                 with at most 64 E variables) */
   double snap_tol;           /* relative residual of the snapshot solves (the first n_snapshots
                                 training samples; default 1e-11, 0: the training tolerance) */
+  int order_samples;         /* ufem_warm_solve groups samples of similar spread of log(E / mean E)
+                                into the same 128-sample groups (outputs in the caller's order;
+                                default 1) */
 } ufem_warm_options;
 
 typedef struct ufem_warm_train_stats {

@@ -42,7 +42,8 @@ class WarmOptions(C.Structure):
     _fields_ = [("n_modes", C.c_int), ("n_hidden", C.c_int), ("n_feat", C.c_int), ("feat_cols", C.c_long * 32),
                 ("feat_log", C.c_int * 32), ("scale_col", C.c_long), ("n_snapshots", C.c_long),
                 ("power_iters", C.c_int), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
-                ("seed", C.c_ulonglong), ("guess_mode", C.c_int), ("n_coarse", C.c_int), ("snap_tol", C.c_double)]
+                ("seed", C.c_ulonglong), ("guess_mode", C.c_int), ("n_coarse", C.c_int), ("snap_tol", C.c_double),
+                ("order_samples", C.c_int)]
 
 
 class WarmTrainStats(C.Structure):

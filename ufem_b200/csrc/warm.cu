@@ -407,6 +407,35 @@ __global__ void k_gather_rows(long nrow, int ncol, const long *__restrict__ idx,
   dst[e] = src[idx[r] * ncol + (e % ncol)];
 }
 
+// rows of src scattered back to the rows idx of a row-major matrix
+template <typename T>
+__global__ void k_scatter_rows(long nrow, int ncol, const long *__restrict__ idx, const T *__restrict__ src,
+                               T *__restrict__ dst) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nrow * ncol) return;
+  const long r = e / ncol;
+  dst[idx[r] * ncol + (e % ncol)] = src[e];
+}
+
+// Ordering score of a sample: the spread (standard deviation) over its E
+// variables of log(a_v / mean a_v).  Samples far from the mean operator --
+// the coarse space's -- need more PCG iterations (correlation 0.77 on the
+// zone beam), and a group of 128 samples iterates until its slowest one.
+__global__ void k_order_score(long nsamp, long ilen, int nmult, const double *__restrict__ ifld,
+                              const int *__restrict__ mcol, const double *__restrict__ log_abar,
+                              double *__restrict__ score) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsamp) return;
+  double m1 = 0.0, m2 = 0.0;
+  for (int v = 1; v < nmult; v++) {
+    const double t = log(fabs(ifld[s * ilen + mcol[v]])) - log_abar[v];
+    m1 += t;
+    m2 += t * t;
+  }
+  const double k = (double)max(1, nmult - 1);
+  score[s] = m2 / k - (m1 / k) * (m1 / k);
+}
+
 // |u0_s - u_s| / |u_s| per sample, both [n][S], in two passes with a fixed
 // order: k_rel_err_part sums a chunk of rows for 32 samples per block (8
 // warps stride the chunk, combined in warp order), k_rel_err adds the chunks.
@@ -612,6 +641,10 @@ struct ufem_warm {
   int novr = 0;
   double guess_scale = 1.0;
   int coarse_modes = 0;                   // modes of the preconditioner's coarse space
+  DBuf<double> log_abar;                  // log of the training samples' mean multipliers (sample ordering)
+  DBuf<double> score, ifperm, ofperm;
+  DBuf<int> stperm;
+  DBuf<long> itperm, sperm;
   // basis and normalisation
   DBuf<double> phi;                       // [n][r]
   DBuf<double> fmean, fsd, cmean, csd;    // feature / coefficient statistics
@@ -790,6 +823,11 @@ int build_coarse(ufem_warm *w, long ntrain, const double *d_ifld) {
     for (long s = 0; s < ntrain; s++) t += ifl[(size_t)s * ilen + mcol[v]];
     abar[v] = t / (double)ntrain;
   }
+  {
+    std::vector<double> la(nmult);
+    for (int v = 0; v < nmult; v++) la[v] = std::log(std::fabs(abar[v]));
+    if ((rv = w->log_abar.upload(la.data(), nmult))) return rv;
+  }
   // Ebar (rc x rc), then its Cholesky factor in place (lower triangle)
   std::vector<double> L((size_t)rc * rc, 0.0);
   for (int i = 0; i < rc; i++)
@@ -903,6 +941,7 @@ void ufem_warm_default_options(ufem_warm_options *o) {
   o->guess_mode = 0;
   o->n_coarse = 64;
   o->snap_tol = 1e-11;
+  o->order_samples = 1;
 }
 
 int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out) {
@@ -1089,13 +1128,12 @@ int ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u0
   return UFEM_AF_OK;
 }
 
-int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
-                    const ufem_mc_options *opt_in, ufem_warm_stats *ws) {
-  if (!w || !d_ifld) return UFEM_AF_ERR_EMP;
-  if (!w->trained) {
-    set_error("ufem_warm_solve: the warm start is not trained");
-    return UFEM_AF_ERR;
-  }
+}  // extern "C"
+
+namespace {
+// the warm-started solve of the samples in the given order
+int warm_solve_ordered(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
+                       const ufem_mc_options *opt_in, ufem_warm_stats *ws) {
   int rv;
   ufem_mc_options opt;
   if (opt_in) opt = *opt_in;
@@ -1214,6 +1252,51 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
   st.ms_total = (double)a + b + c;
   cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   if (ws) *ws = st;
+  return UFEM_AF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+// Samples are solved in the order of their ordering score (stable, so the
+// same batch gives the same grouping every run) and the outputs returned in
+// the caller's order: similar samples share a 128-sample group.
+int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
+                    const ufem_mc_options *opt_in, ufem_warm_stats *ws) {
+  if (!w || !d_ifld) return UFEM_AF_ERR_EMP;
+  if (!w->trained) {
+    set_error("ufem_warm_solve: the warm start is not trained");
+    return UFEM_AF_ERR;
+  }
+  if (!w->o.order_samples || !w->galerkin || w->nmult < 2 || !w->log_abar.p || nsamp <= 128)
+    return warm_solve_ordered(w, nsamp, d_ifld, d_ofld, d_status, d_iters, opt_in, ws);
+  int rv;
+  const long ilen = w->m->mc_ilen, olen = w->m->mc_olen;
+  if ((rv = w->score.ensure(nsamp)) || (rv = w->sperm.ensure(nsamp)) || (rv = w->ifperm.ensure((size_t)nsamp * ilen)) ||
+      (rv = w->stperm.ensure(nsamp)) || (rv = w->itperm.ensure(nsamp)) ||
+      (rv = w->ofperm.ensure((size_t)nsamp * std::max<long>(1, olen))))
+    return rv;
+  k_order_score<<<grid1(nsamp), 256>>>(nsamp, ilen, w->nmult, d_ifld, w->d_mcol.p, w->log_abar.p, w->score.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  std::vector<double> sc(nsamp);
+  UFEM_CUDA_TRY(cudaMemcpy(sc.data(), w->score.p, nsamp * sizeof(double), cudaMemcpyDeviceToHost));
+  for (auto &x : sc)
+    if (!std::isfinite(x)) x = HUGE_VAL;  // non-finite inputs last
+  std::vector<long> perm(nsamp);
+  std::iota(perm.begin(), perm.end(), 0L);
+  std::stable_sort(perm.begin(), perm.end(), [&](long a, long b) { return sc[a] < sc[b]; });
+  if ((rv = w->sperm.upload(perm.data(), nsamp))) return rv;
+  k_gather_rows<double><<<grid1(nsamp * ilen), 256>>>(nsamp, (int)ilen, w->sperm.p, d_ifld, w->ifperm.p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  if ((rv = warm_solve_ordered(w, nsamp, w->ifperm.p, d_ofld ? w->ofperm.p : nullptr, w->stperm.p, w->itperm.p,
+                               opt_in, ws)))
+    return rv;
+  if (d_ofld && olen > 0)
+    k_scatter_rows<double><<<grid1(nsamp * olen), 256>>>(nsamp, (int)olen, w->sperm.p, w->ofperm.p, d_ofld);
+  if (d_status) k_scatter_rows<int><<<grid1(nsamp), 256>>>(nsamp, 1, w->sperm.p, w->stperm.p, d_status);
+  if (d_iters) k_scatter_rows<long><<<grid1(nsamp), 256>>>(nsamp, 1, w->sperm.p, w->itperm.p, d_iters);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  if (ws) ws->kernel_launches += 5;
   return UFEM_AF_OK;
 }
 
