@@ -1661,6 +1661,29 @@ struct McWork {
 
 static ufem_mc_stats g_stats;
 
+// Per-launch tables of the persistent PCG (mesh descriptors, work lists,
+// grid barrier, counters), kept per device for the life of the process and
+// only grown: a cudaFree per solve would synchronise the device and cost a
+// variable few milliseconds.
+template <typename T>
+struct LaunchBufs {
+  DBuf<BMesh<T>> meshes;
+  DBuf<int4> tiles, c1, c3;
+  DBuf<GridBar> bar;
+  DBuf<int> cnt, rcnt;
+  DBuf<long> itout;
+};
+template <typename T>
+LaunchBufs<T> &launch_bufs() {
+  static std::vector<std::pair<int, std::unique_ptr<LaunchBufs<T>>>> per_dev;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  for (auto &e : per_dev)
+    if (e.first == dev) return *e.second;
+  per_dev.emplace_back(dev, std::unique_ptr<LaunchBufs<T>>(new LaunchBufs<T>()));
+  return *per_dev.back().second;
+}
+
 // ---------------------------------------------------------------------------
 // autotuned launch shapes: (tiles per block, gather unroll) per batch shape,
 // kept in memory and in a text cache file (one "key tpb unroll ms" per line)
@@ -1723,16 +1746,27 @@ static int coarse_modes(int nmesh, ufem_model *const *models, const ufem_mc_opti
 
 static std::string tune_key(int nmesh, ufem_model *const *models, const long *nsamp, int precision,
                             int cmodes = 0) {
-  int dev = 0, nsm = 0;
+  // the device part once per device: cudaGetDeviceProperties takes several
+  // milliseconds, erratically, and this runs on every solve
+  static std::vector<std::pair<int, std::string>> dev_names;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaDeviceProp prop;
-  cudaGetDeviceProperties(&prop, dev);
-  std::string name = prop.name;
-  for (auto &c : name)
-    if (c == ' ') c = '_';
-  std::string k = name + "/sm" + std::to_string(nsm) + "/p" + std::to_string(precision) + "/b" +
-                  std::to_string(models[0]->b);
+  std::string name, *cached = nullptr;
+  for (auto &e : dev_names)
+    if (e.first == dev) cached = &e.second;
+  if (!cached) {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, dev);
+    std::string nm = prop.name;
+    for (auto &c : nm)
+      if (c == ' ') c = '_';
+    dev_names.emplace_back(dev, nm + "/sm" + std::to_string(nsm));
+    cached = &dev_names.back().second;
+  }
+  name = *cached;
+  std::string k = name + "/p" + std::to_string(precision) + "/b" + std::to_string(models[0]->b);
   for (int i = 0; i < nmesh; i++)
     k += "/" + std::to_string(models[i]->nbr) + "x" +
          std::to_string(std::max<long>(128, (nsamp[i] + 127) / 128 * 128));
@@ -1992,15 +2026,16 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     }
   }
   g_stats.coarse_modes = max_cmodes;
-  DBuf<BMesh<T>> d_meshes;
-  DBuf<int4> d_tiles, d_c1, d_c3;
-  DBuf<GridBar> bar;
-  DBuf<int> cnt, rcnt;
-  DBuf<long> itout;
+  LaunchBufs<T> &LB = launch_bufs<T>();
+  auto &d_meshes = LB.meshes;
+  auto &d_tiles = LB.tiles, &d_c1 = LB.c1, &d_c3 = LB.c3;
+  auto &bar = LB.bar;
+  auto &cnt = LB.cnt, &rcnt = LB.rcnt;
+  auto &itout = LB.itout;
   const int zero = 0;
   if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
-      (rv = bar.alloc(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
-      (rv = itout.alloc(1)))
+      (rv = bar.ensure(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
+      (rv = itout.ensure(1)))
     return rv;
   if (!c1items.empty() && ((rv = d_c1.upload(c1items.data(), c1items.size())) ||
                            (rv = d_c3.upload(c3items.data(), c3items.size()))))
