@@ -347,7 +347,8 @@ typedef struct ufem_warm_options {
   int n_coarse;              /* the leading POD modes that become the coarse space of the
                                 PCG preconditioner after training (ufem_mc_set_coarse; at
                                 most n_modes, a multiple of 16; 0: none; default 64; models
-                                with at most 64 E variables) */
+                                with at most 64 E variables); modes with energy below 1e-20
+                                of the first are left out (rounded down to a multiple of 16) */
   double snap_tol;           /* relative residual of the snapshot solves (the first n_snapshots
                                 training samples; default 1e-11, 0: the training tolerance) */
   int order_samples;         /* ufem_warm_solve groups samples of similar spread of log(E / mean E)

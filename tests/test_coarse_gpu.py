@@ -207,7 +207,7 @@ def test_warm_start_sets_coarse_space():
     ws = WarmStart(g, cols, logs, sc, n_modes=32, n_hidden=64, n_snapshots=256, epochs=20, batch=128,
                    n_coarse=32)
     ts = ws.train(mg.warm_samples(m, 512), precision=2)
-    assert ts["coarse_modes"] == 32
+    assert ts["coarse_modes"] in (16, 32)   # the modes above the energy floor, a multiple of 16
     ws.set_guess_mode(1)
     ev = mg.warm_samples(m, 200, first_sample=5000)
     o0, st0, it0, w0 = ws.solve(ev, precision=2, coarse=False)

@@ -806,7 +806,17 @@ int build_galerkin(ufem_warm *w) {
 // be a fixed symmetric positive definite map.  Pivots below 1e-13 of the
 // largest drop their mode.
 int build_coarse(ufem_warm *w, long ntrain, const double *d_ifld) {
-  const int rc = std::min(w->o.n_coarse, w->r);
+  // only modes that carry solution content: energy above 1e-20 of the first
+  // (singular values 1e-10 of the first, far above the error of snapshots
+  // solved to 1e-11) -- beyond the family's numerical rank a mode is solver
+  // noise, and the additive correction would lift it to the top of the
+  // preconditioned spectrum; a multiple of 16 (the MMA's N granularity)
+  int rc = std::min(w->o.n_coarse, w->r);
+  {
+    int keep = 0;
+    while (keep < rc && keep < (int)w->sigma2.size() && w->sigma2[keep] > 1e-20 * w->sigma2[0]) keep++;
+    rc = keep / 16 * 16;
+  }
   w->coarse_modes = 0;
   if (!w->galerkin || rc < 16) return ufem_mc_set_coarse(w->m, 0, nullptr);
   int rv;
