@@ -243,3 +243,31 @@ def test_warm_solve_sample_ordering_returns_callers_order():
     assert (st0 == 0).all() and (st1 == 0).all()
     assert (np.abs(o1 - o0).max(axis=1) <= 1e-6 * np.abs(o0).max(axis=1)).all()
     assert np.abs(it1 - it0).max() <= 2
+
+
+def test_warm_solve_ordering_with_non_finite_samples():
+    """Non-finite inputs sort last (their ordering score is not finite): they
+    report UFEM_ST_NAN at their own positions, every other sample converges
+    to the outputs it has in a batch without them."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import ST_NAN
+    from ufem_b200.warm import WarmStart
+    m = mg.warm_beam(24, 6, 6, zones=8)
+    g = GpuModel(m)
+    cols, logs, sc = mg.warm_features(m)
+    ws = WarmStart(g, cols, logs, sc, n_modes=32, n_hidden=64, n_snapshots=256, epochs=5, batch=128, n_coarse=32)
+    ws.train(mg.warm_samples(m, 512), precision=2)
+    ws.set_guess_mode(1)
+    ev = mg.warm_samples(m, 260, first_sample=3000)
+    bad = [3, 140, 259]
+    evb = ev.copy()
+    evb[bad[0], 0] = np.nan          # an E
+    evb[bad[1], 5] = np.inf          # another E
+    evb[bad[2], len(m.mp_vals)] = np.nan  # the load factor
+    o0, st0, it0, _ = ws.solve(ev, precision=2)
+    o1, st1, it1, _ = ws.solve(evb, precision=2)
+    good = np.setdiff1d(np.arange(ev.shape[0]), bad)
+    assert (st0 == 0).all()
+    assert (st1[bad] == ST_NAN).all() and (st1[good] == 0).all()
+    assert (np.abs(o1[good] - o0[good]).max(axis=1) <= 1e-6 * np.abs(o0[good]).max(axis=1)).all()
