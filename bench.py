@@ -60,8 +60,8 @@ WARM_EVAL = 8192
 EVAL_FIRST = 1 << 20     # evaluation sample ids: disjoint from training
 METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 PCG, 1 B200"
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
-            "warm-started and coarse-corrected (POD {m} modes from 512 solves: Galerkin guess + PCG coarse space; "
-            "MLP 17-256-256-{m} trained on 4096 solves)")
+            "warm-started (POD 64 modes from 512 solves, Galerkin guess; MLP 17-256-256-64 trained on 4096 solves) "
+            "and coarse-corrected (PCG coarse space on {c} POD modes of the same snapshots)")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
           2: "k_batch_pcg<double,3,implicit>"}
@@ -83,8 +83,10 @@ def parse():
     p.add_argument("--no-coarse", action="store_true",
                    help="headline without the coarse correction of the preconditioner (Jacobi PCG)")
     p.add_argument("--coarse-modes", type=int, default=128,
-                   help="POD modes of the basis and of the preconditioner's coarse space (a multiple of 16, "
-                        "at most 128)")
+                   help="POD modes of the preconditioner's coarse space (a multiple of 16, at most 128); the "
+                        "guess and the MLP use the 64-mode basis of the learned-warm-start config")
+    p.add_argument("--big-modes", type=int, default=128,
+                   help="a second warm start whose guess also uses this many modes, reported beside (0: none)")
     p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--guess", type=int, default=1,
@@ -122,7 +124,7 @@ def profile_case(a):
             from ufem_b200.warm import WarmStart
             g = GpuModel(m)
             cols, logs, scale_col = mg.warm_features(m)
-            ws = WarmStart(g, cols, logs, scale_col, n_modes=a.coarse_modes, n_hidden=64, n_snapshots=512, epochs=2,
+            ws = WarmStart(g, cols, logs, scale_col, n_modes=64, n_hidden=64, n_snapshots=512, epochs=2,
                            batch=256, n_coarse=a.coarse_modes)
             ws.train(mg.warm_samples(m, 1024, first_sample=EVAL_FIRST), precision=2)
     else:
@@ -331,7 +333,7 @@ def reference_arm(a):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(m=max(64, a.coarse_modes)), "solver": "reference monte_solution (SSOR PCG, eps 1e-21)",
+            "config": {"workload": WORKLOAD.format(c=a.coarse_modes), "solver": "reference monte_solution (SSOR PCG, eps 1e-21)",
                        "processes": procs},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "reference",
                              "sample": f"per step: {procs} processes x 1 evaluation sample of the 40x10x10 "
@@ -484,7 +486,7 @@ def ours(a):
     m, train, ev = warm_setup(a, rank)
     g = GpuModel(m)
     cols, logs, scale_col = mg.warm_features(m)
-    ws = WarmStart(g, cols, logs, scale_col, n_modes=max(64, a.coarse_modes), n_hidden=256, n_snapshots=512,
+    ws = WarmStart(g, cols, logs, scale_col, n_modes=64, n_hidden=256, n_snapshots=512,
                    epochs=a.epochs, batch=256, lr=2e-3, n_coarse=a.coarse_modes)
     t0 = time.perf_counter()
     tstats = ws.train(train, precision=a.precision)
@@ -624,8 +626,7 @@ def ours(a):
                                                                / np.abs(out_warm).max())}
 
     # ---- the other guess (MLP <-> POD-Galerkin), same precision ------------
-    GUESS = {0: f"the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> {max(64, a.coarse_modes)} "
-                "coefficients)",
+    GUESS = {0: "the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> 64 coefficients)",
              1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the per-zone reduced "
                 "operators) on the learned POD basis"}
     galerkin = None
@@ -650,6 +651,35 @@ def ours(a):
                     "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
                                                               / np.abs(out_warm).max())}
         L.ufem_warm_set_guess_mode(ws.h, a.guess)
+
+    # ---- a larger basis: the same samples with a separately trained warm
+    # start of --big-modes modes (guess and coarse space), same precision.
+    # Its training sets its coarse space on the model: this runs after every
+    # precision-2 section of the headline warm start.
+    big = None
+    if a.big_modes and a.big_modes != 64 and not a.no_other:
+        wsb = WarmStart(g, cols, logs, scale_col, n_modes=a.big_modes, n_hidden=256, n_snapshots=512,
+                        epochs=a.epochs, batch=256, lr=2e-3, n_coarse=max(a.coarse_modes, a.big_modes))
+        tsb = wsb.train(train, precision=a.precision)
+        wsb.set_guess_mode(a.guess)
+        wstb = _lib.WarmStats()
+        argsb = (wsb.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt),
+                 C.byref(wstb))
+        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*argsb))
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*argsb))
+        e1.record()
+        torch.cuda.synchronize()
+        msb = e0.elapsed_time(e1) / a.steps
+        big = {"modes": a.big_modes, "coarse_modes": tsb["coarse_modes"], "value": n / (msb / 1000.0),
+               "unit": "solves/s", "ms_per_step": msb, "iters_mean": wstb.iters_mean, "iters_max": wstb.iters_max,
+               "guess_rel_err_mean": wstb.guess_err_mean, "fallbacks": wstb.fallbacks,
+               "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
+               "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
+                                                         / np.abs(out_warm).max())}
+        del wsb
 
     # ---- the warm start at the other precisions (one warm-up, one timed step)
     PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
@@ -725,7 +755,7 @@ def ours(a):
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if a.precision != 1 else "fp32 inner / fp64 refinement",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(m=max(64, a.coarse_modes)), "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
+            "config": {"workload": WORKLOAD.format(c=a.coarse_modes), "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
                        "precision": PREC[a.precision],
                        "l2_flush": "not needed: every per-sample vector is 0.98 GB (FP64, 8192 samples) and the "
                                    "explicit FP32 values 34 GB per iteration, >> 126 MB L2",
@@ -750,6 +780,7 @@ def ours(a):
             "warm_start_without_coarse": no_coarse,
             "warm_start_other_precisions": other,
             "warm_start_other_guess": galerkin,
+            "warm_start_larger_basis": big,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},

@@ -271,3 +271,28 @@ def test_warm_solve_ordering_with_non_finite_samples():
     assert (st0 == 0).all()
     assert (st1[bad] == ST_NAN).all() and (st1[good] == 0).all()
     assert (np.abs(o1[good] - o0[good]).max(axis=1) <= 1e-6 * np.abs(o0[good]).max(axis=1)).all()
+
+
+def test_coarse_space_wider_than_the_guess_basis():
+    """n_coarse > n_modes: the POD fit computes max(n_modes, n_coarse) modes,
+    the guess and the MLP use the leading n_modes, the coarse space up to
+    n_coarse (above the energy floor); the basis returned has n_modes
+    columns, and the solve matches the one without a coarse space."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.warm import WarmStart
+    m = mg.warm_beam(24, 6, 6, zones=8)
+    g = GpuModel(m)
+    cols, logs, sc = mg.warm_features(m)
+    ws = WarmStart(g, cols, logs, sc, n_modes=32, n_hidden=64, n_snapshots=256, epochs=5, batch=128, n_coarse=64)
+    ts = ws.train(mg.warm_samples(m, 512), precision=2)
+    assert 32 < ts["coarse_modes"] <= 64
+    phi, s2 = ws.basis()
+    assert phi.shape[1] == 32 and np.abs(phi.T @ phi - np.eye(32)).max() < 1e-8
+    ws.set_guess_mode(1)
+    ev = mg.warm_samples(m, 200, first_sample=5000)
+    o0, st0, it0, _ = ws.solve(ev, precision=2, coarse=False)
+    o1, st1, it1, _ = ws.solve(ev, precision=2, coarse=True)
+    assert (st0 == 0).all() and (st1 == 0).all()
+    assert np.abs(o1 - o0).max() <= 1e-6 * np.abs(o0).max()
+    assert it1.mean() < 0.8 * it0.mean()

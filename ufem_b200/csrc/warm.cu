@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduced_solve(long nsamp, int r
                                                                const double *__restrict__ G,
                                                                const double *__restrict__ PF0, int novr,
                                                                const int *__restrict__ ovar,
-                                                               const double *__restrict__ Prow,
+                                                               const double *__restrict__ Prow, int ldg,
                                                                double *__restrict__ c_out) {
   extern __shared__ double s_A[];  // packed lower triangle of the r x r system
   __shared__ double bb[kMaxR];
@@ -554,15 +554,15 @@ __global__ void __launch_bounds__(kRedThreads) k_reduced_solve(long nsamp, int r
   // A[i][k] = sum_v a_v G_v[i][k], k <= i: warp w takes rows w, w + kW, ...
   for (int i = warp; i < r; i += kW)
     for (int k = lane; k <= i; k += 32) {
-      const double *g = G + (size_t)i * r + k;
+      const double *g = G + (size_t)i * ldg + k;  // leading r x r block of each ldg x ldg operator
       double t = 0.0;
 #pragma unroll 4
-      for (int v = 0; v < nmult; v++) t = fma(av[v], __ldg(g + (size_t)v * r * r), t);
+      for (int v = 0; v < nmult; v++) t = fma(av[v], __ldg(g + (size_t)v * ldg * ldg), t);
       s_A[tri(i) + k] = t;
     }
   for (int i = tid; i < r; i += blockDim.x) {
     double t = PF0[i];
-    for (int j = 0; j < novr; j++) t += row[ovar[j]] * Prow[(size_t)j * r + i];
+    for (int j = 0; j < novr; j++) t += row[ovar[j]] * Prow[(size_t)j * ldg + i];
     bb[i] = t;
   }
   __syncthreads();
@@ -627,7 +627,8 @@ using namespace ufem;
 struct ufem_warm {
   ufem_model *m = nullptr;
   ufem_warm_options o;
-  int r = 0, l = 0;
+  int r = 0, l = 0;   // guess / MLP modes; subspace width of the POD fit
+  int rb = 0;         // basis columns computed: max(n_modes, n_coarse) (phi row stride)
   long n = 0;
   ufem_mlp *mlp = nullptr;
   bool trained = false;
@@ -719,7 +720,7 @@ int orthonormalise(ufem_warm *w, long rows, int l, const double *Yin, double *ou
 int fit_basis(ufem_warm *w, int S, long nsnap) {
   int rv;
   const long n = w->n;
-  const int l = w->l, r = w->r;
+  const int l = w->l, r = w->rb;  // every basis column (guess and coarse space)
   const long big = std::max<long>(nsnap, n);
   if ((rv = w->Y.ensure((size_t)big * l)) || (rv = w->Q.ensure((size_t)n * l)) ||
       (rv = w->Z.ensure((size_t)big * l)) || (rv = w->G.ensure((size_t)l * l)) ||
@@ -769,7 +770,7 @@ int build_galerkin(ufem_warm *w) {
   if ((rv = mc_implicit_view(w->m, &v))) return rv;
   w->galerkin = false;
   if (v.nmult > 64) return UFEM_AF_OK;
-  const int r = w->r;
+  const int r = w->rb;  // operators of every basis column; the guess uses the leading n_modes
   const long n = w->n;
   DBuf<double> Y;
   if ((rv = Y.ensure((size_t)n * r)) || (rv = w->Gv.ensure((size_t)v.nmult * r * r)) || (rv = w->PF0.ensure(r)))
@@ -811,7 +812,7 @@ int build_coarse(ufem_warm *w, long ntrain, const double *d_ifld) {
   // solved to 1e-11) -- beyond the family's numerical rank a mode is solver
   // noise, and the additive correction would lift it to the top of the
   // preconditioned spectrum; a multiple of 16 (the MMA's N granularity)
-  int rc = std::min(w->o.n_coarse, w->r);
+  int rc = std::min(w->o.n_coarse, w->rb);
   {
     int keep = 0;
     while (keep < rc && keep < (int)w->sigma2.size() && w->sigma2[keep] > 1e-20 * w->sigma2[0]) keep++;
@@ -820,7 +821,7 @@ int build_coarse(ufem_warm *w, long ntrain, const double *d_ifld) {
   w->coarse_modes = 0;
   if (!w->galerkin || rc < 16) return ufem_mc_set_coarse(w->m, 0, nullptr);
   int rv;
-  const int r = w->r, nmult = w->nmult;
+  const int r = w->rb, nmult = w->nmult;
   const long ilen = w->m->mc_ilen;
   std::vector<int> mcol(nmult);
   std::vector<double> ifl((size_t)ntrain * ilen), G((size_t)nmult * r * r);
@@ -920,7 +921,7 @@ int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
       configured = smem;
     }
     k_reduced_solve<<<(unsigned)nsamp, kRedThreads, smem>>>(nsamp, r, w->nmult, w->m->mc_ilen, d_ifld, w->d_mcol.p, w->Gv.p,
-                                                     w->PF0.p, w->novr, w->d_ovar.p, w->Prow.p, w->c.p);
+                                                     w->PF0.p, w->novr, w->d_ovar.p, w->Prow.p, w->rb, w->c.p);
     if (w->guess_scale != 1.0) k_mul<<<grid1(nsamp * r), 256>>>(nsamp * r, w->guess_scale, w->c.p);
   } else {
     if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) return rv;
@@ -928,7 +929,7 @@ int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
   }
   if (S > nsamp) UFEM_CUDA_TRY(cudaMemsetAsync(w->u0.p, 0, (size_t)w->n * S * sizeof(double)));
   // u0(i, s) = sum_k Phi[i][k] c[s][k]
-  return gemm_f64((int)w->n, (int)nsamp, r, w->phi.p, r, 1, w->c.p, 1, r, w->u0.p, S, 1, w->part);
+  return gemm_f64((int)w->n, (int)nsamp, r, w->phi.p, w->rb, 1, w->c.p, 1, r, w->u0.p, S, 1, w->part);
 }
 
 }  // namespace
@@ -960,11 +961,13 @@ int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out)
     set_error("ufem_warm_create: the model has no Monte Carlo variable table");
     return UFEM_AF_ERR_EMP;
   }
-  if (o->n_modes < 16 || o->n_modes % 16 || o->n_modes + 16 > kMaxL || o->n_feat < 1 || o->n_feat > 32 ||
-      o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 || o->n_snapshots < o->n_modes + 16 ||
+  if (o->n_modes < 16 || o->n_modes % 16 || std::max(o->n_modes, o->n_coarse) + 16 > kMaxL || o->n_feat < 1 ||
+      o->n_feat > 32 ||
+      o->n_hidden < 16 || o->n_hidden > 256 || o->n_hidden % 16 || o->batch < 1 ||
+      o->n_snapshots < std::max(o->n_modes, o->n_coarse) + 16 ||
       o->n_coarse < 0 || o->n_coarse % 16) {
     set_error("ufem_warm_create: n_modes a multiple of 16 up to 128, 1..32 inputs, n_hidden a multiple of 16 up to "
-              "256, n_snapshots >= n_modes + 16, n_coarse a multiple of 16");
+              "256, n_coarse a multiple of 16 up to 128, n_snapshots >= max(n_modes, n_coarse) + 16");
     return UFEM_AF_ERR_SIZ;
   }
   for (int f = 0; f < o->n_feat; f++)
@@ -980,7 +983,8 @@ int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out)
   w->m = m;
   w->o = *o;
   w->r = o->n_modes;
-  w->l = o->n_modes + 16;
+  w->rb = std::max(o->n_modes, o->n_coarse);
+  w->l = w->rb + 16;
   w->n = m->nDOFAct;
   int rv;
   std::vector<int> lg(o->n_feat);
@@ -1096,7 +1100,7 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   if ((rv = make_inputs(w, ntrain, d_ifld, true))) return rv;
   if ((rv = w->c.ensure((size_t)ntrain * r)) || (rv = w->Tt.ensure((size_t)ntrain * r))) return rv;
   // c[s][k] = sum_i U[i][s] Phi[i][k]
-  if ((rv = gemm_f64((int)ntrain, r, n, w->U.p, 1, ntrain, w->phi.p, r, 1, w->c.p, r, 1, w->part))) return rv;
+  if ((rv = gemm_f64((int)ntrain, r, n, w->U.p, 1, ntrain, w->phi.p, w->rb, 1, w->c.p, r, 1, w->part))) return rv;
   k_div_scale<<<grid1(ntrain * r), 256>>>(ntrain, r, w->sc.p, w->c.p);
   k_col_stats<<<1, 128>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p);
   k_targets<<<grid1(ntrain * r), 256>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p, w->Tt.p);
@@ -1332,7 +1336,9 @@ int ufem_warm_get_basis(const ufem_warm *w, double *h_phi, double *h_sigma2) {
     set_error("ufem_warm_get_basis: the warm start is not trained");
     return UFEM_AF_ERR;
   }
-  if (h_phi) UFEM_CUDA_TRY(cudaMemcpy(h_phi, w->phi.p, (size_t)w->n * w->r * sizeof(double), cudaMemcpyDeviceToHost));
+  if (h_phi)
+    UFEM_CUDA_TRY(cudaMemcpy2D(h_phi, w->r * sizeof(double), w->phi.p, w->rb * sizeof(double), w->r * sizeof(double),
+                               w->n, cudaMemcpyDeviceToHost));
   if (h_sigma2) std::memcpy(h_sigma2, w->sigma2.data(), w->r * sizeof(double));
   return UFEM_AF_OK;
 }
