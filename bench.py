@@ -99,6 +99,8 @@ def parse():
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
     p.add_argument("--profile-case", action="store_true",
                    help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
+    p.add_argument("--profile-static", action="store_true",
+                   help="the 128x128x64 block's FP64 PCG capped at 40 iterations (two launches) for ncu captures")
     return p.parse_args()
 
 
@@ -140,6 +142,33 @@ def profile_case(a):
                       "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
                       "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))
+
+
+def profile_static(a):
+    """A bounded case of the single-system FP64 PCG (`k_cg`) for profiler
+    captures: the 128x128x64 block (3,244,995 DOFs, 2.1 GB of FP64 block
+    values, ~2.3 GB on the device), two launches capped at 40 iterations."""
+    import ctypes as C
+    import numpy as np
+    from ufem_b200 import _lib, api, meshgen as mg
+    from ufem_b200.api import GpuModel
+    m = mg.block_brick(128, 128, 64)
+    g = GpuModel(m)
+    g.fill_K(0)
+    g.add_loads()
+    g.add_disps()
+    L = _lib.load()
+    b, nbr, nnzb = g.bsr_shape()
+    n = g.ndof
+    sol_ms, x = C.c_double(), C.c_double()
+    for _ in range(2):
+        g.set_u(np.zeros(n))
+        rv, its = g.solve(api.SOLVER_CGWJ, api.STOP_RELRES, 1e-30, 40, check=False)  # the cap ends it
+        L.ufem_get_phase_ms(g.h, C.byref(x), C.byref(x), C.byref(sol_ms), C.byref(x))
+    by = its * (nnzb * 76.0 + 4.0 * (nbr + 1) + 13.0 * n * 8)
+    print(json.dumps({"profile_static": "128x128x64 block, FP64 PCG, 40 iterations", "iterations": its,
+                      "solve_ms": sol_ms.value, "algorithmic_bytes": by,
+                      "achieved_GBs": by / sol_ms.value / 1e6 if sol_ms.value else None}))
 
 
 def build_meshes(nsamp, rank=0):
@@ -813,6 +842,9 @@ def main():
         return
     if a.profile_case:
         profile_case(a)
+        return
+    if a.profile_static:
+        profile_static(a)
         return
     if a.impl == "reference":
         reference_arm(a)

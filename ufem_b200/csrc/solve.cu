@@ -126,8 +126,14 @@ __device__ __forceinline__ double part_total(const double *part, int G, int off)
   return v;
 }
 
+// Four 256-thread blocks per SM (64 registers a thread): the SpMV's
+// index -> gather chains are latency-bound, and 32 warps per SM hide them
+// (128x128x64 block, FP64 PCG to 1e-8: 764 ms with 2 blocks per SM, 535 with
+// 3, 450 with 4; 5 and 6 spill and gain nothing).
+constexpr int kCgBlocksPerSm = 4;
+
 template <typename TV, int B>
-__global__ void __launch_bounds__(kThreads) k_cg(CgArgsT<TV> A) {
+__global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_cg(CgArgsT<TV> A) {
   __shared__ double s_acc[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
@@ -397,7 +403,7 @@ int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double ep
     return UFEM_AF_ERR;
   }
   // at least two block rows per warp; never more blocks than are co-resident
-  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
   G = std::max(G, 1);
   if ((rv = part.alloc((size_t)G * 4)) != UFEM_AF_OK) return rv;
   if ((rv = bar.alloc(1)) != UFEM_AF_OK) return rv;
@@ -828,7 +834,7 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
     set_error("persistent CG kernel does not fit on an SM");
     return UFEM_AF_ERR;
   }
-  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
   G = std::max(G, 1);
   if ((rv = part.alloc((size_t)G * 4)) || (rv = bar.alloc(1)) || (rv = res.alloc(1))) return rv;
   cudaEvent_t e0, e1;
@@ -1005,7 +1011,7 @@ int cg_jacobi_fp64_noalloc(const DevMatrix &A, const double *d_b, double *d_x, d
     set_error("persistent CG kernel does not fit on an SM");
     return UFEM_AF_ERR;
   }
-  int G = (int)std::min<long>((long)nsm * std::min(occ, 2), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
   G = std::max(1, std::min(G, kNoallocMaxGrid));
   CgArgs a;
   a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
