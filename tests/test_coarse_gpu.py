@@ -296,3 +296,37 @@ def test_coarse_space_wider_than_the_guess_basis():
     assert (st0 == 0).all() and (st1 == 0).all()
     assert np.abs(o1 - o0).max() <= 1e-6 * np.abs(o0).max()
     assert it1.mean() < 0.8 * it0.mean()
+
+
+def test_coarse_on_quads_and_two_coarse_meshes():
+    """The coarse phases on the quad family (2x2 blocks, plane stress), and in
+    one launch with two brick meshes that both carry a coarse space (one
+    launch holds one element family): the same answers as the Jacobi-only
+    solves."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve, set_coarse
+    quad = mg.mc_attach_vars(mg.plate_quad(32, 8, 4.0, 1.0, distort=0.2, seed=3))
+    fq = mg.mc_samples(quad, mesh_id=6, nsamp=150)
+    gq = GpuModel(quad)
+    b1, b2 = mg.warm_beam(16, 4, 4, zones=4), mg.warm_beam(24, 6, 6, zones=8)
+    f1, f2 = mg.warm_samples(b1, 140, first_sample=300), mg.warm_samples(b2, 90, first_sample=700)
+    g1, g2 = GpuModel(b1), GpuModel(b2)
+    refq, _ = mc_solve([gq], [fq], precision=2, coarse=0)
+    refb, _ = mc_solve([g1, g2], [f1, f2], precision=2, coarse=0)
+    tq = mg.mc_samples(quad, mesh_id=7, nsamp=64)
+    t1, t2 = mg.warm_samples(b1, 64), mg.warm_samples(b2, 128)
+    set_coarse(gq, _coarse_space(quad, _solve(gq, tq, coarse=0)[0], tq, 16))
+    set_coarse(g1, _coarse_space(b1, _solve(g1, t1, coarse=0)[0], t1, 16))
+    set_coarse(g2, _coarse_space(b2, _solve(g2, t2, coarse=0)[0], t2, 32))
+    try:
+        resq, sq = mc_solve([gq], [fq], precision=2)
+        resb, sb = mc_solve([g1, g2], [f1, f2], precision=2)
+    finally:
+        for g in (gq, g1, g2):
+            set_coarse(g, None)
+    assert sq.coarse_modes == 16 and sb.coarse_modes == 32
+    for res, ref in ((resq, refq), (resb, refb)):
+        for k in range(len(res)):
+            assert (res[k][1] == 0).all() and (ref[k][1] == 0).all()
+            assert np.abs(res[k][0] - ref[k][0]).max() <= 1e-6 * np.abs(ref[k][0]).max()
