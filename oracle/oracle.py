@@ -49,6 +49,7 @@ def lib():
         L.orc_set_u.argtypes = [C.c_void_p, _d]
         L.orc_solve.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_long, C.POINTER(C.c_long)]
         L.orc_results.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_strains.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_reac_len.restype = C.c_long
         L.orc_reac_len.argtypes = [C.c_void_p]
         L.orc_elem_ke.argtypes = [C.c_void_p, C.c_long, _d]
@@ -144,6 +145,17 @@ class OracleModel:
         if rv != AF_OK:
             raise RuntimeError(f"orc_results rv={rv}")
         return sig.reshape(self.model.eLen, nip, ns), fint, reac[:L.orc_reac_len(self.h)]
+
+    def strains(self):
+        """Strains B u_e at every integration point, laid out like the
+        stresses of ``results``."""
+        quad = int(self.model.e_type[0]) == 2
+        nip, ns = (4, 3) if quad else (27, 6)
+        eps = np.zeros(self.model.eLen * nip * ns, np.float64)
+        rv = lib().orc_strains(self.h, eps.ctypes.data)
+        if rv != AF_OK:
+            raise RuntimeError(f"orc_strains rv={rv}")
+        return eps.reshape(self.model.eLen, nip, ns)
 
     def elem_ke(self, e):
         sz = 8 if int(self.model.e_type[e]) == 2 else 24

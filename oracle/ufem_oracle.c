@@ -858,3 +858,49 @@ int orc_results(void *mv, double *sig, double *fint, double *reac)
 }
 
 long orc_reac_len(void *mv) { return ((orc_model *)mv)->resRLen; }
+
+/* strains eps = B u_e at every integration point, the values the result pass
+ * stores as RES_EX.. (quad: EX, EY, EXY, fem/fem_e002.c:656-658; brick: EX,
+ * EY, EZ, EYZ, EZX, EXY, fem/fem_e009.c:545-556); layout as orc_results' sig. */
+int orc_strains(void *mv, double *eps)
+{
+  orc_model *m = (orc_model *)mv;
+  long e, i, j, lf[24];
+  int rv;
+  for (e = 0; e < m->eLen; e++) {
+    long t = m->eType[e];
+    double ue[24];
+    int sz = elem_nodes(t) * elem_dofs(t), n;
+    loc_vec(m, e, lf);
+    for (i = 0; i < sz; i++) ue[i] = lf[i] ? m->u[lf[i] - 1] : 0.0;
+    if (t == 2) {
+      double xy[8], posgp[2], cartd[2][4], B[3][8], djacb;
+      int ig, jg, ip = 0;
+      for (n = 0; n < 4; n++) { long q = m->eNodes[e * m->nn + n]; xy[2 * n] = m->xyz[3 * q]; xy[2 * n + 1] = m->xyz[3 * q + 1]; }
+      posgp[0] = -QUAD_GP; posgp[1] = -1 * posgp[0];
+      for (ig = 0; ig < 2; ig++)
+        for (jg = 0; jg < 2; jg++, ip++) {
+          if ((rv = quad_cartd(xy, posgp[ig], posgp[jg], cartd, &djacb)) != AF_OK) return rv;
+          quad_B(cartd, B);
+          for (i = 0; i < 3; i++) {
+            double s = 0.0;
+            for (j = 0; j < 8; j++) s += (B[i][j] * ue[j]);
+            eps[(e * 4 + ip) * 3 + i] = s;
+          }
+        }
+    } else {
+      double c[24], H[6][24], mult;
+      int a, b, k, ip = 0;
+      for (n = 0; n < 8; n++) { long q = m->eNodes[e * m->nn + n]; c[3 * n] = m->xyz[3 * q]; c[3 * n + 1] = m->xyz[3 * q + 1]; c[3 * n + 2] = m->xyz[3 * q + 2]; }
+      for (a = 0; a < 3; a++) for (b = 0; b < 3; b++) for (k = 0; k < 3; k++, ip++) {
+        if ((rv = brick_H(c, a, b, k, H, &mult)) != AF_OK) return rv;
+        for (i = 0; i < 6; i++) {
+          double s = 0.0;
+          for (j = 0; j < 24; j++) s += (ue[j] * H[i][j]);
+          eps[(e * 27 + ip) * 6 + i] = s;
+        }
+      }
+    }
+  }
+  return AF_OK;
+}

@@ -11,7 +11,8 @@ loading ``oracle/_ref/serial/libfem_ref.so`` and calling ``monte_init_lib_stuff`
 Run it in a container that has the reference sources (it builds them if
 needed):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             # every fixture
+    python tests/golden/make_golden.py mc_outputs  # the Monte Carlo output fixtures only
 
 The fixtures are committed; tests only read them.
 """
@@ -165,8 +166,78 @@ def save_mc_case(name: str, model: mg.Model, nsamp: int):
         print(f"{name}: {os.path.getsize(path) / 1024:.0f} KiB, rv={r['rv'].tolist()}")
 
 
+def _strength_materials(model: mg.Model, groups: np.ndarray, fy=20e6) -> mg.Model:
+    """Give element e material record groups[e], each of type 5 (DENS, EX,
+    NU, G, F_YC, F_YT, F_UC, F_UT; fem/fem_m005.c:39)."""
+    ng = int(groups.max()) + 1
+    model.e_mp = groups.astype(np.int64)
+    model.mp_type = np.full(ng, mg.MAT_STRENGTH, np.int64)
+    model.mp_vals = [np.array([2500.0, 30e9, 0.2, 12.5e9, fy, 2e6, 30e6, 2e6]) for _ in range(ng)]
+    return model
+
+
+def _scales(model: mg.Model):
+    """Largest von Mises stress and |u| of the model as it stands (oracle)."""
+    from oracle.oracle import OracleModel, SOLVER_SSOR
+    r = OracleModel(model).run_static(SOLVER_SSOR)
+    s = r["sig"]
+    if s.shape[-1] == 3:
+        j2 = ((s[..., 0] - s[..., 1]) ** 2 + s[..., 0] ** 2 + s[..., 1] ** 2) / 6 + s[..., 2] ** 2
+    else:
+        j2 = (((s[..., 0] - s[..., 1]) ** 2 + (s[..., 1] - s[..., 2]) ** 2 + (s[..., 2] - s[..., 0]) ** 2) / 6
+              + (s[..., 3:] ** 2).sum(-1))
+    return float(np.sqrt(3 * j2).max()), float(np.abs(r["u"]).max())
+
+
+def save_mc_outputs_case(name: str, model: mg.Model, nsamp: int):
+    """Every linear-static output of monte_fill_ofld_data and the failure
+    function, from the reference libfem.so as an external driver calls it."""
+    mg.mc_attach_outputs(model)
+    vm, umax = _scales(model)
+    # the max-displacement test compares sqrt(max |u|) with MAX_D
+    # (femVecMaxAbs returns the square root, fem/fem_math.c:2163)
+    ifld = mg.mc_outputs_samples(model, nsamp, vm_scale=vm, u_scale=float(np.sqrt(umax)))
+    nmat = int(np.sum(model.mc_vars[:model.mc_ilen, 1] == mg.MONTE_VTYPE_MAT))
+    with tempfile.TemporaryDirectory() as d:
+        inp = os.path.join(d, "mc.fem")
+        mg.write_fem(model, inp)
+        np.save(os.path.join(d, "ifld.npy"), ifld)
+        drv = os.path.join(d, "drv.py")
+        open(drv, "w").write(MC_DRIVER)
+        subprocess.run([sys.executable, drv, os.path.join(REF_DIR, "libfem_ref.so"), inp,
+                        os.path.join(d, "ifld.npy"), os.path.join(d, "out.npz"), str(nmat)],
+                       check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        r = np.load(os.path.join(d, "out.npz"))
+        out = model_arrays(model)
+        out.update(mc_vars=model.mc_vars, mc_ilen=model.mc_ilen, mc_olen=model.mc_olen, ifld=ifld,
+                   ofld=r["ofld"], rv=r["rv"], inames=r["inames"], onames=r["onames"], ffunc=r["ffunc"])
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{name}: {os.path.getsize(path) / 1024:.0f} KiB, rv={r['rv'].tolist()}, ffunc={int(r['ffunc'])}")
+
+
+def mc_outputs_cases():
+    """The Monte Carlo output fixtures (type-5 materials with F_YC, mixed
+    brick types 9/10, and a type-1 plate whose F_YC reads 0)."""
+    m = mg.plate_quad(6, 3, 1.5, 0.75)
+    _strength_materials(m, (np.arange(m.eLen) % 6 >= 3).astype(np.int64))
+    save_mc_outputs_case("mc_out_plate_6x3", m, 8)
+    b = mg.beam_brick(4, 2, 2, 2.0, 1.0, 1.0)
+    ix = np.arange(b.eLen) % 4
+    _strength_materials(b, (ix >= 2).astype(np.int64))
+    b.e_type = np.where(ix >= 2, mg.ELEM_BRICK_W, mg.ELEM_BRICK).astype(np.int64)
+    b.e_rs = (ix >= 2).astype(np.int64)
+    b.rs_type = np.array([mg.ELEM_BRICK, mg.ELEM_BRICK_W], np.int64)
+    b.rs_vals = [np.zeros(0), np.array([0.0])]
+    save_mc_outputs_case("mc_out_beam_4x2x2", b, 8)
+    save_mc_outputs_case("mc_out_plate_iso_4x2", mg.plate_quad(4, 2, 1.0, 0.5), 3)
+
+
 def main():
     build_ref()
+    if sys.argv[1:] == ["mc_outputs"]:
+        mc_outputs_cases()
+        return
     # config 1: the 64x16 cantilever plate (plane stress), 2,210 DOFs
     save_case("plate_64x16", mg.plate_quad(), full=False, ke_elems=[0, 1, 15, 16, 500, 1023])
     # distorted quads (non-rectangular Jacobians), full dumps, three solvers
@@ -187,6 +258,7 @@ def main():
               ke_elems=[0, 1, 20, 100, 499])
     # the Monte Carlo plugin ABI: per-element E and a random end load
     save_mc_case("mc_beam_4x2x2", mg.beam_brick(4, 2, 2, 2.0, 1.0, 1.0, per_element_material=True), 4)
+    mc_outputs_cases()
 
 
 if __name__ == "__main__":

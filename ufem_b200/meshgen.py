@@ -27,6 +27,7 @@ ELEM_QUAD = 2      # 4-node plane quad, fem/fem_e002.c
 ELEM_BRICK = 9     # 8-node brick, fem/fem_e009.c
 ELEM_BRICK_W = 10  # brick + Winkler foundation, fem/fem_e010.c
 MAT_ISO = 1        # linear isotropic material, fem/fem_m001.c
+MAT_STRENGTH = 5   # isotropic with strengths (DENS, EX, NU, G, F_YC, F_YT, F_UC, F_UT), fem/fem_m005.c
 
 # Monte Carlo variable types, fem/fem_mont.h:28-47
 MONTE_VTYPE_RS = 0
@@ -36,9 +37,23 @@ MONTE_VTYPE_NLD = 3
 MONTE_VTYPE_RES_D = 8
 MONTE_VTYPE_RES_R = 9
 MONTE_VTYPE_RES_E = 10
+MONTE_VTYPE_MAX_D = 7
+MONTE_VTYPE_RES_SUM_E = 11
+MONTE_VTYPE_RES_MAX_E = 12
+MONTE_VTYPE_RES_MIN_E = 13
+MONTE_VTYPE_RES_FAIL_E = 14
+MONTE_VTYPE_RES_D_MAX = 15
+MONTE_VTYPE_RES_D_MIN = 16
+MONTE_VTYPE_RES_D_SUM = 17
+MONTE_VTYPE_RES_A_MAX = 18
+MONTE_VTYPE_RES_FAIL = 19
 
-MAT_EX = 2  # fem/fem_mat.h:41
-RES_SX = 7  # fem/fem_eres.h:39
+MAT_EX = 2     # fem/fem_mat.h:41
+MAT_F_YC = 12  # fem/fem_mat.h:51
+# element result codes, fem/fem_eres.h:39-51
+RES_SX, RES_SY, RES_SZ, RES_SXY, RES_SYZ, RES_SZX = 7, 8, 9, 10, 11, 12
+RES_EX, RES_EY, RES_EZ, RES_EXY, RES_EYZ, RES_EZX = 13, 14, 15, 16, 17, 18
+RES_S1 = 19
 
 
 @dataclasses.dataclass
@@ -333,6 +348,90 @@ def mc_attach_vars(model: Model, kind: str = "element_E", n_out_nodes: int = 4) 
     model.mc_ilen = ilen
     model.mc_olen = len(out)
     return model
+
+
+def mc_attach_outputs(model: Model) -> Model:
+    """Attach a Monte Carlo table that asks for every linear-static output of
+    ``monte_fill_ofld_data`` (fem/fem_mont.c:514-686) and the general failure
+    function (fem/fem_asse.c:271-374).
+
+    Inputs: E of every material, F_YC of every material record that holds one
+    (type 5), every type-3 nodal force, and MAX_D.  Outputs (written to
+    permuted positions): RES_D, RES_R, D_MAX/D_MIN/D_SUM/A_MAX at the last
+    loaded node; RES_E at stored and unstored result points (point 0, the
+    last stored point and the one after it, a result code the element never
+    writes); SUM/MAX/MIN/FAIL_E over stress, strain and unwritten codes; and
+    RES_FAIL.
+    """
+    quad = int(model.e_type[0]) == ELEM_QUAD
+    rows = []
+    for m in range(len(model.mp_vals)):
+        rows.append([MONTE_VTYPE_MAT, m, MAT_EX, 0])
+        if int(model.mp_type[m]) == MAT_STRENGTH and len(model.mp_vals[m]) > 4:
+            rows.append([MONTE_VTYPE_MAT, m, MAT_F_YC, 0])
+    force_idx = np.nonzero(model.nl_type == 3)[0]
+    for i in force_idx:
+        rows.append([MONTE_VTYPE_NLD, int(model.nl_node[i]), 3, int(model.nl_dir[i])])
+    rows.append([MONTE_VTYPE_MAX_D, 0, 0, 0])
+    ilen = len(rows)
+    tip, tdir = int(model.nl_node[force_idx[-1]]), int(model.nl_dir[force_idx[-1]])
+    sup = int(model.nl_node[np.nonzero(model.nl_type == 1)[0][0]])
+    ne = model.eLen
+    last = ne - 1
+    # result points the element stores (fem/fem_e002.c:942, fem/fem_e009.c:825, fem/fem_e010.c:41)
+    npt = 4 if quad else (22 if int(model.e_type[last]) == ELEM_BRICK_W else 19)
+    npt0 = 4 if quad else (22 if int(model.e_type[0]) == ELEM_BRICK_W else 19)
+    out = [[MONTE_VTYPE_RES_D, tip, tdir, 0], [MONTE_VTYPE_RES_R, sup, 1, 0],
+           [MONTE_VTYPE_RES_D_MAX, tip, tdir, 0], [MONTE_VTYPE_RES_D_MIN, tip, tdir, 0],
+           [MONTE_VTYPE_RES_D_SUM, tip, tdir, 0], [MONTE_VTYPE_RES_A_MAX, tip, tdir, 0],
+           [MONTE_VTYPE_RES_E, 0, RES_SX, 1], [MONTE_VTYPE_RES_E, 0, RES_SXY, npt0],
+           [MONTE_VTYPE_RES_E, last, RES_EX, 2], [MONTE_VTYPE_RES_E, last, RES_EXY, 3],
+           [MONTE_VTYPE_RES_E, 0, RES_SX, 0], [MONTE_VTYPE_RES_E, last, RES_SY, npt],
+           [MONTE_VTYPE_RES_E, last, RES_SY, npt + 1], [MONTE_VTYPE_RES_E, ne // 2, RES_S1, 1]]
+    codes = [RES_SX, RES_SXY, RES_EX, RES_EY, RES_S1]
+    if not quad:
+        out += [[MONTE_VTYPE_RES_E, 0, RES_SZ, npt0], [MONTE_VTYPE_RES_E, last, RES_EYZ, 7],
+                [MONTE_VTYPE_RES_E, last, RES_EZX, npt], [MONTE_VTYPE_RES_E, 0, RES_SZX, 27]]
+        codes += [RES_SZ, RES_SYZ, RES_EZX]
+    for c in codes:
+        for t in (MONTE_VTYPE_RES_SUM_E, MONTE_VTYPE_RES_MAX_E, MONTE_VTYPE_RES_MIN_E, MONTE_VTYPE_RES_FAIL_E):
+            out.append([t, 0, c, 0])
+    out.append([MONTE_VTYPE_RES_FAIL, 0, 0, 0])
+    olen = len(out)
+    table = [[i] + r for i, r in enumerate(rows)] + [[olen - 1 - j] + r for j, r in enumerate(out)]
+    model.mc_vars = np.array(table, dtype=np.int64)
+    model.mc_ilen = ilen
+    model.mc_olen = olen
+    return model
+
+
+def mc_outputs_samples(model: Model, nsamp: int, vm_scale: float, u_scale: float,
+                       mesh_id: int = 77, E0: float = 30e9, sigma: float = 0.15) -> np.ndarray:
+    """Seeded inputs for ``mc_attach_outputs``' table: E lognormal around E0,
+    one load factor U(0.8, 1.2) for every force, F_YC = vm_scale x r1 (one
+    r1 per sample for every material) and MAX_D = u_scale x r2, each r drawn
+    from U(0.5, 0.9) or U(1.15, 2) (so that about half of the samples fail
+    each test)."""
+    ty = model.mc_vars[:model.mc_ilen, 1]
+    sub = model.mc_vars[:model.mc_ilen, 3]
+    is_force = ty == MONTE_VTYPE_NLD
+    nl = {(int(n), int(d)): float(v) for n, t, d, v in
+          zip(model.nl_node, model.nl_type, model.nl_dir, model.nl_val) if t == 3}
+    ifld = np.empty((nsamp, model.mc_ilen), dtype=np.float64)
+    for s in range(nsamp):
+        g = mc_rng(mesh_id, s)
+        lf = g.uniform(0.8, 1.2)
+        r1, r2 = (g.uniform(0.5, 0.9) if g.uniform() < 0.5 else g.uniform(1.15, 2.0) for _ in range(2))
+        for i in range(model.mc_ilen):
+            if ty[i] == MONTE_VTYPE_MAT and sub[i] == MAT_EX:
+                ifld[s, i] = E0 * np.exp(sigma * g.standard_normal())
+            elif ty[i] == MONTE_VTYPE_MAT:
+                ifld[s, i] = vm_scale * r1 * g.uniform(0.95, 1.05)
+            elif is_force[i]:
+                ifld[s, i] = nl[(int(model.mc_vars[i, 2]), int(model.mc_vars[i, 4]))] * lf
+            else:
+                ifld[s, i] = u_scale * r2
+    return ifld
 
 
 def mc_samples(model: Model, mesh_id: int, nsamp: int, first_sample: int = 0,
