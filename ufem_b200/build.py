@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libufem_gpu.so")
 
-SOURCES = ["model.cpp", "kernels.cu", "solve.cu", "batch.cu", "capi.cu", "monte.cu", "mlp.cu", "warm.cu"]
+SOURCES = ["model.cpp", "kernels.cu", "solve.cu", "batch.cu", "capi.cu", "monte.cu", "mcout.cu", "mlp.cu", "warm.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

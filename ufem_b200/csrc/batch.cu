@@ -59,8 +59,8 @@ namespace ufem {
 struct McOut {
   int type;    // MONTE_VTYPE_RES_*
   int pos;     // ofld position
-  int row;     // DOF row for RES_D / RES_R (0-based) or -1
-  int elem, ip, comp;  // RES_E
+  int row;     // DOF row for RES_D / RES_R / RES_D_MAX / RES_D_MIN (0-based) or -1;
+               // the constant of RES_D_SUM
   int reac;    // reaction index
 };
 
@@ -75,7 +75,7 @@ struct McPlan {
   DBuf<int> d_ovr_row, d_ovr_var;
   DBuf<int> d_ovr_ptr, d_ovr_rvar;  // the overrides by DOF row (input order within a row)
   std::vector<McOut> outs;
-  DBuf<int> d_out_type, d_out_pos, d_out_row, d_out_elem, d_out_ip, d_out_comp;
+  DBuf<int> d_out_type, d_out_pos, d_out_row;
   DBuf<int> reac_rows;             // DOF rows of the reaction list
   long ilen = 0, olen = 0;
   // host copies for the implicit form
@@ -94,6 +94,8 @@ struct McPlan {
   // as BF16 tensor-core operand tiles, supported rows zero
   int cmodes = 0;
   DBuf<uint8_t> wt1, wt3;
+  // element-result outputs and the failure function (mcout.cu)
+  ElemOutPlan eo;
 };
 
 static std::vector<std::unique_ptr<McPlan>> g_plans;
@@ -148,9 +150,10 @@ static int build_plan(ufem_model *m, McPlan *P) {
   if ((rv = P->gptr.upload(cnt.data(), cnt.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->gel.upload(gel.data(), gel.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->gpair.upload(gpair.data(), gpair.size())) != UFEM_AF_OK) return rv;
-  // inputs: MONTE_VTYPE_MAT (E only) and MONTE_VTYPE_NLD (fem/fem_mont.c:721-760)
-  std::vector<int> mat_var(m->mpVals.size(), -1);
+  // inputs: MONTE_VTYPE_MAT (E, F_YC), MONTE_VTYPE_NLD and MONTE_VTYPE_MAX_D (fem/fem_mont.c:721-797)
+  std::vector<int> mat_var(m->mpVals.size(), -1), fy_var(m->mpVals.size(), -1);
   std::vector<int> load_var(m->loads.size(), -1);
+  int md_col = -1;
   for (long i = 0; i < m->mc_ilen; i++) {
     long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i], it = m->mc_iter[i];
     int col = (int)m->mc_pos[i];
@@ -158,12 +161,18 @@ static int build_plan(ufem_model *m, McPlan *P) {
       set_error("Monte Carlo input position out of range");
       return UFEM_AF_ERR_VAL;
     }
-    if (ty == 1) {  // MONTE_VTYPE_MAT
+    if (ty == 1 && sub == 12 && it == 0 && item >= 0 && item < (long)m->mpVals.size()) {
+      // MAT_F_YC: read by the failure function only; a record without it
+      // ignores the input (femGetRepValIndex gives -1, fem/fem_mont.c:722-735)
+      if (m->mpTypeH[item] == 5 && m->mpVals[item].size() > 4) fy_var[item] = col;
+    } else if (ty == 1) {  // MONTE_VTYPE_MAT
       if (sub != 2 || item < 0 || item >= (long)m->mpVals.size()) {
-        set_error("batched Monte Carlo randomises material E (MAT_EX) only");
+        set_error("batched Monte Carlo randomises material E (MAT_EX) and F_YC only");
         return UFEM_AF_ERR_TYP;
       }
       mat_var[item] = col;
+    } else if (ty == 7) {  // MONTE_VTYPE_MAX_D, fem/fem_mont.c:795-797
+      md_col = col;
     } else if (ty == 3) {  // MONTE_VTYPE_NLD: first load with node/type/dir (fem/fem_mont.c:757-768)
       for (size_t j = 0; j < m->loads.size(); j++)
         if (m->loads[j].node == item && m->loads[j].type == sub && m->loads[j].dir == it) {
@@ -175,7 +184,7 @@ static int build_plan(ufem_model *m, McPlan *P) {
           break;
         }
     } else {
-      set_error("input variable type not on the batched path (MAT E and NLD forces only)");
+      set_error("input variable type not on the batched path (MAT E / F_YC, NLD forces and MAX_D only)");
       return UFEM_AF_ERR_TYP;
     }
   }
@@ -216,17 +225,27 @@ static int build_plan(ufem_model *m, McPlan *P) {
   }
   // outputs (fem/fem_mont.c:514-686)
   P->outs.clear();
-  std::vector<int> ot, op, orow, oel, oip, ocomp;
+  std::vector<int> ot, op, orow;
   for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
-    McOut o{(int)m->mc_type[i], (int)m->mc_pos[i - m->mc_ilen], -1, -1, 0, 0, -1};
+    McOut o{(int)m->mc_type[i], (int)m->mc_pos[i - m->mc_ilen], -1, -1};
     if (o.pos < 0 || o.pos >= m->mc_olen) {
       set_error("Monte Carlo output position out of range");
       return UFEM_AF_ERR_VAL;
     }
     long item = m->mc_item[i], sub = m->mc_sub[i], it = m->mc_iter[i];
-    if (o.type == 8) {  // RES_D: u at node item, DOF sub
+    if (o.type == 8 || o.type == 15 || o.type == 16) {
+      // RES_D, RES_D_MAX, RES_D_MIN: u at node item, DOF sub (fem/fem_mont.c:524-548;
+      // max/min against the zeroed output)
       if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS)
         o.row = (int)m->nDOFfld[item * KNOWN_DOFS + sub - 1] - 1;
+    } else if (o.type == 17) {
+      // RES_D_SUM adds nDOFfld[nDOFfld[pos]], the DOF number of another slot
+      // (fem/fem_mont.c:550-555); kept as a constant in `row`
+      o.row = 0;
+      if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS) {
+        const long p = m->nDOFfld[item * KNOWN_DOFS + sub - 1];
+        if (p >= 0 && p < (long)m->nDOFfld.size()) o.row = (int)m->nDOFfld[p];
+      }
     } else if (o.type == 9) {  // RES_R: reaction of node item, DOF sub
       for (size_t r = 0; r < m->reacNode.size(); r++)
         if (m->reacNode[r] == item && m->reacDof[r] == sub) {
@@ -234,35 +253,19 @@ static int build_plan(ufem_model *m, McPlan *P) {
           o.row = m->reacRow[r];
           break;
         }
-    } else if (o.type == 10) {  // RES_E: element item, result type sub, point it
-      int nip = (m->etype == 2) ? 4 : 27;
-      int ns = (m->etype == 2) ? 3 : 6;
-      // stress result codes RES_SX.. (fem/fem_eres.h:39-44) in the element's order
-      static const int quad_map[3] = {7, 8, 10};
-      static const int brick_map[6] = {7, 8, 9, 11, 12, 10};
-      int comp = -1;
-      for (int c = 0; c < ns; c++)
-        if ((m->etype == 2 ? quad_map[c] : brick_map[c]) == sub) comp = c;
-      if (item < 0 || item >= m->eLen || it < 1 || it > nip || comp < 0) {
-        o.type = -1;  // unsupported result -> 0 (femGetEResVal returns 0, fem/fem_accs.c:269-273)
-      } else {
-        o.elem = (int)item;
-        o.ip = (int)it - 1;
-        o.comp = comp;
-      }
     } else {
-      o.type = -1;  // other outputs report 0 on this path
+      // RES_E, the element sums/extremes and RES_FAIL come from the element
+      // pass (mcout.cu), which writes after this one; RES_A_MAX is 0 outside
+      // dynamics (fem/fem_mont.c:557-563)
+      o.type = -1;
     }
     P->outs.push_back(o);
     ot.push_back(o.type); op.push_back(o.pos); orow.push_back(o.row);
-    oel.push_back(o.elem); oip.push_back(o.ip); ocomp.push_back(o.comp);
   }
   if ((rv = P->d_out_type.upload(ot.data(), ot.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->d_out_pos.upload(op.data(), op.size())) != UFEM_AF_OK) return rv;
   if ((rv = P->d_out_row.upload(orow.data(), orow.size())) != UFEM_AF_OK) return rv;
-  if ((rv = P->d_out_elem.upload(oel.data(), oel.size())) != UFEM_AF_OK) return rv;
-  if ((rv = P->d_out_ip.upload(oip.data(), oip.size())) != UFEM_AF_OK) return rv;
-  if ((rv = P->d_out_comp.upload(ocomp.data(), ocomp.size())) != UFEM_AF_OK) return rv;
+  if ((rv = build_elem_outputs(m, P->eo, &fy_var, md_col)) != UFEM_AF_OK) return rv;
   P->built = true;
   return UFEM_AF_OK;
 }
@@ -1486,18 +1489,15 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
 }
 
 // outputs: RES_D (u), RES_R (reaction = internal force - F at the support),
-// RES_E (stress at one integration point).  thread per (output, sample).
+// RES_D_MAX / RES_D_MIN / RES_D_SUM; thread per (output, sample).  Element
+// results and RES_FAIL: mcout.cu.
 template <int B>
 __global__ void k_outputs(int nout, int S, int nsamp, long olen, const int *__restrict__ otype,
-                          const int *__restrict__ opos, const int *__restrict__ orow, const int *__restrict__ oel,
-                          const int *__restrict__ oip, const int *__restrict__ ocomp, const double *__restrict__ u,
+                          const int *__restrict__ opos, const int *__restrict__ orow, const double *__restrict__ u,
                           const int *__restrict__ rowptr, const int *__restrict__ colind,
                           const int *__restrict__ gptr, const int *__restrict__ gel, const int *__restrict__ gpair,
                           int s_el, const double *__restrict__ Khat, const double *__restrict__ E,
-                          const double *__restrict__ Fraw, const double *__restrict__ xyz,
-                          const int *__restrict__ enodes, const int *__restrict__ node_rank,
-                          const double *__restrict__ eNu, const double *__restrict__ eThick, int etype,
-                          double *__restrict__ ofld) {
+                          const double *__restrict__ Fraw, double *__restrict__ ofld) {
   long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= (long)nout * nsamp) return;
   const int o = (int)(t / nsamp), s = (int)(t % nsamp);
@@ -1523,78 +1523,14 @@ __global__ void k_outputs(int nout, int S, int nsamp, long olen, const int *__re
       }
       val = (0.0 - Fraw[(size_t)row * S + s]) + fint;
     }
-  } else if (ty == 10) {
-    const int e = oel[o], ip = oip[o], comp = ocomp[o];
-    const double Ee = E[(size_t)e * S + s], nu = eNu[e];
-    if (etype == 9) {
-      const double gp[3] = {-0.774596669241483, 0.0, 0.774596669241483};
-      const double nc[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
-                               {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
-      const double x = gp[ip / 9], y = gp[(ip / 3) % 3], z = gp[ip % 3];
-      double dN[8][3], X[8][3], J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      for (int n = 0; n < 8; n++) {
-        dN[n][0] = 0.125 * nc[n][0] * (1.0 + nc[n][1] * y) * (1.0 + nc[n][2] * z);
-        dN[n][1] = 0.125 * nc[n][1] * (1.0 + nc[n][0] * x) * (1.0 + nc[n][2] * z);
-        dN[n][2] = 0.125 * nc[n][2] * (1.0 + nc[n][0] * x) * (1.0 + nc[n][1] * y);
-        for (int d = 0; d < 3; d++) X[n][d] = xyz[3 * (size_t)enodes[(size_t)e * 8 + n] + d];
-      }
-      for (int a = 0; a < 3; a++)
-        for (int c = 0; c < 3; c++)
-          for (int n = 0; n < 8; n++) J[a][c] += dN[n][a] * X[n][c];
-      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
-                   c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-      const double id = 1.0 / (J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02);
-      const double inv[3][3] = {{c00 * id, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id,
-                                 (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id},
-                                {c01 * id, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id,
-                                 (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id},
-                                {c02 * id, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id,
-                                 (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id}};
-      double ep[6] = {0, 0, 0, 0, 0, 0};
-      for (int n = 0; n < 8; n++) {
-        double g[3];
-        for (int d = 0; d < 3; d++) g[d] = inv[d][0] * dN[n][0] + inv[d][1] * dN[n][1] + inv[d][2] * dN[n][2];
-        const size_t r0 = (size_t)node_rank[enodes[(size_t)e * 8 + n]] * 3;
-        const double ux = u[(r0)*S + s], uy = u[(r0 + 1) * S + s], uz = u[(r0 + 2) * S + s];
-        ep[0] += g[0] * ux; ep[1] += g[1] * uy; ep[2] += g[2] * uz;
-        ep[3] += g[2] * uy + g[1] * uz; ep[4] += g[2] * ux + g[0] * uz; ep[5] += g[1] * ux + g[0] * uy;
-      }
-      const double d1 = (Ee * (1.0 - nu)) / ((1.0 + nu) * (1.0 - 2.0 * nu));
-      const double d2 = (Ee * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
-      const double d3 = Ee / (2.0 * (1 + nu));
-      const double sg[6] = {d1 * ep[0] + d2 * ep[1] + d2 * ep[2], d2 * ep[0] + d1 * ep[1] + d2 * ep[2],
-                            d2 * ep[0] + d2 * ep[1] + d1 * ep[2], d3 * ep[3], d3 * ep[4], d3 * ep[5]};
-      val = sg[comp];
-    } else {
-      const double qg = 0.577350569189626;
-      const double sx_ = (ip >> 1) ? qg : -qg, tx_ = (ip & 1) ? qg : -qg;
-      const double dS[4] = {(-1.0 + tx_) * 0.25, (1.0 - tx_) * 0.25, (1.0 + tx_) * 0.25, (-1.0 - tx_) * 0.25};
-      const double dT[4] = {(-1.0 + sx_) * 0.25, (-1.0 - sx_) * 0.25, (1.0 + sx_) * 0.25, (1.0 - sx_) * 0.25};
-      double j00 = 0, j01 = 0, j10 = 0, j11 = 0, X[4][2];
-      for (int n = 0; n < 4; n++) {
-        X[n][0] = xyz[3 * (size_t)enodes[(size_t)e * 4 + n]];
-        X[n][1] = xyz[3 * (size_t)enodes[(size_t)e * 4 + n] + 1];
-        j00 += dS[n] * X[n][0]; j01 += dS[n] * X[n][1]; j10 += dT[n] * X[n][0]; j11 += dT[n] * X[n][1];
-      }
-      const double det = j00 * j11 - j01 * j10;
-      double ex = 0, ey = 0, gxy = 0;
-      for (int n = 0; n < 4; n++) {
-        const double gx = (j11 / det) * dS[n] + (-j01 / det) * dT[n];
-        const double gy = (-j10 / det) * dS[n] + (j00 / det) * dT[n];
-        const size_t r0 = (size_t)node_rank[enodes[(size_t)e * 4 + n]] * 2;
-        const double ux = u[r0 * S + s], uy = u[(r0 + 1) * S + s];
-        ex += gx * ux; ey += gy * uy; gxy += gy * ux + gx * uy;
-      }
-      double Mul, D0, D1, D2, D3;
-      if (eThick[e] > 0.0) {
-        Mul = Ee / (1 - nu * nu); D0 = Mul; D1 = Mul * nu; D2 = Mul; D3 = Mul * 0.5 * (1 - nu);
-      } else {
-        Mul = Ee / ((1 + nu) * (1 - 2 * nu)); D0 = Mul * (1 - nu); D1 = Mul * nu; D2 = Mul * (1 - nu);
-        D3 = Mul * 0.5 * (1 - nu);
-      }
-      const double sg[3] = {D0 * ex + D1 * ey, D1 * ex + D2 * ey, D3 * gxy};
-      val = sg[comp];
+  } else if (ty == 15 || ty == 16) {
+    const int row = orow[o];
+    if (row >= 0) {
+      const double v = u[(size_t)row * S + s];
+      val = (ty == 15) ? (v > 0.0 ? v : 0.0) : (v < 0.0 ? v : 0.0);
     }
+  } else if (ty == 17) {
+    val = (double)orow[o];
   }
   ofld[(size_t)s * olen + opos[o]] = val;
 }
@@ -2281,17 +2217,20 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
         const long tot = (long)nout * w.nsamp;
         if (B == 3)
           k_outputs<3><<<(unsigned)((tot + 127) / 128), 128>>>(
-              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
-              P->d_out_ip.p, P->d_out_comp.p, w.x64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
-              P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
-              m->d_eThick.p, m->etype, d_ofld[k]);
+              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, w.x64.p,
+              m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p, P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p,
+              d_ofld[k]);
         else
           k_outputs<2><<<(unsigned)((tot + 127) / 128), 128>>>(
-              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, P->d_out_elem.p,
-              P->d_out_ip.p, P->d_out_comp.p, w.x64.p, m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p,
-              P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p, m->d_xyz.p, m->d_enodes.p, m->d_noderank.p, m->d_eNu.p,
-              m->d_eThick.p, m->etype, d_ofld[k]);
+              nout, w.S, w.nsamp, P->olen, P->d_out_type.p, P->d_out_pos.p, P->d_out_row.p, w.x64.p,
+              m->d_rowptr.p, m->d_colind.p, P->gptr.p, P->gel.p, P->gpair.p, P->s, P->Khat.p, w.E.p, w.Fraw.p,
+              d_ofld[k]);
         g_stats.kernel_launches += 1;
+        int eo_launches = 0;
+        if ((rv = run_elem_outputs(m, P->eo, w.S, w.nsamp, w.x64.p, w.E.p, d_ifld[k], P->ilen, 0.0, d_ofld[k],
+                                   P->olen, &eo_launches)) != UFEM_AF_OK)
+          return rv;
+        g_stats.kernel_launches += eo_launches;
       }
       if (d_u_out && d_u_out[k])
         UFEM_CUDA_TRY(cudaMemcpyAsync(d_u_out[k], w.x64.p, (size_t)m->nDOFAct * w.S * sizeof(double),

@@ -87,7 +87,9 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
       m->enodes[(size_t)e * m->nn + j] = (int)np;
     }
   }
-  // materials: type 1 (linear isotropic), values DENS, EX, NU, ... (fem/fem_m001.c:38)
+  // materials: type 1 (linear isotropic: DENS, EX, NU, ALPHA, KXX, C, PRICE,
+  // fem/fem_m001.c:39) and type 5 (DENS, EX, NU, G, F_YC, F_YT, F_UC, F_UT,
+  // fem/fem_m005.c:39; isotropic D, fem/fem_pl3d.c:190 and fem/fem_stf2.c:298)
   m->mpVals.resize(t->mpLen);
   m->mpTypeH.assign(t->mpType, t->mpType + t->mpLen);
   for (long p = 0; p < t->mpLen; p++) {
@@ -106,10 +108,10 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
       return UFEM_AF_ERR_VAL;
     }
     if (t->mpType[p] != 1 && t->mpType[p] != 5) {
-      set_error("material types: only linear isotropic (1) is on this path");
+      set_error("material types: only linear isotropic (1, 5) is on this path");
       return UFEM_AF_ERR_TYP;
     }
-    if (m->mpVals[p].size() > 7) {
+    if (m->mpVals[p].size() > (t->mpType[p] == 5 ? 8u : 7u)) {
       // repeating values select the orthotropic plane D (fem/fem_stf2.c:256-266)
       set_error("materials with repeating values are not on this path");
       return UFEM_AF_ERR_TYP;

@@ -45,10 +45,18 @@ ufem_model *g_mc = nullptr;
 char g_name[257];
 double g_max_disp = 0.0;
 
-// position of value type `vt` in a type-1 material record (fem/fem_m001.c:38)
-int mat_index(long vt) {
-  static const long order[7] = {1 /*DENS*/, 2 /*EX*/, 5 /*NU*/, 38 /*ALPHA*/, 37 /*KXX*/, 39 /*C*/, 36 /*PRICE*/};
-  for (int i = 0; i < 7; i++)
+ElemOutPlan g_eo;        // element outputs of the process-wide model (mcout.cu)
+DBuf<double> g_dofld;    // their device output row
+
+// position of value type `vt` in a material record of type `ty`: the type's
+// non-repeating list (type 1 fem/fem_m001.c:39, type 5 fem/fem_m005.c:39)
+int mat_index(long ty, long vt) {
+  static const long t1[7] = {1 /*DENS*/, 2 /*EX*/, 5 /*NU*/, 38 /*ALPHA*/, 37 /*KXX*/, 39 /*C*/, 36 /*PRICE*/};
+  static const long t5[8] = {1 /*DENS*/, 2 /*EX*/, 5 /*NU*/, 6 /*G*/, 12 /*F_YC*/, 14 /*F_YT*/, 15 /*F_UC*/,
+                             17 /*F_UT*/};
+  const long *order = ty == 5 ? t5 : t1;
+  const int n = ty == 5 ? 8 : 7;
+  for (int i = 0; i < n; i++)
     if (order[i] == vt) return i;
   return -1;
 }
@@ -73,7 +81,7 @@ int apply_inputs(ufem_model *m, const double *ifld) {
         break;
       case 1: {  // MONTE_VTYPE_MAT
         if (item < 0 || item >= (long)m->mpVals.size() || it > 0) break;
-        const int idx = mat_index(sub);
+        const int idx = mat_index(m->mpTypeH[item], sub);
         if (idx < 0 || idx >= (int)m->mpVals[item].size()) break;  // femGetRepValIndex -> -1
         m->mpVals[item][idx] = v;
         for (long e = 0; e < m->eLen; e++)
@@ -118,14 +126,52 @@ int apply_inputs(ufem_model *m, const double *ifld) {
   return UFEM_AF_OK;
 }
 
-// stress component of a result code RES_SX.. (fem/fem_eres.h:39-44)
-int stress_comp(const ufem_model *m, long code) {
-  static const int quad_map[3] = {7, 8, 10};
-  static const int brick_map[6] = {7, 8, 9, 11, 12, 10};
-  const int ns = m->etype == 2 ? 3 : 6;
-  for (int c = 0; c < ns; c++)
-    if ((m->etype == 2 ? quad_map[c] : brick_map[c]) == code) return c;
-  return -1;
+// The outputs of the sample just solved in m, as monte_fill_ofld_data writes
+// them into the zeroed row `out` (fem/fem_mont.c:514-686): displacement and
+// reaction outputs from the host copies, element results and RES_FAIL from
+// the GPU element pass (mcout.cu).
+int fill_outputs(ufem_model *m, const std::vector<double> &u, double *out) {
+  for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
+    const long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i];
+    const long pos = m->mc_pos[i - m->mc_ilen];
+    if (pos < 0 || pos >= m->mc_olen) continue;
+    double &o = out[pos];
+    const bool slot = item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS;
+    const long p = slot ? m->nDOFfld[item * KNOWN_DOFS + sub - 1] : 0;
+    const double v = p > 0 ? u[p - 1] : 0.0;
+    switch (ty) {
+      case 8: o = v; break;                                  // RES_D
+      case 15: if (o < v) o = v; break;                      // RES_D_MAX
+      case 16: if (o > v) o = v; break;                      // RES_D_MIN
+      case 17:                                               // RES_D_SUM, fem/fem_mont.c:550-555
+        if (slot && p >= 0 && p < (long)m->nDOFfld.size()) o += (double)m->nDOFfld[p];
+        break;
+      case 9:  // RES_R
+        for (size_t r = 0; r < m->reacNode.size(); r++)
+          if (m->reacNode[r] == item && m->reacDof[r] == sub) {
+            o = m->reacVal[r];
+            break;
+          }
+        break;
+      default:
+        break;  // element results and RES_FAIL below; dynamics outputs are 0
+    }
+  }
+  int rv;
+  if ((rv = build_elem_outputs(m, g_eo, nullptr, -1)) != UFEM_AF_OK) return rv;
+  if (g_eo.nagg == 0 && g_eo.npo == 0) return UFEM_AF_OK;
+  const long olen = m->mc_olen;
+  if ((rv = g_dofld.ensure(olen))) return rv;
+  UFEM_CUDA_TRY(cudaMemset(g_dofld.p, 0, olen * sizeof(double)));
+  int launches = 0;
+  if ((rv = run_elem_outputs(m, g_eo, 1, 1, m->d_u.p, m->d_eE.p, nullptr, 0, g_max_disp, g_dofld.p, olen,
+                             &launches)) != UFEM_AF_OK)
+    return rv;
+  std::vector<double> row(olen);
+  UFEM_CUDA_TRY(cudaMemcpy(row.data(), g_dofld.p, olen * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int q : g_eo.h_apos) out[q] = row[q];
+  for (int q : g_eo.h_ppos) out[q] = row[q];
+  return UFEM_AF_OK;
 }
 
 }  // namespace
@@ -237,7 +283,10 @@ int monte_solution(char *param, double *ifld, double *ofld, long if_type) {
   (void)param;
   if (!g_mc) return UFEM_AF_ERR;
   ufem_model *m = g_mc;
-  for (long i = 0; i < m->mc_olen; i++) ofld[m->mc_pos[m->mc_ilen + i]] = 0;  // fem/fem_mont.c:702-705
+  // the reference zeroes the positions held by table rows 0..olen-1
+  // (monte_io_var_pos[i-monte_i_len], fem/fem_mont.c:702-705)
+  for (long i = 0; i < m->mc_olen; i++)
+    if (m->mc_pos[i] >= 0 && m->mc_pos[i] < m->mc_olen) ofld[m->mc_pos[i]] = 0;
   if (if_type != 0) {
     set_error("only the linear static solution (if_type 0) is on this path");
     return UFEM_AF_ERR_TYP;
@@ -248,71 +297,19 @@ int monte_solution(char *param, double *ifld, double *ofld, long if_type) {
   if ((rv = ufem_fem_solve(m, UFEM_SOLVER_CGWJ, &iters)) != UFEM_AF_OK) return rv;
   std::vector<double> u(m->nDOFAct);
   if ((rv = ufem_get_u(m, u.data())) != UFEM_AF_OK) return rv;
-  const int nip = m->etype == 2 ? 4 : 27, ns = m->etype == 2 ? 3 : 6;
-  std::vector<double> sig;
-  bool have_sig = false;
-  for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
-    const long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i], it = m->mc_iter[i];
-    double &out = ofld[m->mc_pos[i - m->mc_ilen]];
-    if (ty >= 10 && ty <= 14 && !have_sig) {
-      sig.resize((size_t)m->eLen * nip * ns);
-      if ((rv = ufem_get_stresses(m, sig.data(), nullptr)) != UFEM_AF_OK) return rv;
-      have_sig = true;
-    }
-    switch (ty) {
-      case 8: {  // RES_D
-        if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS) {
-          long p = m->nDOFfld[item * KNOWN_DOFS + sub - 1];
-          out = p > 0 ? u[p - 1] : 0.0;
-        }
-        break;
-      }
-      case 9:  // RES_R
-        for (size_t r = 0; r < m->reacNode.size(); r++)
-          if (m->reacNode[r] == item && m->reacDof[r] == sub) {
-            out = m->reacVal[r];
-            break;
-          }
-        break;
-      case 10: {  // RES_E
-        const int c = stress_comp(m, sub);
-        if (c >= 0 && item >= 0 && item < m->eLen && it >= 1 && it <= nip)
-          out = sig[((size_t)item * nip + it - 1) * ns + c];
-        break;
-      }
-      case 11: case 12: case 13: case 14: {  // sums / extremes / failure over elements
-        const int c = stress_comp(m, sub);
-        if (c < 0) break;
-        double acc = (ty == 11) ? 0.0 : 0.0;
-        bool fail = false;
-        for (long e = 0; e < m->eLen; e++)
-          for (int q = 0; q < nip; q++) {
-            const double v = sig[((size_t)e * nip + q) * ns + c];
-            if (ty == 11) acc += v;
-            else if (ty == 12) acc = (v > acc) ? v : acc;
-            else if (ty == 13) acc = (v < acc) ? v : acc;
-            else if (v > 0.0) fail = true;
-          }
-        out = (ty == 14) ? (fail ? 1.0 : 0.0) : acc;
-        break;
-      }
-      default:
-        break;  // dynamics outputs and the general failure function: 0 on this path
-    }
-  }
-  return UFEM_AF_OK;
+  return fill_outputs(m, u, ofld);
 }
 
 int ufem_mc_solve_serial(ufem_model *m, long nsamp, const double *ifld, double *ofld, int *status, long *iters,
                          double tol) {
   if (!m) return UFEM_AF_ERR;
   int rv;
-  const int nip = m->etype == 2 ? 4 : 27, ns = m->etype == 2 ? 3 : 6;
-  std::vector<double> u(m->nDOFAct), sig;
+  std::vector<double> u(m->nDOFAct);
   for (long s = 0; s < nsamp; s++) {
     const double *in = ifld + s * m->mc_ilen;
     double *out = ofld + s * m->mc_olen;
-    for (long i = 0; i < m->mc_olen; i++) out[m->mc_pos[m->mc_ilen + i]] = 0;
+    for (long i = 0; i < m->mc_olen; i++)
+      if (m->mc_pos[i] >= 0 && m->mc_pos[i] < m->mc_olen) out[m->mc_pos[i]] = 0;
     if ((rv = apply_inputs(m, in)) != UFEM_AF_OK) return rv;
     long it = 0;
     if ((rv = ufem_fill_K(m, 0)) != UFEM_AF_OK) return rv;
@@ -324,27 +321,7 @@ int ufem_mc_solve_serial(ufem_model *m, long nsamp, const double *ifld, double *
     if (iters) iters[s] = it;
     if ((rv = ufem_fill_K(m, 1)) != UFEM_AF_OK) return rv;
     if ((rv = ufem_get_u(m, u.data())) != UFEM_AF_OK) return rv;
-    for (long i = m->mc_ilen; i < m->mc_ilen + m->mc_olen; i++) {
-      const long ty = m->mc_type[i], item = m->mc_item[i], sub = m->mc_sub[i], itr = m->mc_iter[i];
-      double &o = out[m->mc_pos[i - m->mc_ilen]];
-      if (ty == 8 && item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS) {
-        long p = m->nDOFfld[item * KNOWN_DOFS + sub - 1];
-        o = p > 0 ? u[p - 1] : 0.0;
-      } else if (ty == 9) {
-        for (size_t r = 0; r < m->reacNode.size(); r++)
-          if (m->reacNode[r] == item && m->reacDof[r] == sub) {
-            o = m->reacVal[r];
-            break;
-          }
-      } else if (ty == 10) {
-        const int c = stress_comp(m, sub);
-        if (c >= 0 && item >= 0 && item < m->eLen && itr >= 1 && itr <= nip) {
-          if (sig.empty()) sig.resize((size_t)m->eLen * nip * ns);
-          if ((rv = ufem_get_stresses(m, sig.data(), nullptr)) != UFEM_AF_OK) return rv;
-          o = sig[((size_t)item * nip + itr - 1) * ns + c];
-        }
-      }
-    }
+    if ((rv = fill_outputs(m, u, out)) != UFEM_AF_OK) return rv;
   }
   return UFEM_AF_OK;
 }

@@ -194,4 +194,27 @@ int mlp_train_graph(ufem_mlp *p, long ntrain, int bs, const float *d_X, const fl
 int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
                     long inner_cap, long *iters, int *outer_steps, float *ms);
 
+// Element-result outputs of a Monte Carlo table (RES_E, RES_SUM/MAX/MIN/FAIL_E)
+// and the general failure function RES_FAIL, as GPU passes (mcout.cu)
+struct ElemOutPlan {
+  int nagg = 0, npo = 0;
+  bool strength = false;  // a RES_FAIL output exists
+  int md_col = -1;        // ifld column of MAX_D, -1: none
+  std::vector<int> h_apos, h_ppos;
+  DBuf<int> akind, acomp, apos;        // aggregates: kind 11..14 / 19, value index, ofld position
+  DBuf<int> pel, pip, pcomp, ppos;     // RES_E: element, point, value index, ofld position
+  DBuf<unsigned char> enpts;           // stored result points per element
+  DBuf<double> fy0;                    // F_YC per element (0: the material holds none)
+  DBuf<int> fycol;                     // ifld column that randomises it, -1: none
+  DBuf<double> part, upart;            // per (element range, sample) records; max |u| per (row chunk, sample)
+};
+int stored_points(long eType);
+double mat_f_yc(const ufem_model *m, long mat);
+// fy_col_by_mat: ifld column of each material's F_YC (nullptr: none)
+int build_elem_outputs(const ufem_model *m, ElemOutPlan &P, const std::vector<int> *fy_col_by_mat, int md_col);
+// S == 1 (u, E per element) or S a multiple of 128 (x[row*S + s], E[e*S + s]);
+// ofld[s*olen + pos]; ifld (device) is read only through the plan's columns
+int run_elem_outputs(const ufem_model *m, ElemOutPlan &P, int S, int nsamp, const double *u, const double *E,
+                     const double *ifld, long ilen, double md0, double *ofld, long olen, int *launches);
+
 }  // namespace ufem
