@@ -101,6 +101,9 @@ def parse():
                    help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
     p.add_argument("--profile-static", action="store_true",
                    help="the 128x128x64 block's FP64 PCG capped at 40 iterations (two launches) for ncu captures")
+    p.add_argument("--profile-outputs", type=int, default=0, metavar="SAMPLES",
+                   help="the Monte Carlo output pass (element sums/extremes, RES_E, RES_FAIL) on the 40x10x10 "
+                        "zone beam with SAMPLES samples, against the same batch with RES_D/RES_R only")
     return p.parse_args()
 
 
@@ -169,6 +172,46 @@ def profile_static(a):
     print(json.dumps({"profile_static": "128x128x64 block, FP64 PCG, 40 iterations", "iterations": its,
                       "solve_ms": sol_ms.value, "algorithmic_bytes": by,
                       "achieved_GBs": by / sol_ms.value / 1e6 if sol_ms.value else None}))
+
+
+def profile_outputs(a):
+    """The Monte Carlo output pass at the warm-start workload's size: the
+    40x10x10 beam with 16 type-5 zones (they hold F_YC), the output table of
+    `mc_attach_outputs` (element sums/maxima/minima/fail flags over stresses
+    and strains, RES_E points, RES_FAIL with F_YC and MAX_D per sample) and
+    the same batch with RES_D/RES_R outputs only; PCG capped at 40
+    iterations (the outputs do not depend on the cap), each run twice (warm,
+    timed).  The pass reads u twice (element gathers, max |u|), E once, and
+    writes and reads one record of 3 x 12 + 1 doubles per (element range,
+    sample)."""
+    import numpy as np
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    from ufem_b200.mc import mc_solve
+    S = a.profile_outputs
+    rows = {}
+    for kind in ("plain", "outputs"):
+        m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
+        m.mp_type = np.full(len(m.mp_vals), mg.MAT_STRENGTH, np.int64)
+        m.mp_vals = [np.array([2500.0, 30e9, 0.2, 12.5e9, 24e6, 2e6, 30e6, 2e6]) for _ in m.mp_vals]
+        if kind == "plain":
+            f = mg.mc_samples(m, mesh_id=4, nsamp=S)
+        else:
+            mg.mc_attach_outputs(m)
+            # stresses of this beam reach ~24 MPa at the support; tip deflection ~1.7 cm
+            f = mg.mc_outputs_samples(m, S, vm_scale=24e6, u_scale=0.13)
+        g = GpuModel(m)
+        for _ in range(2):
+            res, st = mc_solve([g], [f], precision=2, max_iters=40, coarse=0)
+        rows[kind] = dict(ms_outputs=st.ms_outputs, ms_pcg=st.ms_pcg, launches=st.kernel_launches,
+                          olen=m.mc_olen, ne=m.eLen, n=g.ndof)
+    n, ne = rows["outputs"]["n"], rows["outputs"]["ne"]
+    nch = max(1, min(ne, -(-4 * 148 // (S // 128))))
+    by = 2.0 * n * S * 8 + ne * S * 8.0 + 2.0 * nch * 37 * S * 8
+    dt = rows["outputs"]["ms_outputs"] - rows["plain"]["ms_outputs"]
+    print(json.dumps({"profile_outputs": f"40x10x10 16 type-5 zones x {S} samples", "plain": rows["plain"],
+                      "outputs": rows["outputs"], "element_pass_ms": dt, "element_pass_bytes": by,
+                      "achieved_GBs": by / dt / 1e6 if dt > 0 else None}))
 
 
 def build_meshes(nsamp, rank=0):
@@ -845,6 +888,9 @@ def main():
         return
     if a.profile_static:
         profile_static(a)
+        return
+    if a.profile_outputs:
+        profile_outputs(a)
         return
     if a.impl == "reference":
         reference_arm(a)

@@ -69,9 +69,29 @@ __device__ __forceinline__ void point_grad_quad(const double *__restrict__ xyz, 
   }
 }
 
+// D of the isotropic solid (fem/fem_pl3d.c:32-60): d[0] diagonal normal,
+// d[1] off-diagonal normal, d[2] shear; per element and sample
+__device__ __forceinline__ void elem_D_brick(double Ee, double nu, double *__restrict__ d) {
+  d[0] = (Ee * (1.0 - nu)) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  d[1] = (Ee * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  d[2] = Ee / (2.0 * (1 + nu));
+}
+
+// plane D: thick > 0 plane stress, else plane strain (fem/fem_e002.c:400-407,
+// fem/fem_stf2.c:43-89); d = D11, D12, D22, D33
+__device__ __forceinline__ void elem_D_quad(double Ee, double nu, double thick, double *__restrict__ d) {
+  if (thick > 0.0) {
+    const double Mul = Ee / (1 - nu * nu);
+    d[0] = Mul; d[1] = Mul * nu; d[2] = Mul; d[3] = Mul * 0.5 * (1 - nu);
+  } else {
+    const double Mul = Ee / ((1 + nu) * (1 - 2 * nu));
+    d[0] = Mul * (1 - nu); d[1] = Mul * nu; d[2] = Mul * (1 - nu); d[3] = Mul * 0.5 * (1 - nu);
+  }
+}
+
 // v[0..5]: SX, SY, SZ, SYZ, SZX, SXY; v[6..11]: EX, EY, EZ, EYZ, EZX, EXY
 __device__ __forceinline__ void point_values_brick(const double *__restrict__ G, const double *__restrict__ ue,
-                                                   double Ee, double nu, double *__restrict__ v) {
+                                                   const double *__restrict__ d, double *__restrict__ v) {
   double ep[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int n = 0; n < 8; n++) {
@@ -80,48 +100,41 @@ __device__ __forceinline__ void point_values_brick(const double *__restrict__ G,
     ep[0] += g0 * ux; ep[1] += g1 * uy; ep[2] += g2 * uz;
     ep[3] += g2 * uy + g1 * uz; ep[4] += g2 * ux + g0 * uz; ep[5] += g1 * ux + g0 * uy;
   }
-  const double d1 = (Ee * (1.0 - nu)) / ((1.0 + nu) * (1.0 - 2.0 * nu));
-  const double d2 = (Ee * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
-  const double d3 = Ee / (2.0 * (1 + nu));
-  v[0] = d1 * ep[0] + d2 * ep[1] + d2 * ep[2];
-  v[1] = d2 * ep[0] + d1 * ep[1] + d2 * ep[2];
-  v[2] = d2 * ep[0] + d2 * ep[1] + d1 * ep[2];
-  v[3] = d3 * ep[3]; v[4] = d3 * ep[4]; v[5] = d3 * ep[5];
+  v[0] = d[0] * ep[0] + d[1] * ep[1] + d[1] * ep[2];
+  v[1] = d[1] * ep[0] + d[0] * ep[1] + d[1] * ep[2];
+  v[2] = d[1] * ep[0] + d[1] * ep[1] + d[0] * ep[2];
+  v[3] = d[2] * ep[3]; v[4] = d[2] * ep[4]; v[5] = d[2] * ep[5];
 #pragma unroll
   for (int c = 0; c < 6; c++) v[6 + c] = ep[c];
 }
 
-// v[0..2]: SX, SY, SXY; v[3..5]: EX, EY, EXY.  thick > 0: plane stress, else
-// plane strain (fem/fem_e002.c:400-407, D of fem/fem_stf2.c:43-89)
+// v[0..2]: SX, SY, SXY; v[3..5]: EX, EY, EXY
 __device__ __forceinline__ void point_values_quad(const double *__restrict__ G, const double *__restrict__ ue,
-                                                  double Ee, double nu, double thick, double *__restrict__ v) {
+                                                  const double *__restrict__ d, double *__restrict__ v) {
   double ex = 0, ey = 0, gxy = 0;
 #pragma unroll
   for (int n = 0; n < 4; n++) {
     const double gx = G[2 * n], gy = G[2 * n + 1], ux = ue[2 * n], uy = ue[2 * n + 1];
     ex += gx * ux; ey += gy * uy; gxy += gy * ux + gx * uy;
   }
-  double Mul, D0, D1, D2, D3;
-  if (thick > 0.0) {
-    Mul = Ee / (1 - nu * nu); D0 = Mul; D1 = Mul * nu; D2 = Mul; D3 = Mul * 0.5 * (1 - nu);
-  } else {
-    Mul = Ee / ((1 + nu) * (1 - 2 * nu)); D0 = Mul * (1 - nu); D1 = Mul * nu; D2 = Mul * (1 - nu);
-    D3 = Mul * 0.5 * (1 - nu);
-  }
-  v[0] = D0 * ex + D1 * ey; v[1] = D1 * ex + D2 * ey; v[2] = D3 * gxy;
+  v[0] = d[0] * ex + d[1] * ey; v[1] = d[1] * ex + d[2] * ey; v[2] = d[3] * gxy;
   v[3] = ex; v[4] = ey; v[5] = gxy;
 }
 
-// sqrt(3 J2) of the stored stress vector: stress2D_J2 (fem/fem_ch2d.c:46-57)
-// and stress3D_J2 (fem/fem_chen.c:54-74, which reads components 4, 5, 6 as
-// t_zx, t_yz, t_xy; the sum of their squares does not depend on the naming)
-__device__ __forceinline__ double vmis_quad(const double *v) {
-  const double d = v[0] - v[1];
-  return sqrt(((d * d + v[0] * v[0] + v[1] * v[1]) / 6.0 + v[2] * v[2]) * 3.0);
+// 3 J2 of the stored stress vector, the square of the von Mises stress that
+// fem_asse_mat_vmis compares with |F_YC| (sqrt(3 J2) < |F_YC|, J2 of
+// stress2D_J2 fem/fem_ch2d.c:46-57 or stress3D_J2 fem/fem_chen.c:54-74):
+// 3 J2 = ((sx-sy)^2 + sx^2 + sy^2) / 2 + 3 txy^2 (plane),
+//        ((sx-sy)^2 + (sy-sz)^2 + (sz-sx)^2) / 2 + 3 (tyz^2 + tzx^2 + txy^2) (solid).
+// Callers test 3 J2 < F_YC^2, the same order for non-negative values, and a
+// NaN stress fails both forms.
+__device__ __forceinline__ double vmis2_quad(const double *v) {
+  const double a = v[0] - v[1];
+  return 0.5 * (a * a + v[0] * v[0] + v[1] * v[1]) + 3.0 * (v[2] * v[2]);
 }
-__device__ __forceinline__ double vmis_brick(const double *v) {
+__device__ __forceinline__ double vmis2_brick(const double *v) {
   const double a = v[0] - v[1], b = v[1] - v[2], c = v[2] - v[0];
-  return sqrt(((a * a + b * b + c * c) / 6.0 + v[5] * v[5] + v[4] * v[4] + v[3] * v[3]) * 3.0);
+  return 0.5 * (a * a + b * b + c * c) + 3.0 * (v[5] * v[5] + v[4] * v[4] + v[3] * v[3]);
 }
 
 }  // namespace ep

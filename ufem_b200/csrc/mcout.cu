@@ -14,7 +14,8 @@
 // (so they are max(0, ...) and min(0, ...)), FAIL_E is "some value > 0", i.e.
 // MAX_E > 0.  The failure function fails an element whose F_YC reads 0
 // (the zero stress of set 0 is not below it) or any stored point whose
-// sqrt(3 J2) is not below |F_YC|; the displacement test compares
+// sqrt(3 J2) is not below |F_YC| (tested as 3 J2 against F_YC^2); the
+// displacement test compares
 // femVecMaxAbs(u), which returns sqrt(max |u_i|) (fem/fem_math.c:2136-2163),
 // with MAX_D.
 //
@@ -82,16 +83,22 @@ __device__ __forceinline__ void point_grad(const double *xyz, const int *en, int
   else ep::point_grad_quad(xyz, en, ip, G);
 }
 
+// D per element and sample: 3 (solid) or 4 (plane) coefficients
 template <int B>
-__device__ __forceinline__ void point_values(const double *G, const double *ue, double Ee, double nu, double th,
-                                             double *v) {
-  if (B == 3) ep::point_values_brick(G, ue, Ee, nu, v);
-  else ep::point_values_quad(G, ue, Ee, nu, th, v);
+__device__ __forceinline__ void elem_D(double Ee, double nu, double th, double *d) {
+  if (B == 3) ep::elem_D_brick(Ee, nu, d);
+  else ep::elem_D_quad(Ee, nu, th, d);
 }
 
 template <int B>
-__device__ __forceinline__ double point_vmis(const double *v) {
-  return (B == 3) ? ep::vmis_brick(v) : ep::vmis_quad(v);
+__device__ __forceinline__ void point_values(const double *G, const double *ue, const double *d, double *v) {
+  if (B == 3) ep::point_values_brick(G, ue, d, v);
+  else ep::point_values_quad(G, ue, d, v);
+}
+
+template <int B>
+__device__ __forceinline__ double point_vmis2(const double *v) {
+  return (B == 3) ? ep::vmis2_brick(v) : ep::vmis2_quad(v);
 }
 
 // |F_YC| of element e for sample s: the material's value, or the sample's
@@ -138,18 +145,20 @@ __global__ void __launch_bounds__(kEoThreads) k_eo_samples(int ne, int S, int ns
     for (int n = 0; n < R::NN; n++)
 #pragma unroll
       for (int d = 0; d < B; d++) ue[n * B + d] = u[(size_t)(sRow[n] + d) * S + s];
-    const double Ee = E[(size_t)e * S + s], nu = eNu[e], th = eThick[e];
-    double fy = 0.0;
+    double d[4];
+    elem_D<B>(E[(size_t)e * S + s], eNu[e], eThick[e], d);
+    double fy2 = 0.0;
     if (strength) {
-      fy = elem_fy(e, s, nsamp, fy0, fycol, ifld, ilen);
+      const double fy = elem_fy(e, s, nsamp, fy0, fycol, ifld, ilen);
       if (!(0.0 < fy)) a.fail = 1;  // result set 0 (zero stress), fem/fem_asse.c:323-327
+      fy2 = fy * fy;
     }
     __syncthreads();
     for (int p = 0; p < np; p++) {
       double v[R::NV];
-      point_values<B>(sG[p], ue, Ee, nu, th, v);
+      point_values<B>(sG[p], ue, d, v);
       a.add(v);
-      if (strength && !(point_vmis<B>(v) < fy)) a.fail = 1;
+      if (strength && !(point_vmis2<B>(v) < fy2)) a.fail = 1;
     }
     __syncthreads();
   }
@@ -182,16 +191,17 @@ __global__ void __launch_bounds__(kEoThreads) k_eo_elements(int ne, const int *_
 #pragma unroll
       for (int d = 0; d < B; d++) ue[n * B + d] = u[r0 + d];
     }
-    const double Ee = E[e], nu = eNu[e], th = eThick[e];
-    const double fy = strength ? fabs(fy0[e]) : 0.0;
+    double d[4];
+    elem_D<B>(E[e], eNu[e], eThick[e], d);
+    const double fy = strength ? fabs(fy0[e]) : 0.0, fy2 = fy * fy;
     if (strength && !(0.0 < fy)) a.fail = 1;
     const int np = enpts[e];
     for (int p = 0; p < np; p++) {
       double G[R::NG], v[R::NV];
       point_grad<B>(xyz, en, p, G);
-      point_values<B>(G, ue, Ee, nu, th, v);
+      point_values<B>(G, ue, d, v);
       a.add(v);
-      if (strength && !(point_vmis<B>(v) < fy)) a.fail = 1;
+      if (strength && !(point_vmis2<B>(v) < fy2)) a.fail = 1;
     }
   }
   for (int q = 0; q < R::NQ; q++) sh[q][threadIdx.x] = a.get(q);
@@ -294,8 +304,10 @@ __global__ void k_eo_points(int npo, int S, int nsamp, const int *__restrict__ p
     const int r0 = node_rank[en[n]] * B;
     for (int d = 0; d < B; d++) ue[n * B + d] = u[(size_t)(r0 + d) * S + s];
   }
+  double d[4];
+  elem_D<B>(E[(size_t)e * S + s], eNu[e], eThick[e], d);
   point_grad<B>(xyz, en, pip[o], G);
-  point_values<B>(G, ue, E[(size_t)e * S + s], eNu[e], eThick[e], v);
+  point_values<B>(G, ue, d, v);
   double r = 0.0;
   for (int c = 0; c < R::NV; c++)
     if (c == pcomp[o]) r = v[c];
