@@ -101,6 +101,9 @@ def parse():
                    help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
     p.add_argument("--profile-static", action="store_true",
                    help="the 128x128x64 block's FP64 PCG capped at 40 iterations (two launches) for ncu captures")
+    p.add_argument("--profile-ingest", action="store_true",
+                   help="input-file ingest of the 128x128x64 block: text vs binary form (host parse, then the "
+                        "whole ufem_read_input with the model build and upload)")
     p.add_argument("--profile-outputs", type=int, default=0, metavar="SAMPLES",
                    help="the Monte Carlo output pass (element sums/extremes, RES_E, RES_FAIL) on the 40x10x10 "
                         "zone beam with SAMPLES samples, against the same batch with RES_D/RES_R only")
@@ -212,6 +215,35 @@ def profile_outputs(a):
     print(json.dumps({"profile_outputs": f"40x10x10 16 type-5 zones x {S} samples", "plain": rows["plain"],
                       "outputs": rows["outputs"], "element_pass_ms": dt, "element_pass_bytes": by,
                       "achieved_GBs": by / dt / 1e6 if dt > 0 else None}))
+
+
+def profile_ingest(a):
+    """Ingest of the 128x128x64 block's input file (1.1 M nodes, 1 M
+    elements): `ufem_convert_input` from the text form and from the binary
+    form (parse + write of the binary file, host only), then
+    `ufem_read_input` of each form (parse, DOF numbering, pattern, upload)."""
+    import tempfile
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel, convert_input
+    d = tempfile.mkdtemp()
+    m = mg.block_brick(128, 128, 64)
+    txt, b1, b2 = (os.path.join(d, f) for f in ("block.fem", "block.bin", "block2.bin"))
+    mg.write_fem(m, txt)
+    t0 = time.perf_counter()
+    convert_input(txt, b1)
+    t1 = time.perf_counter()
+    convert_input(b1, b2)
+    t2 = time.perf_counter()
+    rd = {}
+    for form, path in (("text", txt), ("binary", b1)):
+        GpuModel(path=path).close()  # first-call set-up out of the timing
+        s0 = time.perf_counter()
+        GpuModel(path=path).close()
+        rd[form] = time.perf_counter() - s0
+    print(json.dumps({"profile_ingest": "128x128x64 block input file", "text_MB": os.path.getsize(txt) / 1e6,
+                      "binary_MB": os.path.getsize(b1) / 1e6, "convert_from_text_s": t1 - t0,
+                      "convert_from_binary_s": t2 - t1, "read_input_text_s": rd["text"],
+                      "read_input_binary_s": rd["binary"]}))
 
 
 def build_meshes(nsamp, rank=0):
@@ -891,6 +923,9 @@ def main():
         return
     if a.profile_outputs:
         profile_outputs(a)
+        return
+    if a.profile_ingest:
+        profile_ingest(a)
         return
     if a.impl == "reference":
         reference_arm(a)

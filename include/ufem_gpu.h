@@ -89,8 +89,19 @@ int ufem_model_create(const ufem_tables *t, ufem_model **out);
 
 /* Reads a preparsed uFEM input file (femReadInput, fem/fem_io.c:380, with
  * femPreparsedData = AF_YES) including its Monte Carlo section
- * (fem_monte_read_data, fem/fem_mont.c:866), then ufem_model_create. */
+ * (fem_monte_read_data, fem/fem_mont.c:866), then ufem_model_create.  A file
+ * written by ufem_convert_input (it starts with "UFEMBIN1") is read in its
+ * binary form: the same tables, no text parsing.  monte_init_lib_stuff reads
+ * through this function, so it takes either form. */
 int ufem_read_input(const char *fname, ufem_model **out);
+
+/* Writes the tables of an input file (text or binary) to bin_fname in the
+ * binary form: "UFEMBIN1", a uint32 byte-order mark 0x01020304, then 28
+ * arrays (int64 count, then int64 or float64 items, little-endian): real
+ * sets, materials, nodes, elements, nodal loads and the Monte Carlo table.
+ * Host only; needs no GPU.  No counterpart in the reference (its reader is
+ * text only, femReadInput fem/fem_io.c:380-635). */
+int ufem_convert_input(const char *text_fname, const char *bin_fname);
 
 void ufem_model_free(ufem_model *m);
 

@@ -74,6 +74,7 @@ _SIGS = {
     "ufem_device_info": (C.c_int, [_i, _i, _i, _l]),
     "ufem_model_create": (C.c_int, [C.POINTER(Tables), C.POINTER(C.c_void_p)]),
     "ufem_read_input": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "ufem_convert_input": (C.c_int, [C.c_char_p, C.c_char_p]),
     "ufem_model_free": (None, [C.c_void_p]),
     "ufem_model_set_mc_vars": (C.c_int, [C.c_void_p, C.c_long, C.c_long, _l]),
     "ufem_ndof": (C.c_long, [C.c_void_p]),

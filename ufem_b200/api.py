@@ -65,6 +65,12 @@ def tables_of(model: Model):
     return t, keep
 
 
+def convert_input(text_path: str, bin_path: str) -> None:
+    """Write the binary form of an input file (``ufem_convert_input``); host
+    only.  ``GpuModel(path=...)`` and the Monte Carlo plugin read either form."""
+    _lib.check("ufem_convert_input", _lib.load().ufem_convert_input(text_path.encode(), bin_path.encode()))
+
+
 class GpuModel:
     """One model on the GPU (``ufem_model`` handle)."""
 

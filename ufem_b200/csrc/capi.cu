@@ -75,6 +75,14 @@ int ufem_read_input(const char *fname, ufem_model **out) {
   return read_input_file(fname, out);
 }
 
+int ufem_convert_input(const char *text_fname, const char *bin_fname) {
+  if (!text_fname || !bin_fname) {
+    set_error("ufem_convert_input: null file name");
+    return UFEM_AF_ERR_VAL;
+  }
+  return convert_input_file(text_fname, bin_fname);
+}
+
 void ufem_model_free(ufem_model *m) {
   if (!m) return;
   drop_plan(m);

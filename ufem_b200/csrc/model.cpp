@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <fstream>
 #include <mutex>
@@ -419,60 +420,64 @@ struct Tok {
 };
 }  // namespace
 
-int read_input_file(const char *fname, ufem_model **out) {
-  std::ifstream f(fname, std::ios::binary);
-  if (!f) {
-    set_error(std::string("cannot open input ") + fname);
-    return UFEM_AF_ERR_IO;
-  }
-  std::stringstream ss;
-  ss << f.rdbuf();
-  std::string buf = ss.str();
+namespace {
+
+// The tables of an input file, as parsed from the text form or the binary
+// form, before the model is built from them.
+struct InputTables {
+  std::vector<long> rsID, rsType, rsFrom;
+  std::vector<double> rsVal;
+  std::vector<long> mpID, mpType, mpFrom;
+  std::vector<double> mpVal;
+  std::vector<long> nID;
+  std::vector<double> nx, ny, nz;
+  std::vector<long> eID, eType, eRS, eMP, eFrom, eNodes;
+  std::vector<long> nlNode, nlType, nlDir;
+  std::vector<double> nlVal;
+  long mc_ilen = 0, mc_olen = 0;
+  std::vector<long> mc_pos, mc_type, mc_item, mc_sub, mc_iter;
+};
+
+int parse_text(const std::string &buf, InputTables &in) {
   Tok t{buf.data(), buf.data() + buf.size()};
   // solution control data (fem/fem_io.c:408-414)
   t.L(); t.L();
   t.L(); t.L(); t.L();
   // real sets (fem/fem_io.c:421-475)
   long rsLen = t.L();
-  std::vector<long> rsID, rsType, rsFrom;
-  std::vector<double> rsVal;
   long sum = 0;
   for (long i = 0; i < rsLen; i++) {
-    rsID.push_back(t.L());
-    rsType.push_back(t.L());
+    in.rsID.push_back(t.L());
+    in.rsType.push_back(t.L());
     long c = t.L();
-    rsFrom.push_back(sum);
+    in.rsFrom.push_back(sum);
     sum += c;
   }
-  long rsLenL = 0;
   if (rsLen > 0) {
-    rsLenL = t.L();
+    long rsLenL = t.L();
     if (rsLenL != sum) {
       set_error("bad number of real set values");
       return UFEM_AF_ERR_SIZ;
     }
-    for (long i = 0; i < rsLenL; i++) rsVal.push_back(t.D());
+    for (long i = 0; i < rsLenL; i++) in.rsVal.push_back(t.D());
   }
   // materials (fem/fem_io.c:478-521)
   long mpLen = t.L();
-  std::vector<long> mpID, mpType, mpFrom;
-  std::vector<double> mpVal;
   sum = 0;
   for (long i = 0; i < mpLen; i++) {
-    mpID.push_back(t.L());
-    mpType.push_back(t.L());
+    in.mpID.push_back(t.L());
+    in.mpType.push_back(t.L());
     long c = t.L();
-    mpFrom.push_back(sum);
+    in.mpFrom.push_back(sum);
     sum += c;
   }
-  long mpLenL = 0;
   if (mpLen > 0) {
-    mpLenL = t.L();
+    long mpLenL = t.L();
     if (mpLenL != sum) {
       set_error("bad number of material property values");
       return UFEM_AF_ERR_SIZ;
     }
-    for (long i = 0; i < mpLenL; i++) mpVal.push_back(t.D());
+    for (long i = 0; i < mpLenL; i++) in.mpVal.push_back(t.D());
   }
   // nodes (fem/fem_io.c:524-540)
   long nLen = t.L();
@@ -480,13 +485,15 @@ int read_input_file(const char *fname, ufem_model **out) {
     set_error("fewer than 2 nodes");
     return UFEM_AF_ERR_SML;
   }
-  std::vector<long> nID(nLen);
-  std::vector<double> nx(nLen), ny(nLen), nz(nLen);
+  in.nID.resize(nLen);
+  in.nx.resize(nLen);
+  in.ny.resize(nLen);
+  in.nz.resize(nLen);
   for (long i = 0; i < nLen; i++) {
-    nID[i] = t.L();
-    nx[i] = t.D();
-    ny[i] = t.D();
-    nz[i] = t.D();
+    in.nID[i] = t.L();
+    in.nx[i] = t.D();
+    in.ny[i] = t.D();
+    in.nz[i] = t.D();
   }
   // elements (fem/fem_io.c:543-598)
   long eLen = t.L();
@@ -494,15 +501,19 @@ int read_input_file(const char *fname, ufem_model **out) {
     set_error("no elements");
     return UFEM_AF_ERR_SML;
   }
-  std::vector<long> eID(eLen), eType(eLen), eRS(eLen), eMP(eLen), eFrom(eLen);
+  in.eID.resize(eLen);
+  in.eType.resize(eLen);
+  in.eRS.resize(eLen);
+  in.eMP.resize(eLen);
+  in.eFrom.resize(eLen);
   sum = 0;
   for (long i = 0; i < eLen; i++) {
-    eID[i] = t.L();
-    eType[i] = t.L();
-    eRS[i] = t.L();
-    eMP[i] = t.L();
+    in.eID[i] = t.L();
+    in.eType[i] = t.L();
+    in.eRS[i] = t.L();
+    in.eMP[i] = t.L();
     long c = t.L();
-    eFrom[i] = sum;
+    in.eFrom[i] = sum;
     sum += c;
   }
   long eLenL = t.L();
@@ -510,8 +521,8 @@ int read_input_file(const char *fname, ufem_model **out) {
     set_error("bad number of element nodes");
     return UFEM_AF_ERR_SIZ;
   }
-  std::vector<long> eNodes(eLenL);
-  for (long i = 0; i < eLenL; i++) eNodes[i] = t.L();
+  in.eNodes.resize(eLenL);
+  for (long i = 0; i < eLenL; i++) in.eNodes[i] = t.L();
   // gravity (fem/fem_io.c:604) -- only zero gravity is on this path
   t.L();
   double grVal = t.D();
@@ -521,13 +532,15 @@ int read_input_file(const char *fname, ufem_model **out) {
   }
   // nodal loads (fem/fem_io.c:92-113)
   long nlLen = t.L();
-  std::vector<long> nlNode(nlLen), nlType(nlLen), nlDir(nlLen);
-  std::vector<double> nlVal(nlLen);
+  in.nlNode.resize(nlLen);
+  in.nlType.resize(nlLen);
+  in.nlDir.resize(nlLen);
+  in.nlVal.resize(nlLen);
   for (long i = 0; i < nlLen; i++) {
-    nlNode[i] = t.L();
-    nlType[i] = t.L();
-    nlDir[i] = t.L();
-    nlVal[i] = t.D();
+    in.nlNode[i] = t.L();
+    in.nlType[i] = t.L();
+    in.nlDir[i] = t.L();
+    in.nlVal[i] = t.D();
   }
   // element loads (fem/fem_io.c:116) -- none on this path
   long elLen = t.L();
@@ -541,36 +554,32 @@ int read_input_file(const char *fname, ufem_model **out) {
   }
   // transient and dynamics counters (fem/fem_io.c:176, :297) and the
   // optional Monte Carlo table (fem/fem_mont.c:873-905)
-  ufem_model *m = new ufem_model();
   if (t.more()) {
     long transNum = t.L(), dynNum = t.L();
     t.D();
     if (dynNum > 0 && transNum > 0) {
-      delete m;
       set_error("transient data are not on this path");
       return UFEM_AF_ERR_TYP;
     }
     if (t.more()) {
       long dynNum0 = t.L();
       if (dynNum0 > 0) {
-        delete m;
         set_error("dynamics data are not on this path");
         return UFEM_AF_ERR_TYP;
       }
       if (t.more()) {
         long ilen = t.L(), olen = t.L();
         if (t.ok && ilen > 0) {
-          m->mc_ilen = ilen;
-          m->mc_olen = olen;
+          in.mc_ilen = ilen;
+          in.mc_olen = olen;
           for (long i = 0; i < ilen + olen; i++) {
-            m->mc_pos.push_back(t.L());
-            m->mc_type.push_back(t.L());
-            m->mc_item.push_back(t.L());
-            m->mc_sub.push_back(t.L());
-            m->mc_iter.push_back(t.L());
+            in.mc_pos.push_back(t.L());
+            in.mc_type.push_back(t.L());
+            in.mc_item.push_back(t.L());
+            in.mc_sub.push_back(t.L());
+            in.mc_iter.push_back(t.L());
           }
           if (!t.ok) {
-            delete m;
             set_error("incomplete or unavailable random data");  // fem/fem_mont.c:885
             return UFEM_AF_ERR_IO;
           }
@@ -578,27 +587,186 @@ int read_input_file(const char *fname, ufem_model **out) {
       }
     }
   }
-  m->nID = nID;
-  m->eID = eID;
-  m->mpID = mpID;
-  m->rsID = rsID;
+  return UFEM_AF_OK;
+}
+
+// ---- binary form (no reference counterpart) --------------------------------
+// "UFEMBIN1", a uint32 byte-order mark 0x01020304, then 28 arrays, each as an
+// int64 count followed by count little-endian int64 (integer tables) or
+// float64 (coordinates and values) items, in the order of kBinOrder below.
+// The MC table's ilen and olen travel as a 2-item array.
+constexpr char kBinMagic[8] = {'U', 'F', 'E', 'M', 'B', 'I', 'N', '1'};
+constexpr uint32_t kBinBom = 0x01020304u;
+
+struct BinArray {
+  std::vector<long> *l;
+  std::vector<double> *d;
+};
+
+std::vector<BinArray> bin_order(InputTables &in, std::vector<long> &mc_len) {
+  return {{&in.rsID, nullptr},   {&in.rsType, nullptr}, {&in.rsFrom, nullptr}, {nullptr, &in.rsVal},
+          {&in.mpID, nullptr},   {&in.mpType, nullptr}, {&in.mpFrom, nullptr}, {nullptr, &in.mpVal},
+          {&in.nID, nullptr},    {nullptr, &in.nx},     {nullptr, &in.ny},     {nullptr, &in.nz},
+          {&in.eID, nullptr},    {&in.eType, nullptr},  {&in.eRS, nullptr},    {&in.eMP, nullptr},
+          {&in.eFrom, nullptr},  {&in.eNodes, nullptr}, {&in.nlNode, nullptr}, {&in.nlType, nullptr},
+          {&in.nlDir, nullptr},  {nullptr, &in.nlVal},  {&mc_len, nullptr},    {&in.mc_pos, nullptr},
+          {&in.mc_type, nullptr}, {&in.mc_item, nullptr}, {&in.mc_sub, nullptr}, {&in.mc_iter, nullptr}};
+}
+
+bool is_binary(const std::string &buf) {
+  return buf.size() >= sizeof(kBinMagic) && std::memcmp(buf.data(), kBinMagic, sizeof(kBinMagic)) == 0;
+}
+
+int parse_binary(const std::string &buf, InputTables &in) {
+  static_assert(sizeof(long) == 8 && sizeof(double) == 8, "64-bit long and double");
+  size_t off = sizeof(kBinMagic);
+  uint32_t bom = 0;
+  if (buf.size() < off + sizeof(bom)) {
+    set_error("truncated binary input");
+    return UFEM_AF_ERR_IO;
+  }
+  std::memcpy(&bom, buf.data() + off, sizeof(bom));
+  off += sizeof(bom);
+  if (bom != kBinBom) {
+    set_error("binary input written with another byte order");
+    return UFEM_AF_ERR_IO;
+  }
+  std::vector<long> mc_len;
+  for (BinArray &a : bin_order(in, mc_len)) {
+    int64_t n = 0;
+    if (buf.size() - off < sizeof(n)) {
+      set_error("truncated binary input");
+      return UFEM_AF_ERR_IO;
+    }
+    std::memcpy(&n, buf.data() + off, sizeof(n));
+    off += sizeof(n);
+    if (n < 0 || (uint64_t)n > (buf.size() - off) / 8) {
+      set_error("truncated binary input");
+      return UFEM_AF_ERR_IO;
+    }
+    if (a.l) {
+      a.l->resize(n);
+      if (n) std::memcpy(a.l->data(), buf.data() + off, n * 8);
+    } else {
+      a.d->resize(n);
+      if (n) std::memcpy(a.d->data(), buf.data() + off, n * 8);
+    }
+    off += n * 8;
+  }
+  // the shapes the text reader would have produced
+  const size_t nLen = in.nID.size(), eLen = in.eID.size();
+  bool ok = in.rsType.size() == in.rsID.size() && in.rsFrom.size() == in.rsID.size() &&
+            in.mpType.size() == in.mpID.size() && in.mpFrom.size() == in.mpID.size() && in.nx.size() == nLen &&
+            in.ny.size() == nLen && in.nz.size() == nLen && in.eType.size() == eLen && in.eRS.size() == eLen &&
+            in.eMP.size() == eLen && in.eFrom.size() == eLen && in.nlType.size() == in.nlNode.size() &&
+            in.nlDir.size() == in.nlNode.size() && in.nlVal.size() == in.nlNode.size() && mc_len.size() == 2;
+  for (size_t i = 0; ok && i < eLen; i++)
+    ok = in.eFrom[i] >= 0 && in.eFrom[i] <= (long)in.eNodes.size() && (i == 0 || in.eFrom[i] >= in.eFrom[i - 1]);
+  for (size_t i = 0; ok && i < in.rsFrom.size(); i++) ok = in.rsFrom[i] >= 0 && in.rsFrom[i] <= (long)in.rsVal.size();
+  for (size_t i = 0; ok && i < in.mpFrom.size(); i++) ok = in.mpFrom[i] >= 0 && in.mpFrom[i] <= (long)in.mpVal.size();
+  if (ok) {
+    in.mc_ilen = mc_len[0];
+    in.mc_olen = mc_len[1];
+    const size_t nmc = in.mc_ilen > 0 ? (size_t)(in.mc_ilen + in.mc_olen) : 0;
+    ok = in.mc_ilen >= 0 && in.mc_olen >= 0 && in.mc_pos.size() == nmc && in.mc_type.size() == nmc &&
+         in.mc_item.size() == nmc && in.mc_sub.size() == nmc && in.mc_iter.size() == nmc;
+  }
+  if (!ok) {
+    set_error("inconsistent binary input");
+    return UFEM_AF_ERR_SIZ;
+  }
+  if (nLen < 2) {
+    set_error("fewer than 2 nodes");
+    return UFEM_AF_ERR_SML;
+  }
+  if (eLen < 1) {
+    set_error("no elements");
+    return UFEM_AF_ERR_SML;
+  }
+  return UFEM_AF_OK;
+}
+
+int write_binary(InputTables &in, const char *fname) {
+  std::ofstream f(fname, std::ios::binary | std::ios::trunc);
+  if (!f) {
+    set_error(std::string("cannot open output ") + fname);
+    return UFEM_AF_ERR_IO;
+  }
+  f.write(kBinMagic, sizeof(kBinMagic));
+  f.write(reinterpret_cast<const char *>(&kBinBom), sizeof(kBinBom));
+  std::vector<long> mc_len = {in.mc_ilen, in.mc_olen};
+  for (BinArray &a : bin_order(in, mc_len)) {
+    const int64_t n = a.l ? (int64_t)a.l->size() : (int64_t)a.d->size();
+    f.write(reinterpret_cast<const char *>(&n), sizeof(n));
+    if (n) f.write(a.l ? reinterpret_cast<const char *>(a.l->data()) : reinterpret_cast<const char *>(a.d->data()),
+                   n * 8);
+  }
+  if (!f) {
+    set_error(std::string("cannot write ") + fname);
+    return UFEM_AF_ERR_IO;
+  }
+  return UFEM_AF_OK;
+}
+
+int read_file(const char *fname, std::string &buf) {
+  std::ifstream f(fname, std::ios::binary);
+  if (!f) {
+    set_error(std::string("cannot open input ") + fname);
+    return UFEM_AF_ERR_IO;
+  }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  buf = ss.str();
+  return UFEM_AF_OK;
+}
+
+}  // namespace
+
+int read_input_file(const char *fname, ufem_model **out) {
+  std::string buf;
+  int rv = read_file(fname, buf);
+  if (rv != UFEM_AF_OK) return rv;
+  InputTables in;
+  rv = is_binary(buf) ? parse_binary(buf, in) : parse_text(buf, in);
+  if (rv != UFEM_AF_OK) return rv;
+  ufem_model *m = new ufem_model();
+  m->mc_ilen = in.mc_ilen;
+  m->mc_olen = in.mc_olen;
+  m->mc_pos = in.mc_pos;
+  m->mc_type = in.mc_type;
+  m->mc_item = in.mc_item;
+  m->mc_sub = in.mc_sub;
+  m->mc_iter = in.mc_iter;
+  m->nID = in.nID;
+  m->eID = in.eID;
+  m->mpID = in.mpID;
+  m->rsID = in.rsID;
   ufem_tables tb{};
-  tb.nLen = nLen; tb.n_x = nx.data(); tb.n_y = ny.data(); tb.n_z = nz.data();
-  tb.eLen = eLen; tb.eType = eType.data(); tb.eRS = eRS.data(); tb.eMP = eMP.data();
-  tb.eFrom = eFrom.data(); tb.eNodesL = eNodes.data();
-  tb.rsLen = rsLen; tb.rsType = rsType.data(); tb.rsFrom = rsFrom.data(); tb.rsLenL = rsLenL;
-  tb.rsValL = rsVal.data();
-  tb.mpLen = mpLen; tb.mpType = mpType.data(); tb.mpFrom = mpFrom.data(); tb.mpLenL = mpLenL;
-  tb.mpValL = mpVal.data();
-  tb.nlLen = nlLen; tb.nlNode = nlNode.data(); tb.nlType = nlType.data(); tb.nlDir = nlDir.data();
-  tb.nlVal = nlVal.data();
-  int rv = model_from_tables(&tb, m);
+  tb.nLen = (long)in.nID.size(); tb.n_x = in.nx.data(); tb.n_y = in.ny.data(); tb.n_z = in.nz.data();
+  tb.eLen = (long)in.eID.size(); tb.eType = in.eType.data(); tb.eRS = in.eRS.data(); tb.eMP = in.eMP.data();
+  tb.eFrom = in.eFrom.data(); tb.eNodesL = in.eNodes.data();
+  tb.rsLen = (long)in.rsID.size(); tb.rsType = in.rsType.data(); tb.rsFrom = in.rsFrom.data();
+  tb.rsLenL = (long)in.rsVal.size(); tb.rsValL = in.rsVal.data();
+  tb.mpLen = (long)in.mpID.size(); tb.mpType = in.mpType.data(); tb.mpFrom = in.mpFrom.data();
+  tb.mpLenL = (long)in.mpVal.size(); tb.mpValL = in.mpVal.data();
+  tb.nlLen = (long)in.nlNode.size(); tb.nlNode = in.nlNode.data(); tb.nlType = in.nlType.data();
+  tb.nlDir = in.nlDir.data(); tb.nlVal = in.nlVal.data();
+  rv = model_from_tables(&tb, m);
   if (rv != UFEM_AF_OK) {
     delete m;
     return rv;
   }
   *out = m;
   return UFEM_AF_OK;
+}
+
+int convert_input_file(const char *text_fname, const char *bin_fname) {
+  std::string buf;
+  int rv = read_file(text_fname, buf);
+  if (rv != UFEM_AF_OK) return rv;
+  InputTables in;
+  if ((rv = is_binary(buf) ? parse_binary(buf, in) : parse_text(buf, in)) != UFEM_AF_OK) return rv;
+  return write_binary(in, bin_fname);
 }
 
 }  // namespace ufem

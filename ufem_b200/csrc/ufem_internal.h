@@ -146,6 +146,7 @@ namespace ufem {
 int build_model(ufem_model *m);
 int setup_loads(ufem_model *m);
 int read_input_file(const char *fname, ufem_model **out);
+int convert_input_file(const char *text_fname, const char *bin_fname);
 int model_from_tables(const ufem_tables *t, ufem_model *m);
 int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, long *len);
 
