@@ -20,6 +20,7 @@
 #include <fstream>
 #include <mutex>
 #include <sstream>
+#include <thread>
 
 #include "ufem_internal.h"
 
@@ -169,6 +170,27 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
   return build_model(m);
 }
 
+namespace {
+// f(begin, end) over [0, n) split into contiguous ranges, one per host
+// thread (at most 32; serial below 4096 items)
+template <typename F>
+void parallel_ranges(long n, F f) {
+  const unsigned hc = std::thread::hardware_concurrency();
+  const long nt = std::min<long>(std::max(1u, std::min(hc, 32u)), std::max(1L, n / 4096));
+  if (nt <= 1) {
+    f(0L, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long per = (n + nt - 1) / nt;
+  for (long t = 0; t < nt; t++) {
+    const long a = t * per, b = std::min(n, a + per);
+    if (a < b) th.emplace_back(f, a, b);
+  }
+  for (auto &x : th) x.join();
+}
+}  // namespace
+
 int build_model(ufem_model *m) {
   const int b = m->b, nn = m->nn;
   // ---- fem_dofs: mark used slots, number them 1..nDOFAct in slot order ----
@@ -219,10 +241,10 @@ int build_model(ufem_model *m) {
     for (long e = 0; e < m->eLen; e++)
       for (int j = 0; j < nn; j++) n2e[fill[m->node_rank[m->enodes[(size_t)e * nn + j]]]++] = (int)e;
   }
+  // rows and elements are independent: both passes below run on host
+  // threads over contiguous ranges, with results identical to a serial build
   m->rowptr.assign(m->nbr + 1, 0);
-  std::vector<int> tmp;
-  std::vector<std::vector<int>> rows(m->nbr);
-  for (int r = 0; r < m->nbr; r++) {
+  auto row_cols = [&](int r, std::vector<int> &tmp) {
     tmp.clear();
     for (int q = n2e_ptr[r]; q < n2e_ptr[r + 1]; q++) {
       int e = n2e[q];
@@ -230,32 +252,42 @@ int build_model(ufem_model *m) {
     }
     std::sort(tmp.begin(), tmp.end());
     tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    rows[r] = tmp;
-    m->rowptr[r + 1] = m->rowptr[r] + (int)tmp.size();
-  }
+  };
+  parallel_ranges(m->nbr, [&](long r0, long r1) {
+    std::vector<int> tmp;
+    for (long r = r0; r < r1; r++) {
+      row_cols((int)r, tmp);
+      m->rowptr[r + 1] = (int)tmp.size();
+    }
+  });
+  for (int r = 0; r < m->nbr; r++) m->rowptr[r + 1] += m->rowptr[r];
   m->nnzb = m->rowptr[m->nbr];
   m->colind.resize(m->nnzb);
   m->diagblk.resize(m->nbr);
-  for (int r = 0; r < m->nbr; r++) {
-    std::copy(rows[r].begin(), rows[r].end(), m->colind.begin() + m->rowptr[r]);
-    auto it = std::lower_bound(rows[r].begin(), rows[r].end(), r);
-    m->diagblk[r] = m->rowptr[r] + (int)(it - rows[r].begin());
-  }
-  rows.clear();
-  rows.shrink_to_fit();
+  parallel_ranges(m->nbr, [&](long r0, long r1) {
+    std::vector<int> tmp;
+    for (long r = r0; r < r1; r++) {
+      row_cols((int)r, tmp);
+      std::copy(tmp.begin(), tmp.end(), m->colind.begin() + m->rowptr[r]);
+      auto it = std::lower_bound(tmp.begin(), tmp.end(), (int)r);
+      m->diagblk[r] = m->rowptr[r] + (int)(it - tmp.begin());
+    }
+  });
   // ---- element->block scatter map ------------------------------------------
   m->emap.resize((size_t)m->eLen * nn * nn);
-  for (long e = 0; e < m->eLen; e++)
-    for (int a = 0; a < nn; a++) {
-      int ra = m->node_rank[m->enodes[(size_t)e * nn + a]];
-      const int *beg = m->colind.data() + m->rowptr[ra];
-      const int *end = m->colind.data() + m->rowptr[ra + 1];
-      for (int c = 0; c < nn; c++) {
-        int rc = m->node_rank[m->enodes[(size_t)e * nn + c]];
-        const int *it = std::lower_bound(beg, end, rc);
-        m->emap[((size_t)e * nn + a) * nn + c] = (int)(it - m->colind.data());
+  parallel_ranges(m->eLen, [&](long e0, long e1) {
+    for (long e = e0; e < e1; e++)
+      for (int a = 0; a < nn; a++) {
+        int ra = m->node_rank[m->enodes[(size_t)e * nn + a]];
+        const int *beg = m->colind.data() + m->rowptr[ra];
+        const int *end = m->colind.data() + m->rowptr[ra + 1];
+        for (int c = 0; c < nn; c++) {
+          int rc = m->node_rank[m->enodes[(size_t)e * nn + c]];
+          const int *it = std::lower_bound(beg, end, rc);
+          m->emap[((size_t)e * nn + a) * nn + c] = (int)(it - m->colind.data());
+        }
       }
-    }
+  });
   // ---- greedy element colouring: no two elements of a colour share a node ---
   std::vector<uint64_t> node_used(m->nbr, 0);
   std::vector<int> ecol(m->eLen);
