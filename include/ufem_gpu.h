@@ -190,10 +190,16 @@ int ufem_eqs_cgwssor(long rows, const long *frompos, const long *defpos, const l
  * blocks); d_b and d_x (initial guess in, solution out) are device vectors
  * of nbr*B doubles.  All scratch lives in one array built into the library:
  * at most 131,072 rows (larger systems return AF_ERR_SIZ), about 6.3 MB held
- * on every GPU that loads the library until the process exits.  Calls share
- * that array: calls that overlap on the GPU race and must be serialised.
- * The first call on each device looks the array up (make it before any
- * stream capture). */
+ * on every GPU where the library's solver code is loaded -- the first use of
+ * any of its solvers on a device (this function's first call included) loads
+ * that code with the array, and both stay until the process exits; a caller
+ * that must reserve nothing later makes one solve through any entry point at
+ * set-up.  Every call shares the array, and two solves whose kernels
+ * overlapped on the GPU would race on it; within one process an internal
+ * lock serialises the calls and each call returns only after its kernels
+ * have finished.  It runs on the legacy default stream with synchronous
+ * copies, so it cannot be called while a stream is being captured.  The
+ * first call on each device looks the array's address up. */
 int ufem_eqs_cgwj_noalloc(int B, int nbr, const int *d_rowptr, const int *d_colind, const double *d_val,
                           const double *d_b, double *d_x, double eps, long maxIt, long *iters);
 

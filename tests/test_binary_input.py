@@ -84,6 +84,63 @@ def test_damaged_binary_is_rejected(tmp_path):
         convert_input(cut, str(tmp_path / "x.bin"))
 
 
+def _write_binary(path, t):
+    parts = [b"UFEMBIN1", np.array([0x01020304], "<u4").tobytes()]
+    for name in ORDER:
+        a = np.asarray(t[name], "<f8" if name in FLOATS else "<i8")
+        parts += [np.array([a.size], "<i8").tobytes(), a.tobytes()]
+    open(path, "wb").write(b"".join(parts))
+
+
+def _rejected(src, tmp_path):
+    from ufem_b200 import _lib
+    from ufem_b200.api import convert_input
+    with pytest.raises(_lib.UfemError):
+        convert_input(src, str(tmp_path / "x.bin"))
+
+
+def test_malformed_element_and_value_ranges_are_rejected(tmp_path):
+    """Both readers check every element's node count against its type and
+    the order of the real-set and material value ranges before any table is
+    indexed (host only: the checks run in ufem_convert_input too)."""
+    from ufem_b200.api import convert_input
+    _, _, txt, binp = _files(tmp_path, "mc_out_beam_4x2x2")
+    convert_input(txt, binp)
+    t = _read_binary(binp)
+    bad = str(tmp_path / "bad.bin")
+    # the last brick loses a node: the list ends one entry early
+    tt = dict(t, eNodes=t["eNodes"][:-1])
+    _write_binary(bad, tt)
+    _rejected(bad, tmp_path)
+    # an element start out of order
+    ef = t["eFrom"].copy()
+    ef[2], ef[3] = ef[3], ef[2]
+    _write_binary(bad, dict(t, eFrom=ef))
+    _rejected(bad, tmp_path)
+    # material value ranges out of order
+    mf = t["mpFrom"].copy()
+    if mf.size >= 2:
+        mf[0], mf[1] = mf[1], mf[0]
+        _write_binary(bad, dict(t, mpFrom=mf))
+        _rejected(bad, tmp_path)
+    # the unchanged tables still pass
+    _write_binary(bad, t)
+    convert_input(bad, str(tmp_path / "ok.bin"))
+    # text form: the first of two bricks declares 7 nodes (the list length 15
+    # matches the counts, so only the per-element check can catch it)
+    from ufem_b200 import meshgen as mg
+    good = str(tmp_path / "two.fem")
+    mg.write_fem(mg.beam_brick(2, 1, 1, 2.0, 1.0, 1.0), good)
+    convert_input(good, str(tmp_path / "two.bin"))
+    body = open(good).read()
+    assert "1 9 0 0 8\n2 9 0 0 8\n16\n0 1 4 3 6 7 10 9\n" in body
+    body = body.replace("1 9 0 0 8\n2 9 0 0 8\n16\n0 1 4 3 6 7 10 9\n",
+                        "1 9 0 0 7\n2 9 0 0 8\n15\n0 1 4 3 6 7 10\n")
+    badtxt = str(tmp_path / "bad.fem")
+    open(badtxt, "w").write(body)
+    _rejected(badtxt, tmp_path)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", CASES)
 def test_binary_and_text_give_the_same_model(tmp_path, name):

@@ -1,22 +1,30 @@
 """The allocation-free Jacobi PCG (ufem_eqs_cgwj_noalloc).
 
-It is meant for callers that may not allocate device memory while they
-solve (an application whose allocator owns the device pool, a solve issued
-from another GPU library's callback, a loop that must not hit cudaMalloc's
-implicit synchronisation).  Its scratch lives in one array built into the
-library, so it takes the matrix and vectors already in device memory.
+It serves callers that cannot allocate device memory while they solve: an
+application whose own allocator already owns the device pool, a solve made
+from inside another GPU library's callback, or a loop that must not pay for
+cudaMalloc's implicit device synchronisation.  Its scratch lives in one array
+built into the library, so it takes a matrix and vectors that are already in
+device memory.
 
-The test solves the same supported beam system through the new entry point
-and through the existing ufem_eqs_cgwj (which uploads the reference's
-row-slot matrix itself), twice in a row, and compares the solutions within
-the 1e-8 relative tolerance of the other displacement tests.  It also checks
-that the second call changes no device memory reservation and that an
-oversized system is refused.  This file is collected last on purpose.
+The tests solve the reference's 20x5x5 beam (the committed golden fixture,
+solved by the reference's own femEqsCGwJ) through the new entry point in
+block form (B = 3) and in plain CSR form (B = 1), twice each, and check:
+the displacements within the 1e-8 relative tolerance of the other
+displacement tests against the reference's solution and against the
+existing ufem_eqs_cgwj; the two calls bitwise equal (the kernel's sums run
+in a fixed order, and the shared array keeps the previous call's contents,
+which the next call must not depend on); and that no call -- the first
+included, once the library's solver kernels have run through another entry
+point -- changes the device memory reservation.  An oversized system is
+refused.  This file is collected last on purpose.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
+
+from golden_util import load, model_from
 
 pytestmark = pytest.mark.gpu
 
@@ -24,10 +32,9 @@ U_TOL = 1e-8
 
 
 def _system():
-    from ufem_b200 import meshgen as mg
     from ufem_b200.api import GpuModel
-    m = mg.beam_brick(20, 5, 5, 8.0, 2.0, 2.0)
-    g = GpuModel(m)
+    z = load("beam_20x5x5")
+    g = GpuModel(model_from(z))
     g.fill_K(0)
     g.add_loads()
     g.add_disps()
@@ -35,65 +42,76 @@ def _system():
     rp, ci = g.bsr_pattern()
     vals = g.K_values()
     F = g.F()
-    return g, b, nbr, rp, ci, vals, F
+    return z, g, b, nbr, rp, ci, vals, F
 
 
-def _to_rowslot(b, nbr, rp, ci, vals):
-    """The same matrix in the reference's row-slot layout (1-based columns)."""
+def _to_csr(b, nbr, rp, ci, vals):
+    """The same matrix as plain CSR (B = 1), block columns expanded in order."""
     n = nbr * b
-    frompos, defpos, pos, data = [], [], [], []
-    off = 0
+    rowptr = np.zeros(n + 1, np.int64)
+    cols, data = [], []
     for I in range(nbr):
         for a in range(b):
-            cols = []
             for k in range(rp[I], rp[I + 1]):
                 for c in range(b):
-                    cols.append((ci[k] * b + c + 1, vals[k, a, c]))
-            frompos.append(off)
-            defpos.append(len(cols))
-            for col, v in cols:
-                pos.append(col)
-                data.append(v)
-            off += len(cols)
-    return (np.array(frompos, np.int64), np.array(defpos, np.int64), np.array(pos, np.int64),
-            np.array(data, np.float64))
+                    cols.append(ci[k] * b + c)
+                    data.append(vals[k, a, c])
+            rowptr[I * b + a + 1] = len(cols)
+    return rowptr, np.array(cols, np.int64), np.array(data, np.float64)
 
 
-def test_noalloc_matches_existing_entry_point_twice():
+def _to_rowslot(rowptr, cols, data):
+    """CSR -> the reference's row-slot layout (1-based columns)."""
+    n = len(rowptr) - 1
+    return (rowptr[:-1].copy(), np.diff(rowptr), cols + 1, data.copy())
+
+
+def test_noalloc_matches_the_reference_and_the_existing_entry_point():
     import torch
     from ufem_b200 import _lib, api
     L = _lib.load()
-    g, b, nbr, rp, ci, vals, F = _system()
+    z, g, b, nbr, rp, ci, vals, F = _system()
+    n = len(F)
+    u_ref = z["u"]
     dev = torch.device("cuda", 0)
-    d_rp = torch.from_numpy(rp.astype(np.int32)).to(dev)
-    d_ci = torch.from_numpy(ci.astype(np.int32)).to(dev)
-    d_val = torch.from_numpy(np.ascontiguousarray(vals.reshape(-1))).to(dev)
+    csr_rp, csr_ci, csr_val = _to_csr(b, nbr, rp, ci, vals)
+    forms = {
+        3: (torch.from_numpy(rp.astype(np.int32)).to(dev), torch.from_numpy(ci.astype(np.int32)).to(dev),
+            torch.from_numpy(np.ascontiguousarray(vals.reshape(-1))).to(dev), nbr),
+        1: (torch.from_numpy(csr_rp.astype(np.int32)).to(dev), torch.from_numpy(csr_ci.astype(np.int32)).to(dev),
+            torch.from_numpy(csr_val).to(dev), n),
+    }
     d_b = torch.from_numpy(F).to(dev)
-    # the existing entry point on the reference's own matrix layout
-    fp, dp, pos, data = _to_rowslot(b, nbr, rp, ci, vals)
-    rv, x_ref = api.eqs("cgwj", fp, dp, pos, data, F, np.zeros(len(F)))
+    d_x = torch.zeros(n, dtype=torch.float64, device=dev)
+    # the existing entry points first: ufem_eqs_cgwj (plain CSR kernels, on the
+    # reference's own row-slot layout) and the model's solve (block kernels)
+    rv, x_cgwj = api.eqs("cgwj", *_to_rowslot(csr_rp, csr_ci, csr_val), F, np.zeros(n))
     assert rv == 0
-    sols = []
-    free_after = []
-    for call in range(2):
-        d_x = torch.zeros(len(F), dtype=torch.float64, device=dev)
-        torch.cuda.synchronize()
-        it = C.c_long()
-        rv = L.ufem_eqs_cgwj_noalloc(b, nbr, d_rp.data_ptr(), d_ci.data_ptr(), d_val.data_ptr(), d_b.data_ptr(),
-                                     d_x.data_ptr(), api.EPS_REF, len(F), C.byref(it))
-        torch.cuda.synchronize()
-        free_after.append(torch.cuda.mem_get_info(0)[0])
-        assert rv == 0, L.ufem_last_error()
-        assert it.value > 0
-        x = d_x.cpu().numpy()
-        err = np.abs(x - x_ref).max() / np.abs(x_ref).max()
-        assert err <= U_TOL, (call, err)
-        sols.append(x)
-    # the shared scratch keeps the previous call's contents; the second call
-    # must not depend on them
-    assert np.abs(sols[0] - sols[1]).max() <= U_TOL * np.abs(sols[0]).max()
-    # nothing was reserved on the device by the second call
-    assert free_after[0] == free_after[1]
+    assert np.abs(x_cgwj - u_ref).max() <= U_TOL * np.abs(u_ref).max()
+    g.set_u(np.zeros(n))
+    g.solve(api.SOLVER_CGWJ, api.STOP_REFERENCE, api.EPS_REF, 0)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for B in (3, 1):
+        d_rp, d_ci, d_val, nrows = forms[B]
+        sols = []
+        for call in range(2):
+            d_x.fill_(0.0)
+            torch.cuda.synchronize()
+            it = C.c_long()
+            rv = L.ufem_eqs_cgwj_noalloc(B, nrows, d_rp.data_ptr(), d_ci.data_ptr(), d_val.data_ptr(),
+                                         d_b.data_ptr(), d_x.data_ptr(), api.EPS_REF, n, C.byref(it))
+            torch.cuda.synchronize()
+            assert rv == 0, L.ufem_last_error()
+            assert it.value > 0
+            # nothing reserved on the device, by the first call either
+            assert torch.cuda.mem_get_info(0)[0] == free0, (B, call)
+            x = d_x.cpu().numpy()
+            scale = np.abs(u_ref).max()
+            assert np.abs(x - u_ref).max() <= U_TOL * scale, (B, call, np.abs(x - u_ref).max() / scale)
+            assert np.abs(x - x_cgwj).max() <= U_TOL * scale, (B, call)
+            sols.append(x)
+        assert np.array_equal(sols[0], sols[1]), B
 
 
 def test_noalloc_refuses_oversized_systems():

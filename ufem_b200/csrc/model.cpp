@@ -20,6 +20,7 @@
 #include <fstream>
 #include <mutex>
 #include <sstream>
+#include <system_error>
 #include <thread>
 
 #include "ufem_internal.h"
@@ -80,6 +81,12 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
   m->b = elem_dofs(t0);
   m->enodes.resize((size_t)m->eLen * m->nn);
   for (long e = 0; e < m->eLen; e++) {
+    // the caller's tables carry no length of eNodesL: every element but the
+    // last is checked against the next element's start
+    if (t->eFrom[e] < 0 || (e + 1 < m->eLen && t->eFrom[e + 1] - t->eFrom[e] != m->nn)) {
+      set_error("element node count does not match its type");
+      return UFEM_AF_ERR_SIZ;
+    }
     for (int j = 0; j < m->nn; j++) {
       long np = t->eNodesL[t->eFrom[e] + j];
       if (np < 0 || np >= m->nLen) {
@@ -97,6 +104,10 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
   for (long p = 0; p < t->mpLen; p++) {
     long from = t->mpFrom[p];
     long to = (p + 1 < t->mpLen) ? t->mpFrom[p + 1] : t->mpLenL;
+    if (from < 0 || to < from || to > t->mpLenL) {
+      set_error("material value ranges out of order or out of range");
+      return UFEM_AF_ERR_SIZ;
+    }
     m->mpVals[p].assign(t->mpValL + from, t->mpValL + to);
   }
   m->eE.resize(m->eLen);
@@ -126,6 +137,10 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
     if (t->rsLen > 0 && r >= 0 && r < t->rsLen) {
       long from = t->rsFrom[r];
       long to = (r + 1 < t->rsLen) ? t->rsFrom[r + 1] : t->rsLenL;
+      if (from < 0 || to > t->rsLenL) {
+        set_error("real set value ranges out of range");
+        return UFEM_AF_ERR_SIZ;
+      }
       if (to > from) {
         if (quad) thick = t->rsValL[from];       // RS_HEIGHT first, fem/fem_e002.c:1019
         else winkler = t->rsValL[from];          // RS_WINKLER, fem/fem_e010.c:79
@@ -183,9 +198,19 @@ void parallel_ranges(long n, F f) {
   }
   std::vector<std::thread> th;
   const long per = (n + nt - 1) / nt;
-  for (long t = 0; t < nt; t++) {
+  long t = 0;
+  for (; t < nt; t++) {
     const long a = t * per, b = std::min(n, a + per);
-    if (a < b) th.emplace_back(f, a, b);
+    if (a >= b) continue;
+    try {
+      th.emplace_back(f, a, b);
+    } catch (const std::system_error &) {
+      break;  // no thread could start (thread or process limit): this thread does the rest
+    }
+  }
+  for (; t < nt; t++) {
+    const long a = t * per, b = std::min(n, a + per);
+    if (a < b) f(a, b);
   }
   for (auto &x : th) x.join();
 }
@@ -740,6 +765,40 @@ int write_binary(InputTables &in, const char *fname) {
   return UFEM_AF_OK;
 }
 
+// Shape checks shared by both readers, before any table is indexed: every
+// quad (4 nodes) and brick (8 nodes) element holds exactly its node count in
+// the element-node list (a truncated list or a miscounted element would make
+// model_from_tables read past it), and the real-set and material value
+// ranges start in order inside their value lists.
+int check_tables(const InputTables &in) {
+  const long eLen = (long)in.eFrom.size(), eLenL = (long)in.eNodes.size();
+  for (long e = 0; e < eLen; e++) {
+    const long from = in.eFrom[e], to = e + 1 < eLen ? in.eFrom[e + 1] : eLenL;
+    if (from < 0 || to < from || to > eLenL) {
+      set_error("element node list out of order or out of range");
+      return UFEM_AF_ERR_SIZ;
+    }
+    const long te = in.eType[e];
+    if ((te == 2 || te == 9 || te == 10) && to - from != elem_nodes(te)) {
+      set_error("element " + std::to_string(e) + " of type " + std::to_string(te) + " has " +
+                std::to_string(to - from) + " nodes, not " + std::to_string(elem_nodes(te)));
+      return UFEM_AF_ERR_SIZ;
+    }
+  }
+  auto ranges_ok = [](const std::vector<long> &from, size_t nvals) {
+    for (size_t i = 0; i < from.size(); i++) {
+      const long next = i + 1 < from.size() ? from[i + 1] : (long)nvals;
+      if (from[i] < 0 || next < from[i] || next > (long)nvals) return false;
+    }
+    return true;
+  };
+  if (!ranges_ok(in.rsFrom, in.rsVal.size()) || !ranges_ok(in.mpFrom, in.mpVal.size())) {
+    set_error("real set or material value ranges out of order or out of range");
+    return UFEM_AF_ERR_SIZ;
+  }
+  return UFEM_AF_OK;
+}
+
 int read_file(const char *fname, std::string &buf) {
   std::ifstream f(fname, std::ios::binary);
   if (!f) {
@@ -761,6 +820,7 @@ int read_input_file(const char *fname, ufem_model **out) {
   InputTables in;
   rv = is_binary(buf) ? parse_binary(buf, in) : parse_text(buf, in);
   if (rv != UFEM_AF_OK) return rv;
+  if ((rv = check_tables(in)) != UFEM_AF_OK) return rv;
   ufem_model *m = new ufem_model();
   m->mc_ilen = in.mc_ilen;
   m->mc_olen = in.mc_olen;
@@ -798,6 +858,7 @@ int convert_input_file(const char *text_fname, const char *bin_fname) {
   if (rv != UFEM_AF_OK) return rv;
   InputTables in;
   if ((rv = is_binary(buf) ? parse_binary(buf, in) : parse_text(buf, in)) != UFEM_AF_OK) return rv;
+  if ((rv = check_tables(in)) != UFEM_AF_OK) return rv;
   return write_binary(in, bin_fname);
 }
 

@@ -410,7 +410,7 @@ int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double ep
   if ((rv = res.alloc(1)) != UFEM_AF_OK) return rv;
   UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
   UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
-  CgArgs a;
+  CgArgs a{};
   a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
   a.M = M.p; a.r = r.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
   a.bar = bar.p; a.res = res.p; a.eps = eps; a.normA = normA; a.normB = normB;
@@ -859,7 +859,7 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
     UFEM_CUDA_TRY(cudaMemsetAsync(p1.p, 0, n * sizeof(float)));
     UFEM_CUDA_TRY(cudaMemsetAsync(bar.p, 0, sizeof(GridBar)));
     UFEM_CUDA_TRY(cudaMemsetAsync(res.p, 0, sizeof(CgResult)));
-    CgArgsT<float> a;
+    CgArgsT<float> a{};
     a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = V32.p; a.b = r32.p;
     a.x = d32.p;
     a.M = M32.p; a.r = ri.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
@@ -906,12 +906,16 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
 // the right-hand side and the solution in device memory.
 //
 // Limits: at most kNoallocMaxRows scalar rows (131,072) and kNoallocMaxGrid
-// blocks; the array takes about 6.3 MB on every GPU that loads the library,
-// until the process exits.  All calls share the one array, so calls that
-// overlap on the GPU (two host threads, or two streams) race; serialise
-// them.  The first call on a device looks the array's device address up
-// (once per device, with that device current) and should come before any
-// stream capture.
+// blocks; the array takes about 6.3 MB on every GPU where the library's
+// solver code is loaded (the first use of any of its solvers on a device
+// loads it, this entry point's first call included), until the process
+// exits.  All calls share the one array, so two solves whose kernels
+// overlapped on the GPU would race on it; this function prevents that in one
+// process: a lock serialises calls, and each call returns only once its
+// kernels have finished.  It runs on the legacy default stream with
+// synchronous copies, so it cannot be called during a stream capture.  The
+// first call on a device looks the array's device address up (once per
+// device, with that device current).
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1013,8 +1017,8 @@ int cg_jacobi_fp64_noalloc(const DevMatrix &A, const double *d_b, double *d_x, d
   }
   int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
   G = std::max(1, std::min(G, kNoallocMaxGrid));
-  CgArgs a;
-  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
+  CgArgs a{};
+  a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.x = d_x;
   a.M = M; a.r = r; a.z = z; a.p0 = p0; a.p1 = p1; a.q = q; a.part = part;
   a.bar = &hdr->bar; a.res = &hdr->res; a.eps = eps; a.normA = normA; a.normB = normB;
   a.maxIt = maxIt; a.stop_rule = UFEM_STOP_REFERENCE;
