@@ -13,6 +13,7 @@ needed):
 
     python tests/golden/make_golden.py             # every fixture
     python tests/golden/make_golden.py mc_outputs  # the Monte Carlo output fixtures only
+    python tests/golden/make_golden.py beam_80x20x20  # config 2's displacements only
 
 The fixtures are committed; tests only read them.
 """
@@ -32,6 +33,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
 from ufem_b200 import meshgen as mg  # noqa: E402
+
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+from golden_util import model_sha  # noqa: E402
 
 REF_DIR = os.path.join(ROOT, "oracle", "_ref", "serial")
 
@@ -233,10 +237,29 @@ def mc_outputs_cases():
     save_mc_outputs_case("mc_out_plate_iso_4x2", mg.plate_quad(4, 2, 1.0, 0.5), 3)
 
 
+def beam_80x20x20_case():
+    """Config 2, the 80x20x20 brick cantilever (107,163 DOFs): the reference's
+    displacements from its own femEqsCGwJ with its stopping rule (about a
+    minute on one core).  Only u, the DOF map's hash and the model's hash are
+    kept (the tables are regenerated by ``mg.beam_brick(80, 20, 20, 8.0, 2.0,
+    2.0)``); u is stored with its last 12 mantissa bits cleared (relative
+    rounding below 2.3e-13), which keeps the file small."""
+    model = mg.beam_brick(80, 20, 20, 8.0, 2.0, 2.0)
+    res = run_harness(model, "cgwj", want_ke=False)
+    u = np.ascontiguousarray(res["u"], np.float64)
+    uq = (u.view(np.uint64) & ~np.uint64(0xFFF)).view(np.float64)
+    np.savez_compressed(os.path.join(HERE, "beam_80x20x20.npz"), u=uq, model_sha=model_sha(model),
+                        ndoffld_sha=sha(res["ndoffld"].astype(np.int64)), rv_solve=res["meta"]["rv_solve"],
+                        t_solve=res["meta"]["t_solve"])
+
+
 def main():
     build_ref()
     if sys.argv[1:] == ["mc_outputs"]:
         mc_outputs_cases()
+        return
+    if sys.argv[1:] == ["beam_80x20x20"]:
+        beam_80x20x20_case()
         return
     # config 1: the 64x16 cantilever plate (plane stress), 2,210 DOFs
     save_case("plate_64x16", mg.plate_quad(), full=False, ke_elems=[0, 1, 15, 16, 500, 1023])
@@ -259,6 +282,7 @@ def main():
     # the Monte Carlo plugin ABI: per-element E and a random end load
     save_mc_case("mc_beam_4x2x2", mg.beam_brick(4, 2, 2, 2.0, 1.0, 1.0, per_element_material=True), 4)
     mc_outputs_cases()
+    beam_80x20x20_case()
 
 
 if __name__ == "__main__":

@@ -1,4 +1,5 @@
 """Load the committed golden fixtures (tests/golden/*.npz) back into models."""
+import hashlib
 import os
 
 import numpy as np
@@ -30,3 +31,19 @@ def model_from(z) -> mg.Model:
         m.mc_ilen = int(z["mc_ilen"])
         m.mc_olen = int(z["mc_olen"])
     return m
+
+
+def model_sha(model: mg.Model) -> str:
+    """One hash over every model table: a fixture that stores only results
+    regenerates its model with the mesh generator and checks it with this."""
+    rs_frm, rs_cnt, rs_vals = model.rs_flat()
+    mp_frm, mp_cnt, mp_vals = model.mp_flat()
+    tables = dict(m_xyz=model.n_xyz, m_etype=model.e_type, m_ers=model.e_rs, m_emp=model.e_mp,
+                  m_enodes=model.e_nodes, m_rstype=model.rs_type, m_rscnt=rs_cnt, m_rsvals=rs_vals,
+                  m_mptype=model.mp_type, m_mpcnt=mp_cnt, m_mpvals=mp_vals, m_nlnode=model.nl_node,
+                  m_nltype=model.nl_type, m_nldir=model.nl_dir, m_nlval=model.nl_val)
+    h = hashlib.sha256()
+    for k, v in sorted(tables.items()):
+        h.update(k.encode())
+        h.update(np.ascontiguousarray(v).tobytes())
+    return h.hexdigest()
