@@ -10,7 +10,13 @@ the preconditioner); 256 fresh samples are solved by
   B. the MLP guess + FP32 PCG with FP64 solution and true-residual
      replacement (precision 1),
 
-each with the stopping rule tightened to a true relative residual of 1e-12.
+  C. the MLP guess + FP32 implicit batched PCG (FP32 work vectors, blocks
+     formed in the kernel in FP64, FP64 solution and true-residual
+     replacement) with the coarse correction (precision 3),
+
+each with the stopping rule tightened to a true relative residual of 1e-10
+(the FP64 floor of |f - K u| / |f| on this beam is about 1e-11:
+|K| |u| / |f| is 1.9e6).
 Eight samples spread over the 128-sample groups are solved by the oracle
 (oracle/ufem_oracle.c: the reference's assembly and femEqsCGwJ with its own
 stopping rule, fem/fem_eqs.c:88-247).  Checked against it:
@@ -32,7 +38,7 @@ from golden_util import load, model_sha
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-8          # the north_star's displacement and stress bar
-SOLVE_TOL = 1e-12   # true relative residual of the GPU solves checked here
+SOLVE_TOL = 1e-10   # true relative residual of the GPU solves checked here
 PICK = (0, 37, 101, 128, 170, 200, 233, 255)
 
 
@@ -176,9 +182,21 @@ def test_mlp_fp32_fp64_within_1e8_of_oracle(warm40):
     _check_outputs(m, ev, of, oracle, "MLP + FP32/FP64, ufem_warm_solve")
 
 
+def test_mlp_fp32_implicit_coarse_within_1e8_of_oracle(warm40):
+    m, g, ws, st, ev, oracle = warm40
+    ws.set_guess_mode(0)
+    u0 = ws.guess(ev)
+    u, status, iters = _solve_from(g, ev, u0, precision=3, tol=SOLVE_TOL)
+    of, st_w, it_w, wst = ws.solve(ev, precision=3, tol=SOLVE_TOL)
+    assert (status == 0).all()
+    assert np.isin(st_w, [0, 4]).all()
+    _check_against_oracle(m, ev, u, oracle, "MLP + FP32 implicit + coarse")
+    _check_outputs(m, ev, of, oracle, "MLP + FP32 implicit + coarse, ufem_warm_solve")
+
+
 def test_beam_80x20x20_within_1e8_of_reference():
     """Config 2 (107,163 DOFs): the FP64 PCG with the reference's stopping
-    rule, and the FP64 PCG to a true relative residual of 1e-12, against the
+    rule, and the FP64 PCG to a relative residual of 1e-10, against the
     reference's own displacements (tests/golden/beam_80x20x20.npz, made by
     make_golden.py with the reference's femEqsCGwJ)."""
     import hashlib

@@ -43,6 +43,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <sys/stat.h>
 #include <memory>
 #include <vector>
@@ -394,6 +395,17 @@ __device__ __forceinline__ void ld64(const double *p, double (&o)[VN]) {
     o[2 * h + 1] = v.y;
   }
 }
+// the same through the non-coherent path, for data no block writes during
+// the kernel (the per-sample multipliers of the implicit form)
+template <typename T, int VN>
+__device__ __forceinline__ void ld64_ro(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2)));
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
 template <typename T, int VN>
 __device__ __forceinline__ void ld64_stream(const double *p, double (&o)[VN]) {
 #pragma unroll
@@ -552,6 +564,12 @@ __global__ void k_make_mult(int nmult, int S, int nsamp, long ilen, const double
   mult[t] = (j == 0 || s >= nsamp) ? 1.0 : ifld[(size_t)s * ilen + mult_col[j]];
 }
 
+// FP32 copy of the Jacobi diagonal (the FP32 implicit form)
+__global__ void k_diag_f32(long n, const double *__restrict__ M, float *__restrict__ M32) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) M32[i] = (float)M[i];
+}
+
 // Jacobi diagonal of the implicit K_s (supported rows: 1)
 template <int B>
 __global__ void k_diag_implicit(int nbr, int S, const int *__restrict__ diagblk, const int *__restrict__ cptr,
@@ -652,29 +670,32 @@ struct BArgs {
 // broadcast; the gathers of U contributions are issued together so that U
 // neighbour loads are in flight per warp.  W and the multipliers are
 // read-only for the whole kernel (non-coherent loads); X is written by
-// other blocks during the kernel (L2 loads).
-template <int B, int VN, int U>
+// other blocks during the kernel (L2 loads).  LT is the kernel's lane
+// layout (double: sample pairs 64 apart; float: 4 adjacent samples), XT the
+// type of X (the FP32 kernel gathers FP32 z, and FP64 x for its true
+// residuals); W, the multipliers and the sums are FP64 either way.
+template <typename LT, typename XT, int B, int VN, int U>
 __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, int cstride,
-                                             const double *__restrict__ mult, const double *X, int S, int sb,
+                                             const double *__restrict__ mult, const XT *X, int S, int sb,
                                              int c0, int c1, double (&acc)[B][VN]) {
+  static_assert(sizeof(XT) == 8 || sizeof(LT) == 4, "FP32 vectors only in the FP32 lane layout");
   const int lane = threadIdx.x & 31;
   for (int cb = c0; cb < c1; cb += 32) {
     const long long mykey = (cb + lane < c1) ? (long long)__ldg(cval + (size_t)(cb + lane) * cstride + B * B) : 0;
     const int cnt = min(32, c1 - cb);
     for (int j = 0; j < cnt; j += U) {
-      double xv[U][B][VN], av[U][VN];
+      XT xv[U][B][VN];
+      double av[U][VN];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const long long key = __shfl_sync(0xffffffffu, mykey, min(j + u, cnt - 1));
         const int J = (int)(key & 0xffffffffLL), var = (int)(key >> 32);
 #pragma unroll
-        for (int b = 0; b < B; b++) ld64<double, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
-#pragma unroll
-        for (int h = 0; h < VN / 2; h++) {
-          const double2 v = __ldg(reinterpret_cast<const double2 *>(mult + (size_t)var * S + sb + h * 64));
-          av[u][2 * h] = v.x;
-          av[u][2 * h + 1] = v.y;
+        for (int b = 0; b < B; b++) {
+          if constexpr (sizeof(XT) == 8) ld64<LT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
+          else ldn<XT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
         }
+        ld64_ro<LT, VN>(mult + (size_t)var * S + sb, av[u]);
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {
@@ -694,7 +715,7 @@ __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, in
           for (int v = 0; v < VN; v++) {
             double t = 0.0;
 #pragma unroll
-            for (int b = 0; b < B; b++) t = fma(W[a * B + b], xv[u][b][v], t);
+            for (int b = 0; b < B; b++) t = fma(W[a * B + b], (double)xv[u][b][v], t);
             acc[a][v] = fma(av[u][v], t, acc[a][v]);
           }
       }
@@ -737,7 +758,9 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 template <typename T, int B, bool IMP, int UN, int VN, int NW>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VN]) {
-  static_assert(!IMP || sizeof(T) == 8, "the implicit form runs in FP64");
+  // the implicit form sums every row in FP64 (its unit blocks and
+  // multipliers are FP64) whatever the vector precision T
+  using AT = typename std::conditional<IMP, double, T>::type;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -750,13 +773,14 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
 #pragma unroll
   for (int v = 0; v < VN; v++) pq[v] = 0;
   for (int I = row0 + warp; I < row1; I += NW) {
-    T acc[B][VN];
+    AT acc[B][VN];
 #pragma unroll
     for (int a = 0; a < B; a++)
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     if constexpr (IMP) {
-      implicit_row<B, VN, UN>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+      implicit_row<T, T, B, VN, UN>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1),
+                                    acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -809,17 +833,20 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           T qo[VN];
           ldn<T, VN>(M.q + o, qo);
 #pragma unroll
-          for (int v = 0; v < VN; v++) acc[a][v] = fma(beta[v], qo[v], acc[a][v]);
+          for (int v = 0; v < VN; v++) acc[a][v] = fma((double)beta[v], (double)qo[v], acc[a][v]);
         }
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
 #pragma unroll
           for (int v = 0; v < VN; v++) acc[a][v] = pi[v];
         }
       }
-      stn<T, VN>(pnew + o, pi);
-      stn<T, VN>(M.q + o, acc[a]);
+      T qv[VN];
 #pragma unroll
-      for (int v = 0; v < VN; v++) pq[v] += (double)pi[v] * (double)acc[a][v];
+      for (int v = 0; v < VN; v++) qv[v] = (T)acc[a][v];
+      stn<T, VN>(pnew + o, pi);
+      stn<T, VN>(M.q + o, qv);
+#pragma unroll
+      for (int v = 0; v < VN; v++) pq[v] += (double)pi[v] * (double)qv[v];
     }
   }
 #pragma unroll
@@ -924,7 +951,8 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
     if constexpr (IMP) {
-      implicit_row<B, VN, UN>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+      implicit_row<T, double, B, VN, UN>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I),
+                                         __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -1027,7 +1055,8 @@ __device__ __forceinline__ void coarse_fail(GridBar *bar) { atomicExch(&bar->err
 
 // c = Wc^T r over row range `range` of group g (GS = 128 samples), by the
 // kCoarseThreads threads of the block.
-__device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range, int par, uint32_t &phase,
+template <typename T>
+__device__ __noinline__ void coarse_c1(const BMesh<T> &M, int g, int range, int par, uint32_t &phase,
                                        GridBar *gb) {
   constexpr int kQ = kCoarseThreads / 128;  // threads per sample
   static_assert(8 % kQ == 0, "the 8 row groups of a chunk split evenly over the threads of a sample");
@@ -1043,19 +1072,19 @@ __device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range,
   const uint32_t idesc = tc::idesc_bf16(128, nmod);
   const int stage_b = nmod * 64 * 2;
   const int m = tid & 127, q = tid >> 7;  // sample of the group staged by this thread, and its share
-  const double *rcol = M.r + (size_t)g * 128 + m;
+  const T *rcol = M.r + (size_t)g * 128 + m;
   // this thread stages row groups kg = q + kQ j (8 rows each) of sample m
-  auto load_chunk = [&](int ch, double (&v)[8 / kQ][8]) {
+  auto load_chunk = [&](int ch, T (&v)[8 / kQ][8]) {
     const int rb = r0 + ch * 64;
 #pragma unroll
     for (int j = 0; j < 8 / kQ; j++)
 #pragma unroll
       for (int e = 0; e < 8; e++) {
         const int row = rb + (q + kQ * j) * 8 + e;
-        v[j][e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : 0.0;
+        v[j][e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : T(0);
       }
   };
-  double cur[8 / kQ][8], nxt[8 / kQ][8];
+  T cur[8 / kQ][8], nxt[8 / kQ][8];
   load_chunk(0, cur);
   bool ok = true;
   for (int ch = 0; ch < nch; ch++) {
@@ -1156,7 +1185,8 @@ __device__ __noinline__ void coarse_c1(const BMesh<double> &M, int g, int range,
 }
 
 // z += Wc c on the 128-row chunk `chunk` of group g.
-__device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk, uint32_t &phase, GridBar *gb) {
+template <typename T>
+__device__ __noinline__ void coarse_c3(const BMesh<T> &M, int g, int chunk, uint32_t &phase, GridBar *gb) {
   constexpr int kRows = 128 / (kCoarseThreads / 128);  // rows of the chunk per thread
   const uint32_t tmem = s_coarse_tmem;
   uint64_t *bar = &s_coarse_mbar;
@@ -1185,13 +1215,13 @@ __device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk,
   // lanes = samples, columns = rows of the chunk: warp w reads TMEM lanes
   // 32 (w % 4) .. +31 and rows kRows (w / 4) .. +kRows-1
   const int ms = (warp & 3) * 32 + lane, j0 = (warp >> 2) * kRows;
-  double *zc = M.z + (size_t)g * 128 + ms;
+  T *zc = M.z + (size_t)g * 128 + ms;
   const int rbase = chunk * 128 + j0;
   const int nrow = min(kRows, M.n - rbase);  // rows of this thread's share in the mesh
   // all z loads of this thread are in flight during the MMAs
-  double zv[kRows];
+  T zv[kRows];
 #pragma unroll
-  for (int e = 0; e < kRows; e++) zv[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : 0.0;
+  for (int e = 0; e < kRows; e++) zv[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : T(0);
   const bool ok = tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
   tc::fence_after_sync();
@@ -1202,7 +1232,7 @@ __device__ __noinline__ void coarse_c3(const BMesh<double> &M, int g, int chunk,
     tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j0 + e0), v);
 #pragma unroll
     for (int e = 0; e < 8; e++)
-      if (e0 + e < nrow) zc[(size_t)(rbase + e0 + e) * S] = zv[e0 + e] + (double)__uint_as_float(v[e]);
+      if (e0 + e < nrow) zc[(size_t)(rbase + e0 + e) * S] = (T)((double)zv[e0 + e] + (double)__uint_as_float(v[e]));
   }
   tc::fence_before_sync();
   __syncthreads();  // the next item restages the operand tiles and reuses the accumulator
@@ -1234,7 +1264,7 @@ constexpr int kMaxMeshes = 8;
 #ifndef UFEM_PCG_MIN_BLOCKS
 #define UFEM_PCG_MIN_BLOCKS 2
 #endif
-// The coarse phases (precision 2 with 128-sample groups): C1 then C3 over the
+// The coarse phases (precisions 2 and 3, 128-sample groups): C1 then C3 over the
 // groups whose z has to be formed from r; two grid barriers.  The parity of
 // the MMA barrier is kept in shared memory between calls.
 template <typename T>
@@ -1242,7 +1272,7 @@ __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_m
   __shared__ int s_go;
   const int G = gridDim.x;
   uint32_t phase = s_coarse_phase;
-  if constexpr (sizeof(T) == 8) {
+  {
     for (int t = blockIdx.x; t < A.nc1; t += G) {
       const int4 it = A.c1items[t];
       const BMesh<T> &M = s_meshes[it.x];
@@ -1673,8 +1703,10 @@ static void tune_save(const std::string &path) {
 
 // the batch shape a tuned choice is valid for: device, precision, element
 // family, and per mesh its block rows and padded sample count
+static bool implicit_form(int precision) { return precision == 2 || precision == 3; }
+
 static int coarse_modes(int nmesh, ufem_model *const *models, const ufem_mc_options &opt) {
-  if (opt.precision != 2 || !opt.coarse) return 0;
+  if (!implicit_form(opt.precision) || !opt.coarse) return 0;
   int cm = 0;
   for (int i = 0; i < nmesh; i++) cm = std::max(cm, get_plan(models[i])->cmodes);
   return cm;
@@ -2112,7 +2144,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       ufem_model *m = models[k];
       McPlan *P = get_plan(m);
       if (!P->built && (rv = build_plan(m, P)) != UFEM_AF_OK) return rv;
-      const bool imp = (opt.precision == 2);
+      const bool imp = implicit_form(opt.precision);
       if (imp && !P->imp_built && (rv = build_implicit(m, P)) != UFEM_AF_OK) return rv;
       plans[k] = P;
       W[k] = get_work(m);
@@ -2135,6 +2167,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       }
       if (opt.precision == 1) {
         if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n))) return rv;
+      } else if (opt.precision == 3) {
+        if ((rv = w.M32.ensure(n))) return rv;
       }
       const long ne = (long)m->eLen * w.S;
       k_make_E<<<(unsigned)((ne + 255) / 256), 256>>>((int)m->eLen, w.S, w.nsamp, P->ilen, d_ifld[k],
@@ -2157,6 +2191,10 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
                                                                     P->cval.p, P->cstride, w.mult.p,
                                                                     m->d_fixed.p, w.M64.p);
         g_stats.kernel_launches += 1;  // two kernels here in place of the assembly
+        if (opt.precision == 3) {
+          k_diag_f32<<<(unsigned)((n + 255) / 256), 256>>>((long)n, w.M64.p, w.M32.p);
+          g_stats.kernel_launches += 1;
+        }
       } else {
         dim3 ga((unsigned)m->nnzb, (unsigned)(w.S / 128));
         float *v32 = opt.precision == 1 ? w.V32.p : nullptr;
@@ -2187,7 +2225,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
     g_stats.ms_assemble = t.stop();
   }
   // ---- launch shape: the caller's, else the autotuned one for this batch --
-  if (opt.tiles_per_block <= 0 || (opt.precision == 2 && (opt.unroll <= 0 || opt.lane_samples <= 0))) {
+  if (opt.tiles_per_block <= 0 || (implicit_form(opt.precision) && (opt.unroll <= 0 || opt.lane_samples <= 0))) {
     const TuneEntry *t = tune_find(tune_key(nmesh, models, nsamp, opt.precision, coarse_modes(nmesh, models, opt)));
     if (t) {
       if (opt.tiles_per_block <= 0) opt.tiles_per_block = t->tpb;
@@ -2198,6 +2236,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   // ---- one persistent launch over every mesh -----------------------------
   long its = 0;
   if (opt.precision == 1) rv = run_pcg<float, false, 4>(nmesh, models, W, plans, opt, &its);
+  // FP32 implicit form: 4 adjacent samples per lane (one 16-byte load per row)
+  else if (opt.precision == 3) rv = run_pcg<float, true, 4>(nmesh, models, W, plans, opt, &its);
   // implicit form: 4 samples per lane unless 2 is asked for (measured best on B200)
   else if (opt.precision == 2 && (opt.lane_samples != 2 || coarse_modes(nmesh, models, opt) > 0))
     rv = run_pcg<double, true, 4>(nmesh, models, W, plans, opt, &its);
@@ -2281,10 +2321,11 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
   }
   const int tpbs[] = {3, 6, 12, 24, 48};
   std::vector<int> unrolls, lanes;
-  if (base.precision == 2) {
+  if (implicit_form(base.precision)) {
     unrolls = {2, 4, 8};
     lanes = {2, 4};
-    if (coarse_modes(nmesh, models, base) > 0) lanes = {4};  // the coarse correction needs 128-sample groups
+    // the coarse correction needs 128-sample groups; the FP32 form holds 4 samples per lane
+    if (coarse_modes(nmesh, models, base) > 0 || base.precision == 3) lanes = {4};
   } else {
     unrolls = {4};
     lanes = {0};
