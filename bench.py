@@ -99,6 +99,8 @@ def parse():
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
     p.add_argument("--profile-case", action="store_true",
                    help="one small bounded batch (60x15x15, 128 samples, 40 PCG iterations) for ncu captures")
+    p.add_argument("--profile-samples", type=int, default=1024,
+                   help="samples of the --profile-case batch (precisions 2 and 3: the 40x10x10 zone beam)")
     p.add_argument("--profile-static", action="store_true",
                    help="the 128x128x64 block's FP64 PCG capped at 40 iterations (two launches) for ncu captures")
     p.add_argument("--profile-ingest", action="store_true",
@@ -124,9 +126,9 @@ def profile_case(a):
     from ufem_b200.api import GpuModel
     from ufem_b200.mc import mc_solve
     from ufem_b200 import meshgen as mg
-    if a.precision == 2:
+    if a.precision in (2, 3):
         m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
-        f = mg.warm_samples(m, 1024)
+        f = mg.warm_samples(m, a.profile_samples)
         if not a.no_coarse:
             # the coarse space from a short warm-start training (sets it on the model)
             from ufem_b200.warm import WarmStart
@@ -139,7 +141,7 @@ def profile_case(a):
         m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
         mg.mc_attach_vars(m)
         f = mg.mc_samples(m, mesh_id=2, nsamp=128)
-    if a.precision != 2 or a.no_coarse:
+    if a.precision not in (2, 3) or a.no_coarse:
         g = GpuModel(m)
     for _ in range(2):
         res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block,
@@ -147,7 +149,8 @@ def profile_case(a):
     print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "coarse_modes": st.coarse_modes,
                       "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,
-                      "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None}))
+                      "achieved_GBs": st.pcg_bytes / st.ms_pcg / 1e6 if st.ms_pcg else None,
+                      "phase_wall_ms": list(st.phase_wall_ms), "phase_busy_ms": list(st.phase_busy_ms)}))
 
 
 def profile_static(a):

@@ -306,6 +306,13 @@ typedef struct ufem_mc_stats {
   double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
   int tiles_per_block, unroll, lane_samples;  /* the launch shape used */
   int coarse_modes;          /* modes of the coarse correction applied (0: Jacobi alone) */
+  /* phase profile of the persistent PCG launches (global timer): per phase
+   * -- 0 initial true residual, 1 S (q = A p, p.q), 2 U (x, r, z updates),
+   * 3 R (true-residual replacement), 4 C1 (c = Wc^T r), 5 C3 (z += Wc c) --
+   * the wall time from the phase's start to the next phase's start (grid
+   * barrier included) and the mean time a block spent on its work items */
+  double phase_wall_ms[6], phase_busy_ms[6];
+  long true_residual_passes; /* R phases run */
 } ufem_mc_stats;
 int ufem_mc_get_stats(ufem_mc_stats *s);
 

@@ -6,10 +6,9 @@ load factor, 14,883 DOFs) is trained once (POD basis, MLP, coarse space of
 the preconditioner); 256 fresh samples are solved by
 
   A. the POD-Galerkin guess + FP64 implicit batched PCG with the coarse
-     correction (the bench's headline form), and
+     correction,
   B. the MLP guess + FP32 PCG with FP64 solution and true-residual
-     replacement (precision 1),
-
+     replacement (precision 1), and
   C. the MLP guess + FP32 implicit batched PCG (FP32 work vectors, blocks
      formed in the kernel in FP64, FP64 solution and true-residual
      replacement) with the coarse correction (precision 3),

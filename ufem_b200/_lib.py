@@ -66,7 +66,9 @@ class McStats(C.Structure):
                 ("ms_outputs", C.c_double), ("ms_total", C.c_double), ("pcg_iterations", C.c_long),
                 ("pcg_bytes", C.c_double), ("spmv_bytes", C.c_double), ("kernel_launches", C.c_long),
                 ("pcg_launches", C.c_long), ("pcg_launch_ms", C.c_double * 16), ("tiles_per_block", C.c_int),
-                ("unroll", C.c_int), ("lane_samples", C.c_int), ("coarse_modes", C.c_int)]
+                ("unroll", C.c_int), ("lane_samples", C.c_int), ("coarse_modes", C.c_int),
+                ("phase_wall_ms", C.c_double * 6), ("phase_busy_ms", C.c_double * 6),
+                ("true_residual_passes", C.c_long)]
 
 
 _SIGS = {

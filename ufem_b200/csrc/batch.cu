@@ -65,6 +65,10 @@ struct McOut {
   int reac;    // reaction index
 };
 
+// FP32 unit blocks of the implicit form: B*B values padded to 12 floats
+// (three 16-byte loads per contribution)
+constexpr int kW32Stride = 12;
+
 struct McPlan {
   bool built = false;
   int s = 0;                       // element matrix size (8 or 24)
@@ -90,6 +94,8 @@ struct McPlan {
   std::vector<int> mult_col;
   DBuf<int> d_mult_col, cptr, crow;  // contributions of block k / of block row I
   DBuf<double> cval;               // [nc][cstride]: B*B values, then (multiplier << 32 | J)
+  DBuf<float> w32;                 // [nc][12]: the B*B values in FP32 (precision 3's SpMV)
+  DBuf<int> sperm;                 // block rows in the order the gathering phases visit them
   long nc = 0;
   // coarse space of the preconditioner (ufem_mc_set_coarse): Wc [n][cmodes]
   // as BF16 tensor-core operand tiles, supported rows zero
@@ -124,8 +130,49 @@ void drop_plan(const ufem_model *m) {
 
 int element_matrices_unitE(ufem_model *m, double *d_out);  // kernels.cu
 
+// The order in which the gathering phases (q = A p, the true residual) visit
+// block rows: by the Morton key of the row's node position (coordinates
+// quantised to 1024 steps per axis over the model's bounding box), so that
+// the rows a block works on at once, and one after another, are neighbours in
+// space and their gathered neighbour vectors stay in the SM's L1.  On the
+// 40x10x10 beam an LRU model of a 128 KB L1 fetches 2x (FP64) to 3x (FP32)
+// fewer bytes from L2 per row than in the natural (x fastest) order.
+static std::vector<int> morton_row_order(const ufem_model *m) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int I = 0; I < m->nbr; I++)
+    for (int d = 0; d < 3; d++) {
+      const double v = m->xyz[(size_t)m->rank_node[I] * 3 + d];
+      lo[d] = std::min(lo[d], v);
+      hi[d] = std::max(hi[d], v);
+    }
+  std::vector<std::pair<unsigned long long, int>> key(m->nbr);
+  for (int I = 0; I < m->nbr; I++) {
+    unsigned long long k = 0;
+    unsigned q[3];
+    for (int d = 0; d < 3; d++) {
+      const double span = hi[d] - lo[d];
+      const double t = span > 0 ? (m->xyz[(size_t)m->rank_node[I] * 3 + d] - lo[d]) / span : 0.0;
+      q[d] = (unsigned)std::min(1023.0, std::max(0.0, t * 1023.0 + 0.5));
+    }
+    for (int b = 0; b < 10; b++)
+      for (int d = 0; d < 3; d++) k |= (unsigned long long)((q[d] >> b) & 1u) << (3 * b + d);
+    key[I] = {k, I};
+  }
+  std::stable_sort(key.begin(), key.end(),
+                   [](const std::pair<unsigned long long, int> &a, const std::pair<unsigned long long, int> &b) {
+                     return a.first < b.first;
+                   });
+  std::vector<int> order(m->nbr);
+  for (int I = 0; I < m->nbr; I++) order[I] = key[I].second;
+  return order;
+}
+
 static int build_plan(ufem_model *m, McPlan *P) {
   int rv;
+  {
+    const std::vector<int> order = morton_row_order(m);
+    if ((rv = P->sperm.upload(order.data(), order.size())) != UFEM_AF_OK) return rv;
+  }
   const int nn = m->nn, B = m->b, s = nn * B;
   P->s = s;
   P->ilen = m->mc_ilen;
@@ -343,6 +390,10 @@ static int build_implicit(ufem_model *m, McPlan *P) {
   P->cstride = stride;
   P->nc = cptr[m->nnzb];
   if (cval.empty()) cval.assign(stride, 0.0);
+  std::vector<float> w32((size_t)std::max<long>(1, P->nc) * kW32Stride, 0.0f);
+  for (long c = 0; c < P->nc; c++)
+    for (int t = 0; t < BB; t++) w32[(size_t)c * kW32Stride + t] = (float)cval[(size_t)c * stride + t];
+  if ((rv = P->w32.upload(w32.data(), w32.size()))) return rv;
   if ((rv = P->cptr.upload(cptr.data(), cptr.size())) || (rv = P->cval.upload(cval.data(), cval.size())) ||
       (rv = P->crow.upload(crow.data(), crow.size())) ||
       (rv = P->d_mult_col.upload(P->mult_col.data(), P->mult_col.size())))
@@ -420,6 +471,39 @@ __device__ __forceinline__ void st64(double *p, const double (&o)[VN]) {
 #pragma unroll
   for (int h = 0; h < VN / 2; h++)
     *reinterpret_cast<double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2)) = make_double2(o[2 * h], o[2 * h + 1]);
+}
+
+// Neighbour gathers through L1: VN values in the lane layout of T, read with
+// default caching.  Only for vectors that no block writes during the phase
+// that gathers them (z in the q = A p phase, x in the true-residual phase):
+// the grid barrier before the phase (an atomic arrival, a gpu-scope fence
+// after the wait, then the block barrier -- the pattern of a cooperative grid
+// sync) orders every earlier write before these loads, so no L1 line can be
+// stale, and the rows that a block gathers from its neighbourhood are reused
+// from L1 instead of being fetched from L2 once per neighbour.
+template <typename T, int VN>
+__device__ __forceinline__ void ld64_l1(const double *p, double (&o)[VN]) {
+#pragma unroll
+  for (int h = 0; h < VN / 2; h++) {
+    const double2 v = *reinterpret_cast<const double2 *>(p + (sizeof(T) == 8 ? h * 64 : h * 2));
+    o[2 * h] = v.x;
+    o[2 * h + 1] = v.y;
+  }
+}
+template <typename T, int VN>
+__device__ __forceinline__ void ldn_l1(const T *p, T (&o)[VN]) {
+  if constexpr (sizeof(T) == 8) {
+    ld64_l1<T, VN>(p, o);
+  } else {
+#pragma unroll
+    for (int h = 0; h < VN / 4; h++) {
+      const float4 v = reinterpret_cast<const float4 *>(p)[h];
+      o[4 * h] = v.x;
+      o[4 * h + 1] = v.y;
+      o[4 * h + 2] = v.z;
+      o[4 * h + 3] = v.w;
+    }
+  }
 }
 
 // VN values of type T at a 16-byte aligned address (double: VN = 2 or 4,
@@ -627,10 +711,14 @@ struct BMesh {
   // of mult[idx_c][s] * W_c, W_c and idx_c in cval[c*cstride ...]
   const int *cptr;
   const int *crow;      // contributions of block row I: [crow[I], crow[I+1])
+  const int *sperm;     // block rows in the visiting order of the gathering phases
   const double *cval;
   const double *mult;
+  const float *w32;     // FP32 copies of the unit blocks (precision 3)
   const unsigned char *fixed;
   int cstride;
+  int nmult;            // multipliers (rows of mult)
+  int smult;            // the tile's multipliers are staged in shared memory
   // coarse correction of the preconditioner (precision 2, 128-sample groups):
   // z = r / M + Wc c with c = Wc^T r, both products on the tensor cores
   int n;                // scalar rows (nbr * B)
@@ -662,65 +750,167 @@ struct BArgs {
   int nc1;
   const int4 *c3items;  // (mesh, group, 128-row chunk) of z += Wc c
   int nc3;
+  // phase profile (global timer, nanoseconds): [p] the blocks' summed time
+  // inside phase p's work items, [kProfWall + p] block 0's time from the
+  // start of phase p to the start of the next phase (its barrier wait
+  // included), [2 kProfWall] true-residual passes run.  Phases: kPh*.
+  unsigned long long *prof;
+  int *wctr;            // [kPhN] next work item of each phase (zero before its first use)
 };
+
+enum { kPhInit = 0, kPhS = 1, kPhU = 2, kPhR = 3, kPhC1 = 4, kPhC3 = 5, kPhN = 6 };
+constexpr int kProfWall = 8;
+
+// Per-block phase clocks, kept by thread 0 in shared memory.
+__shared__ unsigned long long s_prof_busy[kPhN], s_prof_wall[kPhN], s_prof_t0, s_prof_w0;
+__shared__ int s_prof_cur;
+
+__device__ __forceinline__ void prof_init() {
+  if (threadIdx.x == 0) {
+    for (int p = 0; p < kPhN; p++) s_prof_busy[p] = s_prof_wall[p] = 0;
+    s_prof_w0 = s_prof_t0 = global_ns();
+    s_prof_cur = kPhInit;
+  }
+}
+// a phase's work starts (after the barrier that ended the previous phase)
+__device__ __forceinline__ void prof_begin(int ph) {
+  if (threadIdx.x == 0) {
+    const unsigned long long t = global_ns();
+    s_prof_wall[s_prof_cur] += t - s_prof_w0;
+    s_prof_w0 = s_prof_t0 = t;
+    s_prof_cur = ph;
+  }
+}
+// the block's work items of the current phase are done (before its barrier)
+__device__ __forceinline__ void prof_end() {
+  if (threadIdx.x == 0) s_prof_busy[s_prof_cur] += global_ns() - s_prof_t0;
+}
+// The next work item of the current phase for this block.  Items are handed
+// out in order by one global counter per phase, so a block that finishes its
+// items early takes more (the per-item results do not depend on which block
+// computes them).  Block 0 zeroes a phase's counter after the grid barrier
+// that ends the phase: every block has left the phase's loop by then, and the
+// next use comes after further barriers.
+__device__ __forceinline__ int claim(int *ctr) {
+  __shared__ int s_claim;
+  __syncthreads();  // every thread has read the previous claim
+  if (threadIdx.x == 0) s_claim = atomicAdd(ctr, 1);
+  __syncthreads();
+  return s_claim;
+}
+__device__ __forceinline__ void release_counter(int *ctr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(ctr, 0);
+}
+
+__device__ __forceinline__ void prof_flush(unsigned long long *prof) {
+  if (threadIdx.x == 0 && prof) {
+    const unsigned long long t = global_ns();
+    s_prof_wall[s_prof_cur] += t - s_prof_w0;
+    for (int p = 0; p < kPhN; p++) {
+      atomicAdd(prof + p, s_prof_busy[p]);
+      if (blockIdx.x == 0) prof[kProfWall + p] = s_prof_wall[p];
+    }
+  }
+}
+
+// Dynamic shared memory of the persistent PCG: the operand staging of the
+// coarse phases, and during the other phases the multipliers of the tile's
+// sample group (implicit form), never both at once.
+extern __shared__ __align__(1024) uint8_t s_dyn_smem[];
 
 // acc[a][v] += mult[var_c][s] * (W_c X_{J_c})[a] over the contributions
 // [c0, c1) of one block row of the implicit form.  The row's contribution
 // keys (multiplier << 32 | J) are fetched 32 at a time, one per lane, and
 // broadcast; the gathers of U contributions are issued together so that U
 // neighbour loads are in flight per warp.  W and the multipliers are
-// read-only for the whole kernel (non-coherent loads); X is written by
-// other blocks during the kernel (L2 loads).  LT is the kernel's lane
-// layout (double: sample pairs 64 apart; float: 4 adjacent samples), XT the
-// type of X (the FP32 kernel gathers FP32 z, and FP64 x for its true
-// residuals); W, the multipliers and the sums are FP64 either way.
-template <typename LT, typename XT, int B, int VN, int U>
+// read-only for the whole kernel (non-coarse loads); X is written by other
+// blocks during the kernel (L2 loads).  LT is the kernel's lane layout
+// (double: sample pairs 64 apart; float: 4 adjacent samples), XT the type of
+// X, CT the type of the products and sums: FP64 (W and the multipliers in
+// FP64) or FP32 (W from the FP32 copies, the multipliers rounded).  With
+// s_mult the multipliers come from the tile's shared-memory copy
+// ([nmult][GS] of CT, sample sl of the group) instead of global memory.
+template <typename LT, typename XT, typename CT, int B, int VN, int U, bool SMULT>
 __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, int cstride,
-                                             const double *__restrict__ mult, const XT *X, int S, int sb,
-                                             int c0, int c1, double (&acc)[B][VN]) {
+                                             const float *__restrict__ w32, const double *__restrict__ mult,
+                                             const CT *s_mult, const XT *X, int S, int sb, int sl, int c0, int c1,
+                                             CT (&acc)[B][VN]) {
   static_assert(sizeof(XT) == 8 || sizeof(LT) == 4, "FP32 vectors only in the FP32 lane layout");
+  constexpr int GS = 32 * VN;
   const int lane = threadIdx.x & 31;
   for (int cb = c0; cb < c1; cb += 32) {
     const long long mykey = (cb + lane < c1) ? (long long)__ldg(cval + (size_t)(cb + lane) * cstride + B * B) : 0;
     const int cnt = min(32, c1 - cb);
     for (int j = 0; j < cnt; j += U) {
       XT xv[U][B][VN];
-      double av[U][VN];
+      double av[SMULT ? 1 : U][VN];
+      int vars[SMULT ? U : 1];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const long long key = __shfl_sync(0xffffffffu, mykey, min(j + u, cnt - 1));
-        const int J = (int)(key & 0xffffffffLL), var = (int)(key >> 32);
+        const int J = (int)(key & 0xffffffffLL);
 #pragma unroll
         for (int b = 0; b < B; b++) {
-          if constexpr (sizeof(XT) == 8) ld64<LT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
-          else ldn<XT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
+          if constexpr (sizeof(XT) == 8) ld64_l1<LT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
+          else ldn_l1<XT, VN>(X + (size_t)(J * B + b) * S + sb, xv[u][b]);
         }
-        ld64_ro<LT, VN>(mult + (size_t)var * S + sb, av[u]);
+        if constexpr (SMULT) vars[u] = (int)(key >> 32);
+        else ld64_ro<LT, VN>(mult + (size_t)(int)(key >> 32) * S + sb, av[u]);
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {
         if (j + u >= cnt) break;
-        const double *w = cval + (size_t)(cb + j + u) * cstride;
-        double W[B * B];
+        CT W[B * B];
+        if constexpr (sizeof(CT) == 8) {
+          const double *w = cval + (size_t)(cb + j + u) * cstride;
 #pragma unroll
-        for (int h = 0; h < (B * B) / 2; h++) {
-          const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
-          W[2 * h] = v.x;
-          W[2 * h + 1] = v.y;
+          for (int h = 0; h < (B * B) / 2; h++) {
+            const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
+            W[2 * h] = v.x;
+            W[2 * h + 1] = v.y;
+          }
+          if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
+        } else {
+          const float4 *w = reinterpret_cast<const float4 *>(w32 + (size_t)(cb + j + u) * kW32Stride);
+#pragma unroll
+          for (int h = 0; h < (B * B + 3) / 4; h++) {
+            const float4 v = __ldg(w + h);
+            const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (4 * h + q < B * B) W[4 * h + q] = e[q];
+          }
         }
-        if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
+        CT a[VN];
+        if constexpr (SMULT) {
+          const CT *sm = s_mult + vars[u] * GS;
 #pragma unroll
-        for (int a = 0; a < B; a++)
+          for (int v = 0; v < VN; v++) a[v] = sm[lane_sample<LT, VN>(lane, v)];
+        } else {
+#pragma unroll
+          for (int v = 0; v < VN; v++) a[v] = (CT)av[u][v];
+        }
+#pragma unroll
+        for (int r = 0; r < B; r++)
 #pragma unroll
           for (int v = 0; v < VN; v++) {
-            double t = 0.0;
+            CT t = 0;
 #pragma unroll
-            for (int b = 0; b < B; b++) t = fma(W[a * B + b], (double)xv[u][b][v], t);
-            acc[a][v] = fma(av[u][v], t, acc[a][v]);
+            for (int b = 0; b < B; b++) t = fma(W[r * B + b], (CT)xv[u][b][v], t);
+            acc[r][v] = fma(a[v], t, acc[r][v]);
           }
       }
     }
   }
+  (void)sl;
+}
+
+// The multipliers of group g, mult[v][g GS + i], into shared memory as CT
+// (by every thread of the block; the caller synchronises before use).
+template <typename CT, int GS>
+__device__ __forceinline__ void stage_mult(const double *__restrict__ mult, int nmult, int S, int g, CT *s_mult) {
+  for (int i = threadIdx.x; i < nmult * GS; i += blockDim.x)
+    s_mult[i] = (CT)__ldg(mult + (size_t)(i / GS) * S + (size_t)g * GS + (i % GS));
 }
 
 // Called by every tile of group g after it wrote its partials: the last
@@ -758,9 +948,9 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 template <typename T, int B, bool IMP, int UN, int VN, int NW>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VN]) {
-  // the implicit form sums every row in FP64 (its unit blocks and
-  // multipliers are FP64) whatever the vector precision T
-  using AT = typename std::conditional<IMP, double, T>::type;
+  // products and sums in the vector precision T: FP64, or FP32 with the
+  // FP32 copies of the unit blocks (the inner FP32 matrix of precision 3)
+  using AT = T;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -769,18 +959,31 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   T beta[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) beta[v] = s_beta[lane_sample<T, VN>(lane, v)];
+  T *s_mult = nullptr;
+  if constexpr (IMP) {
+    if (M.smult) {
+      s_mult = reinterpret_cast<T *>(s_dyn_smem);
+      stage_mult<T, GS>(M.mult, M.nmult, S, g, s_mult);
+      __syncthreads();
+    }
+  }
   double pq[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) pq[v] = 0;
-  for (int I = row0 + warp; I < row1; I += NW) {
+  for (int ri = row0 + warp; ri < row1; ri += NW) {
+    const int I = __ldg(M.sperm + ri);  // rows in the gathering order (neighbours in space together)
     AT acc[B][VN];
 #pragma unroll
     for (int a = 0; a < B; a++)
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     if constexpr (IMP) {
-      implicit_row<T, T, B, VN, UN>(M.cval, M.cstride, M.mult, M.z, S, sb, __ldg(M.crow + I), __ldg(M.crow + I + 1),
-                                    acc);
+      if (s_mult)
+        implicit_row<T, T, T, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.z, S, sb,
+                                               lane_base<T, VN>(lane), __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+      else
+        implicit_row<T, T, T, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.z, S, sb,
+                                                lane_base<T, VN>(lane), __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -797,10 +1000,10 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           T xv[B][VN];
 #pragma unroll
           for (int c = 0; c < B; c++) {
-            ldn<T, VN>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
+            ldn_l1<T, VN>(M.z + (size_t)(J * B + c) * S + sb, xv[c]);
             if (!first) {
               T pv[VN];
-              ldn<T, VN>(pold + (size_t)(J * B + c) * S + sb, pv);
+              ldn_l1<T, VN>(pold + (size_t)(J * B + c) * S + sb, pv);
 #pragma unroll
               for (int v = 0; v < VN; v++) xv[c][v] = xv[c][v] + beta[v] * pv[v];
             }
@@ -833,7 +1036,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           T qo[VN];
           ldn<T, VN>(M.q + o, qo);
 #pragma unroll
-          for (int v = 0; v < VN; v++) acc[a][v] = fma((double)beta[v], (double)qo[v], acc[a][v]);
+          for (int v = 0; v < VN; v++) acc[a][v] = fma(beta[v], qo[v], acc[a][v]);
         }
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
 #pragma unroll
@@ -944,15 +1147,33 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
-  for (int I = row0 + warp; I < row1; I += NW) {
+  // FP64 multipliers in shared memory (FP64 kernels only: the FP32 kernel
+  // stages FP32 copies for its SpMV, and its true residual is FP64)
+  const double *s_mult = nullptr;
+  if constexpr (IMP && sizeof(T) == 8) {
+    if (M.smult) {
+      double *sm = reinterpret_cast<double *>(s_dyn_smem);
+      stage_mult<double, GS>(M.mult, M.nmult, S, g, sm);
+      __syncthreads();
+      s_mult = sm;
+    }
+  }
+  for (int ri = row0 + warp; ri < row1; ri += NW) {
+    const int I = __ldg(M.sperm + ri);  // rows in the gathering order (neighbours in space together)
     double acc[B][VN];
 #pragma unroll
     for (int a = 0; a < B; a++)
 #pragma unroll
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
     if constexpr (IMP) {
-      implicit_row<T, double, B, VN, UN>(M.cval, M.cstride, M.mult, M.x, S, sb, __ldg(M.crow + I),
-                                         __ldg(M.crow + I + 1), acc);
+      if (s_mult)
+        implicit_row<T, double, double, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.x, S, sb,
+                                                         lane_base<T, VN>(lane), __ldg(M.crow + I),
+                                                         __ldg(M.crow + I + 1), acc);
+      else
+        implicit_row<T, double, double, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.x, S, sb,
+                                                          lane_base<T, VN>(lane), __ldg(M.crow + I),
+                                                          __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -963,7 +1184,7 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
           const int J = __shfl_sync(0xffffffffu, myJ, j);
           double xv[B][VN];
 #pragma unroll
-          for (int c = 0; c < B; c++) ld64<T, VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
+          for (int c = 0; c < B; c++) ld64_l1<T, VN>(M.x + (size_t)(J * B + c) * S + sb, xv[c]);
 #pragma unroll
           for (int a = 0; a < B; a++)
 #pragma unroll
@@ -1048,7 +1269,6 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 __shared__ uint32_t s_coarse_tmem;
 __shared__ uint32_t s_coarse_phase;  // parity of the MMA barrier's next completion
 __shared__ __align__(8) uint64_t s_coarse_mbar;
-extern __shared__ __align__(1024) uint8_t s_coarse_smem[];
 
 // Leaves the kernel at the next grid barrier: every block sees the error.
 __device__ __forceinline__ void coarse_fail(GridBar *bar) { atomicExch(&bar->err, kErrMma); }
@@ -1064,7 +1284,7 @@ __device__ __noinline__ void coarse_c1(const BMesh<T> &M, int g, int range, int 
   __shared__ double s_cc[kCoarseThreads];
   const uint32_t tmem = s_coarse_tmem;
   uint64_t *bar = &s_coarse_mbar;
-  uint8_t *sm = s_coarse_smem;
+  uint8_t *sm = s_dyn_smem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = M.cmodes, S = M.S;
   const int r0 = range * M.rps, r1 = min(M.n, r0 + M.rps);
@@ -1190,7 +1410,7 @@ __device__ __noinline__ void coarse_c3(const BMesh<T> &M, int g, int chunk, uint
   constexpr int kRows = 128 / (kCoarseThreads / 128);  // rows of the chunk per thread
   const uint32_t tmem = s_coarse_tmem;
   uint64_t *bar = &s_coarse_mbar;
-  uint8_t *sm = s_coarse_smem;
+  uint8_t *sm = s_dyn_smem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmod = M.cmodes, S = M.S;
   const int tbytes = 128 * nmod * 2;
@@ -1260,6 +1480,7 @@ __global__ void k_coarse_tiles(int n, int cm, const double *__restrict__ Wc, con
 }
 
 constexpr int kMaxMeshes = 8;
+constexpr size_t kMultSmem = 32 * 1024;  // largest staged multiplier table of a tile's group
 
 #ifndef UFEM_PCG_MIN_BLOCKS
 #define UFEM_PCG_MIN_BLOCKS 2
@@ -1270,10 +1491,10 @@ constexpr int kMaxMeshes = 8;
 template <typename T>
 __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_meshes, int par) {
   __shared__ int s_go;
-  const int G = gridDim.x;
   uint32_t phase = s_coarse_phase;
   {
-    for (int t = blockIdx.x; t < A.nc1; t += G) {
+    prof_begin(kPhC1);
+    for (int t = claim(A.wctr + kPhC1); t < A.nc1; t = claim(A.wctr + kPhC1)) {
       const int4 it = A.c1items[t];
       const BMesh<T> &M = s_meshes[it.x];
       if (threadIdx.x == 0) s_go = __ldcg(M.gcz + it.y);
@@ -1282,8 +1503,11 @@ __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_m
       __syncthreads();
       if (go) coarse_c1(M, it.y, it.z, par, phase, A.bar);
     }
+    prof_end();
     if (!grid_barrier(A.bar)) return false;
-    for (int t = blockIdx.x; t < A.nc3; t += G) {
+    release_counter(A.wctr + kPhC1);
+    prof_begin(kPhC3);
+    for (int t = claim(A.wctr + kPhC3); t < A.nc3; t = claim(A.wctr + kPhC3)) {
       const int4 it = A.c3items[t];
       const BMesh<T> &M = s_meshes[it.x];
       if (threadIdx.x == 0) s_go = __ldcg(M.gcz + it.y);
@@ -1292,7 +1516,9 @@ __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_m
       __syncthreads();
       if (go) coarse_c3(M, it.y, it.z, phase, A.bar);
     }
+    prof_end();
     if (!grid_barrier(A.bar)) return false;
+    release_counter(A.wctr + kPhC3);
   }
   if (threadIdx.x == 0) s_coarse_phase = phase;  // every thread holds the same parity
   __syncthreads();
@@ -1309,13 +1535,13 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
   __shared__ T s_sc[GS];
   __shared__ BMesh<T> s_meshes[kMaxMeshes];
   __shared__ int s_flag;
-  const int G = gridDim.x;
   // the mesh descriptors, once per launch
   for (int i = threadIdx.x; i < A.nmesh * (int)(sizeof(BMesh<T>) / sizeof(int)); i += blockDim.x)
     reinterpret_cast<int *>(s_meshes)[i] = reinterpret_cast<const int *>(A.meshes)[i];
+  prof_init();
   __syncthreads();
   // phase 0: the true residual of the initial guess (parity slot 0)
-  for (int t = blockIdx.x; t < A.ntiles; t += G) {
+  for (int t = claim(A.wctr + kPhInit); t < A.ntiles; t = claim(A.wctr + kPhInit)) {
     const int4 ti = A.tiles[t];
     const BMesh<T> &M = s_meshes[ti.x];
     int any = 0;
@@ -1331,7 +1557,9 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
     }
     __syncthreads();
   }
+  prof_end();
   if (!grid_barrier(A.bar)) return;
+  release_counter(A.wctr + kPhInit);
   if constexpr (kCoarse) {
     if (A.coarse && !coarse_phases<T>(A, s_meshes, 0)) return;
   }
@@ -1340,7 +1568,8 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
     const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
     const bool first = (k == 1);
     // ---- phase S: convergence on true residuals, beta, q = A p -------------
-    for (int t = blockIdx.x; t < A.ntiles; t += G) {
+    prof_begin(kPhS);
+    for (int t = claim(A.wctr + kPhS); t < A.ntiles; t = claim(A.wctr + kPhS)) {
       const int4 ti = A.tiles[t];
       const BMesh<T> &M = s_meshes[ti.x];
       if (threadIdx.x == 0) s_flag = __ldcg(M.gtrue + ti.y);
@@ -1411,12 +1640,15 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
       T *pnew = (k & 1) ? M.p1 : M.p0;
       tile_spmv<T, B, IMP, UN, VN, NW>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
+    prof_end();
     if (!grid_barrier(A.bar)) return;
+    release_counter(A.wctr + kPhS);
     // The group counter changes only in phase S: read between the barriers,
     // every block takes the same exit decision.
     const int remaining = atomicAdd(A.active_count, 0);
     // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
-    for (int t = blockIdx.x; t < A.ntiles; t += G) {
+    prof_begin(kPhU);
+    for (int t = claim(A.wctr + kPhU); t < A.ntiles; t = claim(A.wctr + kPhU)) {
       const int4 ti = A.tiles[t];
       const BMesh<T> &M = s_meshes[ti.x];
       __syncthreads();
@@ -1452,11 +1684,15 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
       if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
       if (M.cmodes && threadIdx.x == 0) M.gcz[g] = 1;
     }
+    prof_end();
     if (!grid_barrier(A.bar)) return;
+    release_counter(A.wctr + kPhU);
     // ---- phase R (when a group asked): replace the recursive residual -------
     const int nrep = atomicAdd(A.rcount, 0);  // changes only in phase U
     if (nrep > 0) {
-      for (int t = blockIdx.x; t < A.ntiles; t += G) {
+      prof_begin(kPhR);
+      if (blockIdx.x == 0 && threadIdx.x == 0 && A.prof) A.prof[2 * kProfWall] += 1;
+      for (int t = claim(A.wctr + kPhR); t < A.ntiles; t = claim(A.wctr + kPhR)) {
         const int4 ti = A.tiles[t];
         const BMesh<T> &M = s_meshes[ti.x];
         if (threadIdx.x == 0) s_flag = __ldcg(M.gneed + ti.y);
@@ -1472,7 +1708,9 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
         }
         if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
       }
+      prof_end();
       if (!grid_barrier(A.bar)) return;
+      release_counter(A.wctr + kPhR);
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(A.rcount, 0);  // read again only after the next U
     }
     if (remaining <= 0 || k > A.maxit + 1) break;
@@ -1481,6 +1719,7 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
       if (A.coarse && !coarse_phases<T>(A, s_meshes, par)) return;
     }
   }
+  prof_flush(A.prof);
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
 }
 
@@ -1638,6 +1877,8 @@ struct LaunchBufs {
   DBuf<GridBar> bar;
   DBuf<int> cnt, rcnt;
   DBuf<long> itout;
+  DBuf<unsigned long long> prof;
+  DBuf<int> wctr;
 };
 template <typename T>
 LaunchBufs<T> &launch_bufs() {
@@ -1841,10 +2082,18 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       }
     }
   }
-  const size_t dsmem = coarse ? kCoarseSmem : 0;
+  // The multipliers of a tile's sample group go to shared memory when the
+  // largest mesh's fit in kMultSmem bytes (zone models; per-element E
+  // models read them from global memory); the coarse phases reuse the space.
+  int max_nmult = 0;
+  if constexpr (IMP)
+    for (int k = 0; k < nmesh; k++) max_nmult = std::max(max_nmult, plans[k]->nmult);
+  const size_t mult_bytes = (size_t)max_nmult * GS * sizeof(T);
+  const bool smult = IMP && max_nmult > 0 && mult_bytes <= kMultSmem;
+  const size_t dsmem = std::max(coarse ? kCoarseSmem : (size_t)0, smult ? mult_bytes : (size_t)0);
   // one block per SM either way (tensor memory): the rest of the unified
   // L1 / shared memory stays L1 for the contribution records
-  if (coarse) UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+  if (dsmem) UFEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
   const int nthreads = coarse ? kCoarseThreads : kThreads, nwarps = nthreads / 32;
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nthreads, dsmem));
   if (occ < 1) {
@@ -1895,6 +2144,10 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     b.mult = w.mult.p;
     b.fixed = m->d_fixed.p;
     b.cstride = plans[k]->cstride;
+    b.w32 = plans[k]->w32.p;
+    b.sperm = plans[k]->sperm.p;
+    b.nmult = plans[k]->nmult;
+    b.smult = smult ? 1 : 0;
     const size_t n = (size_t)m->nDOFAct * w.S;
     const size_t np = (size_t)b.ngroups * b.ntpg * GS;
     if constexpr (sizeof(T) == 4) {
@@ -2003,8 +2256,10 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   const int zero = 0;
   if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
       (rv = bar.ensure(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
-      (rv = itout.ensure(1)))
+      (rv = itout.ensure(1)) || (rv = LB.prof.ensure(2 * kProfWall + 1)) || (rv = LB.wctr.ensure(kPhN)))
     return rv;
+  UFEM_CUDA_TRY(cudaMemsetAsync(LB.wctr.p, 0, kPhN * sizeof(int)));
+  UFEM_CUDA_TRY(cudaMemsetAsync(LB.prof.p, 0, (2 * kProfWall + 1) * sizeof(unsigned long long)));
   if (!c1items.empty() && ((rv = d_c1.upload(c1items.data(), c1items.size())) ||
                            (rv = d_c3.upload(c3items.data(), c3items.size()))))
     return rv;
@@ -2026,13 +2281,15 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   a.nc1 = (int)c1items.size();
   a.c3items = d_c3.p;
   a.nc3 = (int)c3items.size();
+  a.prof = LB.prof.p;
+  a.wctr = LB.wctr.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0);
-  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, a.coarse ? dsmem : 0, 0));
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
   cudaEventRecord(ev1);
   g_stats.kernel_launches += 1;
   long its = 0;
@@ -2050,6 +2307,15 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     set_error(hb.err == kErrMma ? "batched PCG: a tensor-core wait of the coarse correction timed out"
                                 : "batched PCG: grid barrier timed out");
     return UFEM_AF_ERR;
+  }
+  {
+    unsigned long long pr[2 * kProfWall + 1];
+    UFEM_CUDA_TRY(cudaMemcpy(pr, LB.prof.p, sizeof(pr), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < kPhN; p++) {
+      g_stats.phase_wall_ms[p] += pr[kProfWall + p] * 1e-6;
+      g_stats.phase_busy_ms[p] += pr[p] * 1e-6 / grid;
+    }
+    g_stats.true_residual_passes += (long)pr[2 * kProfWall];
   }
   *iters_run = its;
   // Algorithmic bytes.  A group of GS samples moves data only while it is
