@@ -343,10 +343,14 @@ int  ufem_tc_gemm_bf16(int M, int N, int K, const void *d_A, const void *d_B, fl
  * monte_linear_solver, fem/fem_mont.c:493-504) ------------------------------
  * Training: the batched solver solves ntrain samples from zero; a POD basis
  * of n_modes modes is built from the first n_snapshots solutions (FP64,
- * randomised subspace iteration + Rayleigh-Ritz); the MLP above learns the
- * map from the chosen inputs to the solutions' POD coefficients (divided by
- * the sample's value in scale_col: the solution is linear in the load).
- * Solving: u0 = scale * Phi * MLP(inputs) is the initial guess of the
+ * randomised subspace iteration + Rayleigh-Ritz); the solutions' POD
+ * coefficients (divided by the sample's value in scale_col: the solution is
+ * linear in the load) are modelled as a least-squares quadratic polynomial
+ * of the standardised inputs (FP64, fitted by normal equations; linear
+ * terms only below 4 training samples per quadratic term) plus the MLP
+ * above, trained on that polynomial's residual over one common scale, so
+ * the network's squared error is the coefficients' squared error.
+ * Solving: u0 = scale * Phi * (poly + MLP)(inputs) is the initial guess of the
  * batched PCG, which still iterates to the same tolerance; its iteration cap
  * is the largest cold iteration count seen in training (when solving at the
  * training's precision), and a sample that does not converge within it is
@@ -357,7 +361,9 @@ typedef struct ufem_warm_options {
   int n_hidden;              /* MLP width: a multiple of 16, at most 256 */
   int n_feat;                /* network inputs, 1..32 */
   long feat_cols[32];        /* ifld column of each input */
-  int feat_log[32];          /* nonzero: the input enters as log|value| */
+  int feat_log[32];          /* 1: the input enters as log|value|; 2: as 1/value (a compliance:
+                                for a modulus E, displacements are close to linear in 1/E);
+                                0: as is */
   long scale_col;            /* ifld column the solution is proportional to, or -1 */
   long n_snapshots;          /* solutions the basis is built from (>= n_modes + 16) */
   int power_iters;           /* subspace iterations of the POD */
@@ -414,7 +420,10 @@ int  ufem_warm_guess(ufem_warm *w, long nsamp, const double *d_ifld, double *d_u
 /* warm-started batched solve; d_ofld nsamp*olen, d_status, d_iters nsamp (device; may be NULL) */
 int  ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_ofld, int *d_status, long *d_iters,
                      const ufem_mc_options *opt, ufem_warm_stats *st);
-/* switches the guess between the MLP (0) and the POD-Galerkin system (1) */
+/* switches the guess between the MLP (0: the least-squares quadratic model
+ * of the coefficients plus the network's correction), the POD-Galerkin
+ * system (1) and, as a diagnostic of what the network adds, the
+ * least-squares model alone (2) */
 int  ufem_warm_set_guess_mode(ufem_warm *w, int mode);
 /* multiplies every guess by factor (1 by default): a diagnostic that makes the
  * guesses bad on purpose, to exercise the fallback */

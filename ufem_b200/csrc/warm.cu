@@ -326,7 +326,8 @@ __global__ void k_feat_raw(long nsamp, int nf, long ilen, const double *__restri
   const long s = e / nf;
   const int f = (int)(e % nf);
   double v = ifld[s * ilen + col[f]];
-  if (lg[f]) v = log(fabs(v));
+  if (lg[f] == 2) v = v != 0.0 ? 1.0 / v : 0.0;  // compliance-like inputs (1/E)
+  else if (lg[f]) v = log(fabs(v));
   raw[e] = v;
 }
 
@@ -387,14 +388,72 @@ __global__ void k_targets(long nsamp, int r, const double *__restrict__ c, const
   t[e] = (float)((c[e] - mean[k]) / sd[k]);
 }
 
-// network outputs -> coefficients: c[s][k] = (y * sd + mean) * sc[s]
-__global__ void k_coeffs(long nsamp, int r, const float *__restrict__ y, const double *__restrict__ mean,
-                         const double *__restrict__ sd, const double *__restrict__ sc, double gscale,
+// Least-squares part of the coefficient model: a full quadratic polynomial
+// in the standardised features xs (1, xs_f, xs_i xs_j for i <= j),
+// lin(x)[k] = sum_j W[j][k] phi_j(xs).  The MLP learns only what this misses,
+// so its BF16 arithmetic and its fitting error act on a small residual
+// instead of the whole coefficient.  nterms(nf) = 1 + nf + nf (nf + 1) / 2.
+// With fewer than 4 training samples per quadratic term the model keeps the
+// linear terms only (quad = 0).
+__host__ __device__ __forceinline__ int poly_terms(int nf, int quad) { return 1 + nf + (quad ? nf * (nf + 1) / 2 : 0); }
+
+__device__ __forceinline__ void poly_features(int nf, int quad, const double *__restrict__ raw,
+                                              const double *__restrict__ fmean, const double *__restrict__ fsd,
+                                              double *phi) {
+  double xs[32];
+  for (int f = 0; f < nf; f++) xs[f] = (raw[f] - fmean[f]) / fsd[f];
+  int j = 0;
+  phi[j++] = 1.0;
+  for (int f = 0; f < nf; f++) phi[j++] = xs[f];
+  if (quad)
+    for (int a = 0; a < nf; a++)
+      for (int b = a; b < nf; b++) phi[j++] = xs[a] * xs[b];
+}
+
+__device__ __forceinline__ double lin_model(int nf, int quad, int r, int k, const double *__restrict__ raw,
+                                            const double *__restrict__ fmean, const double *__restrict__ fsd,
+                                            const double *__restrict__ W) {
+  double xs[32];
+  for (int f = 0; f < nf; f++) xs[f] = (raw[f] - fmean[f]) / fsd[f];
+  double t = W[k];
+  int j = 1;
+  for (int f = 0; f < nf; f++) t = fma(xs[f], W[(size_t)(j++) * r + k], t);
+  if (quad)
+    for (int a = 0; a < nf; a++)
+      for (int b = a; b < nf; b++) t = fma(xs[a] * xs[b], W[(size_t)(j++) * r + k], t);
+  return t;
+}
+
+// network outputs -> coefficients: c[s][k] = (lin(x_s)[k] + y * sd + mean) * sc[s]
+// (W == nullptr: no least-squares part)
+__global__ void k_coeffs(long nsamp, int r, int nf, int quad, const float *__restrict__ y, const double *__restrict__ mean,
+                         const double *__restrict__ sd, const double *__restrict__ raw,
+                         const double *__restrict__ fmean, const double *__restrict__ fsd,
+                         const double *__restrict__ W, const double *__restrict__ sc, double gscale,
                          double *__restrict__ c) {
   const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nsamp * r) return;
   const int k = (int)(e % r);
-  c[e] = ((double)y[e] * sd[k] + mean[k]) * sc[e / r] * gscale;
+  const long s = e / r;
+  const double lin = W ? lin_model(nf, quad, r, k, raw + s * nf, fmean, fsd, W) : 0.0;
+  c[e] = (lin + (double)y[e] * sd[k] + mean[k]) * sc[s] * gscale;
+}
+
+// design matrix of the least-squares model: D[s] = phi(xs_s), one thread per sample
+__global__ void k_design(long nsamp, int nf, int quad, const double *__restrict__ raw, const double *__restrict__ fmean,
+                         const double *__restrict__ fsd, double *__restrict__ D) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsamp) return;
+  poly_features(nf, quad, raw + s * nf, fmean, fsd, D + s * poly_terms(nf, quad));
+}
+
+// c[s][k] -= lin(x_s)[k]: the residual the MLP is trained on
+__global__ void k_lin_resid(long nsamp, int r, int nf, int quad, const double *__restrict__ raw,
+                            const double *__restrict__ fmean, const double *__restrict__ fsd,
+                            const double *__restrict__ W, double *__restrict__ c) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsamp * r) return;
+  c[e] -= lin_model(nf, quad, r, (int)(e % r), raw + (e / r) * nf, fmean, fsd, W);
 }
 
 // rows of a row-major matrix picked by idx (minibatches)
@@ -649,6 +708,9 @@ struct ufem_warm {
   // basis and normalisation
   DBuf<double> phi;                       // [n][r]
   DBuf<double> fmean, fsd, cmean, csd;    // feature / coefficient statistics
+  DBuf<double> linW;                      // [terms][r] least-squares (quadratic) model of the coefficients
+  DBuf<double> design, gram;              // [ntrain][terms] design matrix; normal equations
+  int lin_quad = 0;                       // the least-squares model has the quadratic terms
   DBuf<long> fcol;
   DBuf<int> flog;
   std::vector<double> sigma2;             // Rayleigh-Ritz energies of the modes
@@ -907,6 +969,80 @@ int padded_S(long nsamp) { return (int)std::max<long>(128, (nsamp + 127) / 128 *
 
 // u0 [n][S] = Phi c^T for nsamp samples: c from the MLP (inputs in w->X /
 // w->sc), or from the POD-Galerkin system of each sample (guess mode 1)
+// The coefficient model's least-squares part, fitted over the training
+// samples (normal equations (D^T D + lambda I) W = D^T C, D the quadratic
+// design matrix of the standardised features, formed on the GPU and solved
+// by Cholesky on the host: 1 + nf + nf (nf + 1) / 2 unknowns, 171 for 17
+// inputs, shared by every mode); c becomes the
+// residual, and the MLP's targets are that residual over one common scale
+// (its RMS over samples and modes), so the network's squared error is the
+// squared error of the coefficients themselves -- the error of the guess
+// in the 2-norm, Phi being orthonormal.
+int fit_linear(ufem_warm *w, long ntrain) {
+  int rv;
+  const int r = w->r, nf = w->o.n_feat;
+  w->lin_quad = ntrain >= 4L * poly_terms(nf, 1) ? 1 : 0;
+  const int nd = poly_terms(nf, w->lin_quad);
+  if ((rv = w->design.ensure((size_t)ntrain * nd)) || (rv = w->gram.ensure((size_t)nd * (nd + r))) ||
+      (rv = w->linW.ensure((size_t)nd * r)))
+    return rv;
+  k_design<<<grid1(ntrain, 128), 128>>>(ntrain, nf, w->lin_quad, w->raw.p, w->fmean.p, w->fsd.p, w->design.p);
+  // G = D^T D [nd][nd], H = D^T C [nd][r]
+  if ((rv = gemm_f64(nd, nd, ntrain, w->design.p, 1, nd, w->design.p, nd, 1, w->gram.p, nd, 1, w->part)) ||
+      (rv = gemm_f64(nd, r, ntrain, w->design.p, 1, nd, w->c.p, r, 1, w->gram.p + (size_t)nd * nd, r, 1, w->part)))
+    return rv;
+  std::vector<double> G((size_t)nd * nd), H((size_t)nd * r);
+  UFEM_CUDA_TRY(cudaMemcpy(G.data(), w->gram.p, G.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(H.data(), w->gram.p + (size_t)nd * nd, H.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  double tr = 0.0;
+  for (int i = 0; i < nd; i++) tr += G[(size_t)i * nd + i];
+  for (int i = 0; i < nd; i++) G[(size_t)i * nd + i] += 1e-12 * tr / nd;  // keeps a constant feature solvable
+  // Cholesky G = L L^T (lower, in place)
+  for (int j = 0; j < nd; j++) {
+    double d = G[(size_t)j * nd + j];
+    for (int k = 0; k < j; k++) d -= G[(size_t)j * nd + k] * G[(size_t)j * nd + k];
+    if (!(d > 0.0)) {
+      set_error("warm start: the linear coefficient model's normal equations are not positive definite");
+      return UFEM_AF_ERR;
+    }
+    const double ljj = std::sqrt(d);
+    G[(size_t)j * nd + j] = ljj;
+    for (int i = j + 1; i < nd; i++) {
+      double t = G[(size_t)i * nd + j];
+      for (int k = 0; k < j; k++) t -= G[(size_t)i * nd + k] * G[(size_t)j * nd + k];
+      G[(size_t)i * nd + j] = t / ljj;
+    }
+  }
+  for (int k = 0; k < r; k++) {  // L y = h, L^T w = y, column by column
+    std::vector<double> y(nd);
+    for (int i = 0; i < nd; i++) {
+      double t = H[(size_t)i * r + k];
+      for (int j = 0; j < i; j++) t -= G[(size_t)i * nd + j] * y[j];
+      y[i] = t / G[(size_t)i * nd + i];
+    }
+    for (int i = nd - 1; i >= 0; i--) {
+      double t = y[i];
+      for (int j = i + 1; j < nd; j++) t -= G[(size_t)j * nd + i] * H[(size_t)j * r + k];
+      H[(size_t)i * r + k] = t / G[(size_t)i * nd + i];
+    }
+  }
+  UFEM_CUDA_TRY(cudaMemcpy(w->linW.p, H.data(), H.size() * sizeof(double), cudaMemcpyHostToDevice));
+  k_lin_resid<<<grid1(ntrain * r), 256>>>(ntrain, r, nf, w->lin_quad, w->raw.p, w->fmean.p, w->fsd.p, w->linW.p,
+                                          w->c.p);
+  // one common scale for every mode: the RMS of the residual
+  k_col_stats<<<1, 128>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p);
+  std::vector<double> mu(r), sd(r);
+  UFEM_CUDA_TRY(cudaMemcpy(mu.data(), w->cmean.p, r * sizeof(double), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(sd.data(), w->csd.p, r * sizeof(double), cudaMemcpyDeviceToHost));
+  double ms = 0.0;
+  for (int k = 0; k < r; k++) ms += sd[k] * sd[k] + mu[k] * mu[k];
+  const double scale = ms > 0.0 ? std::sqrt(ms / r) : 1.0;
+  for (int k = 0; k < r; k++) sd[k] = scale;
+  UFEM_CUDA_TRY(cudaMemcpy(w->csd.p, sd.data(), r * sizeof(double), cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_AF_OK;
+}
+
 int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
   int rv;
   const int r = w->r;
@@ -924,8 +1060,13 @@ int make_guess(ufem_warm *w, long nsamp, int S, const double *d_ifld) {
                                                      w->PF0.p, w->novr, w->d_ovar.p, w->Prow.p, w->rb, w->c.p);
     if (w->guess_scale != 1.0) k_mul<<<grid1(nsamp * r), 256>>>(nsamp * r, w->guess_scale, w->c.p);
   } else {
-    if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) return rv;
-    k_coeffs<<<grid1(nsamp * r), 256>>>(nsamp, r, w->Yo.p, w->cmean.p, w->csd.p, w->sc.p, w->guess_scale, w->c.p);
+    if (w->o.guess_mode == 2) {  // the least-squares part alone: a zero network output
+      UFEM_CUDA_TRY(cudaMemsetAsync(w->Yo.p, 0, (size_t)nsamp * r * sizeof(float)));
+    } else if ((rv = ufem_mlp_forward(w->mlp, nsamp, w->X.p, w->Yo.p))) {
+      return rv;
+    }
+    k_coeffs<<<grid1(nsamp * r), 256>>>(nsamp, r, w->o.n_feat, w->lin_quad, w->Yo.p, w->cmean.p, w->csd.p, w->raw.p, w->fmean.p,
+                                        w->fsd.p, w->linW.p, w->sc.p, w->guess_scale, w->c.p);
   }
   if (S > nsamp) UFEM_CUDA_TRY(cudaMemsetAsync(w->u0.p, 0, (size_t)w->n * S * sizeof(double)));
   // u0(i, s) = sum_k Phi[i][k] c[s][k]
@@ -988,7 +1129,7 @@ int ufem_warm_create(ufem_model *m, const ufem_warm_options *o, ufem_warm **out)
   w->n = m->nDOFAct;
   int rv;
   std::vector<int> lg(o->n_feat);
-  for (int f = 0; f < o->n_feat; f++) lg[f] = o->feat_log[f] ? 1 : 0;
+  for (int f = 0; f < o->n_feat; f++) lg[f] = o->feat_log[f] == 2 ? 2 : (o->feat_log[f] ? 1 : 0);
   if ((rv = w->fcol.upload(o->feat_cols, o->n_feat)) || (rv = w->flog.upload(lg.data(), o->n_feat)) ||
       (rv = w->fmean.ensure(32)) || (rv = w->fsd.ensure(32)) || (rv = w->cmean.ensure(w->r)) ||
       (rv = w->csd.ensure(w->r)) ||
@@ -1102,7 +1243,7 @@ int ufem_warm_train(ufem_warm *w, long ntrain, const double *d_ifld, const ufem_
   // c[s][k] = sum_i U[i][s] Phi[i][k]
   if ((rv = gemm_f64((int)ntrain, r, n, w->U.p, 1, ntrain, w->phi.p, w->rb, 1, w->c.p, r, 1, w->part))) return rv;
   k_div_scale<<<grid1(ntrain * r), 256>>>(ntrain, r, w->sc.p, w->c.p);
-  k_col_stats<<<1, 128>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p);
+  if ((rv = fit_linear(w, ntrain))) return rv;
   k_targets<<<grid1(ntrain * r), 256>>>(ntrain, r, w->c.p, w->cmean.p, w->csd.p, w->Tt.p);
   UFEM_CUDA_TRY(cudaGetLastError());
   // 4. training: shuffled minibatches, cosine learning rate; every step is
@@ -1316,8 +1457,8 @@ int ufem_warm_solve(ufem_warm *w, long nsamp, const double *d_ifld, double *d_of
 
 int ufem_warm_set_guess_mode(ufem_warm *w, int mode) {
   if (!w) return UFEM_AF_ERR_EMP;
-  if (mode != 0 && mode != 1) {
-    set_error("ufem_warm_set_guess_mode: 0 (MLP) or 1 (POD-Galerkin)");
+  if (mode < 0 || mode > 2) {
+    set_error("ufem_warm_set_guess_mode: 0 (MLP), 1 (POD-Galerkin) or 2 (least-squares part alone)");
     return UFEM_AF_ERR_VAL;
   }
   w->o.guess_mode = mode;

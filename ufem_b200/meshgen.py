@@ -466,12 +466,14 @@ def warm_beam(nx=40, ny=10, nz=10, zones=16, lx=8.0, ly=2.0, lz=2.0, n_out_nodes
 
 
 def warm_features(model: Model):
-    """Network inputs of the warm start: the zone E values and the first tip
-    force (all tip forces share one random load factor), both as log|.|, and
-    the solution's scale column (the first tip force: u is linear in it)."""
+    """Network inputs of the warm start: the zone E values as compliances 1/E
+    (displacements of an elastic body are close to linear in them: for a
+    statically determinate beam, exactly so in beam theory) and the first tip
+    force (all tip forces share one random load factor) as log|.|, and the
+    solution's scale column (the first tip force: u is linear in it)."""
     nmat = len(model.mp_vals)
     cols = list(range(nmat)) + [nmat]
-    return cols, [1] * len(cols), nmat
+    return cols, [2] * nmat + [1], nmat
 
 
 def warm_samples(model: Model, nsamp: int, first_sample: int = 0, mesh_id: int = 5) -> np.ndarray:
