@@ -48,6 +48,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -60,11 +62,24 @@ WARM_EVAL = 8192
 EVAL_FIRST = 1 << 20     # evaluation sample ids: disjoint from training
 METRIC = "MC solves/s at rel-res 1e-8: learned+FP32/FP64 batched vs plain FP64 PCG, 1 B200"
 WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inputs), 8192 fresh samples "
-            "warm-started (POD 64 modes from 512 solves, Galerkin guess; MLP 17-256-256-64 trained on 4096 solves) "
-            "and coarse-corrected (PCG coarse space on {c} POD modes of the same snapshots)")
+            "warm-started by the learned guess (POD 64 modes from 512 solves; least-squares quadratic model of the "
+            "POD coefficients in the zone compliances 1/E + MLP 17-256-256-64 on its residual, trained on 4096 "
+            "solves) and solved by FP32 PCG with FP64 solution and true-residual replacement, preconditioner "
+            "coarse-corrected on {c} POD modes of the same snapshots")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
-          2: "k_batch_pcg<double,3,implicit>"}
+          2: "k_batch_pcg<double,3,implicit>", 3: "k_batch_pcg<float,3,implicit>"}
+PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
+        1: "FP32 PCG on explicit FP32 matrices, FP64 solution and true-residual replacement",
+        2: "FP64 PCG, blocks formed in the kernel from shared unit-E element blocks",
+        3: "FP32 PCG (FP32 vectors and products, blocks formed in the kernel from FP32 copies of the unit-E "
+           "blocks), FP64 solution and FP64 true-residual replacement"}
+GUESS = {0: "learned: least-squares quadratic model + MLP (BF16 tcgen05 network) of the POD coefficients",
+         1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s) on the learned POD basis",
+         2: "the least-squares quadratic model alone (no network)"}
+EPS_ORACLE = 1e-17 / 10000.0  # the reference's stopping rule, FEM_ZERO/10000 (fem/fem.h:59, fem/fem_sol.c:1722)
+FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (non-tensor) peak, datasheet figure: not measured here
+BRICK_FLOP = 2.3e5           # FP64 flops of the reference's 27-point brick integration per element
 
 
 def parse():
@@ -76,7 +91,7 @@ def parse():
     p.add_argument("--nsamp", type=int, default=NSAMP, help="samples per mesh of the uneven batch")
     p.add_argument("--train", type=int, default=WARM_TRAIN, help="warm-start training samples")
     p.add_argument("--eval", type=int, default=WARM_EVAL, help="warm-started samples per step and rank")
-    p.add_argument("--epochs", type=int, default=400, help="MLP training epochs")
+    p.add_argument("--epochs", type=int, default=100, help="MLP training epochs")
     p.add_argument("--plain-samples", type=int, default=16, help="samples timed by the plain method")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     p.add_argument("--no-other", action="store_true", help="skip the other precisions of the warm start")
@@ -85,16 +100,18 @@ def parse():
     p.add_argument("--coarse-modes", type=int, default=128,
                    help="POD modes of the preconditioner's coarse space (a multiple of 16, at most 128); the "
                         "guess and the MLP use the 64-mode basis of the learned-warm-start config")
-    p.add_argument("--big-modes", type=int, default=128,
-                   help="a second warm start whose guess also uses this many modes, reported beside (0: none)")
     p.add_argument("--no-static", action="store_true", help="skip the single-system configs (80x20x20, 128x128x64)")
     p.add_argument("--tiles-per-block", type=int, default=0, help=argparse.SUPPRESS)
-    p.add_argument("--guess", type=int, default=1,
-                   help="warm-start guess: 1 = each sample's POD-Galerkin coefficients on the learned basis "
-                        "(default), 0 = the MLP's coefficients")
-    p.add_argument("--precision", type=int, default=2,
-                   help="2: FP64 PCG, blocks formed in the kernel (default); 1: FP32 PCG on explicit FP32 "
-                        "matrices with FP64 solution and true-residual replacement; 0: FP64 explicit")
+    p.add_argument("--guess", type=int, default=0,
+                   help="warm-start guess: 0 = the learned coefficients (least-squares model + MLP, default), "
+                        "1 = each sample's POD-Galerkin coefficients on the learned basis, 2 = the least-squares "
+                        "model alone")
+    p.add_argument("--precision", type=int, default=3,
+                   help="3: FP32 PCG with FP64 solution and true-residual replacement, blocks formed in the kernel "
+                        "(default); 2: FP64 PCG, blocks formed in the kernel; 1: FP32 PCG on explicit FP32 "
+                        "matrices; 0: FP64 explicit")
+    p.add_argument("--oracle-samples", type=int, default=64,
+                   help="evaluation samples checked against the FP64 oracle (displacements, von Mises)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     p.add_argument("--ref-worker", nargs="*", help=argparse.SUPPRESS)
     p.add_argument("--profile-case", action="store_true",
@@ -113,6 +130,9 @@ def parse():
 
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
+           3: ("k_batch_pcg_fp32_coarse_40x10x10_2048samples.md",
+               "40x10x10 16 E zones x 2048 samples, FP32 implicit form, coarse space of a short warm-start "
+               "training, 40 iterations"),
            2: ("k_batch_pcg_coarse_40x10x10_1024samples.md",
                "40x10x10 16 E zones x 1024 samples, coarse space of a short warm-start training, 40 iterations")}
 
@@ -479,7 +499,7 @@ def uneven_section(a, rank, dev):
     ns = np.array([f.shape[0] for f in iflds], np.int64)
     null = (C.c_void_p * nm)()
     out = {"workload": UNEVEN}
-    for prec, label in ((1, "fp32_explicit_fp64_refinement"), (2, "fp64_implicit")):
+    for prec, label in ((1, "fp32_explicit_fp64_refinement"), (2, "fp64_implicit"), (3, "fp32_implicit_fp64_refinement")):
         opt = default_options()
         opt.precision = prec
         opt.tol = 1e-8
@@ -525,13 +545,31 @@ def static_section(a, peak):
         g.add_loads()
         g.add_disps()
         setup_s = time.perf_counter() - t0
+        # element integration + colour-ordered assembly (fem_fill_K(0)): the
+        # second call, CUDA events inside the library
+        fills = []
+        for _ in range(3):
+            g.fill_K(0)
+            fills.append(g.phase_ms()["fill"])
+        g.add_loads()
+        g.add_disps()
+        fill_ms = min(fills)
         b, nbr, nnzb = g.bsr_shape()
         n = g.ndof
         fill_ms = C.c_double(); bc_ms = C.c_double(); sol_ms = C.c_double(); res_ms = C.c_double()
         L = g.L if hasattr(g, "L") else None
         from ufem_b200 import _lib
         L = _lib.load()
-        res = {"ndof": n, "blocks": nnzb, "setup_s": setup_s}
+        res = {"ndof": n, "blocks": nnzb, "setup_s": setup_s,
+               "fill_K": {"ms": fill_ms, "elements": int(m.eLen),
+                          "elements_per_s": m.eLen / (fill_ms / 1000.0),
+                          "reference_equivalent_TFLOPs": m.eLen * BRICK_FLOP / (fill_ms / 1000.0) / 1e12,
+                          "frac_of_nominal_fp64": m.eLen * BRICK_FLOP / (fill_ms / 1000.0) / 1e12
+                          / FP64_NOMINAL_TFLOPS,
+                          "note": "integration of every brick (closed-form isotropic H^T D H at 27 points) and "
+                                  "the colour-ordered scatter into the block-sparse K; FLOPs counted as the "
+                                  "reference's 2.3e5 per brick (27 x (H^T D + (H^T D) H)); FP64 peak: the "
+                                  "B200 datasheet's 37 TFLOP/s, not measured"}}
         g.set_u(np.zeros(n))
         g.solve(api.SOLVER_CGWJ, api.STOP_RELRES, 1e-12, 0)
         uref = g.u()
@@ -558,6 +596,130 @@ def static_section(a, peak):
         out[name] = res
         del g
     return out
+
+
+def _von_mises(sig):
+    """von Mises stress of (SX, SY, SZ, SYZ, SZX, SXY) records."""
+    sx, sy, sz, syz, szx, sxy = (sig[..., k] for k in range(6))
+    return (0.5 * ((sx - sy) ** 2 + (sy - sz) ** 2 + (sz - sx) ** 2) + 3.0 * (sxy ** 2 + syz ** 2 + szx ** 2)) ** 0.5
+
+
+def _oracle_job(job):
+    """One process of the oracle leg: the samples' static solves by the C
+    restatement of the reference (oracle/ufem_oracle.c).  eps > 0: the
+    reference's own stopping rule (FEM_ZERO/10000: converged to FP64, the
+    checker); eps < 0: the relative residual |eps| (the CPU leg at the GPU's
+    tolerance).  Returns per sample (u, von Mises at the brick's stored
+    points 1-19, iterations, seconds)."""
+    from oracle.oracle import OracleModel
+    from ufem_b200 import meshgen as mg
+    model, rows, eps, want_fields = job
+    out = []
+    for row in rows:
+        ms = mg.model_for_sample(model, row)
+        t0 = time.perf_counter()
+        o = OracleModel(ms).run_static(eps=eps)
+        dt = time.perf_counter() - t0
+        out.append((o["u"] if want_fields else None, _von_mises(o["sig"][:, :19, :]) if want_fields else None,
+                    o["iters"], dt, o["rv_solve"]))
+    return out
+
+
+def oracle_leg(model, rows, eps, procs, want_fields=True):
+    """The oracle over `rows` in `procs` spawned processes (spawned: this
+    process already holds a CUDA context); returns the per-sample results and
+    the wall time."""
+    import multiprocessing as mp
+    chunks = [rows[i::procs] for i in range(procs) if len(rows[i::procs])]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(len(chunks)) as pool:
+        parts = pool.map(_oracle_job, [(model, c, eps, want_fields) for c in chunks])
+    wall = time.perf_counter() - t0
+    res = [None] * len(rows)
+    for i, part in enumerate(parts):
+        for j, r in enumerate(part):
+            res[i + j * len(chunks)] = r
+    return res, wall
+
+
+def warm_run(L, ws, d, guess, precision, coarse, steps, tol=1e-8):
+    """ufem_warm_solve with the given guess, precision and coarse correction:
+    one warm-up call, then `steps` timed calls (CUDA events)."""
+    import ctypes as C
+    import torch
+    from ufem_b200 import _lib
+    from ufem_b200.mc import default_options
+    n = d["in"].shape[0]
+    L.ufem_warm_set_guess_mode(ws.h, guess)
+    o = default_options()
+    o.precision = precision
+    o.tol = tol
+    o.coarse = int(bool(coarse))
+    st = _lib.WarmStats()
+    args = (ws.h, n, d["in"].data_ptr(), d["out"].data_ptr(), d["st"].data_ptr(), d["it"].data_ptr(), C.byref(o),
+            C.byref(st))
+    _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pcg_ms = pcg_by = 0.0
+    for _ in range(steps):
+        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args))
+        pcg_ms += st.pcg_ms
+        pcg_by += st.pcg_bytes
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    it = d["it"].cpu().numpy()
+    return {"guess": GUESS[guess], "precision": PREC[precision], "coarse": bool(coarse),
+            "value": n / (ms / 1000.0), "unit": "solves/s", "ms_per_step": ms, "iters_mean": float(it.mean()),
+            "iters_max": int(it.max()), "guess_rel_err_mean": st.guess_err_mean, "guess_rel_err_max": st.guess_err_max,
+            "fallbacks": st.fallbacks, "all_converged": bool(np.isin(d["st"].cpu().numpy(), [0, 4]).all()),
+            "pcg_GBs": pcg_by / (pcg_ms / 1000.0) / 1e9 if pcg_ms else None}, d["out"].cpu().numpy().copy()
+
+
+def solve_u(L, g, ws, rows, guess, precision, coarse, tol=1e-8):
+    """The displacements of `rows` by the same method (ufem_warm_guess, then
+    the batched solve from the guesses), u [nsamp][ndof]."""
+    import ctypes as C
+    import torch
+    from ufem_b200 import _lib
+    from ufem_b200.mc import default_options
+    L.ufem_warm_set_guess_mode(ws.h, guess)
+    u0 = ws.guess(rows)
+    n = rows.shape[0]
+    S = max(128, (n + 127) // 128 * 128)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d_in, d_g = t(rows), t(u0)
+    d_out = torch.zeros((n, max(1, g.model.mc_olen)), dtype=torch.float64, device="cuda")
+    d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_it = torch.zeros(n, dtype=torch.int64, device="cuda")
+    d_u = torch.zeros((g.ndof, S), dtype=torch.float64, device="cuda")
+    vp = lambda x: (C.c_void_p * 1)(x.data_ptr())
+    o = default_options()
+    o.precision = precision
+    o.tol = tol
+    o.coarse = int(bool(coarse))
+    _lib.check("ufem_mc_solve_device", L.ufem_mc_solve_device(
+        1, (C.c_void_p * 1)(g.h.value), np.array([n], np.int64).ctypes.data_as(C.POINTER(C.c_long)), vp(d_in),
+        vp(d_out), vp(d_st), vp(d_it), vp(d_g), vp(d_u), C.byref(o)))
+    return d_u[:, :n].T.cpu().numpy(), d_st.cpu().numpy()
+
+
+def gpu_von_mises(model, row, u):
+    """von Mises at the stored points 1-19 from the GPU result pass on u."""
+    from ufem_b200 import meshgen as mg
+    from ufem_b200.api import GpuModel
+    ms = mg.model_for_sample(model, row)
+    gs = GpuModel(ms)
+    gs.fill_K(0)
+    gs.add_loads()
+    gs.add_disps()
+    gs.set_u(u)
+    gs.fill_K(1)
+    _, vm = gs.stresses(ms.eLen, False)
+    gs.close()
+    return vm.reshape(ms.eLen, 27)[:, :19]
 
 
 def ours(a):
@@ -651,6 +813,9 @@ def ours(a):
     iters = d_it.cpu().numpy()
     out_warm = d_out.cpu().numpy().copy()
     warm_info = {f: getattr(wst, f) for f, _ in wst._fields_}
+    mcs = _lib.McStats()
+    L.ufem_mc_get_stats(C.byref(mcs))
+    phases = {k: round(mcs.phase_wall_ms[i], 3) for i, k in enumerate(["init", "S", "U", "R", "C1", "C3"])}
 
     # ---- e2e: host (pinned) inputs -> device -> ufem_warm_solve -> host outputs
     h_in = torch.from_numpy(ev).pin_memory()
@@ -673,15 +838,31 @@ def ours(a):
     d2h = h_out.numel() * 8 + h_st.numel() * 4 + h_it.numel() * 8
     e2e_ok = bool(np.array_equal(h_out.numpy(), out_warm))
 
-    # ---- the same samples without the warm start (one batched launch) --------
+    # ---- the same samples by the other forms: guess x precision x coarse ----
+    dd = {"in": d_in, "out": d_out, "st": d_st, "it": d_it}
+    forms = []
+    if not a.no_other:
+        combos = [(a.guess, a.precision, 0), (a.guess, 2, 1), (a.guess, 2, 0), (1, a.precision, 1), (1, 2, 1),
+                  (2, a.precision, 1), (a.guess, 1, 0), (a.guess, 0, 0)]
+        seen = {(a.guess, a.precision, opt.coarse)}
+        for gm, pr, co in combos:
+            if (gm, pr, co) in seen:
+                continue
+            seen.add((gm, pr, co))
+            row, out_f = warm_run(L, ws, dd, gm, pr, co, 1 if pr in (0, 1) else a.steps)
+            row["outputs_max_rel_diff_vs_headline"] = float(np.abs(out_f - out_warm).max() / np.abs(out_warm).max())
+            forms.append(row)
+        L.ufem_warm_set_guess_mode(ws.h, a.guess)
+
+    # ---- the same samples without a guess (one batched launch) --------------
     one = np.array([n], np.int64).ctypes.data_as(C.POINTER(C.c_long))
     d_out2 = torch.zeros_like(d_out)
     d_st2 = torch.zeros_like(d_st)
     d_it2 = torch.zeros_like(d_it)
 
-    def cold_run(coarse):
+    def cold_run(precision, coarse):
         o = default_options()
-        o.precision = a.precision
+        o.precision = precision
         o.tol = 1e-8
         o.coarse = coarse
         cold_args = (1, (C.c_void_p * 1)(g.h.value), one, _vp([d_in]), _vp([d_out2]), _vp([d_st2]), _vp([d_it2]),
@@ -694,130 +875,18 @@ def ours(a):
         cold_ms = e0.elapsed_time(e1)
         it_cold = d_it2.cpu().numpy()
         out_cold = d_out2.cpu().numpy()
-        return {"value": n / (cold_ms / 1000.0), "unit": "solves/s", "iters_mean": float(it_cold.mean()),
-                "iters_max": int(it_cold.max()), "all_converged": bool((d_st2.cpu().numpy() == 0).all()),
+        return {"precision": PREC[precision], "coarse": bool(coarse), "value": n / (cold_ms / 1000.0),
+                "unit": "solves/s", "iters_mean": float(it_cold.mean()), "iters_max": int(it_cold.max()),
+                "all_converged": bool((d_st2.cpu().numpy() == 0).all()),
                 "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}
 
-    # Jacobi PCG from zero: the batched solver alone
-    cold = cold_run(0)
-    cold["method"] = "Jacobi PCG from zero"
+    cold = cold_run(a.precision, 0)
+    cold["method"] = "PCG from zero, Jacobi preconditioner"
     cold_coarse = None
     if tstats["coarse_modes"] and opt.coarse:
-        cold_coarse = cold_run(1)
+        cold_coarse = cold_run(a.precision, 1)
         cold_coarse["method"] = f"PCG from zero, Jacobi + coarse correction on {tstats['coarse_modes']} POD modes"
     del d_out2, d_st2, d_it2
-
-    # ---- the warm start without the coarse correction -----------------------
-    no_coarse = None
-    if tstats["coarse_modes"] and opt.coarse and not a.no_other:
-        opt_nc = default_options()
-        opt_nc.precision = a.precision
-        opt_nc.tol = 1e-8
-        opt_nc.coarse = 0
-        wst4 = _lib.WarmStats()
-        args4 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt_nc),
-                 C.byref(wst4))
-        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args4))
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(a.steps):
-            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args4))
-        e1.record()
-        torch.cuda.synchronize()
-        ms4 = e0.elapsed_time(e1) / a.steps
-        no_coarse = {"method": "same warm start, Jacobi PCG (no coarse correction)", "value": n / (ms4 / 1000.0),
-                     "unit": "solves/s", "iters_mean": wst4.iters_mean, "iters_max": wst4.iters_max,
-                     "pcg_GBs": wst4.pcg_bytes / (wst4.pcg_ms / 1000.0) / 1e9 if wst4.pcg_ms else None,
-                     "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
-                     "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
-                                                               / np.abs(out_warm).max())}
-
-    # ---- the other guess (MLP <-> POD-Galerkin), same precision ------------
-    GUESS = {0: "the MLP's POD coefficients (BF16 tcgen05 network, 17 inputs -> 64 coefficients)",
-             1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s from the per-zone reduced "
-                "operators) on the learned POD basis"}
-    galerkin = None
-    if not a.no_other:
-        L.ufem_warm_set_guess_mode(ws.h, 1 - a.guess)
-        wst3 = _lib.WarmStats()
-        args3 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt),
-                 C.byref(wst3))
-        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args3))
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(a.steps):
-            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args3))
-        e1.record()
-        torch.cuda.synchronize()
-        ms3 = e0.elapsed_time(e1) / a.steps
-        galerkin = {"guess": GUESS[1 - a.guess], "value": n / (ms3 / 1000.0),
-                    "unit": "solves/s", "iters_mean": wst3.iters_mean, "iters_max": wst3.iters_max,
-                    "guess_rel_err_mean": wst3.guess_err_mean, "guess_rel_err_max": wst3.guess_err_max,
-                    "fallbacks": wst3.fallbacks, "ms_guess": wst3.ms_guess,
-                    "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
-                    "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
-                                                              / np.abs(out_warm).max())}
-        L.ufem_warm_set_guess_mode(ws.h, a.guess)
-
-    # ---- a larger basis: the same samples with a separately trained warm
-    # start of --big-modes modes (guess and coarse space), same precision.
-    # Its training sets its coarse space on the model: this runs after every
-    # precision-2 section of the headline warm start.
-    big = None
-    if a.big_modes and a.big_modes != 64 and not a.no_other:
-        wsb = WarmStart(g, cols, logs, scale_col, n_modes=a.big_modes, n_hidden=256, n_snapshots=512,
-                        epochs=a.epochs, batch=256, lr=2e-3, n_coarse=max(a.coarse_modes, a.big_modes))
-        tsb = wsb.train(train, precision=a.precision)
-        wsb.set_guess_mode(a.guess)
-        wstb = _lib.WarmStats()
-        argsb = (wsb.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt),
-                 C.byref(wstb))
-        _lib.check("ufem_warm_solve", L.ufem_warm_solve(*argsb))
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(a.steps):
-            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*argsb))
-        e1.record()
-        torch.cuda.synchronize()
-        msb = e0.elapsed_time(e1) / a.steps
-        big = {"modes": a.big_modes, "coarse_modes": tsb["coarse_modes"], "value": n / (msb / 1000.0),
-               "unit": "solves/s", "ms_per_step": msb, "iters_mean": wstb.iters_mean, "iters_max": wstb.iters_max,
-               "guess_rel_err_mean": wstb.guess_err_mean, "fallbacks": wstb.fallbacks,
-               "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
-               "outputs_max_rel_diff_vs_headline": float(np.abs(d_out.cpu().numpy() - out_warm).max()
-                                                         / np.abs(out_warm).max())}
-        del wsb
-
-    # ---- the warm start at the other precisions (one warm-up, one timed step)
-    PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
-            1: "FP32 PCG on explicit FP32 matrices, FP64 solution and true-residual replacement",
-            2: "FP64 PCG, blocks formed in the kernel from shared unit-E element blocks"}
-    other = {}
-    if not a.no_other:
-        for p_alt in (1, 0):
-            if p_alt == a.precision:
-                continue
-            opt_alt = default_options()
-            opt_alt.precision = p_alt
-            opt_alt.tol = 1e-8
-            wst2 = _lib.WarmStats()
-            args2 = (ws.h, n, d_in.data_ptr(), d_out.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), C.byref(opt_alt),
-                     C.byref(wst2))
-            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args2))
-            torch.cuda.synchronize()
-            e0.record()
-            _lib.check("ufem_warm_solve", L.ufem_warm_solve(*args2))
-            e1.record()
-            torch.cuda.synchronize()
-            ms2 = e0.elapsed_time(e1)
-            other[str(p_alt)] = {"method": PREC[p_alt], "value": n / (ms2 / 1000.0), "unit": "solves/s",
-                                 "iters_mean": wst2.iters_mean, "iters_max": wst2.iters_max,
-                                 "all_converged": bool(np.isin(d_st.cpu().numpy(), [0, 4]).all()),
-                                 "pcg_GBs": wst2.pcg_bytes / (wst2.pcg_ms / 1000.0) / 1e9 if wst2.pcg_ms else None,
-                                 "outputs_max_rel_diff": float(np.abs(d_out.cpu().numpy() - out_warm).max()
-                                                               / np.abs(out_warm).max())}
-            if p_alt == 0:
-                break  # FP64 explicit needs the most memory: last
 
     result = None
     if rank == 0:
@@ -831,17 +900,50 @@ def ours(a):
         plain_t = time.perf_counter() - t0
         plain = sub.shape[0] / plain_t
         plain_diff = float(np.abs(o_plain - out_warm[:sub.shape[0]]).max() / np.abs(o_plain).max())
+        # ---- the headline method against the FP64 oracle ----------------------
+        parity, cpu_matched = None, None
+        procs = host_cores()
+        if a.oracle_samples > 0 and not a.no_cpu:
+            rows = ev[:a.oracle_samples]
+            u_gpu, st_gpu = solve_u(L, g, ws, rows, a.guess, a.precision, opt.coarse)
+            L.ufem_warm_set_guess_mode(ws.h, a.guess)
+            tight, tight_wall = oracle_leg(m, rows, EPS_ORACLE, procs)
+            eu = evm = eo = 0.0
+            rows_d = [(int(r[2]), int(r[3]), int(r[0])) for r in m.mc_vars[m.mc_ilen:] if r[1] == mg.MONTE_VTYPE_RES_D]
+            ndf = g.ndoffld(m.nLen)
+            for s in range(rows.shape[0]):
+                uo, vmo = tight[s][0], tight[s][1]
+                eu = max(eu, float(np.abs(u_gpu[s] - uo).max() / np.abs(uo).max()))
+                vm = gpu_von_mises(m, rows[s], u_gpu[s])
+                evm = max(evm, float(np.abs(vm - vmo).max() / np.abs(vmo).max()))
+                want = np.array([uo[ndf[node * 7 + d - 1] - 1] for node, d, _ in rows_d])
+                got = out_warm[s, [p for _, _, p in rows_d]]
+                eo = max(eo, float(np.abs(got - want).max() / np.abs(want).max()))
+            parity = {"samples": int(rows.shape[0]), "method": "the headline's guess, precision and coarse space, "
+                      "solved to true relative residual 1e-8",
+                      "oracle": "oracle/ufem_oracle.c (the reference's assembly and femEqsCGwJ restated, pinned "
+                                "bit-exact against the reference build), reference stopping rule FEM_ZERO/10000",
+                      "u_rel_err_vs_oracle": eu, "vm_rel_err_vs_oracle": evm,
+                      "outputs_rel_err_vs_oracle": eo, "all_converged": bool((st_gpu == 0).all()),
+                      "vm_points": "the brick's stored result points 1-19 of every element (fem/fem_e009.c:825)",
+                      "errors": "max over samples of max|x - x_oracle| / max|x_oracle|"}
+            # the CPU leg at the GPU's tolerance: the oracle's Jacobi PCG to
+            # relative residual 1e-8, one process per host core
+            matched, wall = oracle_leg(m, rows, -1e-8, procs, want_fields=False)
+            cpu_matched = {"value": rows.shape[0] / wall, "unit": "solves/s", "cores": procs, "kind": "port",
+                           "iters_mean": float(np.mean([r[2] for r in matched])),
+                           "sample": f"{rows.shape[0]} evaluation samples, oracle Jacobi PCG (femEqsCGwJ restated) "
+                                     f"to relative residual 1e-8 with assembly, {procs} processes ({wall:.1f} s)",
+                           "oracle_tight_wall_s": tight_wall}
         uneven = None if a.no_uneven else uneven_section(a, rank, dev)
         peak, peak_kind = measured_peaks()
         static = None if a.no_static else static_section(a, peak)
         achieved = pcg_bytes / (pcg_ms / 1000.0) / 1e9 if pcg_ms > 0 else 0.0
-        # DRAM traffic per launch: the ncu-measured traffic / algorithmic
-        # ratio of this kernel (profiles/, a smaller case of the same kernel)
-        # times this run's algorithmic bytes per launch
+        # DRAM traffic per launch: the ncu-measured traffic / algorithmic ratio
+        # of this kernel (profiles/, a smaller case of the same kernel) times
+        # this run's algorithmic bytes per launch
         traffic = None
         pf = PROFILE.get(a.precision, ("none", ""))[0]
-        if a.precision == 2 and not (tstats["coarse_modes"] and opt.coarse):
-            pf = "k_batch_pcg_implicit_40x10x10_1024samples.md"  # the Jacobi-only instance
         tf = os.path.join(ROOT, "profiles", pf)
         if os.path.exists(tf) and pcg_launches > 0:
             for line in open(tf):
@@ -850,22 +952,23 @@ def ours(a):
         # ---- CPU baseline: the reference on a bounded sample ------------------
         cpu = None
         if os.path.exists(REF_LIB) and not a.no_cpu:
-            procs = host_cores()
             with tempfile.TemporaryDirectory() as d:
                 files = ref_files([m], [ev[:max(1, procs)]], d)
                 nref, wall = run_reference_sample(files, procs, 1, d)
             cpu = {"value": nref / wall, "unit": "solves/s", "cores": procs, "kind": "reference",
-                   "sample": f"{procs} processes x 1 evaluation sample via monte_solution, SSOR PCG ({wall:.1f} s)"}
+                   "sample": f"{procs} processes x 1 evaluation sample via monte_solution, SSOR PCG to the "
+                             f"reference's rule ({wall:.1f} s)",
+                   "matched_tolerance": cpu_matched}
         s2 = tstats["sigma2"][:64]
         result = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if a.precision != 1 else "fp32 inner / fp64 refinement",
+            "vs_baseline": None, "dtype": "fp32 inner / fp64 refinement" if a.precision in (1, 3) else "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(c=a.coarse_modes), "samples_per_step": solves_step, "rel_res": 1e-8, "ndof": g.ndof,
-                       "precision": PREC[a.precision],
-                       "l2_flush": "not needed: every per-sample vector is 0.98 GB (FP64, 8192 samples) and the "
-                                   "explicit FP32 values 34 GB per iteration, >> 126 MB L2",
+            "config": {"workload": WORKLOAD.format(c=a.coarse_modes), "samples_per_step": solves_step, "rel_res": 1e-8,
+                       "ndof": g.ndof, "precision": PREC[a.precision], "guess": GUESS[a.guess],
+                       "l2_flush": "not needed: every per-sample vector is 0.49 GB (FP32) / 0.98 GB (FP64) at "
+                                   "8192 samples, >> 126 MB L2",
                        "parallelism": f"samples sharded over {world} GPU(s), no collective"},
             "all_converged": bool(np.isin(status, [0, 4]).all()),
             "warm_start": {"guess": GUESS[a.guess], "coarse_modes": tstats["coarse_modes"] if opt.coarse else 0,
@@ -876,27 +979,26 @@ def ours(a):
                            "guess_rel_err_max": warm_info["guess_err_max"],
                            "fallback_rate": fallbacks / max(1, n * a.steps), "cold_cap": warm_info["cold_cap"],
                            "ms_guess": warm_info["ms_guess"], "ms_solve": warm_info["ms_solve"],
+                           "pcg_phase_wall_ms": phases, "true_residual_passes": mcs.true_residual_passes,
                            "train": {"samples": int(train.shape[0]), "seconds": train_s,
                                      "cold_iters_mean": tstats["cold_iters_mean"],
                                      "ms_solve": tstats["ms_solve"], "ms_basis": tstats["ms_basis"],
                                      "ms_mlp": tstats["ms_train"], "epochs": tstats["epochs"],
                                      "loss_first": tstats["loss_first"], "loss_last": tstats["loss_last"],
                                      "pod_energy_mode64_over_mode1": (s2[63] / s2[0]) if s2[0] else None}},
-            "batched_without_warm_start": cold,
+            "oracle_parity": parity,
+            "other_forms": forms,
+            "batched_without_guess": cold,
             "batched_coarse_without_guess": cold_coarse,
-            "warm_start_without_coarse": no_coarse,
-            "warm_start_other_precisions": other,
-            "warm_start_other_guess": galerkin,
-            "warm_start_larger_basis": big,
             "plain_fp64_one_at_a_time": {"value": plain, "unit": "solves/s", "samples_timed": int(sub.shape[0]),
                                          "iters_mean": float(it_plain.mean()),
                                          "outputs_max_rel_diff_vs_warm": plain_diff},
             "speedup_vs_plain": value / plain,
             "roofline": {"bound": "hbm",
                          "kernel": KERNEL[a.precision] + (" + coarse phases (tcgen05)"
-                                                          if tstats["coarse_modes"] and opt.coarse else ""), "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "pcg_ms_per_step": pcg_ms / a.steps,
+                                                          if tstats["coarse_modes"] and opt.coarse else ""),
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "pcg_ms_per_step": pcg_ms / a.steps,
                          "pcg_launches_per_step": pcg_launches / a.steps},
             "e2e": {"value": solves_step / (e2e_ms / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "matches_device_run": e2e_ok},

@@ -480,3 +480,24 @@ def warm_samples(model: Model, nsamp: int, first_sample: int = 0, mesh_id: int =
     """Warm-start inputs: zone E = 30 GPa * exp(0.15 z) (median 30 GPa), load
     factor U(0.8, 1.2).  Training and evaluation draw disjoint sample ids."""
     return mc_samples(model, mesh_id=mesh_id, nsamp=nsamp, first_sample=first_sample, mean_one=False)
+
+
+def model_for_sample(model: Model, row) -> Model:
+    """A copy of ``model`` with one Monte Carlo sample's inputs applied, as
+    monte_solution applies ifld before solving (fem/fem_mont.c:715-800): E
+    of materials (``MONTE_VTYPE_MAT`` / MAT_EX) and nodal force values
+    (``MONTE_VTYPE_NLD``)."""
+    import copy
+    ms = copy.deepcopy(model)
+    ms.mp_vals = [v.copy() for v in model.mp_vals]
+    ms.nl_val = model.nl_val.copy()
+    for var in model.mc_vars[:model.mc_ilen]:
+        pos, ty, item, sub, it = [int(x) for x in var]
+        if ty == MONTE_VTYPE_MAT and sub == MAT_EX:
+            ms.mp_vals[item][1] = row[pos]
+        elif ty == MONTE_VTYPE_NLD:
+            for j in range(len(ms.nl_node)):
+                if ms.nl_node[j] == item and ms.nl_type[j] == sub and ms.nl_dir[j] == it:
+                    ms.nl_val[j] = row[pos]
+                    break
+    return ms
