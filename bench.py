@@ -690,7 +690,9 @@ def solve_u(L, g, ws, rows, guess, precision, coarse, tol=1e-8):
     n = rows.shape[0]
     S = max(128, (n + 127) // 128 * 128)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    d_in, d_g = t(rows), t(u0)
+    g0 = np.zeros((g.ndof, S))
+    g0[:, :n] = u0.T  # the device guess layout: [nDOFAct][S], sample fastest
+    d_in, d_g = t(rows), t(g0)
     d_out = torch.zeros((n, max(1, g.model.mc_olen)), dtype=torch.float64, device="cuda")
     d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
     d_it = torch.zeros(n, dtype=torch.int64, device="cuda")

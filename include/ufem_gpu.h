@@ -262,7 +262,9 @@ int ufem_mc_solve_serial(ufem_model *m, long nsamp, const double *ifld, double *
                          double tol);
 
 /* Same, with every input and output already in device memory (for timing the
- * kernels without host transfers). */
+ * kernels without host transfers).  d_u_guess[k] and d_u_out[k] (either may
+ * be NULL) are [nDOFAct][S] with S = nsamp[k] rounded up to a multiple of
+ * 128 -- DOF-major, sample fastest, the solver's own layout. */
 int ufem_mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp,
                          const double *const *d_ifld, double *const *d_ofld, int *const *d_status,
                          long *const *d_iters, const double *const *d_u_guess,

@@ -100,7 +100,9 @@ def _solve_from(g, ifld, u0, precision, tol):
     d_out = torch.zeros((n, max(1, g.model.mc_olen)), dtype=torch.float64, device="cuda")
     d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
     d_it = torch.zeros(n, dtype=torch.int64, device="cuda")
-    d_g = torch.from_numpy(np.ascontiguousarray(u0)).cuda()
+    g0 = np.zeros((g.ndof, S))
+    g0[:, :n] = u0.T  # the device guess layout: [nDOFAct][S], sample fastest
+    d_g = torch.from_numpy(g0).cuda()
     d_u = torch.zeros((g.ndof, S), dtype=torch.float64, device="cuda")
     vp = lambda t: (C.c_void_p * 1)(t.data_ptr())
     opt = default_options()
