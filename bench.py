@@ -553,7 +553,7 @@ def static_section(a, peak):
             fills.append(g.phase_ms()["fill"])
         g.add_loads()
         g.add_disps()
-        fill_ms = min(fills)
+        fill_best = min(fills)
         b, nbr, nnzb = g.bsr_shape()
         n = g.ndof
         fill_ms = C.c_double(); bc_ms = C.c_double(); sol_ms = C.c_double(); res_ms = C.c_double()
@@ -561,10 +561,10 @@ def static_section(a, peak):
         from ufem_b200 import _lib
         L = _lib.load()
         res = {"ndof": n, "blocks": nnzb, "setup_s": setup_s,
-               "fill_K": {"ms": fill_ms, "elements": int(m.eLen),
-                          "elements_per_s": m.eLen / (fill_ms / 1000.0),
-                          "reference_equivalent_TFLOPs": m.eLen * BRICK_FLOP / (fill_ms / 1000.0) / 1e12,
-                          "frac_of_nominal_fp64": m.eLen * BRICK_FLOP / (fill_ms / 1000.0) / 1e12
+               "fill_K": {"ms": fill_best, "elements": int(m.eLen),
+                          "elements_per_s": m.eLen / (fill_best / 1000.0),
+                          "reference_equivalent_TFLOPs": m.eLen * BRICK_FLOP / (fill_best / 1000.0) / 1e12,
+                          "frac_of_nominal_fp64": m.eLen * BRICK_FLOP / (fill_best / 1000.0) / 1e12
                           / FP64_NOMINAL_TFLOPS,
                           "note": "integration of every brick (closed-form isotropic H^T D H at 27 points) and "
                                   "the colour-ordered scatter into the block-sparse K; FLOPs counted as the "
