@@ -65,10 +65,6 @@ struct McOut {
   int reac;    // reaction index
 };
 
-// FP32 unit blocks of the implicit form: B*B values padded to 12 floats
-// (three 16-byte loads per contribution)
-constexpr int kW32Stride = 12;
-
 struct McPlan {
   bool built = false;
   int s = 0;                       // element matrix size (8 or 24)
@@ -94,7 +90,6 @@ struct McPlan {
   std::vector<int> mult_col;
   DBuf<int> d_mult_col, cptr, crow;  // contributions of block k / of block row I
   DBuf<double> cval;               // [nc][cstride]: B*B values, then (multiplier << 32 | J)
-  DBuf<float> w32;                 // [nc][12]: the B*B values in FP32 (precision 3's SpMV)
   DBuf<int> sperm;                 // block rows in the order the gathering phases visit them
   long nc = 0;
   // coarse space of the preconditioner (ufem_mc_set_coarse): Wc [n][cmodes]
@@ -390,10 +385,6 @@ static int build_implicit(ufem_model *m, McPlan *P) {
   P->cstride = stride;
   P->nc = cptr[m->nnzb];
   if (cval.empty()) cval.assign(stride, 0.0);
-  std::vector<float> w32((size_t)std::max<long>(1, P->nc) * kW32Stride, 0.0f);
-  for (long c = 0; c < P->nc; c++)
-    for (int t = 0; t < BB; t++) w32[(size_t)c * kW32Stride + t] = (float)cval[(size_t)c * stride + t];
-  if ((rv = P->w32.upload(w32.data(), w32.size()))) return rv;
   if ((rv = P->cptr.upload(cptr.data(), cptr.size())) || (rv = P->cval.upload(cval.data(), cval.size())) ||
       (rv = P->crow.upload(crow.data(), crow.size())) ||
       (rv = P->d_mult_col.upload(P->mult_col.data(), P->mult_col.size())))
@@ -714,7 +705,6 @@ struct BMesh {
   const int *sperm;     // block rows in the visiting order of the gathering phases
   const double *cval;
   const double *mult;
-  const float *w32;     // FP32 copies of the unit blocks (precision 3)
   const unsigned char *fixed;
   int cstride;
   int nmult;            // multipliers (rows of mult)
@@ -819,22 +809,20 @@ __device__ __forceinline__ void prof_flush(unsigned long long *prof) {
 extern __shared__ __align__(1024) uint8_t s_dyn_smem[];
 
 // acc[a][v] += mult[var_c][s] * (W_c X_{J_c})[a] over the contributions
-// [c0, c1) of one block row of the implicit form.  The row's contribution
-// keys (multiplier << 32 | J) are fetched 32 at a time, one per lane, and
-// broadcast; the gathers of U contributions are issued together so that U
-// neighbour loads are in flight per warp.  W and the multipliers are
-// read-only for the whole kernel (non-coarse loads); X is written by other
-// blocks during the kernel (L2 loads).  LT is the kernel's lane layout
-// (double: sample pairs 64 apart; float: 4 adjacent samples), XT the type of
-// X, CT the type of the products and sums: FP64 (W and the multipliers in
-// FP64) or FP32 (W from the FP32 copies, the multipliers rounded).  With
-// s_mult the multipliers come from the tile's shared-memory copy
-// ([nmult][GS] of CT, sample sl of the group) instead of global memory.
-template <typename LT, typename XT, typename CT, int B, int VN, int U, bool SMULT>
+// [c0, c1) of one block row of the implicit form, in FP64.  The row's
+// contribution keys (multiplier << 32 | J) are fetched 32 at a time, one per
+// lane, and broadcast; the gathers of U contributions are issued together so
+// that U neighbour loads are in flight per warp.  W and the multipliers are
+// read-only for the whole kernel (non-coherent loads); X is written by other
+// blocks during the kernel (loads after the phase's grid barrier).  LT is the
+// kernel's lane layout (double: sample pairs 64 apart; float: 4 adjacent
+// samples), XT the type of X (the FP32 kernel gathers FP32 z, and FP64 x for
+// its true residuals).  SMULT: the multipliers come from the tile's
+// shared-memory copy ([nmult][GS] doubles) instead of global memory.
+template <typename LT, typename XT, int B, int VN, int U, bool SMULT>
 __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, int cstride,
-                                             const float *__restrict__ w32, const double *__restrict__ mult,
-                                             const CT *s_mult, const XT *X, int S, int sb, int sl, int c0, int c1,
-                                             CT (&acc)[B][VN]) {
+                                             const double *__restrict__ mult, const double *s_mult, const XT *X,
+                                             int S, int sb, int c0, int c1, double (&acc)[B][VN]) {
   static_assert(sizeof(XT) == 8 || sizeof(LT) == 4, "FP32 vectors only in the FP32 lane layout");
   constexpr int GS = 32 * VN;
   const int lane = threadIdx.x & 31;
@@ -860,49 +848,36 @@ __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, in
 #pragma unroll
       for (int u = 0; u < U; u++) {
         if (j + u >= cnt) break;
-        CT W[B * B];
-        if constexpr (sizeof(CT) == 8) {
-          const double *w = cval + (size_t)(cb + j + u) * cstride;
+        const double *w = cval + (size_t)(cb + j + u) * cstride;
+        double W[B * B];
 #pragma unroll
-          for (int h = 0; h < (B * B) / 2; h++) {
-            const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
-            W[2 * h] = v.x;
-            W[2 * h + 1] = v.y;
-          }
-          if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
-        } else {
-          const float4 *w = reinterpret_cast<const float4 *>(w32 + (size_t)(cb + j + u) * kW32Stride);
-#pragma unroll
-          for (int h = 0; h < (B * B + 3) / 4; h++) {
-            const float4 v = __ldg(w + h);
-            const float e[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-              if (4 * h + q < B * B) W[4 * h + q] = e[q];
-          }
+        for (int h = 0; h < (B * B) / 2; h++) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
+          W[2 * h] = v.x;
+          W[2 * h + 1] = v.y;
         }
-        CT a[VN];
+        if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
+        double a[VN];
         if constexpr (SMULT) {
-          const CT *sm = s_mult + vars[u] * GS;
+          const double *sm = s_mult + vars[u] * GS;
 #pragma unroll
           for (int v = 0; v < VN; v++) a[v] = sm[lane_sample<LT, VN>(lane, v)];
         } else {
 #pragma unroll
-          for (int v = 0; v < VN; v++) a[v] = (CT)av[u][v];
+          for (int v = 0; v < VN; v++) a[v] = av[u][v];
         }
 #pragma unroll
         for (int r = 0; r < B; r++)
 #pragma unroll
           for (int v = 0; v < VN; v++) {
-            CT t = 0;
+            double t = 0.0;
 #pragma unroll
-            for (int b = 0; b < B; b++) t = fma(W[r * B + b], (CT)xv[u][b][v], t);
+            for (int b = 0; b < B; b++) t = fma(W[r * B + b], (double)xv[u][b][v], t);
             acc[r][v] = fma(a[v], t, acc[r][v]);
           }
       }
     }
   }
-  (void)sl;
 }
 
 // The multipliers of group g, mult[v][g GS + i], into shared memory as CT
@@ -948,9 +923,11 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 template <typename T, int B, bool IMP, int UN, int VN, int NW>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VN]) {
-  // products and sums in the vector precision T: FP64, or FP32 with the
-  // FP32 copies of the unit blocks (the inner FP32 matrix of precision 3)
-  using AT = T;
+  // the implicit form forms every product and sum in FP64 (its unit blocks
+  // and multipliers are FP64) whatever the vector precision T: with FP32
+  // products the FP32 form took 565 instead of 289 Jacobi iterations from
+  // zero on the 16-zone beam, and stagnated with the coarse correction
+  using AT = typename std::conditional<IMP, double, T>::type;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -959,11 +936,11 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
   T beta[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) beta[v] = s_beta[lane_sample<T, VN>(lane, v)];
-  T *s_mult = nullptr;
+  AT *s_mult = nullptr;
   if constexpr (IMP) {
     if (M.smult) {
-      s_mult = reinterpret_cast<T *>(s_dyn_smem);
-      stage_mult<T, GS>(M.mult, M.nmult, S, g, s_mult);
+      s_mult = reinterpret_cast<AT *>(s_dyn_smem);
+      stage_mult<AT, GS>(M.mult, M.nmult, S, g, s_mult);
       __syncthreads();
     }
   }
@@ -979,11 +956,11 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     if constexpr (IMP) {
       if (s_mult)
-        implicit_row<T, T, T, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.z, S, sb,
-                                               lane_base<T, VN>(lane), __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+        implicit_row<T, T, B, VN, UN, true>(M.cval, M.cstride, M.mult, s_mult, M.z, S, sb, __ldg(M.crow + I),
+                                            __ldg(M.crow + I + 1), acc);
       else
-        implicit_row<T, T, T, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.z, S, sb,
-                                                lane_base<T, VN>(lane), __ldg(M.crow + I), __ldg(M.crow + I + 1), acc);
+        implicit_row<T, T, B, VN, UN, false>(M.cval, M.cstride, M.mult, nullptr, M.z, S, sb, __ldg(M.crow + I),
+                                             __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -1036,7 +1013,7 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
           T qo[VN];
           ldn<T, VN>(M.q + o, qo);
 #pragma unroll
-          for (int v = 0; v < VN; v++) acc[a][v] = fma(beta[v], qo[v], acc[a][v]);
+          for (int v = 0; v < VN; v++) acc[a][v] = fma((AT)beta[v], (AT)qo[v], acc[a][v]);
         }
         if (M.fixed[I * B + a]) {  // supported DOF: identity row
 #pragma unroll
@@ -1147,10 +1124,9 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
-  // FP64 multipliers in shared memory (FP64 kernels only: the FP32 kernel
-  // stages FP32 copies for its SpMV, and its true residual is FP64)
+  // the FP64 multipliers of the tile's group in shared memory
   const double *s_mult = nullptr;
-  if constexpr (IMP && sizeof(T) == 8) {
+  if constexpr (IMP) {
     if (M.smult) {
       double *sm = reinterpret_cast<double *>(s_dyn_smem);
       stage_mult<double, GS>(M.mult, M.nmult, S, g, sm);
@@ -1167,13 +1143,11 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
     if constexpr (IMP) {
       if (s_mult)
-        implicit_row<T, double, double, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.x, S, sb,
-                                                         lane_base<T, VN>(lane), __ldg(M.crow + I),
-                                                         __ldg(M.crow + I + 1), acc);
+        implicit_row<T, double, B, VN, UN, true>(M.cval, M.cstride, M.mult, s_mult, M.x, S, sb, __ldg(M.crow + I),
+                                                 __ldg(M.crow + I + 1), acc);
       else
-        implicit_row<T, double, double, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.x, S, sb,
-                                                          lane_base<T, VN>(lane), __ldg(M.crow + I),
-                                                          __ldg(M.crow + I + 1), acc);
+        implicit_row<T, double, B, VN, UN, false>(M.cval, M.cstride, M.mult, nullptr, M.x, S, sb, __ldg(M.crow + I),
+                                                  __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
       for (int kb = k0; kb < k1; kb += 32) {
@@ -2088,7 +2062,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   int max_nmult = 0;
   if constexpr (IMP)
     for (int k = 0; k < nmesh; k++) max_nmult = std::max(max_nmult, plans[k]->nmult);
-  const size_t mult_bytes = (size_t)max_nmult * GS * sizeof(T);
+  const size_t mult_bytes = (size_t)max_nmult * GS * sizeof(double);
   const bool smult = IMP && max_nmult > 0 && mult_bytes <= kMultSmem;
   const size_t dsmem = std::max(coarse ? kCoarseSmem : (size_t)0, smult ? mult_bytes : (size_t)0);
   // one block per SM either way (tensor memory): the rest of the unified
@@ -2144,7 +2118,6 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     b.mult = w.mult.p;
     b.fixed = m->d_fixed.p;
     b.cstride = plans[k]->cstride;
-    b.w32 = plans[k]->w32.p;
     b.sperm = plans[k]->sperm.p;
     b.nmult = plans[k]->nmult;
     b.smult = smult ? 1 : 0;
