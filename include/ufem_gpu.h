@@ -35,9 +35,10 @@ extern "C" {
 #define UFEM_SOLVER_CGWJ  0   /* femEqsCGwJ    fem/fem_eqs.c:88   */
 #define UFEM_SOLVER_SSOR  1   /* femEqsCGwSSOR fem/fem_eqs.c:1001 */
 #define UFEM_SOLVER_BICG  2   /* femEqsBiCCSwJ fem/fem_eqs.c:262  */
-#define UFEM_SOLVER_CGWJ_MIXED 3 /* Jacobi PCG with an FP32 matrix and FP32 vectors inside
-                                    FP64 iterative refinement (no reference counterpart);
-                                    always stops on the FP64 true residual |b - Ax| <= eps |b| */
+#define UFEM_SOLVER_CGWJ_MIXED 3 /* Jacobi PCG on an FP32 copy of the matrix (FP64 vectors and
+                                    sums), FP64 true-residual replacement without a Krylov
+                                    restart (no reference counterpart); always stops on the
+                                    FP64 true residual |b - Ax| <= eps |b| */
 
 /* stopping rules */
 #define UFEM_STOP_REFERENCE 0 /* |r| <= eps(|A||x| + |b|) with the recursive r

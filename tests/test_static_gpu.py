@@ -255,10 +255,10 @@ def _assembled_csr(g):
 
 @pytest.mark.parametrize("shape", [(20, 5, 5), (80, 20, 20)])
 def test_mixed_precision_pcg(shape):
-    """FP32 inner PCG in FP64 iterative refinement (UFEM_SOLVER_CGWJ_MIXED) to
-    true relative residual 1e-8, checked in numpy with the GPU's FP64 K, and
-    against the plain FP64 PCG solution to 1e-10 (displacements within 1e-6
-    relative: the residual-to-solution amplification of the cantilever)."""
+    """PCG on the FP32 matrix copy with FP64 true-residual replacement
+    (UFEM_SOLVER_CGWJ_MIXED) to true relative residual 1e-8, checked in numpy
+    with the GPU's FP64 K, and against the plain FP64 PCG solution to 1e-10
+    (displacements within 1e-6 relative)."""
     from ufem_b200 import api, meshgen as mg
     m = mg.beam_brick(*shape, 8.0, 2.0, 2.0)
     ref = gpu_model(m)

@@ -778,29 +778,205 @@ double true_relres(const DevMatrix &A, const double *d_b, const double *d_x) {
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision: FP32 inner Jacobi PCG inside FP64 iterative refinement.
-// Every outer step forms the true residual r = b - A x with the FP64 matrix,
-// solves A d = r with an FP32 copy of the matrix and FP32 vectors (the same
-// persistent kernel, products and dots accumulated in FP64) to inner_tol
-// relative, and adds d to x in FP64.  Converged when |b - A x| / |b| <= eps,
-// always decided on the FP64 true residual.
+// Mixed precision: Jacobi PCG on an FP32 copy of the matrix (half the value
+// bytes of the SpMV) with an FP64 solution and FP64 true-residual
+// replacement, in one persistent launch.  The work vectors r, z, p, q are
+// FP32 or FP64 (VT), products and dot products accumulate in FP64, x +=
+// alpha p in FP64.  The recursive
+// residual r is replaced by the true residual b - A x (FP64 matrix, FP64 x)
+// whenever it has dropped by `near` since the last replacement, every
+// `every` iterations, and when it reaches eps |b|; the search direction is
+// kept across replacements (no Krylov restart), so the count stays close to
+// the FP64 one.  Converged only on a true residual: |b - A x| <= eps |b|.
 namespace {
 __global__ void k_to_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
 }
-__global__ void k_add_f32(long n, const float *__restrict__ d, double *__restrict__ x) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i < n) x[i] += (double)d[i];
+
+// One block row of y = A (z + beta p) with an FP32 matrix copy and VT
+// vectors (the mapping of warp_row_spmv); products and sums in FP64.
+template <int B, typename VT>
+__device__ __forceinline__ double warp_row_spmv_mix(int I, const int *__restrict__ rowptr,
+                                                    const int *__restrict__ colind, const float *__restrict__ val,
+                                                    const VT *z, const VT *p, double beta, bool use_p,
+                                                    double *s_acc) {
+  constexpr int L = 32 - (32 % B);
+  const int lane = threadIdx.x & 31;
+  const int k0 = __ldg(rowptr + I), k1 = __ldg(rowptr + I + 1);
+  const int nitems = (k1 - k0) * B;
+  double acc = 0.0;
+  if (lane < L) {
+    const int a = lane % B;
+    for (int t = lane; t < nitems; t += L) {
+      const int k = k0 + t / B;
+      const int J = __ldg(colind + k);
+      const float *v = val + (size_t)k * B * B + a * B;
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        double xj = (double)__ldcg(z + (size_t)J * B + c);
+        if (use_p) xj = xj + beta * (double)__ldcg(p + (size_t)J * B + c);
+        acc += (double)__ldg(v + c) * xj;
+      }
+    }
+  }
+  if (B == 1) {
+    return warp_sum(acc);
+  } else if (B == 2) {
+#pragma unroll
+    for (int o = 16; o >= 2; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    return acc;
+  } else {
+    s_acc[lane] = acc;
+    __syncwarp();
+    double y = 0.0;
+    if (lane < B)
+      for (int l = lane; l < L; l += B) y += s_acc[l];
+    __syncwarp();
+    return y;
+  }
+}
+
+// VT: the type of the work vectors r, z, p, q and of the diagonal (FP32, or
+// FP64 with only the matrix copy in FP32)
+template <typename VT>
+struct CgMixArgs {
+  int nbr;
+  const int *rowptr, *colind;
+  const float *val;      // FP32 copy of K [nnzb][B][B]
+  const double *val64;   // FP64 K, for the true residuals
+  const double *b;       // right-hand side
+  double *x;             // solution (in: the initial guess)
+  const VT *M;           // diagonal
+  VT *r, *z, *p0, *p1, *q;
+  double *part;          // [grid][4]: r.r, -, r.z, p.q
+  GridBar *bar;
+  CgResult *res;
+  double eps, normB, near2;
+  long maxIt, every;
+  long *replacements;
+};
+
+// r = b - A x in FP64 (true residual), r (FP32), z = r / M and the partials
+// of the true r.r and of r.z, over the warp's block rows
+template <int B, typename VT>
+__device__ __forceinline__ void mix_true_residual(const CgMixArgs<VT> &A, int I0, int I1, double *s_acc,
+                                                  double *mypart) {
+  const int lane = threadIdx.x & 31;
+  double rr = 0.0, rz = 0.0;
+  for (int I = I0; I < I1; I++) {
+    const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val64, A.x, nullptr, 0.0, false, s_acc);
+    if (lane < B) {
+      const size_t i = (size_t)I * B + lane;
+      const double r64 = A.b[i] - y;
+      const VT ri = (VT)r64, zi = ri / A.M[i];
+      A.r[i] = ri;
+      A.z[i] = zi;
+      rr += r64 * r64;
+      rz += (double)ri * (double)zi;
+    }
+  }
+  double v[3] = {rr, 0.0, rz};
+  block_partials<3>(v, mypart);
+}
+
+template <int B, typename VT>
+__global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_cg_mixed(CgMixArgs<VT> A) {
+  __shared__ double s_acc[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
+  const int rpw = (A.nbr + nw - 1) / nw;
+  const int I0 = min(A.nbr, gw * rpw), I1 = min(A.nbr, I0 + rpw);
+  const int G = gridDim.x;
+  double *mypart = A.part + (size_t)blockIdx.x * 4;
+  const double tol2 = (A.eps * A.normB) * (A.eps * A.normB);
+  mix_true_residual<B, VT>(A, I0, I1, s_acc[warp], mypart);
+  if (!grid_barrier(A.bar)) return;
+  double rr_true = part_total(A.part, G, 0), rho = part_total(A.part, G, 2), rhoold = 1.0, rr_last = rr_true;
+  long it = 0, it_last = 0, nrep = 0;
+  int status = UFEM_AF_ERR;
+  if (rr_true <= tol2) status = UFEM_AF_OK;
+  for (it = 1; status != UFEM_AF_OK && it <= A.maxIt; it++) {
+    const bool first = (it == 1);
+    const double beta = first ? 0.0 : rho / rhoold;
+    const VT *pold = (it & 1) ? A.p0 : A.p1;
+    VT *pnew = (it & 1) ? A.p1 : A.p0;
+    // phase S: q = A p with p = z + beta p_old, partial p.q
+    {
+      double pq = 0.0;
+      for (int I = I0; I < I1; I++) {
+        const double y = warp_row_spmv_mix<B, VT>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
+        if (lane < B) {
+          const size_t i = (size_t)I * B + lane;
+          const VT pi = (VT)(first ? (double)A.z[i] : ((double)A.z[i] + beta * (double)pold[i]));
+          const VT qi = (VT)y;
+          pnew[i] = pi;
+          A.q[i] = qi;
+          pq += (double)pi * (double)qi;
+        }
+      }
+      double v[1] = {pq};
+      block_partials<1>(v, mypart + 3);
+    }
+    if (!grid_barrier(A.bar)) return;
+    const double pq = part_total(A.part, G, 3);
+    if (!(pq > 0.0) || !isfinite(pq)) break;  // breakdown
+    const double alpha = rho / pq;
+    // phase U: x += alpha p (FP64), r -= alpha q, z = r / M
+    {
+      double rr = 0.0, rz = 0.0;
+      const size_t i0 = (size_t)I0 * B, i1 = (size_t)I1 * B;
+      for (size_t i = i0 + lane; i < i1; i += 32) {
+        A.x[i] += alpha * (double)pnew[i];
+        const VT ri = (VT)((double)A.r[i] - alpha * (double)A.q[i]);
+        const VT zi = ri / A.M[i];
+        A.r[i] = ri;
+        A.z[i] = zi;
+        rr += (double)ri * (double)ri;
+        rz += (double)ri * (double)zi;
+      }
+      double v[3] = {rr, 0.0, rz};
+      block_partials<3>(v, mypart);
+    }
+    if (!grid_barrier(A.bar)) return;
+    const double rr_rec = part_total(A.part, G, 0);
+    double rz_new = part_total(A.part, G, 2);
+    if (!isfinite(rr_rec)) break;
+    // a true-residual pass: on the residual drop, every `every` iterations,
+    // and to verify convergence (every block takes the same decision)
+    if (rr_rec <= tol2 || rr_rec <= A.near2 * rr_last || it - it_last >= A.every) {
+      mix_true_residual<B, VT>(A, I0, I1, s_acc[warp], mypart);
+      if (!grid_barrier(A.bar)) return;
+      rr_true = part_total(A.part, G, 0);
+      rz_new = part_total(A.part, G, 2);
+      nrep++;
+      if (rr_true <= tol2) {
+        status = UFEM_AF_OK;
+        break;
+      }
+      rr_last = rr_true;
+      it_last = it;
+    }
+    rhoold = rho;
+    rho = rz_new;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.res->iters = it > A.maxIt ? A.maxIt : it;
+    A.res->status = status;
+    A.res->normRes = sqrt(rr_true);
+    *A.replacements = nrep;
+  }
 }
 }  // namespace
 
-int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
-                    long inner_cap, long *iters, int *outer_steps, float *ms) {
+namespace {
+template <typename VT>
+int run_cg_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double replace_near,
+                 long replace_every, long *iters, int *replacements, float *ms) {
   const long n = (long)A.nbr * A.B, nv = A.nnzb * A.B * A.B;
   int rv;
   if (iters) *iters = 0;
-  if (outer_steps) *outer_steps = 0;
+  if (replacements) *replacements = 0;
   double normA = 0.0;
   int zero_row = 0;
   DBuf<double> M;
@@ -814,21 +990,25 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
     set_error("matrix member on the diagonal has zero size");  // fem/fem_eqs.c:134-145
     return UFEM_AF_ERR_ZER;
   }
-  DBuf<float> V32, M32, r32, d32, ri, z, p0, p1, q;
-  DBuf<double> r64, part;
+  DBuf<float> V32;
+  DBuf<VT> M32, r, z, p0, p1, q;
+  DBuf<double> part;
   DBuf<GridBar> bar;
   DBuf<CgResult> res;
-  if ((rv = V32.alloc(nv)) || (rv = M32.alloc(n)) || (rv = r32.alloc(n)) || (rv = d32.alloc(n)) ||
-      (rv = ri.alloc(n)) || (rv = z.alloc(n)) || (rv = p0.alloc(n)) || (rv = p1.alloc(n)) || (rv = q.alloc(n)) ||
-      (rv = r64.alloc(n)))
+  DBuf<long> nrep;
+  if ((rv = V32.alloc(nv)) || (rv = M32.alloc(n)) || (rv = r.alloc(n)) || (rv = z.alloc(n)) || (rv = p0.alloc(n)) ||
+      (rv = p1.alloc(n)) || (rv = q.alloc(n)) || (rv = nrep.alloc(1)))
     return rv;
   const unsigned gv = (unsigned)((nv + 255) / 256), gn = (unsigned)((n + 255) / 256);
   k_to_f32<<<gv, 256>>>(nv, A.val, V32.p);
-  k_to_f32<<<gn, 256>>>(n, M.p, M32.p);
+  if constexpr (sizeof(VT) == 4) k_to_f32<<<gn, 256>>>(n, M.p, M32.p);
+  else UFEM_CUDA_TRY(cudaMemcpy(M32.p, M.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+  UFEM_CUDA_TRY(cudaMemset(p0.p, 0, n * sizeof(VT)));
+  UFEM_CUDA_TRY(cudaMemset(p1.p, 0, n * sizeof(VT)));
   int dev = 0, nsm = 0, occ = 0;
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  void (*kern)(CgArgsT<float>) = A.B == 1 ? k_cg<float, 1> : (A.B == 2 ? k_cg<float, 2> : k_cg<float, 3>);
+  void (*kern)(CgMixArgs<VT>) = A.B == 1 ? k_cg_mixed<1, VT> : (A.B == 2 ? k_cg_mixed<2, VT> : k_cg_mixed<3, VT>);
   UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     set_error("persistent CG kernel does not fit on an SM");
@@ -837,59 +1017,50 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
   int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
   G = std::max(G, 1);
   if ((rv = part.alloc((size_t)G * 4)) || (rv = bar.alloc(1)) || (rv = res.alloc(1))) return rv;
+  UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
+  UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
+  CgMixArgs<VT> a{};
+  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = V32.p; a.val64 = A.val; a.b = d_b; a.x = d_x;
+  a.M = M32.p; a.r = r.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p; a.bar = bar.p;
+  a.res = res.p; a.eps = eps; a.normB = normB; a.near2 = replace_near * replace_near; a.maxIt = maxIt;
+  a.every = std::max<long>(1, replace_every); a.replacements = nrep.p;
+  void *args[] = {&a};
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0);
-  long total = 0;
-  int outer = 0, status = UFEM_AF_ERR;
-  for (; outer < 40 && total < maxIt; outer++) {
-    // r = b - A x (FP64)
-    spmv_launch(A, d_x, r64.p);
-    k_sub<<<gn, 256>>>(n, d_b, r64.p, r64.p);
-    const double normR = host_norm(n, r64.p);
-    if (!std::isfinite(normR)) break;
-    if (normR <= eps * normB) {
-      status = UFEM_AF_OK;
-      break;
-    }
-    k_to_f32<<<gn, 256>>>(n, r64.p, r32.p);
-    UFEM_CUDA_TRY(cudaMemsetAsync(d32.p, 0, n * sizeof(float)));
-    UFEM_CUDA_TRY(cudaMemsetAsync(p0.p, 0, n * sizeof(float)));
-    UFEM_CUDA_TRY(cudaMemsetAsync(p1.p, 0, n * sizeof(float)));
-    UFEM_CUDA_TRY(cudaMemsetAsync(bar.p, 0, sizeof(GridBar)));
-    UFEM_CUDA_TRY(cudaMemsetAsync(res.p, 0, sizeof(CgResult)));
-    CgArgsT<float> a{};
-    a.nbr = A.nbr; a.nnzb = A.nnzb; a.rowptr = A.rowptr; a.colind = A.colind; a.val = V32.p; a.b = r32.p;
-    a.x = d32.p;
-    a.M = M32.p; a.r = ri.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.part = part.p;
-    a.bar = bar.p; a.res = res.p; a.eps = inner_tol; a.normA = normA; a.normB = normR;
-    a.maxIt = std::min(inner_cap, maxIt - total); a.stop_rule = UFEM_STOP_RELRES;
-    void *args[] = {&a};
-    UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
-    GridBar hb;
-    CgResult hr;
-    UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
-    UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
-    if (hb.err) {
-      set_error("persistent CG: grid barrier timed out");
-      return UFEM_AF_ERR;
-    }
-    total += hr.iters < 0 ? -hr.iters : hr.iters;
-    // the correction, even from an inner solve that stopped at its cap
-    k_add_f32<<<gn, 256>>>(n, d32.p, d_x);
-  }
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
   cudaEventRecord(e1);
-  cudaEventSynchronize(e1);
+  UFEM_CUDA_TRY(cudaEventSynchronize(e1));
   float t = 0;
   cudaEventElapsedTime(&t, e0, e1);
   if (ms) *ms = t;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (iters) *iters = total;
-  if (outer_steps) *outer_steps = outer;
-  if (status != UFEM_AF_OK) set_error("unconverged solution");
-  return status;
+  GridBar hb;
+  CgResult hr;
+  long hrep = 0;
+  UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
+  UFEM_CUDA_TRY(cudaMemcpy(&hrep, nrep.p, sizeof(hrep), cudaMemcpyDeviceToHost));
+  if (hb.err) {
+    set_error("persistent CG: grid barrier timed out");
+    return UFEM_AF_ERR;
+  }
+  if (iters) *iters = hr.iters;
+  if (replacements) *replacements = (int)hrep;
+  if (hr.status != UFEM_AF_OK) set_error("unconverged solution");
+  return hr.status;
+}
+}  // namespace
+
+// fp32_vectors: the work vectors in FP32 as well (else FP64, only the matrix
+// copy in FP32)
+int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double replace_near,
+                    long replace_every, bool fp32_vectors, long *iters, int *replacements, float *ms) {
+  return fp32_vectors ? run_cg_mixed<float>(A, d_b, d_x, eps, maxIt, replace_near, replace_every, iters, replacements, ms)
+                      : run_cg_mixed<double>(A, d_b, d_x, eps, maxIt, replace_near, replace_every, iters, replacements,
+                                             ms);
 }
 
 // ---------------------------------------------------------------------------

@@ -192,8 +192,8 @@ int mc_implicit_view(ufem_model *m, McImplicitView *v);
 int mlp_train_graph(ufem_mlp *p, long ntrain, int bs, const float *d_X, const float *d_T,
                     const std::vector<float> &sched, int epochs, unsigned long long seed, float *loss_first,
                     float *loss_last, long *steps);
-int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double inner_tol,
-                    long inner_cap, long *iters, int *outer_steps, float *ms);
+int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, double replace_near,
+                    long replace_every, bool fp32_vectors, long *iters, int *replacements, float *ms);
 
 // Element-result outputs of a Monte Carlo table (RES_E, RES_SUM/MAX/MIN/FAIL_E)
 // and the general failure function RES_FAIL, as GPU passes (mcout.cu)
