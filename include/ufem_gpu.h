@@ -441,6 +441,19 @@ int  ufem_sym_eig(int l, const double *h_A, double *h_V, double *h_lam, int *swe
 
 /* ---- device / diagnostics ------------------------------------------------ */
 int ufem_device_info(int *sm_count, int *cc_major, int *cc_minor, long *mem_bytes);
+
+/* Self-tests of the bounded device waits (no reference counterpart).  Every
+ * spin-wait of the library's kernels ends after a limit with an error the
+ * host reads, so the CUDA context stays usable.  The first makes the grid
+ * barrier of the persistent solvers run out: nblocks co-resident blocks, one
+ * of which leaves without arriving, the others waiting limit_ms (1 to 2000)
+ * before they give up; it returns AF_ERR ("grid barrier timed out") with the
+ * number of blocks that timed out and the kernel's duration.  The second
+ * waits on a tensor-core completion barrier that nothing signals, for
+ * spin_limit polls (the coarse phases and the MLP use 2^24); it returns
+ * AF_ERR with *timed_out = 1. */
+int ufem_selftest_barrier_timeout(int nblocks, int limit_ms, int *blocks_timed_out, double *ms);
+int ufem_selftest_mma_wait_timeout(long spin_limit, int *timed_out);
 const char *ufem_last_error(void);
 
 #ifdef __cplusplus

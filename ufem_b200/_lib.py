@@ -74,6 +74,8 @@ class McStats(C.Structure):
 _SIGS = {
     "ufem_last_error": (C.c_char_p, []),
     "ufem_device_info": (C.c_int, [_i, _i, _i, _l]),
+    "ufem_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int, _i, _d]),
+    "ufem_selftest_mma_wait_timeout": (C.c_int, [C.c_long, _i]),
     "ufem_model_create": (C.c_int, [C.POINTER(Tables), C.POINTER(C.c_void_p)]),
     "ufem_read_input": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "ufem_convert_input": (C.c_int, [C.c_char_p, C.c_char_p]),

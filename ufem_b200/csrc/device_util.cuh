@@ -7,13 +7,14 @@
 namespace ufem {
 
 // Generation-counting grid barrier.  Every wait is bounded: after
-// kBarrierTimeoutNs of global time the waiting block records an error, leaves
-// the barrier and the kernel returns; the host turns the flag into AF_ERR.
+// kBarrierTimeoutNs of global time (or limit_ms, when set) the waiting block
+// records an error, leaves the barrier and the kernel returns; the host turns
+// the flag into AF_ERR.
 struct GridBar {
   unsigned int count;
   unsigned int gen;
   int err;
-  int pad;
+  int limit_ms;  // 0: kBarrierTimeoutNs; set shorter by the self-test of the wait
 };
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
@@ -39,13 +40,15 @@ __device__ __forceinline__ bool grid_barrier(GridBar *gb) {
       __threadfence();
       atomicAdd(&gb->gen, 1u);
     } else {
-      unsigned long long t0 = global_ns();
+      const unsigned long long t0 = global_ns();
+      const int lim = gb->limit_ms;
+      const unsigned long long limit_ns = lim > 0 ? (unsigned long long)lim * 1000000ull : kBarrierTimeoutNs;
       while (*vgen == g) {
         if (*verr) {
           ok = 0;
           break;
         }
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
+        if (global_ns() - t0 > limit_ns) {
           atomicExch(&gb->err, 1);
           ok = 0;
           break;

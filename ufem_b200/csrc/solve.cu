@@ -1,8 +1,8 @@
 // Single-system FP64 solvers on the GPU block-sparse K (block size B = 1, 2
-// or 3; B = 1 is plain CSR):
+// or 3; B = 1 is plain CSR), each one persistent cooperative kernel:
 //
-//   Jacobi PCG      femEqsCGwJ    fem/fem_eqs.c:88-247   (one persistent kernel)
-//   Jacobi BiCGStab femEqsBiCCSwJ fem/fem_eqs.c:262-468  (stream of kernels)
+//   Jacobi PCG      femEqsCGwJ    fem/fem_eqs.c:88-247
+//   Jacobi BiCGStab femEqsBiCCSwJ fem/fem_eqs.c:262-468
 //   SSOR PCG        femEqsCGwSSOR fem/fem_eqs.c:1001-1217 (multicolour sweeps)
 //
 // Jacobi PCG: one cooperative launch runs every iteration; the grid meets at
@@ -442,58 +442,233 @@ int cg_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double ep
 }
 
 // ---- BiCGStab (femEqsBiCCSwJ) ------------------------------------------------
-
+//
+// One persistent cooperative launch runs every iteration of the reference's
+// Jacobi BiCGStab (fem/fem_eqs.c:262-468): scalars stay on the device, every
+// block sums the per-block partials in the same fixed order, and the grid
+// meets at a bounded barrier after each of the five phases of an iteration
+// (p and pp = p / M; v = A pp with rr.v; s and ss = s / M with s.s;
+// t = A ss with t.s and t.t; x, r with the next rr.r and the stopping
+// sums), plus one for the true residual under the relative-residual rule.
 namespace {
-struct BiScal {  // device scalars
-  double ro, roro, alpha, omega, beta, rrv, ts, tt;
-};
 
-__global__ void k_bicg_p(long n, int first, const double *__restrict__ dv, const double *__restrict__ r,
-                         double *__restrict__ p, const double *__restrict__ v, const double *__restrict__ M,
-                         double *__restrict__ pp) {
-  // dv: [0]=ro [1]=roro [2]=alpha [3]=omega
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double pi;
-  if (first) {
-    pi = r[i];
-  } else {
-    double beta = (dv[0] / dv[1]) * (dv[2] / dv[3]);  // fem/fem_eqs.c:386
-    pi = r[i] + beta * (p[i] - (dv[3] * v[i]));
-  }
-  p[i] = pi;
-  pp[i] = pi / M[i];
-}
-__global__ void k_bicg_s(long n, const double *__restrict__ dv, const double *__restrict__ r,
-                         const double *__restrict__ v, const double *__restrict__ M, double *__restrict__ s,
-                         double *__restrict__ ss) {
-  // dv[2] = alpha = ro / (rr.v) computed by k_bicg_alpha
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double si = r[i] - (dv[2] * v[i]);
-  s[i] = si;
-  ss[i] = si / M[i];
-}
-__global__ void k_bicg_alpha(double *dv, const double *rrv) { dv[2] = dv[0] / *rrv; }
-__global__ void k_bicg_omega(double *dv, const double *ts, const double *tt) { dv[3] = *ts / *tt; }
-__global__ void k_bicg_xr(long n, const double *__restrict__ dv, double *__restrict__ x, double *__restrict__ r,
-                          const double *__restrict__ pp, const double *__restrict__ ss,
-                          const double *__restrict__ s, const double *__restrict__ t) {
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  x[i] += dv[2] * pp[i] + (dv[3] * ss[i]);
-  r[i] = s[i] - (dv[3] * t[i]);
-}
-__global__ void k_axpy_last(long n, const double *__restrict__ dv, double *__restrict__ x,
-                            const double *__restrict__ pp) {
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i < n) x[i] += dv[2] * pp[i];
-}
 __global__ void k_sub(long n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c) {
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i < n) c[i] = a[i] - b[i];
 }
-__global__ void k_copy_scalar(double *dst, const double *src) { *dst = *src; }
+
+struct BiArgs {
+  int nbr;
+  const int *rowptr, *colind;
+  const double *val, *b, *M;
+  double *x, *r, *rr, *p, *pp, *s, *ss, *t, *v, *Ab;
+  double *part;  // [grid][4]
+  GridBar *bar;
+  CgResult *res;
+  double eps, normA, normB;
+  long maxIt;
+  int stop_rule;
+};
+
+template <int B>
+__global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_bicgstab(BiArgs A) {
+  __shared__ double s_acc[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
+  const int rpw = (A.nbr + nw - 1) / nw;
+  const int I0 = min(A.nbr, gw * rpw), I1 = min(A.nbr, I0 + rpw);
+  const size_t i0 = (size_t)I0 * B, i1 = (size_t)I1 * B;
+  const int G = gridDim.x;
+  double *mypart = A.part + (size_t)blockIdx.x * 4;
+  // phase 0: r = b - A x, rr = r (fem/fem_eqs.c:340-350); A b for the
+  // reference's stopping test
+  {
+    double r2 = 0.0;
+    for (int I = I0; I < I1; I++) {
+      const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
+      double yb = 0.0;
+      if (A.stop_rule == UFEM_STOP_REFERENCE)
+        yb = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.b, nullptr, 0.0, false, s_acc[warp]);
+      if (lane < B) {
+        const size_t i = (size_t)I * B + lane;
+        const double ri = A.b[i] - y;
+        A.r[i] = ri;
+        A.rr[i] = ri;
+        if (A.stop_rule == UFEM_STOP_REFERENCE) A.Ab[i] = yb;
+        r2 += ri * ri;
+      }
+    }
+    double v3[1] = {r2};
+    block_partials<1>(v3, mypart);
+  }
+  if (!grid_barrier(A.bar)) return;
+  double ro = part_total(A.part, G, 0);  // rr.r = r.r at the start
+  long it = 0;
+  double normRes = sqrt(ro), normX = 0.0;
+  if (!(sqrt(ro) <= FEM_ZERO)) {
+    double roro = 1.0, alpha = 0.0, omega = 1.0;
+    for (it = 1; it <= A.maxIt; it++) {
+      if (fabs(ro) <= 0.0) break;  // fem/fem_eqs.c:373-379
+      // p = r + beta (p - omega v) (fem/fem_eqs.c:381-392), pp = p / M
+      {
+        const double beta = (it == 1) ? 0.0 : (ro / roro) * (alpha / omega);
+        for (size_t i = i0 + lane; i < i1; i += 32) {
+          const double pi = (it == 1) ? A.r[i] : A.r[i] + beta * (A.p[i] - (omega * A.v[i]));
+          A.p[i] = pi;
+          A.pp[i] = pi / A.M[i];
+        }
+      }
+      if (!grid_barrier(A.bar)) return;
+      // v = A pp, rr.v
+      {
+        double rv = 0.0;
+        for (int I = I0; I < I1; I++) {
+          const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.pp, nullptr, 0.0, false,
+                                                    s_acc[warp]);
+          if (lane < B) {
+            const size_t i = (size_t)I * B + lane;
+            A.v[i] = y;
+            rv += A.rr[i] * y;
+          }
+        }
+        double v1[1] = {rv};
+        block_partials<1>(v1, mypart);
+      }
+      if (!grid_barrier(A.bar)) return;
+      alpha = ro / part_total(A.part, G, 0);
+      // s = r - alpha v, ss = s / M, s.s
+      {
+        double s2 = 0.0;
+        for (size_t i = i0 + lane; i < i1; i += 32) {
+          const double si = A.r[i] - (alpha * A.v[i]);
+          A.s[i] = si;
+          A.ss[i] = si / A.M[i];
+          s2 += si * si;
+        }
+        double v1[1] = {s2};
+        block_partials<1>(v1, mypart + 1);
+      }
+      if (!grid_barrier(A.bar)) return;
+      if (sqrt(part_total(A.part, G, 1)) <= FEM_ZERO) {  // fem/fem_eqs.c:407-417
+        for (size_t i = i0 + lane; i < i1; i += 32) A.x[i] += alpha * A.pp[i];
+        break;
+      }
+      // t = A ss, t.s and t.t
+      {
+        double ts = 0.0, tt = 0.0;
+        for (int I = I0; I < I1; I++) {
+          const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.ss, nullptr, 0.0, false,
+                                                    s_acc[warp]);
+          if (lane < B) {
+            const size_t i = (size_t)I * B + lane;
+            A.t[i] = y;
+            ts += y * A.s[i];
+            tt += y * y;
+          }
+        }
+        double v2[2] = {ts, tt};
+        block_partials<2>(v2, mypart + 2);
+      }
+      if (!grid_barrier(A.bar)) return;
+      omega = part_total(A.part, G, 2) / part_total(A.part, G, 3);
+      // x += alpha pp + omega ss, r = s - omega t; the next rr.r and the
+      // reference's stopping sums |A b - x|^2 and |x|^2 (its residual call
+      // at fem/fem_eqs.c:425 swaps the arguments: res = A b - x)
+      {
+        double rr_r = 0.0, res2 = 0.0, x2 = 0.0;
+        for (size_t i = i0 + lane; i < i1; i += 32) {
+          const double xi = A.x[i] + (alpha * A.pp[i] + (omega * A.ss[i]));
+          const double ri = A.s[i] - (omega * A.t[i]);
+          A.x[i] = xi;
+          A.r[i] = ri;
+          rr_r += A.rr[i] * ri;
+          if (A.stop_rule == UFEM_STOP_REFERENCE) {
+            const double d = A.Ab[i] - xi;
+            res2 += d * d;
+          }
+          x2 += xi * xi;
+        }
+        double v3[3] = {rr_r, res2, x2};
+        block_partials<3>(v3, mypart);
+      }
+      if (!grid_barrier(A.bar)) return;
+      roro = ro;
+      ro = part_total(A.part, G, 0);
+      normX = sqrt(part_total(A.part, G, 2));
+      bool conv;
+      if (A.stop_rule == UFEM_STOP_REFERENCE) {
+        normRes = sqrt(part_total(A.part, G, 1));
+        conv = normRes < (A.eps * ((A.normA * normX) + A.normB));
+      } else {
+        // the true residual b - A x
+        double r2 = 0.0;
+        for (int I = I0; I < I1; I++) {
+          const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false,
+                                                    s_acc[warp]);
+          if (lane < B) {
+            const double d = A.b[(size_t)I * B + lane] - y;
+            r2 += d * d;
+          }
+        }
+        double v1[1] = {r2};
+        block_partials<1>(v1, mypart + 3);
+        if (!grid_barrier(A.bar)) return;
+        normRes = sqrt(part_total(A.part, G, 3));
+        conv = normRes <= A.eps * A.normB;
+      }
+      if (!isfinite(normRes)) break;
+      if (conv) break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.res->iters = it > A.maxIt ? A.maxIt : it;
+    A.res->status = UFEM_AF_OK;
+    A.res->normRes = normRes;
+    A.res->normX = normX;
+  }
+}
+
+// Launches a persistent cooperative solver kernel over the matrix rows with
+// the grid of k_cg (at least two block rows per warp, never more blocks than
+// are co-resident); returns the kernel's milliseconds.
+template <typename Args>
+int launch_persistent(void (*kern)(Args), const DevMatrix &A, Args &a, DBuf<double> &part, DBuf<GridBar> &bar,
+                      float *ms) {
+  int dev = 0, nsm = 0, occ = 0, rv;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  UFEM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+  if (occ < 1) {
+    set_error("persistent solver kernel does not fit on an SM");
+    return UFEM_AF_ERR;
+  }
+  int G = (int)std::min<long>((long)nsm * std::min(occ, kCgBlocksPerSm), (A.nbr + 2 * kWarps - 1) / (2 * kWarps));
+  G = std::max(G, 1);
+  if ((rv = part.alloc((size_t)G * 4)) || (rv = bar.alloc(1))) return rv;
+  UFEM_CUDA_TRY(cudaMemset(bar.p, 0, sizeof(GridBar)));
+  a.part = part.p;
+  a.bar = bar.p;
+  void *args[] = {&a};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kThreads), args, 0, 0));
+  cudaEventRecord(e1);
+  UFEM_CUDA_TRY(cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t;
+  GridBar hb;
+  UFEM_CUDA_TRY(cudaMemcpy(&hb, bar.p, sizeof(hb), cudaMemcpyDeviceToHost));
+  if (hb.err) {
+    set_error("persistent solver: grid barrier timed out");
+    return UFEM_AF_ERR;
+  }
+  return UFEM_AF_OK;
+}
 }  // namespace
 
 int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps, long maxIt, int stop_rule,
@@ -505,75 +680,27 @@ int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, dou
   int zero_row = 0;
   DBuf<double> M;
   if ((rv = setup_common(A, M, &normA, &zero_row)) != UFEM_AF_OK) return rv;
-  double normB = host_norm(n, d_b);
+  const double normB = host_norm(n, d_b);
   // the reference leaves through memFree and still returns AF_OK (fem/fem_eqs.c:352-360, :467)
   if (zero_row != 0x7fffffff) return UFEM_AF_OK;
-  DBuf<double> r, rr, p, pp, s, ss, t, v, res;
+  DBuf<double> r, rr, p, pp, s, ss, t, v, Ab, part;
+  DBuf<GridBar> bar;
+  DBuf<CgResult> res;
   if ((rv = r.alloc(n)) || (rv = rr.alloc(n)) || (rv = p.alloc(n)) || (rv = pp.alloc(n)) || (rv = s.alloc(n)) ||
-      (rv = ss.alloc(n)) || (rv = t.alloc(n)) || (rv = v.alloc(n)) || (rv = res.alloc(n)))
+      (rv = ss.alloc(n)) || (rv = t.alloc(n)) || (rv = v.alloc(n)) || (rv = Ab.alloc(n)) || (rv = res.alloc(1)))
     return rv;
-  Dots D;
-  if ((rv = D.init(8)) != UFEM_AF_OK) return rv;
-  DBuf<double> dv;
-  if ((rv = dv.alloc(4)) != UFEM_AF_OK) return rv;
-  UFEM_CUDA_TRY(cudaMemset(dv.p, 0, 4 * sizeof(double)));
-  unsigned g = (unsigned)((n + 255) / 256);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0);
-  spmv_launch(A, d_x, r.p);
-  k_sub<<<g, 256>>>(n, d_b, r.p, r.p);
-  UFEM_CUDA_TRY(cudaMemcpy(rr.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
-  long it = 0;
-  if (!(host_norm(n, r.p) <= FEM_ZERO)) {
-    for (it = 1; it <= maxIt; it++) {
-      D.dot(n, rr.p, r.p, 0);                       // ro
-      k_copy_scalar<<<1, 1>>>(dv.p + 0, D.vals.p + 0);
-      double ro = 0;
-      UFEM_CUDA_TRY(cudaMemcpy(&ro, D.vals.p, sizeof(double), cudaMemcpyDeviceToHost));
-      if (fabs(ro) <= 0.0) break;                   // fem/fem_eqs.c:373-379
-      k_bicg_p<<<g, 256>>>(n, it == 1, dv.p, r.p, p.p, v.p, M.p, pp.p);
-      spmv_launch(A, pp.p, v.p);
-      D.dot(n, rr.p, v.p, 1);
-      k_bicg_alpha<<<1, 1>>>(dv.p, D.vals.p + 1);
-      k_bicg_s<<<g, 256>>>(n, dv.p, r.p, v.p, M.p, s.p, ss.p);
-      if (host_norm(n, s.p) <= FEM_ZERO) {          // fem/fem_eqs.c:407-417
-        k_axpy_last<<<g, 256>>>(n, dv.p, d_x, pp.p);
-        break;
-      }
-      spmv_launch(A, ss.p, t.p);
-      D.dot(n, t.p, s.p, 2);
-      D.dot(n, t.p, t.p, 3);
-      k_bicg_omega<<<1, 1>>>(dv.p, D.vals.p + 2, D.vals.p + 3);
-      k_bicg_xr<<<g, 256>>>(n, dv.p, d_x, r.p, pp.p, ss.p, s.p, t.p);
-      k_copy_scalar<<<1, 1>>>(dv.p + 1, dv.p + 0);  // roro = ro
-      double normRes;
-      if (stop_rule == UFEM_STOP_REFERENCE) {
-        // eqsCompResid(a, b, x, &res) as called at fem/fem_eqs.c:425: the
-        // arguments are swapped against its prototype, so res = A b - x
-        spmv_launch(A, d_b, res.p);
-        k_sub<<<g, 256>>>(n, res.p, d_x, res.p);
-        normRes = host_norm(n, res.p);
-        double normX = host_norm(n, d_x);
-        if (normRes < (eps * ((normA * normX) + normB))) break;
-      } else {
-        spmv_launch(A, d_x, res.p);
-        k_sub<<<g, 256>>>(n, d_b, res.p, res.p);
-        normRes = host_norm(n, res.p);
-        if (normRes <= eps * normB) break;
-      }
-    }
-  }
-  UFEM_CUDA_TRY(cudaGetLastError());
-  cudaEventRecord(e1);
-  cudaEventSynchronize(e1);
-  float tm = 0;
-  cudaEventElapsedTime(&tm, e0, e1);
-  if (ms) *ms = tm;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (iters) *iters = it > maxIt ? maxIt : it;
+  UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
+  UFEM_CUDA_TRY(cudaMemset(p.p, 0, n * sizeof(double)));
+  UFEM_CUDA_TRY(cudaMemset(v.p, 0, n * sizeof(double)));
+  BiArgs a{};
+  a.nbr = A.nbr; a.rowptr = A.rowptr; a.colind = A.colind; a.val = A.val; a.b = d_b; a.M = M.p; a.x = d_x;
+  a.r = r.p; a.rr = rr.p; a.p = p.p; a.pp = pp.p; a.s = s.p; a.ss = ss.p; a.t = t.p; a.v = v.p; a.Ab = Ab.p;
+  a.res = res.p; a.eps = eps; a.normA = normA; a.normB = normB; a.maxIt = maxIt; a.stop_rule = stop_rule;
+  void (*kern)(BiArgs) = A.B == 1 ? k_bicgstab<1> : (A.B == 2 ? k_bicgstab<2> : k_bicgstab<3>);
+  if ((rv = launch_persistent(kern, A, a, part, bar, ms)) != UFEM_AF_OK) return rv;
+  CgResult hr;
+  UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
+  if (iters) *iters = hr.iters;
   return UFEM_AF_OK;  // the reference always returns AF_OK (fem/fem_eqs.c:467)
 }
 
@@ -584,69 +711,170 @@ int bicgstab_jacobi_fp64(const DevMatrix &A, const double *d_b, double *d_x, dou
 // of a colour are coupled; the forward sweep visits colours in order and the
 // backward sweep in reverse, rows of a colour in parallel, the B DOFs of a
 // node in order.  This is symmetric Gauss-Seidel for a permuted ordering: an
-// SPD preconditioner like the reference's, with different iterates.
-
+// SPD preconditioner like the reference's, with different iterates.  One
+// persistent cooperative launch runs every iteration: a bounded grid barrier
+// after each colour of each sweep (r.z accumulates as the backward sweep
+// finalises each row's z), after q = A p with p = z + beta p_old formed on
+// the fly, and after the x, r update.
 namespace {
+
+__global__ void k_recip(long n, const double *__restrict__ M, double *__restrict__ Minv) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) Minv[i] = 1.0 / M[i];
+}
+
+struct SsorArgs {
+  int nbr, ncol;
+  const int *rowptr, *colind, *colour_of, *cptr, *crow;  // cptr [ncol+1], crow: rows by colour
+  const double *val, *b, *Minv;
+  double *x, *r, *zz, *z, *p0, *p1, *q;
+  double *part;  // [grid][4]
+  GridBar *bar;
+  CgResult *res;
+  double eps, normA, normB;
+  long maxIt;
+  int stop_rule;
+};
+
+// one block row of a sweep (the row's thread): FWD, out = zz from rhs = r;
+// backward, out = z from rhs = zz (returns the row's r.z contribution)
 template <int B, bool FWD>
-__global__ void k_sgs_sweep(int nrows, const int *__restrict__ rows, const int *__restrict__ colour_of,
-                            int colour, const int *__restrict__ rowptr, const int *__restrict__ colind,
-                            const double *__restrict__ val, const double *__restrict__ Minv,
-                            const double *__restrict__ rhs, double *__restrict__ out) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nrows) return;
-  const int I = rows[t];
+__device__ __forceinline__ double sgs_row(const SsorArgs &A, int I, int colour, const double *rhs, double *out) {
   double loc[B];
 #pragma unroll
   for (int a = 0; a < B; a++) loc[a] = 0.0;
-  // coupling to other rows of earlier (FWD) or later (!FWD) colours
-  for (int k = rowptr[I]; k < rowptr[I + 1]; k++) {
-    const int J = colind[k];
-    if (J == I) continue;
-    const int cj = colour_of[J];
+  const int k0 = A.rowptr[I], k1 = A.rowptr[I + 1];
+  int kd = k0;
+  for (int k = k0; k < k1; k++) {
+    const int J = A.colind[k];
+    if (J == I) {
+      kd = k;
+      continue;
+    }
+    const int cj = A.colour_of[J];
     if (FWD ? (cj < colour) : (cj > colour)) {
 #pragma unroll
       for (int a = 0; a < B; a++)
 #pragma unroll
-        for (int c = 0; c < B; c++) loc[a] += val[(size_t)k * B * B + a * B + c] * out[(size_t)J * B + c];
+        for (int c = 0; c < B; c++) loc[a] += A.val[(size_t)k * B * B + a * B + c] * __ldcg(out + (size_t)J * B + c);
     }
   }
-  int kd = rowptr[I];
-  while (colind[kd] != I) kd++;
-  const double *D = val + (size_t)kd * B * B;
+  const double *D = A.val + (size_t)kd * B * B;
+  double rz = 0.0;
   if (FWD) {
 #pragma unroll
     for (int a = 0; a < B; a++) {
       double s = loc[a];
       for (int c = 0; c < a; c++) s += D[a * B + c] * out[(size_t)I * B + c];
-      out[(size_t)I * B + a] = Minv[(size_t)I * B + a] * (rhs[(size_t)I * B + a] - s);
+      out[(size_t)I * B + a] = A.Minv[(size_t)I * B + a] * (__ldcg(rhs + (size_t)I * B + a) - s);
     }
   } else {
 #pragma unroll
     for (int a = B - 1; a >= 0; a--) {
       double s = loc[a];
       for (int c = a + 1; c < B; c++) s += D[a * B + c] * out[(size_t)I * B + c];
-      out[(size_t)I * B + a] = rhs[(size_t)I * B + a] - Minv[(size_t)I * B + a] * s;
+      const double zi = __ldcg(rhs + (size_t)I * B + a) - A.Minv[(size_t)I * B + a] * s;
+      out[(size_t)I * B + a] = zi;
+      rz += __ldcg(A.r + (size_t)I * B + a) * zi;
     }
   }
+  return rz;
 }
-__global__ void k_recip(long n, const double *__restrict__ M, double *__restrict__ Minv) {
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i < n) Minv[i] = 1.0 / M[i];
-}
-__global__ void k_cg_p(long n, int first, const double *__restrict__ sc, const double *__restrict__ z,
-                       double *__restrict__ p) {
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  p[i] = first ? z[i] : (z[i] + ((sc[0] / sc[1]) * p[i]));
-}
-__global__ void k_cg_xr(long n, const double *__restrict__ sc, const double *__restrict__ pq,
-                        double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                        const double *__restrict__ q) {
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double alpha = sc[0] / *pq;
-  x[i] = x[i] + (alpha * p[i]);
-  r[i] = r[i] - (alpha * q[i]);
+
+template <int B>
+__global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_cg_ssor(SsorArgs A) {
+  __shared__ double s_acc[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
+  const int rpw = (A.nbr + nw - 1) / nw;
+  const int I0 = min(A.nbr, gw * rpw), I1 = min(A.nbr, I0 + rpw);
+  const size_t i0 = (size_t)I0 * B, i1 = (size_t)I1 * B;
+  const int G = gridDim.x;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  double *mypart = A.part + (size_t)blockIdx.x * 4;
+  // r = b - A x
+  for (int I = I0; I < I1; I++) {
+    const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
+    if (lane < B) A.r[(size_t)I * B + lane] = A.b[(size_t)I * B + lane] - y;
+  }
+  if (!grid_barrier(A.bar)) return;
+  int status = UFEM_AF_ERR;
+  double rho = 0.0, rhoold = 1.0, normRes = 0.0, normX = 0.0;
+  long it;
+  for (it = 1; it <= A.maxIt; it++) {
+    // z = (symmetric multicolour Gauss-Seidel)^-1 r
+    for (int c = 0; c < A.ncol; c++) {
+      const int r0 = __ldg(A.cptr + c), nr = __ldg(A.cptr + c + 1) - r0;
+      for (int t = gtid; t < nr; t += nthr) sgs_row<B, true>(A, __ldg(A.crow + r0 + t), c, A.r, A.zz);
+      if (!grid_barrier(A.bar)) return;
+    }
+    double rz = 0.0;
+    for (int c = A.ncol - 1; c >= 0; c--) {
+      const int r0 = __ldg(A.cptr + c), nr = __ldg(A.cptr + c + 1) - r0;
+      for (int t = gtid; t < nr; t += nthr) rz += sgs_row<B, false>(A, __ldg(A.crow + r0 + t), c, A.zz, A.z);
+      if (c > 0 && !grid_barrier(A.bar)) return;
+    }
+    {
+      double v1[1] = {rz};
+      block_partials<1>(v1, mypart + 2);
+    }
+    if (!grid_barrier(A.bar)) return;
+    rho = part_total(A.part, G, 2);
+    const bool first = (it == 1);
+    const double beta = first ? 0.0 : rho / rhoold;
+    const double *pold = (it & 1) ? A.p0 : A.p1;
+    double *pnew = (it & 1) ? A.p1 : A.p0;
+    // q = A p with p = z + beta p_old, p.q
+    {
+      double pq = 0.0;
+      for (int I = I0; I < I1; I++) {
+        const double y = warp_row_spmv<B, double>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
+        if (lane < B) {
+          const size_t i = (size_t)I * B + lane;
+          const double zi = __ldcg(A.z + i);  // written by the sweeps' row mapping
+          const double pi = first ? zi : (zi + (beta * pold[i]));
+          pnew[i] = pi;
+          A.q[i] = y;
+          pq += pi * y;
+        }
+      }
+      double v1[1] = {pq};
+      block_partials<1>(v1, mypart + 3);
+    }
+    if (!grid_barrier(A.bar)) return;
+    const double alpha = rho / part_total(A.part, G, 3);
+    // x += alpha p, r -= alpha q, |r|^2 and |x|^2
+    {
+      double rr = 0.0, xx = 0.0;
+      for (size_t i = i0 + lane; i < i1; i += 32) {
+        const double xi = A.x[i] + (alpha * pnew[i]);
+        const double ri = A.r[i] - (alpha * A.q[i]);
+        A.x[i] = xi;
+        A.r[i] = ri;
+        rr += ri * ri;
+        xx += xi * xi;
+      }
+      double v2[2] = {rr, xx};
+      block_partials<2>(v2, mypart);
+    }
+    if (!grid_barrier(A.bar)) return;
+    normRes = sqrt(part_total(A.part, G, 0));
+    normX = sqrt(part_total(A.part, G, 1));
+    const bool conv = A.stop_rule == UFEM_STOP_REFERENCE ? normRes <= (A.eps * ((A.normA * normX) + A.normB))
+                                                         : normRes <= A.eps * A.normB;
+    if (!isfinite(normRes)) break;
+    if (conv) {
+      status = UFEM_AF_OK;
+      break;
+    }
+    rhoold = rho;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.res->iters = it > A.maxIt ? A.maxIt : it;
+    A.res->status = status;
+    A.res->normRes = normRes;
+    A.res->normX = normX;
+  }
 }
 }  // namespace
 
@@ -691,79 +919,33 @@ int cg_ssor_fp64(const DevMatrix &A, const double *d_b, double *d_x, double eps,
     std::vector<int> f(cptr.begin(), cptr.end() - 1);
     for (int I = 0; I < A.nbr; I++) crow[f[col[I]]++] = I;
   }
-  DBuf<int> d_col, d_crow;
-  DBuf<double> Minv, r, z, zz, p, q, sc;
-  if ((rv = d_col.upload(col.data(), col.size())) || (rv = d_crow.upload(crow.data(), crow.size()))) return rv;
-  if ((rv = Minv.alloc(n)) || (rv = r.alloc(n)) || (rv = z.alloc(n)) || (rv = zz.alloc(n)) || (rv = p.alloc(n)) ||
-      (rv = q.alloc(n)) || (rv = sc.alloc(2)))
+  DBuf<int> d_col, d_crow, d_cptr;
+  DBuf<double> Minv, r, z, zz, p0, p1, q, part;
+  DBuf<GridBar> bar;
+  DBuf<CgResult> res;
+  if ((rv = d_col.upload(col.data(), col.size())) || (rv = d_crow.upload(crow.data(), crow.size())) ||
+      (rv = d_cptr.upload(cptr.data(), cptr.size())))
     return rv;
-  Dots D;
-  if ((rv = D.init(4)) != UFEM_AF_OK) return rv;
-  unsigned g = (unsigned)((n + 255) / 256);
-  k_recip<<<g, 256>>>(n, M.p, Minv.p);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0);
-  spmv_launch(A, d_x, r.p);
-  k_sub<<<g, 256>>>(n, d_b, r.p, r.p);
-  long it;
-  int status = UFEM_AF_ERR;
-  for (it = 1; it <= maxIt; it++) {
-    for (int c = 0; c < ncol; c++) {
-      int nr = cptr[c + 1] - cptr[c];
-      unsigned gg = (unsigned)((nr + 127) / 128);
-      if (A.B == 3)
-        k_sgs_sweep<3, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                           r.p, zz.p);
-      else if (A.B == 2)
-        k_sgs_sweep<2, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                           r.p, zz.p);
-      else
-        k_sgs_sweep<1, true><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                           r.p, zz.p);
-    }
-    for (int c = ncol - 1; c >= 0; c--) {
-      int nr = cptr[c + 1] - cptr[c];
-      unsigned gg = (unsigned)((nr + 127) / 128);
-      if (A.B == 3)
-        k_sgs_sweep<3, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                            zz.p, z.p);
-      else if (A.B == 2)
-        k_sgs_sweep<2, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                            zz.p, z.p);
-      else
-        k_sgs_sweep<1, false><<<gg, 128>>>(nr, d_crow.p + cptr[c], d_col.p, c, A.rowptr, A.colind, A.val, Minv.p,
-                                            zz.p, z.p);
-    }
-    D.dot(n, r.p, z.p, 0);  // ro
-    if (it > 1) k_copy_scalar<<<1, 1>>>(sc.p + 1, sc.p + 0);
-    k_copy_scalar<<<1, 1>>>(sc.p + 0, D.vals.p + 0);
-    // sc[0] = ro, sc[1] = roro (beta = ro/roro)
-    k_cg_p<<<g, 256>>>(n, it == 1, sc.p, z.p, p.p);
-    spmv_launch(A, p.p, q.p);
-    D.dot(n, p.p, q.p, 1);
-    k_cg_xr<<<g, 256>>>(n, sc.p, D.vals.p + 1, d_x, r.p, p.p, q.p);
-    double normRes = host_norm(n, r.p);
-    double normX = host_norm(n, d_x);
-    bool conv = stop_rule == UFEM_STOP_REFERENCE ? normRes <= (eps * ((normA * normX) + normB))
-                                                 : normRes <= eps * normB;
-    if (!std::isfinite(normRes)) break;
-    if (conv) {
-      status = UFEM_AF_OK;
-      break;
-    }
-  }
+  if ((rv = Minv.alloc(n)) || (rv = r.alloc(n)) || (rv = z.alloc(n)) || (rv = zz.alloc(n)) || (rv = p0.alloc(n)) ||
+      (rv = p1.alloc(n)) || (rv = q.alloc(n)) || (rv = res.alloc(1)))
+    return rv;
+  UFEM_CUDA_TRY(cudaMemset(res.p, 0, sizeof(CgResult)));
+  UFEM_CUDA_TRY(cudaMemset(p0.p, 0, n * sizeof(double)));
+  UFEM_CUDA_TRY(cudaMemset(p1.p, 0, n * sizeof(double)));
+  k_recip<<<(unsigned)((n + 255) / 256), 256>>>(n, M.p, Minv.p);
   UFEM_CUDA_TRY(cudaGetLastError());
-  cudaEventRecord(e1);
-  cudaEventSynchronize(e1);
-  float tm = 0;
-  cudaEventElapsedTime(&tm, e0, e1);
-  if (ms) *ms = tm;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (iters) *iters = it > maxIt ? maxIt : it;
-  return status;
+  SsorArgs a{};
+  a.nbr = A.nbr; a.ncol = ncol; a.rowptr = A.rowptr; a.colind = A.colind; a.colour_of = d_col.p;
+  a.cptr = d_cptr.p; a.crow = d_crow.p; a.val = A.val; a.b = d_b; a.Minv = Minv.p; a.x = d_x; a.r = r.p;
+  a.zz = zz.p; a.z = z.p; a.p0 = p0.p; a.p1 = p1.p; a.q = q.p; a.res = res.p; a.eps = eps; a.normA = normA;
+  a.normB = normB; a.maxIt = maxIt; a.stop_rule = stop_rule;
+  void (*kern)(SsorArgs) = A.B == 1 ? k_cg_ssor<1> : (A.B == 2 ? k_cg_ssor<2> : k_cg_ssor<3>);
+  if ((rv = launch_persistent(kern, A, a, part, bar, ms)) != UFEM_AF_OK) return rv;
+  CgResult hr;
+  UFEM_CUDA_TRY(cudaMemcpy(&hr, res.p, sizeof(hr), cudaMemcpyDeviceToHost));
+  if (iters) *iters = hr.iters;
+  if (hr.status != UFEM_AF_OK) set_error("unconverged solution");
+  return hr.status;
 }
 
 // true residual |b - A x| / |b| in FP64 (host helper for the RELRES rule)
