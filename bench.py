@@ -68,12 +68,15 @@ WORKLOAD = ("MC 40x10x10 brick beam, 16 lognormal E zones + load factor (17 inpu
             "coarse-corrected on {c} POD modes of the same snapshots")
 UNEVEN = "MC brick beams 20x5x5 + 40x10x10 + 60x15x15, 512 samples each, one launch"
 KERNEL = {0: "k_batch_pcg<double,3,explicit>", 1: "k_batch_pcg<float,3,explicit>",
-          2: "k_batch_pcg<double,3,implicit>", 3: "k_batch_pcg<float,3,implicit>"}
+          2: "k_batch_pcg<double,3,implicit>", 3: "k_batch_pcg<float,3,implicit>",
+          4: "k_batch_pcg<float,3,implicit,fp32 products>"}
 PREC = {0: "FP64 PCG, explicit FP64 matrix per sample",
         1: "FP32 PCG on explicit FP32 matrices, FP64 solution and true-residual replacement",
         2: "FP64 PCG, blocks formed in the kernel from shared unit-E element blocks",
-        3: "FP32 PCG (FP32 vectors and products, blocks formed in the kernel from FP32 copies of the unit-E "
-           "blocks), FP64 solution and FP64 true-residual replacement"}
+        3: "FP32 PCG (FP32 vectors, FP64 products of blocks formed in the kernel from the unit-E blocks), "
+           "FP64 solution and FP64 true-residual replacement",
+        4: "FP32 PCG (FP32 vectors and FP32 SpMV products: blocks formed in the kernel from FP32 copies of the "
+           "unit-E blocks), FP64 solution and FP64 true-residual replacement"}
 GUESS = {0: "learned: least-squares quadratic model + MLP (BF16 tcgen05 network) of the POD coefficients",
          1: "each sample's POD-Galerkin coefficients (Phi^T K_s Phi c = Phi^T f_s) on the learned POD basis",
          2: "the least-squares quadratic model alone (no network)"}
@@ -106,10 +109,10 @@ def parse():
                    help="warm-start guess: 0 = the learned coefficients (least-squares model + MLP, default), "
                         "1 = each sample's POD-Galerkin coefficients on the learned basis, 2 = the least-squares "
                         "model alone")
-    p.add_argument("--precision", type=int, default=3,
-                   help="3: FP32 PCG with FP64 solution and true-residual replacement, blocks formed in the kernel "
-                        "(default); 2: FP64 PCG, blocks formed in the kernel; 1: FP32 PCG on explicit FP32 "
-                        "matrices; 0: FP64 explicit")
+    p.add_argument("--precision", type=int, default=4,
+                   help="4: FP32 PCG with FP32 SpMV products, FP64 solution and true-residual replacement, blocks "
+                        "formed in the kernel (default); 3: the same with FP64 products; 2: FP64 PCG, blocks formed "
+                        "in the kernel; 1: FP32 PCG on explicit FP32 matrices; 0: FP64 explicit")
     p.add_argument("--oracle-samples", type=int, default=64,
                    help="evaluation samples checked against the FP64 oracle (displacements, von Mises)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
@@ -130,6 +133,9 @@ def parse():
 
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
+           4: ("k_batch_pcg_fp32prod_coarse_40x10x10_2048samples.md",
+               "40x10x10 16 E zones x 2048 samples, FP32 implicit form with FP32 products, coarse space of a short "
+               "warm-start training, 40 iterations"),
            3: ("k_batch_pcg_fp32_coarse_40x10x10_2048samples.md",
                "40x10x10 16 E zones x 2048 samples, FP32 implicit form, coarse space of a short warm-start "
                "training, 40 iterations"),
@@ -146,7 +152,7 @@ def profile_case(a):
     from ufem_b200.api import GpuModel
     from ufem_b200.mc import mc_solve
     from ufem_b200 import meshgen as mg
-    if a.precision in (2, 3):
+    if a.precision in (2, 3, 4):
         m = mg.warm_beam(*WARM_MESH, zones=WARM_ZONES)
         f = mg.warm_samples(m, a.profile_samples)
         if not a.no_coarse:
@@ -161,7 +167,7 @@ def profile_case(a):
         m = mg.beam_brick(60, 15, 15, 8.0, 2.0, 2.0, per_element_material=True)
         mg.mc_attach_vars(m)
         f = mg.mc_samples(m, mesh_id=2, nsamp=128)
-    if a.precision not in (2, 3) or a.no_coarse:
+    if a.precision not in (2, 3, 4) or a.no_coarse:
         g = GpuModel(m)
     for _ in range(2):
         res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block,
@@ -856,8 +862,8 @@ def ours(a):
     dd = {"in": d_in, "out": d_out, "st": d_st, "it": d_it}
     forms = []
     if not a.no_other:
-        combos = [(a.guess, a.precision, 0), (a.guess, 2, 1), (a.guess, 2, 0), (1, a.precision, 1), (1, 2, 1),
-                  (2, a.precision, 1), (a.guess, 1, 0), (a.guess, 0, 0)]
+        combos = [(a.guess, 3, 1), (a.guess, 3, 0), (a.guess, 2, 1), (a.guess, 2, 0), (1, a.precision, 1),
+                  (1, 2, 1), (2, a.precision, 1), (a.guess, 1, 0), (a.guess, 0, 0)]
         seen = {(a.guess, a.precision, opt.coarse)}
         for gm, pr, co in combos:
             if (gm, pr, co) in seen:
@@ -977,7 +983,7 @@ def ours(a):
         result = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32 inner / fp64 refinement" if a.precision in (1, 3) else "f64",
+            "vs_baseline": None, "dtype": "fp32 inner / fp64 refinement" if a.precision in (1, 3, 4) else "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD.format(c=a.coarse_modes), "samples_per_step": solves_step, "rel_res": 1e-8,
                        "ndof": g.ndof, "precision": PREC[a.precision], "guess": GUESS[a.guess],

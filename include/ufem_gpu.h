@@ -226,8 +226,14 @@ int monte_solution_batch(char *param, long nsamp, const double *ifld, double *of
  * f - K u from time to time; 2: FP64 PCG with no per-sample matrix -- every
  * block is formed inside the PCG kernel from the mesh's unit-E element blocks
  * (summed per random E variable) times the sample's E values, which holds
- * because K_e is linear in E for the isotropic material.  A sample converges
- * when its true relative residual |f - K u| / |f| <= tol. */
+ * because K_e is linear in E for the isotropic material; 3: the same implicit
+ * form with FP32 work vectors (r, z, p, q, the diagonal) and FP64 products,
+ * FP64 solution and FP64 true-residual replacement as in 1; 4: as 3 with the
+ * SpMV's products and sums in FP32 (FP32 unit blocks and multipliers: the
+ * inner FP32 matrix) -- fastest with a warm start and the coarse space, but
+ * from zero it needs far more iterations (the warm start's fallback re-solves
+ * in precision 3).  A sample converges when its true relative residual
+ * |f - K u| / |f| <= tol. */
 typedef struct ufem_mc_options {
   int precision;
   double tol;

@@ -11,7 +11,8 @@ the preconditioner); 256 fresh samples are solved by
      replacement (precision 1), and
   C. the MLP guess + FP32 implicit batched PCG (FP32 work vectors, blocks
      formed in the kernel in FP64, FP64 solution and true-residual
-     replacement) with the coarse correction (precision 3),
+     replacement) with the coarse correction (precision 3), and the same
+     with FP32 SpMV products (precision 4, the bench headline's form),
 
 each with the stopping rule tightened to a true relative residual of 1e-10
 (the FP64 floor of |f - K u| / |f| on this beam is about 1e-11:
@@ -193,6 +194,20 @@ def test_mlp_fp32_implicit_coarse_within_1e8_of_oracle(warm40):
     assert np.isin(st_w, [0, 4]).all()
     _check_against_oracle(m, ev, u, oracle, "MLP + FP32 implicit + coarse")
     _check_outputs(m, ev, of, oracle, "MLP + FP32 implicit + coarse, ufem_warm_solve")
+
+
+def test_mlp_fp32_products_coarse_within_1e8_of_oracle(warm40):
+    """Precision 4: FP32 SpMV products (the inner FP32 matrix) with the warm
+    start and the coarse correction, FP64 true-residual replacement."""
+    m, g, ws, st, ev, oracle = warm40
+    ws.set_guess_mode(0)
+    u0 = ws.guess(ev)
+    u, status, iters = _solve_from(g, ev, u0, precision=4, tol=SOLVE_TOL)
+    of, st_w, it_w, wst = ws.solve(ev, precision=4, tol=SOLVE_TOL)
+    assert (status == 0).all()
+    assert np.isin(st_w, [0, 4]).all()
+    _check_against_oracle(m, ev, u, oracle, "MLP + FP32 products + coarse")
+    _check_outputs(m, ev, of, oracle, "MLP + FP32 products + coarse, ufem_warm_solve")
 
 
 def test_beam_80x20x20_within_1e8_of_reference():

@@ -65,6 +65,10 @@ struct McOut {
   int reac;    // reaction index
 };
 
+// FP32 unit blocks of the implicit form: B*B values padded to 12 floats
+// (three 16-byte loads per contribution)
+constexpr int kW32Stride = 12;
+
 struct McPlan {
   bool built = false;
   int s = 0;                       // element matrix size (8 or 24)
@@ -90,6 +94,7 @@ struct McPlan {
   std::vector<int> mult_col;
   DBuf<int> d_mult_col, cptr, crow;  // contributions of block k / of block row I
   DBuf<double> cval;               // [nc][cstride]: B*B values, then (multiplier << 32 | J)
+  DBuf<float> w32;                 // [nc][12]: the B*B values in FP32 (precision 4's SpMV products)
   DBuf<int> sperm;                 // block rows in the order the gathering phases visit them
   long nc = 0;
   // coarse space of the preconditioner (ufem_mc_set_coarse): Wc [n][cmodes]
@@ -385,6 +390,12 @@ static int build_implicit(ufem_model *m, McPlan *P) {
   P->cstride = stride;
   P->nc = cptr[m->nnzb];
   if (cval.empty()) cval.assign(stride, 0.0);
+  {
+    std::vector<float> w32((size_t)std::max<long>(1, P->nc) * kW32Stride, 0.0f);
+    for (long c = 0; c < P->nc; c++)
+      for (int t = 0; t < BB; t++) w32[(size_t)c * kW32Stride + t] = (float)cval[(size_t)c * stride + t];
+    if ((rv = P->w32.upload(w32.data(), w32.size()))) return rv;
+  }
   if ((rv = P->cptr.upload(cptr.data(), cptr.size())) || (rv = P->cval.upload(cval.data(), cval.size())) ||
       (rv = P->crow.upload(crow.data(), crow.size())) ||
       (rv = P->d_mult_col.upload(P->mult_col.data(), P->mult_col.size())))
@@ -705,6 +716,7 @@ struct BMesh {
   const int *sperm;     // block rows in the visiting order of the gathering phases
   const double *cval;
   const double *mult;
+  const float *w32;     // FP32 copies of the unit blocks (precision 4)
   const unsigned char *fixed;
   int cstride;
   int nmult;            // multipliers (rows of mult)
@@ -809,20 +821,23 @@ __device__ __forceinline__ void prof_flush(unsigned long long *prof) {
 extern __shared__ __align__(1024) uint8_t s_dyn_smem[];
 
 // acc[a][v] += mult[var_c][s] * (W_c X_{J_c})[a] over the contributions
-// [c0, c1) of one block row of the implicit form, in FP64.  The row's
-// contribution keys (multiplier << 32 | J) are fetched 32 at a time, one per
-// lane, and broadcast; the gathers of U contributions are issued together so
-// that U neighbour loads are in flight per warp.  W and the multipliers are
+// [c0, c1) of one block row of the implicit form.  The row's contribution
+// keys (multiplier << 32 | J) are fetched 32 at a time, one per lane, and
+// broadcast; the gathers of U contributions are issued together so that U
+// neighbour loads are in flight per warp.  W and the multipliers are
 // read-only for the whole kernel (non-coherent loads); X is written by other
 // blocks during the kernel (loads after the phase's grid barrier).  LT is the
 // kernel's lane layout (double: sample pairs 64 apart; float: 4 adjacent
-// samples), XT the type of X (the FP32 kernel gathers FP32 z, and FP64 x for
-// its true residuals).  SMULT: the multipliers come from the tile's
-// shared-memory copy ([nmult][GS] doubles) instead of global memory.
-template <typename LT, typename XT, int B, int VN, int U, bool SMULT>
+// samples), XT the type of X (the FP32 kernels gather FP32 z, and FP64 x for
+// their true residuals), CT the type of the products and sums: FP64 (W and
+// the multipliers in FP64) or FP32 (W from the FP32 copies, the multipliers
+// rounded: precision 4).  SMULT: the multipliers come from the tile's
+// shared-memory copy ([nmult][GS] of CT) instead of global memory.
+template <typename LT, typename XT, typename CT, int B, int VN, int U, bool SMULT>
 __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, int cstride,
-                                             const double *__restrict__ mult, const double *s_mult, const XT *X,
-                                             int S, int sb, int c0, int c1, double (&acc)[B][VN]) {
+                                             const float *__restrict__ w32, const double *__restrict__ mult,
+                                             const CT *s_mult, const XT *X, int S, int sb, int c0, int c1,
+                                             CT (&acc)[B][VN]) {
   static_assert(sizeof(XT) == 8 || sizeof(LT) == 4, "FP32 vectors only in the FP32 lane layout");
   constexpr int GS = 32 * VN;
   const int lane = threadIdx.x & 31;
@@ -848,31 +863,43 @@ __device__ __forceinline__ void implicit_row(const double *__restrict__ cval, in
 #pragma unroll
       for (int u = 0; u < U; u++) {
         if (j + u >= cnt) break;
-        const double *w = cval + (size_t)(cb + j + u) * cstride;
-        double W[B * B];
+        CT W[B * B];
+        if constexpr (sizeof(CT) == 8) {
+          const double *w = cval + (size_t)(cb + j + u) * cstride;
 #pragma unroll
-        for (int h = 0; h < (B * B) / 2; h++) {
-          const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
-          W[2 * h] = v.x;
-          W[2 * h + 1] = v.y;
+          for (int h = 0; h < (B * B) / 2; h++) {
+            const double2 v = __ldg(reinterpret_cast<const double2 *>(w) + h);
+            W[2 * h] = v.x;
+            W[2 * h + 1] = v.y;
+          }
+          if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
+        } else {
+          const float4 *w = reinterpret_cast<const float4 *>(w32 + (size_t)(cb + j + u) * kW32Stride);
+#pragma unroll
+          for (int h = 0; h < (B * B + 3) / 4; h++) {
+            const float4 v = __ldg(w + h);
+            const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (4 * h + q < B * B) W[4 * h + q] = e[q];
+          }
         }
-        if ((B * B) & 1) W[B * B - 1] = __ldg(w + B * B - 1);
-        double a[VN];
+        CT a[VN];
         if constexpr (SMULT) {
-          const double *sm = s_mult + vars[u] * GS;
+          const CT *sm = s_mult + vars[u] * GS;
 #pragma unroll
           for (int v = 0; v < VN; v++) a[v] = sm[lane_sample<LT, VN>(lane, v)];
         } else {
 #pragma unroll
-          for (int v = 0; v < VN; v++) a[v] = av[u][v];
+          for (int v = 0; v < VN; v++) a[v] = (CT)av[u][v];
         }
 #pragma unroll
         for (int r = 0; r < B; r++)
 #pragma unroll
           for (int v = 0; v < VN; v++) {
-            double t = 0.0;
+            CT t = 0;
 #pragma unroll
-            for (int b = 0; b < B; b++) t = fma(W[r * B + b], (double)xv[u][b][v], t);
+            for (int b = 0; b < B; b++) t = fma(W[r * B + b], (CT)xv[u][b][v], t);
             acc[r][v] = fma(a[v], t, acc[r][v]);
           }
       }
@@ -920,14 +947,17 @@ __device__ __forceinline__ void group_close(int *cnt, int ntpg, int g, const dou
 // samples; pnew = p on the own rows; partial p.q per sample.  Explicit form:
 // p is formed at every gathered neighbour.  Implicit form: q = A z + beta
 // q_old (A p_old is the previous q), so only z is gathered.
-template <typename T, int B, bool IMP, int UN, int VN, int NW>
+template <typename T, int B, bool IMP, int UN, int VN, int NW, bool F32P = false>
 __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, const T *s_beta, bool first,
                                           const T *pold, T *pnew, double (*s_red)[32 * VN]) {
-  // the implicit form forms every product and sum in FP64 (its unit blocks
-  // and multipliers are FP64) whatever the vector precision T: with FP32
-  // products the FP32 form took 565 instead of 289 Jacobi iterations from
-  // zero on the 16-zone beam, and stagnated with the coarse correction
-  using AT = typename std::conditional<IMP, double, T>::type;
+  // The implicit form forms every product and sum in FP64 (its unit blocks
+  // and multipliers are FP64) whatever the vector precision T, except in
+  // precision 4 (F32P: FP32 unit blocks, multipliers and sums, the inner FP32
+  // matrix).  FP32 products lose the cancellation of K z for smooth z: from
+  // zero on the 16-zone beam 565 instead of 289 Jacobi iterations, and no
+  // convergence with the coarse correction; warm-started with the coarse
+  // correction they keep the iteration count and are faster.
+  using AT = typename std::conditional<IMP, typename std::conditional<F32P, float, double>::type, T>::type;
   constexpr int GS = 32 * VN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = M.S;
@@ -956,10 +986,10 @@ __device__ __forceinline__ void tile_spmv(const BMesh<T> &M, int g, int chunk, c
       for (int v = 0; v < VN; v++) acc[a][v] = 0;
     if constexpr (IMP) {
       if (s_mult)
-        implicit_row<T, T, B, VN, UN, true>(M.cval, M.cstride, M.mult, s_mult, M.z, S, sb, __ldg(M.crow + I),
+        implicit_row<T, T, AT, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.z, S, sb, __ldg(M.crow + I),
                                             __ldg(M.crow + I + 1), acc);
       else
-        implicit_row<T, T, B, VN, UN, false>(M.cval, M.cstride, M.mult, nullptr, M.z, S, sb, __ldg(M.crow + I),
+        implicit_row<T, T, AT, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.z, S, sb, __ldg(M.crow + I),
                                              __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
@@ -1143,10 +1173,10 @@ __device__ __forceinline__ void tile_true_residual(const BMesh<T> &M, int g, int
       for (int v = 0; v < VN; v++) acc[a][v] = 0.0;
     if constexpr (IMP) {
       if (s_mult)
-        implicit_row<T, double, B, VN, UN, true>(M.cval, M.cstride, M.mult, s_mult, M.x, S, sb, __ldg(M.crow + I),
+        implicit_row<T, double, double, B, VN, UN, true>(M.cval, M.cstride, M.w32, M.mult, s_mult, M.x, S, sb, __ldg(M.crow + I),
                                                  __ldg(M.crow + I + 1), acc);
       else
-        implicit_row<T, double, B, VN, UN, false>(M.cval, M.cstride, M.mult, nullptr, M.x, S, sb, __ldg(M.crow + I),
+        implicit_row<T, double, double, B, VN, UN, false>(M.cval, M.cstride, M.w32, M.mult, nullptr, M.x, S, sb, __ldg(M.crow + I),
                                                   __ldg(M.crow + I + 1), acc);
     } else {
       const int k0 = __ldg(M.rowptr + I), k1 = __ldg(M.rowptr + I + 1);
@@ -1499,7 +1529,7 @@ __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_m
   return true;
 }
 
-template <typename T, int B, bool IMP, int UN, int VN, bool CO, int NW>
+template <typename T, int B, bool IMP, int UN, int VN, bool CO, int NW, bool F32P>
 __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
   constexpr int GS = 32 * VN;
   constexpr bool kCoarse = CO;
@@ -1612,7 +1642,7 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
       }
       const T *pold = (k & 1) ? M.p0 : M.p1;
       T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B, IMP, UN, VN, NW>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+      tile_spmv<T, B, IMP, UN, VN, NW, F32P>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
     }
     prof_end();
     if (!grid_barrier(A.bar)) return;
@@ -1705,7 +1735,7 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
 // block (the Jacobi instance: two blocks of kThreads); the block holds
 // kCoarseCols TMEM columns and kCoarseSmem bytes of dynamic shared memory
 // for the whole launch.
-template <typename T, int B, bool IMP, int UN, int VN, bool CO = false>
+template <typename T, int B, bool IMP, int UN, int VN, bool CO = false, bool F32P = false>
 __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP ? UFEM_PCG_MIN_BLOCKS : 2))
     k_batch_pcg(BArgs<T> A) {
   constexpr bool kCoarse = CO;
@@ -1721,7 +1751,7 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
       tc::fence_after_sync();
     }
   }
-  pcg_body<T, B, IMP, UN, VN, CO, (CO ? kCoarseThreads : kThreads) / 32>(A);
+  pcg_body<T, B, IMP, UN, VN, CO, (CO ? kCoarseThreads : kThreads) / 32, F32P>(A);
   if constexpr (kCoarse) {
     if (A.coarse) {
       tc::fence_before_sync();
@@ -1918,7 +1948,7 @@ static void tune_save(const std::string &path) {
 
 // the batch shape a tuned choice is valid for: device, precision, element
 // family, and per mesh its block rows and padded sample count
-static bool implicit_form(int precision) { return precision == 2 || precision == 3; }
+static bool implicit_form(int precision) { return precision >= 2 && precision <= 4; }
 
 static int coarse_modes(int nmesh, ufem_model *const *models, const ufem_mc_options &opt) {
   if (!implicit_form(opt.precision) || !opt.coarse) return 0;
@@ -2026,7 +2056,7 @@ struct EvTimer {
   }
 };
 
-template <typename T, bool IMP, int VN>
+template <typename T, bool IMP, int VN, bool F32P = false>
 int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, const std::vector<McPlan *> &plans,
             const ufem_mc_options &opt, long *iters_run) {
   constexpr int GS = 32 * VN;
@@ -2043,6 +2073,15 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   void (*kern)(BArgs<T>) = nullptr;
   if constexpr (!IMP) {
     kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 1, VN> : k_batch_pcg<T, 2, IMP, 1, VN>;
+  } else if constexpr (F32P) {
+    // FP32 products (precision 4): 2 or 4 contributions in flight
+    const int un = opt.unroll > 0 ? opt.unroll : 2;
+    if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN, false, true> : k_batch_pcg<T, 2, IMP, 2, VN, false, true>;
+    else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN, false, true> : k_batch_pcg<T, 2, IMP, 4, VN, false, true>;
+    if (coarse) {
+      if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN, true, true> : k_batch_pcg<T, 2, IMP, 2, VN, true, true>;
+      else kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 4, VN, true, true> : k_batch_pcg<T, 2, IMP, 4, VN, true, true>;
+    }
   } else {
     const int un = opt.unroll > 0 ? opt.unroll : 2;
     if (un <= 2) kern = (B == 3) ? k_batch_pcg<T, 3, IMP, 2, VN> : k_batch_pcg<T, 2, IMP, 2, VN>;
@@ -2062,7 +2101,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   int max_nmult = 0;
   if constexpr (IMP)
     for (int k = 0; k < nmesh; k++) max_nmult = std::max(max_nmult, plans[k]->nmult);
-  const size_t mult_bytes = (size_t)max_nmult * GS * sizeof(double);
+  const size_t mult_bytes = (size_t)max_nmult * GS * sizeof(double);  // the true residual stages FP64
   const bool smult = IMP && max_nmult > 0 && mult_bytes <= kMultSmem;
   const size_t dsmem = std::max(coarse ? kCoarseSmem : (size_t)0, smult ? mult_bytes : (size_t)0);
   // one block per SM either way (tensor memory): the rest of the unified
@@ -2119,6 +2158,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     b.fixed = m->d_fixed.p;
     b.cstride = plans[k]->cstride;
     b.sperm = plans[k]->sperm.p;
+    b.w32 = plans[k]->w32.p;
     b.nmult = plans[k]->nmult;
     b.smult = smult ? 1 : 0;
     const size_t n = (size_t)m->nDOFAct * w.S;
@@ -2363,6 +2403,10 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   else ufem_mc_default_options(&opt);
   std::memset(&g_stats, 0, sizeof(g_stats));
   int rv;
+  if (opt.precision < 0 || opt.precision > 4) {
+    set_error("batched Monte Carlo: precision 0 to 4");
+    return UFEM_AF_ERR_VAL;
+  }
   if (nmesh < 1 || nmesh > kMaxMeshes) {
     set_error("batched Monte Carlo: 1 to 8 meshes per launch");
     return UFEM_AF_ERR_SIZ;
@@ -2406,7 +2450,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
       }
       if (opt.precision == 1) {
         if ((rv = w.V32.ensure(nv)) || (rv = w.M32.ensure(n))) return rv;
-      } else if (opt.precision == 3) {
+      } else if (opt.precision >= 3) {
         if ((rv = w.M32.ensure(n))) return rv;
       }
       const long ne = (long)m->eLen * w.S;
@@ -2430,7 +2474,7 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
                                                                     P->cval.p, P->cstride, w.mult.p,
                                                                     m->d_fixed.p, w.M64.p);
         g_stats.kernel_launches += 1;  // two kernels here in place of the assembly
-        if (opt.precision == 3) {
+        if (opt.precision >= 3) {
           k_diag_f32<<<(unsigned)((n + 255) / 256), 256>>>((long)n, w.M64.p, w.M32.p);
           g_stats.kernel_launches += 1;
         }
@@ -2477,6 +2521,8 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
   if (opt.precision == 1) rv = run_pcg<float, false, 4>(nmesh, models, W, plans, opt, &its);
   // FP32 implicit form: 4 adjacent samples per lane (one 16-byte load per row)
   else if (opt.precision == 3) rv = run_pcg<float, true, 4>(nmesh, models, W, plans, opt, &its);
+  // FP32 vectors and FP32 SpMV products on the implicit form
+  else if (opt.precision == 4) rv = run_pcg<float, true, 4, true>(nmesh, models, W, plans, opt, &its);
   // implicit form: 4 samples per lane unless 2 is asked for (measured best on B200)
   else if (opt.precision == 2 && (opt.lane_samples != 2 || coarse_modes(nmesh, models, opt) > 0))
     rv = run_pcg<double, true, 4>(nmesh, models, W, plans, opt, &its);
@@ -2564,7 +2610,8 @@ extern "C" int ufem_mc_autotune(int nmesh, ufem_model *const *models, const long
     unrolls = {2, 4, 8};
     lanes = {2, 4};
     // the coarse correction needs 128-sample groups; the FP32 form holds 4 samples per lane
-    if (coarse_modes(nmesh, models, base) > 0 || base.precision == 3) lanes = {4};
+    if (coarse_modes(nmesh, models, base) > 0 || base.precision >= 3) lanes = {4};
+    if (base.precision == 4) unrolls = {2, 4};
   } else {
     unrolls = {4};
     lanes = {0};

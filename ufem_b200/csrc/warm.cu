@@ -1351,7 +1351,11 @@ int warm_solve_ordered(ufem_warm *w, long nsamp, const double *d_ifld, double *d
     const int Sf = padded_S(nf);
     if ((rv = ufb.ensure((size_t)n * Sf))) return rv;
     double *pu = ufb.p;
-    if ((rv = mc_solve_device(1, &m, &nf, &pin, d_ofld ? &pof : nullptr, &ps, &pi, nullptr, &pu, &opt))) return rv;
+    // from zero, FP32 SpMV products (precision 4) converge poorly: the
+    // fallback forms the products in FP64 (precision 3)
+    ufem_mc_options fopt = opt;
+    if (fopt.precision == 4) fopt.precision = 3;
+    if ((rv = mc_solve_device(1, &m, &nf, &pin, d_ofld ? &pof : nullptr, &ps, &pi, nullptr, &pu, &fopt))) return rv;
     ufem_mc_stats ms;
     ufem_mc_get_stats(&ms);
     st.kernel_launches += ms.kernel_launches + 1;  // + the input gather
