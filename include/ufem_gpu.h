@@ -127,6 +127,9 @@ int ufem_export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *
 int ufem_bsr_shape(const ufem_model *m, long *b, long *nbr, long *nnzb);
 int ufem_get_bsr_pattern(const ufem_model *m, int *rowptr, int *colind);
 long ufem_num_colours(const ufem_model *m);
+/* the colour of every element (eLen ints): elements of one colour share no
+ * node, and the assembly adds the colours in order */
+int ufem_get_element_colours(const ufem_model *m, int *colour);
 
 /* ---- the static path (replaces femSolve's body, fem/fem_sol.c:1655-1760) -- */
 
@@ -164,6 +167,11 @@ int ufem_get_stresses(const ufem_model *m, double *sig, double *von_mises);
 /* reactions in the order of fem_sol_res_alloc (fem/fem_sol.c:676-722) */
 long ufem_num_reactions(const ufem_model *m);
 int ufem_get_reactions(const ufem_model *m, long *node, long *dof, double *val);
+/* wall-clock milliseconds of the model's set-up by ufem_read_input or
+ * ufem_model_from_tables, six stages: [0] file read, [1] parse, [2] host
+ * tables, [3] DOF numbering + block pattern + scatter map + element colouring
+ * (device kernels), [4] supports and loads, [5] upload of the rest */
+int ufem_get_ingest_ms(const ufem_model *m, double *ms);
 /* timing of the last call of each phase, milliseconds (CUDA events) */
 int ufem_get_phase_ms(const ufem_model *m, double *fill_ms, double *bc_ms, double *solve_ms,
                       double *results_ms);

@@ -87,6 +87,7 @@ _SIGS = {
     "ufem_bsr_shape": (C.c_int, [C.c_void_p, _l, _l, _l]),
     "ufem_get_bsr_pattern": (C.c_int, [C.c_void_p, _i, _i]),
     "ufem_num_colours": (C.c_long, [C.c_void_p]),
+    "ufem_get_element_colours": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "ufem_fill_K": (C.c_int, [C.c_void_p, C.c_long]),
     "ufem_add_loads": (C.c_int, [C.c_void_p]),
     "ufem_add_disps": (C.c_int, [C.c_void_p]),
@@ -101,6 +102,7 @@ _SIGS = {
     "ufem_num_reactions": (C.c_long, [C.c_void_p]),
     "ufem_get_reactions": (C.c_int, [C.c_void_p, _l, _l, _d]),
     "ufem_get_phase_ms": (C.c_int, [C.c_void_p, _d, _d, _d, _d]),
+    "ufem_get_ingest_ms": (C.c_int, [C.c_void_p, _d]),
     "ufem_eqs_cgwj": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),
     "ufem_eqs_bicgs": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),
     "ufem_eqs_cgwssor": (C.c_int, [C.c_long, _l, _l, _l, _d, _d, _d, C.c_double, C.c_long]),

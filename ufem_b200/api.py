@@ -137,6 +137,12 @@ class GpuModel:
     def colours(self) -> int:
         return _lib.load().ufem_num_colours(self.h)
 
+    def element_colours(self, n_elements: int | None = None):
+        """Colour of each element (a model read from a file needs its element count)."""
+        col = np.zeros(n_elements if n_elements is not None else self.model.eLen, np.int32)
+        _lib.check("ufem_get_element_colours", _lib.load().ufem_get_element_colours(self.h, _ip(col)))
+        return col
+
     # ---- the femSolve steps ----------------------------------------------------
     def fill_K(self, mode: int = 0):
         _lib.check("ufem_fill_K", _lib.load().ufem_fill_K(self.h, mode))
@@ -200,6 +206,11 @@ class GpuModel:
         node, dof, val = np.zeros(n, np.int64), np.zeros(n, np.int64), np.zeros(n)
         _lib.check("ufem_get_reactions", L.ufem_get_reactions(self.h, _lp(node), _lp(dof), _dp(val)))
         return node, dof, val
+
+    def ingest_ms(self):
+        v = np.zeros(6)
+        _lib.check("ufem_get_ingest_ms", _lib.load().ufem_get_ingest_ms(self.h, _dp(v)))
+        return dict(zip(("read", "parse", "tables", "pattern", "loads", "upload"), v.tolist()))
 
     def phase_ms(self):
         v = [C.c_double() for _ in range(4)]

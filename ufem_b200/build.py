@@ -23,7 +23,7 @@ OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libufem_gpu.so")
 
 SOURCES = ["model.cpp", "kernels.cu", "solve.cu", "batch.cu", "capi.cu", "monte.cu", "mcout.cu", "mlp.cu", "warm.cu",
-           "selftest.cu"]
+           "selftest.cu", "pattern.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMPILE_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17",

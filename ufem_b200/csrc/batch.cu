@@ -169,6 +169,7 @@ static std::vector<int> morton_row_order(const ufem_model *m) {
 
 static int build_plan(ufem_model *m, McPlan *P) {
   int rv;
+  if ((rv = host_pattern(m)) != UFEM_AF_OK) return rv;
   {
     const std::vector<int> order = morton_row_order(m);
     if ((rv = P->sperm.upload(order.data(), order.size())) != UFEM_AF_OK) return rv;
@@ -250,7 +251,7 @@ static int build_plan(ufem_model *m, McPlan *P) {
       return UFEM_AF_ERR_TYP;
     }
     if (l.type != 3) continue;
-    long p = m->nDOFfld[l.node * KNOWN_DOFS + l.dir - 1];
+    long p = m->dof(l.node * KNOWN_DOFS + l.dir - 1);
     if (p <= 0) continue;
     if (load_var[j] >= 0) {
       P->ovr_row.push_back((int)(p - 1));
@@ -285,14 +286,14 @@ static int build_plan(ufem_model *m, McPlan *P) {
       // RES_D, RES_D_MAX, RES_D_MIN: u at node item, DOF sub (fem/fem_mont.c:524-548;
       // max/min against the zeroed output)
       if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS)
-        o.row = (int)m->nDOFfld[item * KNOWN_DOFS + sub - 1] - 1;
+        o.row = (int)m->dof(item * KNOWN_DOFS + sub - 1) - 1;
     } else if (o.type == 17) {
       // RES_D_SUM adds nDOFfld[nDOFfld[pos]], the DOF number of another slot
       // (fem/fem_mont.c:550-555); kept as a constant in `row`
       o.row = 0;
       if (item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS) {
-        const long p = m->nDOFfld[item * KNOWN_DOFS + sub - 1];
-        if (p >= 0 && p < (long)m->nDOFfld.size()) o.row = (int)m->nDOFfld[p];
+        const long p = m->dof(item * KNOWN_DOFS + sub - 1);
+        if (p >= 0 && p < m->dof_slots()) o.row = (int)m->dof(p);
       }
     } else if (o.type == 9) {  // RES_R: reaction of node item, DOF sub
       for (size_t r = 0; r < m->reacNode.size(); r++)
@@ -324,6 +325,7 @@ static int build_plan(ufem_model *m, McPlan *P) {
 // identity (fem/fem_loads.c:158-166).
 static int build_implicit(ufem_model *m, McPlan *P) {
   int rv;
+  if ((rv = host_pattern(m)) != UFEM_AF_OK) return rv;
   const int B = m->b, nn = m->nn, se = P->s, BB = B * B;
   const int stride = (BB + 2) & ~1;  // values + index, a multiple of 16 bytes
   std::vector<double> Kh((size_t)m->eLen * se * se);

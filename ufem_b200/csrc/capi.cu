@@ -112,7 +112,7 @@ int ufem_model_set_mc_vars(ufem_model *m, long ilen, long olen, const long *vars
 long ufem_ndof(const ufem_model *m) { return m ? m->nDOFAct : 0; }
 
 int ufem_get_ndoffld(const ufem_model *m, long *nDOFfld) {
-  std::memcpy(nDOFfld, m->nDOFfld.data(), m->nDOFfld.size() * sizeof(long));
+  for (long s = 0; s < m->dof_slots(); s++) nDOFfld[s] = m->dof(s);
   return UFEM_AF_OK;
 }
 
@@ -128,12 +128,21 @@ int ufem_bsr_shape(const ufem_model *m, long *b, long *nbr, long *nnzb) {
 }
 
 int ufem_get_bsr_pattern(const ufem_model *m, int *rowptr, int *colind) {
+  const int rv = host_pattern(m);
+  if (rv != UFEM_AF_OK) return rv;
   if (rowptr) std::memcpy(rowptr, m->rowptr.data(), m->rowptr.size() * sizeof(int));
   if (colind) std::memcpy(colind, m->colind.data(), m->colind.size() * sizeof(int));
   return UFEM_AF_OK;
 }
 
 long ufem_num_colours(const ufem_model *m) { return m->ncolours; }
+
+int ufem_get_element_colours(const ufem_model *m, int *colour) {
+  if (!colour) return UFEM_AF_OK;
+  for (int c = 0; c < m->ncolours; c++)
+    for (int k = m->colour_ptr[c]; k < m->colour_ptr[c + 1]; k++) colour[m->colour_elems[k]] = c;
+  return UFEM_AF_OK;
+}
 
 int ufem_fill_K(ufem_model *m, long mode) {
   if (mode == 0) return gpu_fill_K(m);
@@ -237,6 +246,11 @@ int ufem_get_reactions(const ufem_model *m, long *node, long *dof, double *val) 
     if (dof) dof[r] = m->reacDof[r];
     if (val) val[r] = r < m->reacVal.size() ? m->reacVal[r] : 0.0;
   }
+  return UFEM_AF_OK;
+}
+
+int ufem_get_ingest_ms(const ufem_model *m, double *ms) {
+  if (ms) std::memcpy(ms, m->ms_ingest, sizeof(m->ms_ingest));
   return UFEM_AF_OK;
 }
 

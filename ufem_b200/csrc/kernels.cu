@@ -512,21 +512,10 @@ __global__ void __launch_bounds__(EPB * 32) k_quad_results(const int *__restrict
 
 // ---------------------------------------------------------------------------
 int upload_model(ufem_model *m) {
+  // the element nodes, pattern, scatter map, colour groups and block rows
+  // are already on the device (gpu_build_pattern)
   int rv;
-  UFEM_CUDA_TRY(cudaGetDevice(&m->device));
-  std::vector<int> blkrow(m->nnzb);
-  for (int r = 0; r < m->nbr; r++)
-    for (int k = m->rowptr[r]; k < m->rowptr[r + 1]; k++) blkrow[k] = r;
-  std::vector<int> nrank(m->node_rank.begin(), m->node_rank.end());
   if ((rv = m->d_xyz.upload(m->xyz.data(), m->xyz.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_enodes.upload(m->enodes.data(), m->enodes.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_emap.upload(m->emap.data(), m->emap.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_colour_elems.upload(m->colour_elems.data(), m->colour_elems.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_rowptr.upload(m->rowptr.data(), m->rowptr.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_colind.upload(m->colind.data(), m->colind.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_diagblk.upload(m->diagblk.data(), m->diagblk.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_blkrow.upload(blkrow.data(), blkrow.size())) != UFEM_AF_OK) return rv;
-  if ((rv = m->d_noderank.upload(nrank.data(), nrank.size())) != UFEM_AF_OK) return rv;
   if ((rv = m->d_eE.upload(m->eE.data(), m->eE.size())) != UFEM_AF_OK) return rv;
   if ((rv = m->d_eNu.upload(m->eNu.data(), m->eNu.size())) != UFEM_AF_OK) return rv;
   if ((rv = m->d_eThick.upload(m->eThick.data(), m->eThick.size())) != UFEM_AF_OK) return rv;
@@ -655,7 +644,7 @@ static int bc_launch(ufem_model *m) {
   std::vector<int> reac_slot;
   for (const auto &l : m->loads) {
     if (l.type != 1) continue;
-    long p = m->nDOFfld[l.node * KNOWN_DOFS + l.dir - 1];
+    long p = m->dof(l.node * KNOWN_DOFS + l.dir - 1);
     rows.push_back((int)(p - 1));
     vals.push_back(l.val);
   }

@@ -12,16 +12,17 @@
 //   fem_sol_res_alloc      fem/fem_sol.c:676-722 (reaction list)
 //   femGetRepVal           fem/fem_accs.c:196-288 (value lookup by position)
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <mutex>
-#include <sstream>
-#include <system_error>
-#include <thread>
 
 #include "ufem_internal.h"
 
@@ -50,6 +51,7 @@ static double rec_val(const std::vector<double> &rec, size_t idx) {
 }
 
 int model_from_tables(const ufem_tables *t, ufem_model *m) {
+  const auto t_start = std::chrono::steady_clock::now();
   if (!t || t->nLen < 2 || t->eLen < 1) {
     set_error("model tables: fewer than 2 nodes or no elements");
     return UFEM_AF_ERR_SML;  // fem/fem_io.c:516, :534
@@ -182,165 +184,26 @@ int model_from_tables(const ufem_tables *t, ufem_model *m) {
     m->mpID.resize(t->mpLen);
     for (long i = 0; i < t->mpLen; i++) m->mpID[i] = i + 1;
   }
+  m->ms_ingest[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   return build_model(m);
 }
 
-namespace {
-// f(begin, end) over [0, n) split into contiguous ranges, one per host
-// thread (at most 32; serial below 4096 items)
-template <typename F>
-void parallel_ranges(long n, F f) {
-  const unsigned hc = std::thread::hardware_concurrency();
-  const long nt = std::min<long>(std::max(1u, std::min(hc, 32u)), std::max(1L, n / 4096));
-  if (nt <= 1) {
-    f(0L, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  const long per = (n + nt - 1) / nt;
-  long t = 0;
-  for (; t < nt; t++) {
-    const long a = t * per, b = std::min(n, a + per);
-    if (a >= b) continue;
-    try {
-      th.emplace_back(f, a, b);
-    } catch (const std::system_error &) {
-      break;  // no thread could start (thread or process limit): this thread does the rest
-    }
-  }
-  for (; t < nt; t++) {
-    const long a = t * per, b = std::min(n, a + per);
-    if (a < b) f(a, b);
-  }
-  for (auto &x : th) x.join();
-}
-}  // namespace
-
 int build_model(ufem_model *m) {
-  const int b = m->b, nn = m->nn;
-  // ---- fem_dofs: mark used slots, number them 1..nDOFAct in slot order ----
-  m->nDOFfld.assign((size_t)m->nLen * KNOWN_DOFS, 0);
-  long act = 0;
-  for (long e = 0; e < m->eLen; e++)
-    for (int j = 0; j < nn; j++) {
-      long np = m->enodes[(size_t)e * nn + j];
-      for (int k = 0; k < b; k++) {
-        long d = np * KNOWN_DOFS + k;  // ndof = {U_X, U_Y[, U_Z]}
-        if (m->nDOFfld[d] == 0) {
-          m->nDOFfld[d] = 1;
-          act++;
-        }
-      }
-    }
-  if (act < 1) {
-    set_error("no degrees of freedom found");
-    return UFEM_AF_ERR_SIZ;
-  }
-  m->nDOFAct = act;
-  long num = 1;
-  for (size_t i = 0; i < m->nDOFfld.size(); i++)
-    if (m->nDOFfld[i] != 0) m->nDOFfld[i] = num++;
-  // block rows: used nodes in node order; DOF = b*rank + d + 1
-  m->node_rank.assign(m->nLen, -1);
-  m->rank_node.clear();
-  for (long n = 0; n < m->nLen; n++) {
-    if (m->nDOFfld[n * KNOWN_DOFS] != 0) {
-      m->node_rank[n] = (int)m->rank_node.size();
-      m->rank_node.push_back((int)n);
-      for (int d = 0; d < b; d++)
-        if (m->nDOFfld[n * KNOWN_DOFS + d] != (long)b * m->node_rank[n] + d + 1) {
-          set_error("DOF numbering is not node-uniform");
-          return UFEM_AF_ERR_TYP;
-        }
-    }
-  }
-  m->nbr = (int)m->rank_node.size();
-  // ---- block pattern: node adjacency through elements ---------------------
-  std::vector<int> n2e_ptr(m->nbr + 1, 0), n2e;
-  for (long e = 0; e < m->eLen; e++)
-    for (int j = 0; j < nn; j++) n2e_ptr[m->node_rank[m->enodes[(size_t)e * nn + j]] + 1]++;
-  for (int r = 0; r < m->nbr; r++) n2e_ptr[r + 1] += n2e_ptr[r];
-  n2e.resize(n2e_ptr[m->nbr]);
-  {
-    std::vector<int> fill(n2e_ptr.begin(), n2e_ptr.end() - 1);
-    for (long e = 0; e < m->eLen; e++)
-      for (int j = 0; j < nn; j++) n2e[fill[m->node_rank[m->enodes[(size_t)e * nn + j]]]++] = (int)e;
-  }
-  // rows and elements are independent: both passes below run on host
-  // threads over contiguous ranges, with results identical to a serial build
-  m->rowptr.assign(m->nbr + 1, 0);
-  auto row_cols = [&](int r, std::vector<int> &tmp) {
-    tmp.clear();
-    for (int q = n2e_ptr[r]; q < n2e_ptr[r + 1]; q++) {
-      int e = n2e[q];
-      for (int j = 0; j < nn; j++) tmp.push_back(m->node_rank[m->enodes[(size_t)e * nn + j]]);
-    }
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-  };
-  parallel_ranges(m->nbr, [&](long r0, long r1) {
-    std::vector<int> tmp;
-    for (long r = r0; r < r1; r++) {
-      row_cols((int)r, tmp);
-      m->rowptr[r + 1] = (int)tmp.size();
-    }
-  });
-  for (int r = 0; r < m->nbr; r++) m->rowptr[r + 1] += m->rowptr[r];
-  m->nnzb = m->rowptr[m->nbr];
-  m->colind.resize(m->nnzb);
-  m->diagblk.resize(m->nbr);
-  parallel_ranges(m->nbr, [&](long r0, long r1) {
-    std::vector<int> tmp;
-    for (long r = r0; r < r1; r++) {
-      row_cols((int)r, tmp);
-      std::copy(tmp.begin(), tmp.end(), m->colind.begin() + m->rowptr[r]);
-      auto it = std::lower_bound(tmp.begin(), tmp.end(), (int)r);
-      m->diagblk[r] = m->rowptr[r] + (int)(it - tmp.begin());
-    }
-  });
-  // ---- element->block scatter map ------------------------------------------
-  m->emap.resize((size_t)m->eLen * nn * nn);
-  parallel_ranges(m->eLen, [&](long e0, long e1) {
-    for (long e = e0; e < e1; e++)
-      for (int a = 0; a < nn; a++) {
-        int ra = m->node_rank[m->enodes[(size_t)e * nn + a]];
-        const int *beg = m->colind.data() + m->rowptr[ra];
-        const int *end = m->colind.data() + m->rowptr[ra + 1];
-        for (int c = 0; c < nn; c++) {
-          int rc = m->node_rank[m->enodes[(size_t)e * nn + c]];
-          const int *it = std::lower_bound(beg, end, rc);
-          m->emap[((size_t)e * nn + a) * nn + c] = (int)(it - m->colind.data());
-        }
-      }
-  });
-  // ---- greedy element colouring: no two elements of a colour share a node ---
-  std::vector<uint64_t> node_used(m->nbr, 0);
-  std::vector<int> ecol(m->eLen);
-  int ncol = 0;
-  for (long e = 0; e < m->eLen; e++) {
-    uint64_t busy = 0;
-    for (int j = 0; j < nn; j++) busy |= node_used[m->node_rank[m->enodes[(size_t)e * nn + j]]];
-    if (busy == ~0ull) {
-      set_error("element colouring needs more than 64 colours");
-      return UFEM_AF_ERR_BIG;
-    }
-    int c = __builtin_ctzll(~busy);
-    ecol[e] = c;
-    ncol = std::max(ncol, c + 1);
-    for (int j = 0; j < nn; j++) node_used[m->node_rank[m->enodes[(size_t)e * nn + j]]] |= (1ull << c);
-  }
-  m->ncolours = ncol;
-  m->colour_ptr.assign(ncol + 1, 0);
-  for (long e = 0; e < m->eLen; e++) m->colour_ptr[ecol[e] + 1]++;
-  for (int c = 0; c < ncol; c++) m->colour_ptr[c + 1] += m->colour_ptr[c];
-  m->colour_elems.resize(m->eLen);
-  {
-    std::vector<int> fill(m->colour_ptr.begin(), m->colour_ptr.end() - 1);
-    for (long e = 0; e < m->eLen; e++) m->colour_elems[fill[ecol[e]]++] = (int)e;
-  }
-  int rv = setup_loads(m);
+  // DOF numbering (fem_dofs, fem/fem_sol.c:1263), the block pattern
+  // (femKhit, fem/fem_mloc.c:83), the scatter map and the element colouring
+  // are built on the device
+  auto t0 = std::chrono::steady_clock::now();
+  int rv = gpu_build_pattern(m);
   if (rv != UFEM_AF_OK) return rv;
-  return upload_model(m);
+  auto t1 = std::chrono::steady_clock::now();
+  if ((rv = setup_loads(m)) != UFEM_AF_OK) return rv;
+  auto t2 = std::chrono::steady_clock::now();
+  rv = upload_model(m);
+  auto t3 = std::chrono::steady_clock::now();
+  m->ms_ingest[3] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  m->ms_ingest[4] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  m->ms_ingest[5] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+  return rv;
 }
 
 
@@ -357,7 +220,7 @@ int setup_loads(ufem_model *m) {
   m->reacRow.clear();
   m->fixedMask.assign(m->nDOFAct, 0);
   for (const auto &l : m->loads) {
-    long p = (l.dir >= 1 && l.dir <= KNOWN_DOFS) ? m->nDOFfld[l.node * KNOWN_DOFS + l.dir - 1] : 0;
+    long p = (l.dir >= 1 && l.dir <= KNOWN_DOFS) ? m->dof(l.node * KNOWN_DOFS + l.dir - 1) : 0;
     if (l.type == 3) {
       if (p > 0) m->F_loads[p - 1] += l.val;
     } else if (l.type == 1) {
@@ -391,7 +254,7 @@ int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, 
   for (long e = 0; e < m->eLen; e++)
     for (int j = 0; j < nn; j++)
       for (int k = 0; k < b; k++) {
-        long p = m->nDOFfld[(long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k];
+        long p = m->dof((long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k);
         if (p >= 1) krows[p - 1] += s;
       }
   long sum = 0;
@@ -409,7 +272,7 @@ int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, 
   for (long e = 0; e < m->eLen; e++) {
     int q = 0;
     for (int j = 0; j < nn; j++)
-      for (int k = 0; k < b; k++) lf[q++] = m->nDOFfld[(long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k];
+      for (int k = 0; k < b; k++) lf[q++] = m->dof((long)m->enodes[(size_t)e * nn + j] * KNOWN_DOFS + k);
     for (int i = 0; i < s; i++) {
       long r = lf[i] - 1;
       for (int j = 0; j < s; j++) {
@@ -701,12 +564,27 @@ int parse_binary(const std::string &buf, InputTables &in) {
       set_error("truncated binary input");
       return UFEM_AF_ERR_IO;
     }
+    // one copy pass (the array may sit at any byte offset of the file)
     if (a.l) {
-      a.l->resize(n);
-      if (n) std::memcpy(a.l->data(), buf.data() + off, n * 8);
+      a.l->clear();
+      a.l->reserve(n);
+      const char *src = buf.data() + off;
+      for (int64_t i = 0; i < n; i += 4096) {
+        long tmp[4096];
+        const int64_t c = std::min<int64_t>(4096, n - i);
+        std::memcpy(tmp, src + i * 8, c * 8);
+        a.l->insert(a.l->end(), tmp, tmp + c);
+      }
     } else {
-      a.d->resize(n);
-      if (n) std::memcpy(a.d->data(), buf.data() + off, n * 8);
+      a.d->clear();
+      a.d->reserve(n);
+      const char *src = buf.data() + off;
+      for (int64_t i = 0; i < n; i += 4096) {
+        double tmp[4096];
+        const int64_t c = std::min<int64_t>(4096, n - i);
+        std::memcpy(tmp, src + i * 8, c * 8);
+        a.d->insert(a.d->end(), tmp, tmp + c);
+      }
     }
     off += n * 8;
   }
@@ -799,29 +677,46 @@ int check_tables(const InputTables &in) {
   return UFEM_AF_OK;
 }
 
+// the whole file in one buffer, read with one pass of read(2)
 int read_file(const char *fname, std::string &buf) {
-  std::ifstream f(fname, std::ios::binary);
-  if (!f) {
+  const int fd = ::open(fname, O_RDONLY);
+  struct stat st;
+  if (fd < 0 || ::fstat(fd, &st) != 0) {
+    if (fd >= 0) ::close(fd);
     set_error(std::string("cannot open input ") + fname);
     return UFEM_AF_ERR_IO;
   }
-  std::stringstream ss;
-  ss << f.rdbuf();
-  buf = ss.str();
+  buf.resize((size_t)st.st_size);
+  size_t got = 0;
+  while (got < buf.size()) {
+    const ssize_t r = ::read(fd, &buf[got], buf.size() - got);
+    if (r <= 0) break;
+    got += (size_t)r;
+  }
+  ::close(fd);
+  if (got != buf.size()) {
+    set_error(std::string("cannot read input ") + fname);
+    return UFEM_AF_ERR_IO;
+  }
   return UFEM_AF_OK;
 }
 
 }  // namespace
 
 int read_input_file(const char *fname, ufem_model **out) {
+  const auto t0 = std::chrono::steady_clock::now();
   std::string buf;
   int rv = read_file(fname, buf);
   if (rv != UFEM_AF_OK) return rv;
+  const auto t1 = std::chrono::steady_clock::now();
   InputTables in;
   rv = is_binary(buf) ? parse_binary(buf, in) : parse_text(buf, in);
   if (rv != UFEM_AF_OK) return rv;
   if ((rv = check_tables(in)) != UFEM_AF_OK) return rv;
+  const auto t2 = std::chrono::steady_clock::now();
   ufem_model *m = new ufem_model();
+  m->ms_ingest[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  m->ms_ingest[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
   m->mc_ilen = in.mc_ilen;
   m->mc_olen = in.mc_olen;
   m->mc_pos = in.mc_pos;

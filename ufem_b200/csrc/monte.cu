@@ -137,14 +137,14 @@ int fill_outputs(ufem_model *m, const std::vector<double> &u, double *out) {
     if (pos < 0 || pos >= m->mc_olen) continue;
     double &o = out[pos];
     const bool slot = item >= 0 && item < m->nLen && sub >= 1 && sub <= KNOWN_DOFS;
-    const long p = slot ? m->nDOFfld[item * KNOWN_DOFS + sub - 1] : 0;
+    const long p = slot ? m->dof(item * KNOWN_DOFS + sub - 1) : 0;
     const double v = p > 0 ? u[p - 1] : 0.0;
     switch (ty) {
       case 8: o = v; break;                                  // RES_D
       case 15: if (o < v) o = v; break;                      // RES_D_MAX
       case 16: if (o > v) o = v; break;                      // RES_D_MIN
       case 17:                                               // RES_D_SUM, fem/fem_mont.c:550-555
-        if (slot && p >= 0 && p < (long)m->nDOFfld.size()) o += (double)m->nDOFfld[p];
+        if (slot && p >= 0 && p < m->dof_slots()) o += (double)m->dof(p);
         break;
       case 9:  // RES_R
         for (size_t r = 0; r < m->reacNode.size(); r++)

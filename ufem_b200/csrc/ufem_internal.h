@@ -102,15 +102,30 @@ struct ufem_model {
 
   // ---- DOF map and pattern -------------------------------------------------
   long nDOFAct = 0;
-  std::vector<long> nDOFfld;          // nLen*7, 1-based DOF numbers, 0 unused
   std::vector<int> node_rank;         // nLen, block row of a node or -1
   std::vector<int> rank_node;         // nbr
+  // the reference's nDOFfld[s], s = node * KNOWN_DOFS + slot: 1-based DOF
+  // number, 0 for an unused slot; slots 1..b of every used node, numbered
+  // node by node (fem_dofs, fem/fem_sol.c:1263)
+  long dof(long s) const {
+    if (s < 0 || s >= nLen * ufem::KNOWN_DOFS) return 0;
+    const long n = s / ufem::KNOWN_DOFS;
+    const int d = (int)(s % ufem::KNOWN_DOFS);
+    return (d < b && node_rank[n] >= 0) ? (long)b * node_rank[n] + d + 1 : 0;
+  }
+  long dof_slots() const { return nLen * ufem::KNOWN_DOFS; }
   int nbr = 0;                        // block rows
   long nnzb = 0;                      // blocks
-  std::vector<int> rowptr, colind, diagblk;
+  // the pattern and the scatter map are built on the device (pattern.cu);
+  // these host copies are filled on first use by host_pattern()
+  mutable std::vector<int> rowptr, colind, diagblk;
+  mutable std::vector<int> emap;      // eLen*nn*nn block index per node pair
+  mutable bool host_pattern_ok = false;
   int ncolours = 0;
   std::vector<int> colour_ptr, colour_elems;  // elements grouped by colour
-  std::vector<int> emap;              // eLen*nn*nn block index per node pair
+  // wall-clock milliseconds of model set-up: file read, parse, tables,
+  // DOF numbering + pattern + colouring, supports/loads, upload
+  double ms_ingest[6] = {0, 0, 0, 0, 0, 0};
 
   // ---- supports / loads ----------------------------------------------------
   std::vector<double> F_loads;        // F after fem_add_loads (host, reference order)
@@ -149,6 +164,10 @@ int read_input_file(const char *fname, ufem_model **out);
 int convert_input_file(const char *text_fname, const char *bin_fname);
 int model_from_tables(const ufem_tables *t, ufem_model *m);
 int export_rowslot(const ufem_model *m, long *frompos, long *defpos, long *pos, long *len);
+
+// device build of DOF numbering, pattern, scatter map, colouring (pattern.cu)
+int gpu_build_pattern(ufem_model *m);
+int host_pattern(const ufem_model *m);
 
 // device work (kernels.cu)
 int upload_model(ufem_model *m);
