@@ -67,23 +67,22 @@ struct CgArgsT {
 };
 using CgArgs = CgArgsT<double>;
 
-// One block row of y = A (z + beta p) (use_p) or y = A z: the B row sums come
-// back on lanes < B.
+// The items [k0, k1) of one block row of y = A (z + beta p) (use_p) or
+// y = A z: the B row sums come back on lanes < B.  Jf >= 0: the column index
+// of the lane's first item, already loaded by the caller.
 template <int B, typename TV>
-__device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ rowptr,
-                                                const int *__restrict__ colind, const TV *__restrict__ val,
-                                                const TV *z, const TV *p, double beta, bool use_p,
-                                                double *s_acc) {
+__device__ __forceinline__ double warp_items_spmv(int k0, int k1, int Jf, const int *__restrict__ colind,
+                                                  const TV *__restrict__ val, const TV *z, const TV *p,
+                                                  double beta, bool use_p, double *s_acc) {
   constexpr int L = 32 - (32 % B);
   const int lane = threadIdx.x & 31;
-  const int k0 = __ldg(rowptr + I), k1 = __ldg(rowptr + I + 1);
   const int nitems = (k1 - k0) * B;
   double acc = 0.0;
   if (lane < L) {
     const int a = lane % B;
     for (int t = lane; t < nitems; t += L) {
       const int k = k0 + t / B;
-      const int J = __ldg(colind + k);
+      const int J = (t == lane && Jf >= 0) ? Jf : __ldg(colind + k);
       const TV *v = val + (size_t)k * B * B + a * B;
 #pragma unroll
       for (int c = 0; c < B; c++) {
@@ -107,6 +106,45 @@ __device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ r
       for (int l = lane; l < L; l += B) y += s_acc[l];
     __syncwarp();
     return y;
+  }
+}
+
+// One block row I (bounds read from rowptr).
+template <int B, typename TV>
+__device__ __forceinline__ double warp_row_spmv(int I, const int *__restrict__ rowptr,
+                                                const int *__restrict__ colind, const TV *__restrict__ val,
+                                                const TV *z, const TV *p, double beta, bool use_p,
+                                                double *s_acc) {
+  return warp_items_spmv<B, TV>(__ldg(rowptr + I), __ldg(rowptr + I + 1), -1, colind, val, z, p, beta, use_p,
+                                s_acc);
+}
+
+// A warp's consecutive block rows [I0, I1) with the next row's bounds and
+// first column indices loaded while the current row computes, and the row's
+// own epilogue operands loaded before its SpMV: the loads that only depend on
+// the row number leave the per-row chain (row bounds -> column index ->
+// neighbour gathers -> epilogue).  pre(I) loads the epilogue operands (lanes
+// < B) and returns them; post(I, y, ops) consumes them.
+template <int B, typename TV, typename Pre, typename Post>
+__device__ __forceinline__ void warp_rows_spmv(int I0, int I1, const int *__restrict__ rowptr,
+                                               const int *__restrict__ colind, const TV *__restrict__ val,
+                                               const TV *z, const TV *p, double beta, bool use_p, double *s_acc,
+                                               Pre pre, Post post) {
+  constexpr int L = 32 - (32 % B);
+  const int lane = threadIdx.x & 31;
+  if (I0 >= I1) return;
+  const int kend = __ldg(rowptr + I1);
+  int k0 = __ldg(rowptr + I0), k1 = __ldg(rowptr + I0 + 1);
+  int Jf = (lane < L && k0 + lane / B < kend) ? __ldg(colind + k0 + lane / B) : 0;
+  for (int I = I0; I < I1; I++) {
+    const int k1n = (I + 1 < I1) ? __ldg(rowptr + I + 2) : k1;
+    const int Jfn = (lane < L && k1 + lane / B < kend) ? __ldg(colind + k1 + lane / B) : 0;
+    const auto ops = pre(I);
+    const double y = warp_items_spmv<B, TV>(k0, k1, Jf, colind, val, z, p, beta, use_p, s_acc);
+    post(I, y, ops);
+    k0 = k1;
+    k1 = k1n;
+    Jf = Jfn;
   }
 }
 
@@ -144,19 +182,28 @@ __global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_cg(CgArgsT<TV> A) 
   // phase 0: r = b - A x; z = r / M (fem/fem_eqs.c:150-162)
   {
     double rr = 0.0, xx = 0.0, rz = 0.0;
-    for (int I = I0; I < I1; I++) {
-      double y = warp_row_spmv<B, TV>(I, A.rowptr, A.colind, A.val, A.x, nullptr, 0.0, false, s_acc[warp]);
+    auto pre = [&](int I) {
+      double3 o = make_double3(0.0, 0.0, 1.0);
+      if (lane < B) {
+        const size_t i = (size_t)I * B + lane;
+        o = make_double3((double)A.b[i], (double)A.x[i], (double)A.M[i]);
+      }
+      return o;
+    };
+    auto post = [&](int I, double y, double3 o) {
       if (lane < B) {
         size_t i = (size_t)I * B + lane;
-        const TV ri = (TV)((double)A.b[i] - y);
-        const TV zi = (TV)((double)ri / (double)A.M[i]);
+        const TV ri = (TV)(o.x - y);
+        const TV zi = (TV)((double)ri / o.z);
         A.r[i] = ri;
         A.z[i] = zi;
         rr += (double)ri * (double)ri;
-        xx += (double)A.x[i] * (double)A.x[i];
+        xx += o.y * o.y;
         rz += (double)ri * (double)zi;
       }
-    }
+    };
+    warp_rows_spmv<B, TV>(I0, I1, A.rowptr, A.colind, A.val, A.x, (const TV *)nullptr, 0.0, false, s_acc[warp], pre,
+                          post);
     double v[3] = {rr, xx, rz};
     block_partials<3>(v, mypart);
   }
@@ -173,18 +220,25 @@ __global__ void __launch_bounds__(kThreads, kCgBlocksPerSm) k_cg(CgArgsT<TV> A) 
     // phase S: q = A p, p = z + beta p_old (fem/fem_eqs.c:168-186), partial p.q
     {
       double pq = 0.0;
-      for (int I = I0; I < I1; I++) {
-        double y = warp_row_spmv<B, TV>(I, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp]);
+      auto pre = [&](int I) {
+        double2 o = make_double2(0.0, 0.0);
+        if (lane < B) {
+          const size_t i = (size_t)I * B + lane;
+          o = make_double2((double)A.z[i], first ? 0.0 : (double)pold[i]);
+        }
+        return o;
+      };
+      auto post = [&](int I, double y, double2 o) {
         if (lane < B) {
           size_t i = (size_t)I * B + lane;
-          const double zi = (double)A.z[i];
-          const TV pi = (TV)(first ? zi : (zi + (beta * (double)pold[i])));
+          const TV pi = (TV)(first ? o.x : (o.x + (beta * o.y)));
           const TV qi = (TV)y;
           pnew[i] = pi;
           A.q[i] = qi;
           pq += (double)pi * (double)qi;
         }
-      }
+      };
+      warp_rows_spmv<B, TV>(I0, I1, A.rowptr, A.colind, A.val, A.z, pold, beta, !first, s_acc[warp], pre, post);
       double v[1] = {pq};
       block_partials<1>(v, mypart + 3);
     }
