@@ -903,7 +903,9 @@ def ours(a):
         cold_ms = e0.elapsed_time(e1)
         it_cold = d_it2.cpu().numpy()
         out_cold = d_out2.cpu().numpy()
-        return {"precision": PREC[precision], "coarse": bool(coarse), "value": n / (cold_ms / 1000.0),
+        # precision 4 needs a guess: the library runs a launch without one in precision 3
+        return {"precision": PREC[3 if precision == 4 else precision], "coarse": bool(coarse),
+                "value": n / (cold_ms / 1000.0),
                 "unit": "solves/s", "iters_mean": float(it_cold.mean()), "iters_max": int(it_cold.max()),
                 "all_converged": bool((d_st2.cpu().numpy() == 0).all()),
                 "outputs_max_rel_diff_vs_warm": float(np.abs(out_cold - out_warm).max() / np.abs(out_cold).max())}

@@ -238,9 +238,10 @@ int monte_solution_batch(char *param, long nsamp, const double *ifld, double *of
  * form with FP32 work vectors (r, z, p, q, the diagonal) and FP64 products,
  * FP64 solution and FP64 true-residual replacement as in 1; 4: as 3 with the
  * SpMV's products and sums in FP32 (FP32 unit blocks and multipliers: the
- * inner FP32 matrix) -- fastest with a warm start and the coarse space, but
- * from zero it needs far more iterations (the warm start's fallback re-solves
- * in precision 3).  A sample converges when its true relative residual
+ * inner FP32 matrix) -- fastest with a warm start and the coarse space; it
+ * needs a starting guess for every mesh of the launch: without one the
+ * launch runs in precision 3 (and the warm start's fallback re-solves in
+ * precision 3).  A sample converges when its true relative residual
  * |f - K u| / |f| <= tol. */
 typedef struct ufem_mc_options {
   int precision;

@@ -330,3 +330,19 @@ def test_coarse_on_quads_and_two_coarse_meshes():
         for k in range(len(res)):
             assert (res[k][1] == 0).all() and (ref[k][1] == 0).all()
             assert np.abs(res[k][0] - ref[k][0]).max() <= 1e-6 * np.abs(ref[k][0]).max()
+
+
+def test_precision4_without_a_guess_runs_in_precision3(beam):
+    """FP32 SpMV products need a starting guess: a launch without one runs in
+    precision 3 (same iterations and answer, bitwise), and converges with the
+    coarse space where FP32 products from zero would not."""
+    from ufem_b200.mc import set_coarse
+    m, g, train, ev, u_train = beam
+    set_coarse(g, _coarse_space(m, u_train, train, 32))
+    try:
+        u3, st3, it3, o3, _ = _solve(g, ev, precision=3)
+        u4, st4, it4, o4, _ = _solve(g, ev, precision=4)
+    finally:
+        set_coarse(g, None)
+    assert (st4 == 0).all()
+    assert np.array_equal(u3, u4) and np.array_equal(it3, it4) and np.array_equal(o3, o4)

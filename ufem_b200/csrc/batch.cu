@@ -2413,6 +2413,13 @@ int mc_solve_device(int nmesh, ufem_model *const *models, const long *nsamp, con
     set_error("batched Monte Carlo: 1 to 8 meshes per launch");
     return UFEM_AF_ERR_SIZ;
   }
+  // FP32 products need a starting guess: from zero they lose the cancellation
+  // of K z for smooth z (about twice the iterations, and no convergence to
+  // 1e-8 with the coarse space), so a launch with a mesh that has no guess
+  // runs in precision 3
+  if (opt.precision == 4)
+    for (int k = 0; k < nmesh; k++)
+      if (!d_u_guess || !d_u_guess[k]) opt.precision = 3;
   const int B = models[0]->b;
   for (int k = 0; k < nmesh; k++)
     if (models[k]->b != B) {
