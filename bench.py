@@ -134,8 +134,8 @@ def parse():
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
            4: ("k_batch_pcg_fp32prod_coarse_40x10x10_2048samples.md",
-               "40x10x10 16 E zones x 2048 samples, FP32 implicit form with FP32 products, coarse space of a short "
-               "warm-start training, 40 iterations"),
+               "40x10x10 16 E zones x 2048 samples, FP32 implicit form with FP32 products, coarse space and learned "
+               "guess of a short warm-start training, PCG to 1e-8"),
            3: ("k_batch_pcg_fp32_coarse_40x10x10_2048samples.md",
                "40x10x10 16 E zones x 2048 samples, FP32 implicit form, coarse space of a short warm-start "
                "training, 40 iterations"),
@@ -169,9 +169,19 @@ def profile_case(a):
         f = mg.mc_samples(m, mesh_id=2, nsamp=128)
     if a.precision not in (2, 3, 4) or a.no_coarse:
         g = GpuModel(m)
-    for _ in range(2):
-        res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block,
-                           coarse=0 if a.no_coarse else 1)
+    if a.precision == 4 and not a.no_coarse:
+        # precision 4 (FP32 products) runs warm-started only: the short
+        # training's learned guess, the PCG to 1e-8
+        import ctypes as C
+        from ufem_b200 import _lib
+        for _ in range(2):
+            ws.solve(f, precision=4, tiles_per_block=a.tiles_per_block)
+        st = _lib.McStats()
+        _lib.load().ufem_mc_get_stats(C.byref(st))
+    else:
+        for _ in range(2):
+            res, st = mc_solve([g], [f], precision=a.precision, max_iters=40, tiles_per_block=a.tiles_per_block,
+                               coarse=0 if a.no_coarse else 1)
     print(json.dumps({"profile_case": PROFILE.get(a.precision, ("", ""))[1], "coarse_modes": st.coarse_modes,
                       "pcg_ms": st.ms_pcg,
                       "pcg_bytes": st.pcg_bytes, "pcg_iterations": st.pcg_iterations,

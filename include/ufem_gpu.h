@@ -207,8 +207,9 @@ int ufem_eqs_cgwssor(long rows, const long *frompos, const long *defpos, const l
  * overlapped on the GPU would race on it; within one process an internal
  * lock serialises the calls and each call returns only after its kernels
  * have finished.  It runs on the legacy default stream with synchronous
- * copies, so it cannot be called while a stream is being captured.  The
- * first call on each device looks the array's address up. */
+ * copies.  The first call on each device looks the array's address up
+ * (cudaGetSymbolAddress); make that first call before any stream capture
+ * begins. */
 int ufem_eqs_cgwj_noalloc(int B, int nbr, const int *d_rowptr, const int *d_colind, const double *d_val,
                           const double *d_b, double *d_x, double eps, long maxIt, long *iters);
 

@@ -1590,12 +1590,12 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
         const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
         const double tol2 = M.tol2[s];
         const int st = __ldcg(M.state + s);
-        // FP64 inner iterations: the recursive residual tracks the true one,
-        // so a sample whose recursive residual reaches tol is frozen until
-        // the group's next true-residual pass.  FP32: the recursive residual
-        // drifts, so such a sample keeps iterating and asks for a true
-        // residual every iteration until one confirms convergence.
-        constexpr bool kFreeze = sizeof(T) == 8;
+        // A sample whose recursive residual reaches tol / 2 is frozen until
+        // the group's next true-residual pass confirms it (or it resumes).
+        // FP32 inner iterations too: the residual is replaced every time it
+        // has dropped by replace_near, so the recursive residual's drift is
+        // small against tol when it gets there.
+        constexpr bool kFreeze = true;
         int nst = st;
         if (st == ST_ACTIVE || st == ST_CAND) {
           if (!(rr == rr) || isinf(rr)) nst = ST_NAN;
@@ -1631,12 +1631,13 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
           atomicSub(A.active_count, 1);
         }
         // a true-residual pass.  FP32: on the residual drop and every
-        // rr_every iterations.  FP64 (no drift to correct): only to verify
-        // candidates, once no sample of the group still iterates or rr_every
-        // iterations after the last pass.
+        // rr_every iterations, and to verify candidates once no sample of
+        // the group still iterates.  FP64 (no drift to correct): only to
+        // verify candidates, once no sample of the group still iterates or
+        // rr_every iterations after the last pass.
         const bool due = (k - M.glast[g] >= A.rr_every);
         if (sizeof(T) == 8) M.gneed[g] = wait && (!upd || due);
-        else M.gneed[g] = upd && (near || due);
+        else M.gneed[g] = (upd && (near || due)) || (wait && !upd);
       }
       if (!upd) {
         __syncthreads();

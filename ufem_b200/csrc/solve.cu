@@ -1320,9 +1320,9 @@ int cg_jacobi_mixed(const DevMatrix &A, const double *d_b, double *d_x, double e
 // overlapped on the GPU would race on it; this function prevents that in one
 // process: a lock serialises calls, and each call returns only once its
 // kernels have finished.  It runs on the legacy default stream with
-// synchronous copies, so it cannot be called during a stream capture.  The
-// first call on a device looks the array's device address up (once per
-// device, with that device current).
+// synchronous copies.  The first call on a device looks the array's device
+// address up (once per device, with that device current); make that first
+// call before any stream capture begins.
 // ---------------------------------------------------------------------------
 namespace {
 

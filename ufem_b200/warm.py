@@ -96,10 +96,12 @@ class WarmStart:
     def set_guess_scale(self, factor: float) -> None:
         _lib.check("ufem_warm_set_guess_scale", self.L.ufem_warm_set_guess_scale(self.h, float(factor)))
 
-    def solve(self, ifld, precision: int = 1, tol: float = 1e-8, coarse: bool = True):
+    def solve(self, ifld, precision: int = 1, tol: float = 1e-8, coarse: bool = True, tiles_per_block: int = 0):
         """Warm-started batched solve: (ofld, status, iters, stats).  With
         ``coarse`` (precision 2) the preconditioner adds the coarse correction
-        on the leading POD modes that training set on the model."""
+        on the leading POD modes that training set on the model;
+        ``tiles_per_block`` > 0 overrides the launch shape's work tiles per
+        persistent block."""
         import torch
         d = _dev(ifld, torch.float64)
         n = d.shape[0]
@@ -109,6 +111,7 @@ class WarmStart:
         it = torch.zeros(n, dtype=torch.int64, device="cuda")
         ws = _lib.WarmStats()
         opt = self._mc_opts(precision, tol, coarse)
+        opt.tiles_per_block = int(tiles_per_block)
         _lib.check("ufem_warm_solve", self.L.ufem_warm_solve(self.h, n, d.data_ptr(), of.data_ptr(), st.data_ptr(),
                                                              it.data_ptr(), C.byref(opt), C.byref(ws)))
         return (of.cpu().numpy()[:, :self.model.model.mc_olen], st.cpu().numpy(), it.cpu().numpy(), _fields(ws))
