@@ -1116,17 +1116,25 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
   double rr[VN], rz[VN];
 #pragma unroll
   for (int v = 0; v < VN; v++) rr[v] = rz[v] = 0;
+  // the vectors do not overlap: the loads of a row's next DOFs may be issued
+  // ahead of the stores of its first (more loads in flight per warp)
+  const T *__restrict__ Md = M.M;
+  const T *__restrict__ pd = pnew;
+  const T *__restrict__ qd = M.q;
+  T *__restrict__ rd = M.r;
+  T *__restrict__ zd = M.z;
+  double *__restrict__ xd = M.x;
   for (int I = row0 + warp; I < row1; I += NW) {
 #pragma unroll
     for (int a = 0; a < B; a++) {
       const size_t o = (size_t)(I * B + a) * S + sb;
       T ri[VN], mi[VN], pi[VN], qi[VN], zi[VN];
       double xi[VN];
-      ldn<T, VN>(M.M + o, mi);
-      ldn<T, VN>(M.r + o, ri);
-      ldn<T, VN>(pnew + o, pi);
-      ldn<T, VN>(M.q + o, qi);
-      ld64<T, VN>(M.x + o, xi);
+      ldn<T, VN>(Md + o, mi);
+      ldn<T, VN>(rd + o, ri);
+      ldn<T, VN>(pd + o, pi);
+      ldn<T, VN>(qd + o, qi);
+      ld64<T, VN>(xd + o, xi);
 #pragma unroll
       for (int v = 0; v < VN; v++) {
         xi[v] += (double)alpha[v] * (double)pi[v];
@@ -1135,9 +1143,9 @@ __device__ __forceinline__ void tile_update(const BMesh<T> &M, int g, int chunk,
         rr[v] += (double)ri[v] * (double)ri[v];
         rz[v] += (double)ri[v] * (double)zi[v];
       }
-      st64<T, VN>(M.x + o, xi);
-      stn<T, VN>(M.r + o, ri);
-      stn<T, VN>(M.z + o, zi);  // with a coarse space the C3 phase adds Wc c
+      st64<T, VN>(xd + o, xi);
+      stn<T, VN>(rd + o, ri);
+      stn<T, VN>(zd + o, zi);  // with a coarse space the C3 phase adds Wc c
     }
   }
   tile_partials<T, VN, NW>(M, g, chunk, par, rr, rz, s_red, s_red2);

@@ -75,11 +75,75 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return cdf + x * pdf;
 }
 
+// 8 x 8 transpose of BF16 values held as 8 rows of 16 bytes: in[k] holds
+// rows m = 0..7 of column k, out[m] holds columns k = 0..7 of row m.  Pairs
+// of 16-bit halves are exchanged with byte permutes; the rest is renaming.
+__device__ __forceinline__ void transpose8x8_bf16(const uint4 (&in)[8], uint4 (&out)[8]) {
+  uint32_t w[8][4];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    w[k][0] = in[k].x; w[k][1] = in[k].y; w[k][2] = in[k].z; w[k][3] = in[k].w;
+  }
+  uint32_t o[8][4];
+#pragma unroll
+  for (int kp = 0; kp < 4; kp++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t a = w[2 * kp][j], b = w[2 * kp + 1][j];  // rows 2j, 2j+1 of columns 2kp, 2kp+1
+      o[2 * j][kp] = __byte_perm(a, b, 0x5410);               // row 2j: columns 2kp, 2kp+1
+      o[2 * j + 1][kp] = __byte_perm(a, b, 0x7632);           // row 2j+1
+    }
+#pragma unroll
+  for (int m = 0; m < 8; m++) out[m] = make_uint4(o[m][0], o[m][1], o[m][2], o[m][3]);
+}
+
+// Stages rows [r_base, r_base + nrows) x columns [k0, k0 + KC) of an operand
+// X(r, k) = src[r * s_r + k * s_k] (rows >= r_lim and columns >= K read 0)
+// into the core-matrix layout.  One 8 x 8 core matrix per thread step: a
+// K-contiguous operand is read as 8 rows of 16 bytes, an R-contiguous one
+// (the backward products' transposed operands) as 8 columns of 16 bytes and
+// transposed in registers; edge and unaligned tiles element by element.
+__device__ __forceinline__ void stage_operand(const __nv_bfloat16 *__restrict__ src, long s_r, long s_k, int r_base,
+                                              int r_lim, int K, int k0, int nrows, uint8_t *dst) {
+  const bool kvec = s_k == 1 && (s_r & 7) == 0 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+  const bool rvec = s_r == 1 && (s_k & 7) == 0 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+  const int ntiles = (nrows / 8) * (kKC / 8);
+  for (int t = threadIdx.x; t < ntiles; t += kGemmThreads) {
+    const int r0 = (t / (kKC / 8)) * 8, kk = (t % (kKC / 8)) * 8;
+    const int gr = r_base + r0, gk = k0 + kk;
+    const bool full = gr + 8 <= r_lim && gk + 8 <= K;
+    uint8_t *d = dst + cm_offset(r0, kk);  // the tile's 8 rows of 16 bytes
+    if (full && kvec) {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        *reinterpret_cast<uint4 *>(d + 16 * i) =
+            __ldg(reinterpret_cast<const uint4 *>(src + (long)(gr + i) * s_r + gk));
+    } else if (full && rvec) {
+      uint4 in[8], out[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) in[i] = __ldg(reinterpret_cast<const uint4 *>(src + gr + (long)(gk + i) * s_k));
+      transpose8x8_bf16(in, out);
+#pragma unroll
+      for (int i = 0; i < 8; i++) *reinterpret_cast<uint4 *>(d + 16 * i) = out[i];
+    } else {
+      for (int i = 0; i < 8; i++)
+        for (int e = 0; e < 8; e++) {
+          __nv_bfloat16 v = __float2bfloat16(0.0f);
+          if (gr + i < r_lim && gk + e < K) v = src[(long)(gr + i) * s_r + (long)(gk + e) * s_k];
+          *reinterpret_cast<__nv_bfloat16 *>(d + 16 * i + 2 * e) = v;
+        }
+    }
+  }
+}
+
+// Two operand stages: the next K chunk is staged while the tensor cores work
+// on the current one; the MMAs of a stage arrive on that stage's mbarrier.
+constexpr int kStageA = kTileM * kKC * 2;        // 16 KB
+constexpr int kStageBytes = kStageA + kMaxN * kKC * 2;  // + 32 KB
+
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t *sA = smem;                              // 128 x KC bf16 = 16 KB
-  uint8_t *sB = smem + kTileM * kKC * 2;           // 256 x KC bf16 = 32 KB
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int s_bad;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -88,7 +152,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
   const int ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
   if (threadIdx.x == 0) {
     s_bad = 0;
-    tc::mbar_init(&mbar, 1);
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
   }
   if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
   tc::fence_before_sync();
@@ -97,43 +162,47 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::idesc_bf16(kTileM, N);
   const uint32_t sbo = (kKC / 8) * 128;
-  uint32_t phase = 0;
+  uint32_t phase[2] = {0u, 0u};
   const int nchunks = (g.K + kKC - 1) / kKC;
+  auto stage = [&](int c) {
+    uint8_t *sA = smem + (c & 1) * kStageBytes;
+    stage_operand(g.A, g.a_sm, g.a_sk, m0, g.M, g.K, c * kKC, kTileM, sA);
+    stage_operand(g.B, g.b_sn, g.b_sk, 0, N, g.K, c * kKC, N, sA + kStageA);
+  };
+  stage(0);
   for (int c = 0; c < nchunks; c++) {
-    const int k0 = c * kKC;
-    // stage A (128 x KC) and B (N x KC), zero-padded
-    for (int i = threadIdx.x; i < kTileM * kKC; i += kGemmThreads) {
-      const int r = i / kKC, k = i % kKC;
-      const int m = m0 + r, kk = k0 + k;
-      __nv_bfloat16 v = __float2bfloat16(0.0f);
-      if (m < g.M && kk < g.K) v = g.A[(long)m * g.a_sm + (long)kk * g.a_sk];
-      *reinterpret_cast<__nv_bfloat16 *>(sA + cm_offset(r, k)) = v;
-    }
-    for (int i = threadIdx.x; i < N * kKC; i += kGemmThreads) {
-      const int r = i / kKC, k = i % kKC;
-      const int kk = k0 + k;
-      __nv_bfloat16 v = __float2bfloat16(0.0f);
-      if (kk < g.K) v = g.B[(long)r * g.b_sn + (long)kk * g.b_sk];
-      *reinterpret_cast<__nv_bfloat16 *>(sB + cm_offset(r, k)) = v;
-    }
+    const int buf = c & 1;
     // make the generic-proxy shared stores visible to the tensor core
     tc::fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
       tc::fence_after_sync();
+      const uint8_t *sA = smem + buf * kStageBytes, *sB = sA + kStageA;
       for (int ks = 0; ks < kKC / 16; ks++) {
-        const uint64_t da = tc::desc_kmajor(smem_u32(sA) + ks * 256, 128, sbo);
-        const uint64_t db = tc::desc_kmajor(smem_u32(sB) + ks * 256, 128, sbo);
+        const uint64_t da = tc::desc_kmajor(tc::smem_u32(sA) + ks * 256, 128, sbo);
+        const uint64_t db = tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, sbo);
         tc::mma_bf16(tmem, da, db, idesc, c > 0 || ks > 0);
       }
-      tc::commit(&mbar);
+      tc::commit(&mbar[buf]);
     }
-    // wait for the MMAs of this chunk (they also release the staged tiles)
-    if (!tc::mbar_wait(&mbar, phase, kSpinLimit)) s_bad = 1;
-    phase ^= 1u;
-    __syncthreads();
-    if (s_bad) break;
+    if (c + 1 < nchunks) {
+      const int nb = buf ^ 1;
+      // the other stage is free once the MMAs of chunk c - 1 have read it
+      if (c >= 1) {
+        if (!tc::mbar_wait(&mbar[nb], phase[nb], kSpinLimit)) s_bad = 1;
+        phase[nb] ^= 1u;
+      }
+      __syncthreads();
+      if (s_bad) break;
+      stage(c + 1);
+    }
   }
+  // the last commit arrives once every MMA of the block has completed
+  if (!s_bad) {
+    const int lb = (nchunks - 1) & 1;
+    if (!tc::mbar_wait(&mbar[lb], phase[lb], kSpinLimit)) s_bad = 1;
+  }
+  __syncthreads();
   tc::fence_after_sync();
   if (!s_bad) {
     // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows m0+32w+lane
@@ -177,11 +246,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
   if (threadIdx.x == 0 && s_bad) atomicExch(g.err, 1);
 }
 
-// The operand tiles take 48 KB; the request is padded to 100 KB so that at
-// most two CTAs share an SM, which keeps their TMEM allocations (<= 256
+// The two operand stages take 96 KB; the request is padded to 100 KB so that
+// at most two CTAs share an SM, which keeps their TMEM allocations (<= 256
 // columns each) within the SM's 512 columns without any CTA waiting.
 constexpr size_t kGemmSmem = 100 * 1024;
-static_assert((size_t)(kTileM + kMaxN) * kKC * 2 <= kGemmSmem, "operand tiles exceed the shared-memory request");
+static_assert(2 * (size_t)kStageBytes <= kGemmSmem, "operand stages exceed the shared-memory request");
 
 // ---- small elementwise kernels ---------------------------------------------
 __global__ void k_to_bf16_pad(long rows, int cols, int ld_out, const float *__restrict__ x,
