@@ -10,7 +10,11 @@
 //   backward products read transposed operands without copies) into shared
 //   memory in the canonical no-swizzle K-major layout of the UMMA
 //   descriptors: 8-row x 16-byte core matrices, K-adjacent core matrices
-//   128 B apart (LBO), 8-row groups KC/8 * 128 B apart (SBO);
+//   128 B apart (LBO), 8-row groups KC/8 * 128 B apart (SBO).  A thread
+//   stages a whole core matrix with eight 16-byte loads (K-contiguous
+//   operands directly, M-contiguous ones through an 8 x 8 register
+//   transpose); two operand stages let the next K chunk be staged while the
+//   tensor cores work on the current one;
 // * one elected thread issues tcgen05.mma.cta_group::1.kind::f16 (M = 128,
 //   N <= 256, K = 16 per instruction) into an FP32 accumulator in tensor
 //   memory (TMEM) and tcgen05.commit arrives on an mbarrier; all waits are
