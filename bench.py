@@ -133,9 +133,9 @@ def parse():
 
 
 PROFILE = {1: ("k_batch_pcg_60x15x15_128samples.md", "60x15x15 per-element E x 128 samples, 40 iterations"),
-           4: ("k_batch_pcg_fp32prod_coarse_40x10x10_2048samples.md",
-               "40x10x10 16 E zones x 2048 samples, FP32 implicit form with FP32 products, coarse space and learned "
-               "guess of a short warm-start training, PCG to 1e-8"),
+           4: ("k_batch_pcg_fp32prod_coarse_40x10x10_4096samples.md",
+               "40x10x10 16 E zones, FP32 implicit form with FP32 products, coarse space and learned guess of a "
+               "short warm-start training, PCG to 1e-8"),
            3: ("k_batch_pcg_fp32_coarse_40x10x10_2048samples.md",
                "40x10x10 16 E zones x 2048 samples, FP32 implicit form, coarse space of a short warm-start "
                "training, 40 iterations"),
