@@ -1318,8 +1318,21 @@ __device__ __noinline__ void coarse_c1(const BMesh<T> &M, int g, int range, int 
         v[j][e] = row < r1 ? __ldcg(rcol + (size_t)row * S) : T(0);
       }
   };
+  // this thread's 16-byte pieces of a chunk's Wc^T tile (at most 2: the
+  // tile is cmodes x 64 BF16 <= 16 KB)
+  constexpr int kBp = (kCoarseMaxModes * 64 * 2 / 16 + kCoarseThreads - 1) / kCoarseThreads;
+  auto load_tile = [&](int ch, uint4 (&b)[kBp]) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(M.wt1 + (size_t)(r0 / 64 + ch) * stage_b);
+#pragma unroll
+    for (int j = 0; j < kBp; j++) {
+      const int i = tid + j * kCoarseThreads;
+      if (i < stage_b / 16) b[j] = __ldg(src + i);
+    }
+  };
   T cur[8 / kQ][8], nxt[8 / kQ][8];
+  uint4 bcur[kBp], bnxt[kBp];
   load_chunk(0, cur);
+  load_tile(0, bcur);
   bool ok = true;
   for (int ch = 0; ch < nch; ch++) {
     uint8_t *sA = sm + (ch & 1) * kCoarseStage, *sB = sA + 128 * 64 * 2;
@@ -1333,11 +1346,18 @@ __device__ __noinline__ void coarse_c1(const BMesh<T> &M, int g, int range, int 
       pk.w = pack_bf16x2((float)cur[j][6], (float)cur[j][7]);
       *reinterpret_cast<uint4 *>(sA + tc::cm_offset(m, (q + kQ * j) * 8, 64)) = pk;
     }
-    // B = the chunk's Wc^T tile (cmodes x 64), stored in operand order
-    const uint4 *src = reinterpret_cast<const uint4 *>(M.wt1 + (size_t)(r0 / 64 + ch) * stage_b);
-    for (int i = tid; i < stage_b / 16; i += kCoarseThreads) reinterpret_cast<uint4 *>(sB)[i] = __ldg(src + i);
-    // the next chunk's residuals are in flight during the MMAs of this one
-    if (ch + 1 < nch) load_chunk(ch + 1, nxt);
+    // B = the chunk's Wc^T tile (cmodes x 64), stored in operand order; it
+    // was loaded one chunk ahead
+#pragma unroll
+    for (int j = 0; j < kBp; j++) {
+      const int i = tid + j * kCoarseThreads;
+      if (i < stage_b / 16) reinterpret_cast<uint4 *>(sB)[i] = bcur[j];
+    }
+    // the next chunk's residuals and tile are in flight during the MMAs of this one
+    if (ch + 1 < nch) {
+      load_chunk(ch + 1, nxt);
+      load_tile(ch + 1, bnxt);
+    }
     tc::fence_proxy_async();
     // the MMAs of the previous chunk read the other buffer; wait for them
     // before the next staging round overwrites it
@@ -1358,6 +1378,8 @@ __device__ __noinline__ void coarse_c1(const BMesh<T> &M, int g, int range, int 
     for (int j = 0; j < 8 / kQ; j++)
 #pragma unroll
       for (int e = 0; e < 8; e++) cur[j][e] = nxt[j][e];
+#pragma unroll
+    for (int j = 0; j < kBp; j++) bcur[j] = bnxt[j];
   }
   ok = ok && tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
