@@ -24,14 +24,16 @@
 // sample group, block-row chunk) of every mesh.  The solution is kept in
 // FP64 (x += alpha p in FP64), and the recursive residual is replaced by the
 // true residual f - K x, computed in FP64 from the FP64 values, every
-// replace_every iterations and whenever it falls to replace_near * tol: the
-// CG keeps its search direction across replacements (no restart), so FP32
-// costs about the FP64 iteration count.  A sample converges only on a true
-// residual, |f - K x| / |f| <= tol.  Two bounded grid barriers per
-// iteration (three when a replacement runs); per-sample masks freeze
-// converged samples, a group of GS samples drops out when all of its
-// samples are done, the launch ends when no group is left or at the
-// iteration cap.  Per-sample scalars come from per-tile partials reduced in
+// replace_every iterations and whenever it has dropped by the factor
+// replace_near since the last replacement: the CG keeps its search direction
+// across replacements (no restart), so FP32 costs about the FP64 iteration
+// count.  A sample converges only on a true residual, |f - K x| / |f| <=
+// tol: once its recursive residual is below tol / 2 it is frozen until a
+// true-residual pass of its group confirms it (or it resumes).  Two bounded
+// grid barriers per iteration (three when a replacement runs, two more for
+// the coarse correction); per-sample masks freeze converged samples, a
+// group of GS samples drops out when all of its samples are done, the launch
+// ends when no group is left or at the iteration cap.  Per-sample scalars come from per-tile partials reduced in
 // a fixed order (run-to-run identical); partial buffers are double-buffered
 // by iteration parity so no block overwrites what another still reads.
 #include <cuda_bf16.h>
@@ -763,6 +765,7 @@ struct BArgs {
 };
 
 enum { kPhInit = 0, kPhS = 1, kPhU = 2, kPhR = 3, kPhC1 = 4, kPhC3 = 5, kPhN = 6 };
+constexpr int kRepAlign = 4;  // FP32: iterations on which drop-triggered replacements run
 constexpr int kProfWall = 8;
 
 // Per-block phase clocks, kept by thread 0 in shared memory.
@@ -1283,6 +1286,21 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 __shared__ uint32_t s_coarse_tmem;
 __shared__ uint32_t s_coarse_phase;  // parity of the MMA barrier's next completion
 __shared__ __align__(8) uint64_t s_coarse_mbar;
+__shared__ uint32_t s_tile_phase;   // parity of the operand-tile barrier's next completion
+__shared__ __align__(8) uint64_t s_tile_mbar;
+
+// Bulk (non-tensor) copies global -> shared memory that complete on an
+// mbarrier: one thread announces the bytes, then issues the copies.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   tc::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+               : "memory");
+}
 
 // Leaves the kernel at the next grid barrier: every block sees the error.
 __device__ __forceinline__ void coarse_fail(GridBar *bar) { atomicExch(&bar->err, kErrMma); }
@@ -1451,22 +1469,17 @@ __device__ __noinline__ void coarse_c3(const BMesh<T> &M, int g, int chunk, uint
   const int nmod = M.cmodes, S = M.S;
   const int tbytes = 128 * nmod * 2;
   uint8_t *sA = sm, *sB = sm + tbytes;
-  // A = c of the group (written in this launch: L2 loads), B = Wc rows of the chunk
-  const uint4 *ca = reinterpret_cast<const uint4 *>(M.cb + (size_t)g * tbytes);
-  const uint4 *wb = reinterpret_cast<const uint4 *>(M.wt3 + (size_t)chunk * tbytes);
-  for (int i = tid; i < tbytes / 16; i += kCoarseThreads) {
-    reinterpret_cast<uint4 *>(sA)[i] = __ldcg(ca + i);
-    reinterpret_cast<uint4 *>(sB)[i] = __ldg(wb + i);
-  }
-  tc::fence_proxy_async();
-  __syncthreads();
+  // A = c of the group, B = Wc rows of the chunk: both tiles lie contiguous
+  // in global memory in operand order, so one bulk copy each brings them in
+  // while the threads' z loads are in flight.  c was written in this launch
+  // by other blocks (before the grid barrier that started the phase), and
+  // shared memory by this block's threads in earlier phases: the proxy
+  // fence orders both before the copies.
   if (tid == 0) {
-    tc::fence_after_sync();
-    const uint32_t idesc = tc::idesc_bf16(128, 128), sbo = (uint32_t)(nmod / 8) * 128;
-    for (int ks = 0; ks < nmod / 16; ks++)
-      tc::mma_bf16(tmem, tc::desc_kmajor(tc::smem_u32(sA) + ks * 256, 128, sbo),
-                   tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, sbo), idesc, ks > 0);
-    tc::commit(bar);
+    asm volatile("fence.proxy.async;" ::: "memory");
+    mbar_expect_tx(&s_tile_mbar, 2u * (uint32_t)tbytes);
+    bulk_g2s(sA, M.cb + (size_t)g * tbytes, (uint32_t)tbytes, &s_tile_mbar);
+    bulk_g2s(sB, M.wt3 + (size_t)chunk * tbytes, (uint32_t)tbytes, &s_tile_mbar);
   }
   // lanes = samples, columns = rows of the chunk: warp w reads TMEM lanes
   // 32 (w % 4) .. +31 and rows kRows (w / 4) .. +kRows-1
@@ -1474,10 +1487,23 @@ __device__ __noinline__ void coarse_c3(const BMesh<T> &M, int g, int chunk, uint
   T *zc = M.z + (size_t)g * 128 + ms;
   const int rbase = chunk * 128 + j0;
   const int nrow = min(kRows, M.n - rbase);  // rows of this thread's share in the mesh
-  // all z loads of this thread are in flight during the MMAs
+  // all z loads of this thread are in flight during the copies and the MMAs
   T zv[kRows];
 #pragma unroll
   for (int e = 0; e < kRows; e++) zv[e] = e < nrow ? __ldcg(zc + (size_t)(rbase + e) * S) : T(0);
+  const uint32_t tph = s_tile_phase;
+  const bool tok = tc::mbar_wait(&s_tile_mbar, tph, kMmaSpinLimit);
+  __syncthreads();
+  if (tid == 0) {
+    s_tile_phase = tph ^ 1u;
+    if (!tok) coarse_fail(gb);
+    tc::fence_after_sync();
+    const uint32_t idesc = tc::idesc_bf16(128, 128), sbo = (uint32_t)(nmod / 8) * 128;
+    for (int ks = 0; ks < nmod / 16; ks++)
+      tc::mma_bf16(tmem, tc::desc_kmajor(tc::smem_u32(sA) + ks * 256, 128, sbo),
+                   tc::desc_kmajor(tc::smem_u32(sB) + ks * 256, 128, sbo), idesc, ks > 0);
+    tc::commit(bar);
+  }
   const bool ok = tc::mbar_wait(bar, phase, kMmaSpinLimit);
   phase ^= 1u;
   tc::fence_after_sync();
@@ -1661,13 +1687,15 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
           atomicSub(A.active_count, 1);
         }
         // a true-residual pass.  FP32: on the residual drop and every
-        // rr_every iterations, and to verify candidates once no sample of
-        // the group still iterates.  FP64 (no drift to correct): only to
-        // verify candidates, once no sample of the group still iterates or
-        // rr_every iterations after the last pass.
+        // rr_every iterations -- both only on every kRepAlign-th iteration,
+        // so that the groups' replacements share passes (a pass over few
+        // groups leaves most SMs idle) -- and at once to verify candidates
+        // once no sample of the group still iterates.  FP64 (no drift to
+        // correct): only to verify candidates, once no sample of the group
+        // still iterates or rr_every iterations after the last pass.
         const bool due = (k - M.glast[g] >= A.rr_every);
         if (sizeof(T) == 8) M.gneed[g] = wait && (!upd || due);
-        else M.gneed[g] = (upd && (near || due)) || (wait && !upd);
+        else M.gneed[g] = (upd && (near || due) && (k % kRepAlign) == 0) || (wait && !upd);
       }
       if (!upd) {
         __syncthreads();
@@ -1777,6 +1805,8 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
       if (threadIdx.x == 0) {
         tc::mbar_init(&s_coarse_mbar, 1);
         s_coarse_phase = 0;
+        tc::mbar_init(&s_tile_mbar, 1);
+        s_tile_phase = 0;
       }
       if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s_coarse_tmem, kCoarseCols);
       tc::fence_before_sync();
