@@ -19,7 +19,7 @@
 // (block, row-in-block) items with stride L, so a lane's row-in-block
 // a = lane % B is fixed; each lane reads the B consecutive values of its block
 // row (contiguous across the warp) and the B gathered neighbour values; the B
-// sums are combined in a fixed order.
+// sums are combined by warp shuffles in a fixed order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -67,6 +67,18 @@ struct CgArgsT {
 };
 using CgArgs = CgArgsT<double>;
 
+// B = 3 (L = 30 lanes): lane l holds a partial of row l % 3 (lanes 30, 31
+// hold 0).  Lanes l, l + 15, l + 6, l + 3 and l + 12 share a row (the
+// offsets are multiples of 3), so four shuffles leave each row's sum of its
+// 10 lanes on lanes 0..2, in a fixed order (identical run to run).
+__device__ __forceinline__ double row_sums3(double acc) {
+  const double t1 = acc + __shfl_down_sync(0xffffffffu, acc, 15);  // lanes 0..14: l, l + 15
+  double t = t1 + __shfl_down_sync(0xffffffffu, t1, 6);            // lanes 0..8: + l + 6, l + 21
+  t += __shfl_down_sync(0xffffffffu, t, 3);                        // lanes 0..5: + l + 3, 9, 18, 24
+  t += __shfl_down_sync(0xffffffffu, t1, 12);                      // lanes 0..2: + l + 12, l + 27
+  return t;
+}
+
 // The items [k0, k1) of one block row of y = A (z + beta p) (use_p) or
 // y = A z: the B row sums come back on lanes < B.  Jf >= 0: the column index
 // of the lane's first item, already loaded by the caller.
@@ -99,13 +111,8 @@ __device__ __forceinline__ double warp_items_spmv(int k0, int k1, int Jf, const 
     for (int o = 16; o >= 2; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     return acc;
   } else {
-    s_acc[lane] = acc;
-    __syncwarp();
-    double y = 0.0;
-    if (lane < B)
-      for (int l = lane; l < L; l += B) y += s_acc[l];
-    __syncwarp();
-    return y;
+    (void)s_acc;
+    return row_sums3(acc);
   }
 }
 
@@ -1063,13 +1070,8 @@ __device__ __forceinline__ double warp_row_spmv_mix(int I, const int *__restrict
     for (int o = 16; o >= 2; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     return acc;
   } else {
-    s_acc[lane] = acc;
-    __syncwarp();
-    double y = 0.0;
-    if (lane < B)
-      for (int l = lane; l < L; l += B) y += s_acc[l];
-    __syncwarp();
-    return y;
+    (void)s_acc;
+    return row_sums3(acc);
   }
 }
 
