@@ -33,9 +33,10 @@
 // grid barriers per iteration (three when a replacement runs, two more for
 // the coarse correction); per-sample masks freeze converged samples, a
 // group of GS samples drops out when all of its samples are done, the launch
-// ends when no group is left or at the iteration cap.  Per-sample scalars come from per-tile partials reduced in
-// a fixed order (run-to-run identical); partial buffers are double-buffered
-// by iteration parity so no block overwrites what another still reads.
+// ends when no group is left or at the iteration cap.  Per-sample scalars
+// come from per-tile partials reduced in a fixed order (run-to-run
+// identical); partial buffers are double-buffered by iteration parity so no
+// block overwrites what another still reads.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
