@@ -763,6 +763,12 @@ struct BArgs {
   // included), [2 kProfWall] true-residual passes run.  Phases: kPh*.
   unsigned long long *prof;
   int *wctr;            // [kPhN] next work item of each phase (zero before its first use)
+  // Split iterations (the coarse-corrected FP32 kernels): kstep >= 0 runs
+  // one iteration's phases U, R, C1, C3 (kstep = 0: the initial residual
+  // and coarse correction), phase S runs in k_batch_s; -1: every iteration
+  // in this launch.
+  long kstep;
+  int *done;            // split: set when the iterations end (later launches return at once)
 };
 
 enum { kPhInit = 0, kPhS = 1, kPhU = 2, kPhR = 3, kPhC1 = 4, kPhC3 = 5, kPhN = 6 };
@@ -816,7 +822,7 @@ __device__ __forceinline__ void prof_flush(unsigned long long *prof) {
     s_prof_wall[s_prof_cur] += t - s_prof_w0;
     for (int p = 0; p < kPhN; p++) {
       atomicAdd(prof + p, s_prof_busy[p]);
-      if (blockIdx.x == 0) prof[kProfWall + p] = s_prof_wall[p];
+      if (blockIdx.x == 0) prof[kProfWall + p] += s_prof_wall[p];
     }
   }
 }
@@ -1588,16 +1594,183 @@ __device__ __noinline__ bool coarse_phases(const BArgs<T> A, const BMesh<T> *s_m
   return true;
 }
 
+// Phase S of iteration k: per-sample convergence on true residuals, beta,
+// q = A p with p = z + beta p_old, p.q (the tiles' work items).
+template <typename T, int B, bool IMP, int UN, int VN, int NW, bool F32P>
+__device__ __forceinline__ void phase_S(const BArgs<T> &A, const BMesh<T> *s_meshes, long k,
+                                        double (*s_red)[32 * VN], T *s_sc) {
+  constexpr int GS = 32 * VN;
+  __shared__ int s_flag;
+  const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
+  const bool first = (k == 1);
+  prof_begin(kPhS);
+  for (int t = claim(A.wctr + kPhS); t < A.ntiles; t = claim(A.wctr + kPhS)) {
+    const int4 ti = A.tiles[t];
+    const BMesh<T> &M = s_meshes[ti.x];
+    if (threadIdx.x == 0) s_flag = __ldcg(M.gtrue + ti.y);
+    __syncthreads();
+    const int g = ti.y;
+    const bool is_true = s_flag != 0;
+    int upd = 0, near = 0, wait = 0;
+    if (threadIdx.x < GS) {
+      const int sl = threadIdx.x, s = g * GS + sl;
+      const double rr = __ldcg(M.tot_rr + (size_t)parm1 * M.S + s);
+      const double rzn = __ldcg(M.tot_rz + (size_t)parm1 * M.S + s);
+      const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
+      const double tol2 = M.tol2[s];
+      const int st = __ldcg(M.state + s);
+      // A sample whose recursive residual reaches tol / 2 is frozen until
+      // the group's next true-residual pass confirms it (or it resumes).
+      // FP32 inner iterations too: the residual is replaced every time it
+      // has dropped by replace_near, so the recursive residual's drift is
+      // small against tol when it gets there.
+      constexpr bool kFreeze = true;
+      int nst = st;
+      if (st == ST_ACTIVE || st == ST_CAND) {
+        if (!(rr == rr) || isinf(rr)) nst = ST_NAN;
+        else if (is_true && (double)rr <= tol2) nst = ST_CONV;
+        else if (k > A.maxit) nst = ST_MAXIT;
+        else if (is_true) nst = ST_ACTIVE;  // a candidate that failed its check resumes
+        else if (kFreeze && rr <= 0.25 * tol2) nst = ST_CAND;
+      }
+      upd = (nst == ST_ACTIVE);
+      wait = (nst == ST_CAND);
+      // replace once the recursive residual has dropped by the factor
+      // near since the last replacement (FP32: also to verify convergence)
+      near = upd && !is_true &&
+             (rr <= A.near2 * __ldcg(M.rrlast + s) || (!kFreeze && rr <= 0.25 * tol2));
+      s_sc[sl] = upd ? (first ? T(0) : (T)(rzn / rzo)) : T(0);
+      if (ti.z == 0) {  // the group's first tile records per-sample results
+        if (sl == 0 && M.cmodes) M.gcz[g] = 0;  // z was formed in the last coarse phase
+        if (nst != st) {
+          M.state[s] = nst;
+          // a verified candidate keeps the count of the iterate it froze at
+          if (!(st == ST_CAND && nst == ST_CONV)) M.iters[s] = (int)(k - 1);
+        }
+        M.rho[(size_t)par * M.S + s] = rzn;
+        if (is_true) M.rrlast[s] = rr;
+      }
+    }
+    upd = __syncthreads_or(upd);
+    near = __syncthreads_or(near);
+    wait = __syncthreads_or(wait);
+    if (ti.z == 0 && threadIdx.x == 0) {
+      if (!upd && !wait && M.gactive[g]) {
+        M.gactive[g] = 0;
+        atomicSub(A.active_count, 1);
+      }
+      // a true-residual pass.  FP32: on the residual drop and every
+      // rr_every iterations -- both only on every kRepAlign-th iteration,
+      // so that the groups' replacements share passes (a pass over few
+      // groups leaves most SMs idle) -- and at once to verify candidates
+      // once no sample of the group still iterates.  FP64 (no drift to
+      // correct): only to verify candidates, once no sample of the group
+      // still iterates or rr_every iterations after the last pass.
+      const bool due = (k - M.glast[g] >= A.rr_every);
+      if (sizeof(T) == 8) M.gneed[g] = wait && (!upd || due);
+      else M.gneed[g] = (upd && (near || due) && (k % kRepAlign) == 0) || (wait && !upd);
+    }
+    if (!upd) {
+      __syncthreads();
+      continue;
+    }
+    const T *pold = (k & 1) ? M.p0 : M.p1;
+    T *pnew = (k & 1) ? M.p1 : M.p0;
+    tile_spmv<T, B, IMP, UN, VN, NW, F32P>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
+  }
+}
+
+// Phase U of iteration k: alpha, x += alpha p, r -= alpha q, z = r / M, and
+// the groups that asked for a true-residual pass counted in A.rcount.
+template <typename T, int B, int VN, int NW>
+__device__ __forceinline__ void phase_U(const BArgs<T> &A, const BMesh<T> *s_meshes, long k,
+                                        double (*s_red)[32 * VN], double (*s_red2)[32 * VN], T *s_sc) {
+  constexpr int GS = 32 * VN;
+  const int par = (int)(k & 1);
+  prof_begin(kPhU);
+  for (int t = claim(A.wctr + kPhU); t < A.ntiles; t = claim(A.wctr + kPhU)) {
+    const int4 ti = A.tiles[t];
+    const BMesh<T> &M = s_meshes[ti.x];
+    __syncthreads();
+    const int g = ti.y;
+    int upd = 0;
+    if (threadIdx.x < GS) {
+      const int sl = threadIdx.x, s = g * GS + sl;
+      const int st = __ldcg(M.state + s);
+      T alpha = 0;
+      if (st == ST_ACTIVE) {
+        const double pq = __ldcg(M.tot_pq + s);
+        const double rho = __ldcg(M.rho + (size_t)par * M.S + s);
+        if (pq > 0.0 && isfinite(pq)) {
+          alpha = (T)(rho / pq);
+          upd = 1;
+        } else if (ti.z == 0) {
+          M.state[s] = isfinite(pq) ? ST_BREAK : ST_NAN;  // p.q <= 0 or not finite: the sample is frozen
+          M.iters[s] = (int)k;
+        }
+      }
+      s_sc[sl] = alpha;
+    }
+    upd = __syncthreads_or(upd);
+    int live = 0;
+    if (threadIdx.x < GS) live = (__ldcg(M.state + g * GS + threadIdx.x) == ST_ACTIVE);
+    live = __syncthreads_or(live) | upd;
+    // groups due for a true-residual pass are counted whether or not they
+    // update (a group of frozen candidates only waits for that pass)
+    if (ti.z == 0 && threadIdx.x == 0 && __ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
+    if (!live) continue;
+    const T *pnew = (k & 1) ? M.p1 : M.p0;
+    tile_update<T, B, VN, NW>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
+    if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
+    if (M.cmodes && threadIdx.x == 0) M.gcz[g] = 1;
+  }
+}
+
+// Phase R of iteration k: the groups that asked replace their recursive
+// residual by the true one.
+template <typename T, int B, bool IMP, int UN, int VN, int NW>
+__device__ __forceinline__ void phase_R(const BArgs<T> &A, const BMesh<T> *s_meshes, long k,
+                                        double (*s_red)[32 * VN], double (*s_red2)[32 * VN]) {
+  __shared__ int s_flag;
+  const int par = (int)(k & 1);
+  prof_begin(kPhR);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.prof) A.prof[2 * kProfWall] += 1;
+  for (int t = claim(A.wctr + kPhR); t < A.ntiles; t = claim(A.wctr + kPhR)) {
+    const int4 ti = A.tiles[t];
+    const BMesh<T> &M = s_meshes[ti.x];
+    if (threadIdx.x == 0) s_flag = __ldcg(M.gneed + ti.y);
+    __syncthreads();
+    if (!s_flag) {
+      __syncthreads();  // thread 0 rewrites s_flag for the next tile
+      continue;
+    }
+    tile_true_residual<T, B, IMP, UN, VN, NW>(M, ti.y, ti.z, par, s_red, s_red2);
+    if (ti.z == 0 && threadIdx.x == 0) {
+      M.gtrue[ti.y] = 1;
+      M.glast[ti.y] = (int)k;
+    }
+    if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
+  }
+}
+
+// The block's shared state of the PCG launches (declared once per kernel).
+template <typename T, int NW, int GS>
+struct PcgShared {
+  double red[NW][GS];   // per-warp partial sums
+  double red2[NW][GS];
+  T sc[GS];             // per-sample scalars of the tile's group
+  BMesh<T> meshes[kMaxMeshes];
+};
+
 template <typename T, int B, bool IMP, int UN, int VN, bool CO, int NW, bool F32P>
-__device__ __forceinline__ void pcg_body(const BArgs<T> A) {
+__device__ __forceinline__ void pcg_body(const BArgs<T> A, PcgShared<T, NW, 32 * VN> &sh) {
   constexpr int GS = 32 * VN;
   constexpr bool kCoarse = CO;
   static_assert(!CO || (IMP && VN == 4), "the coarse correction runs with the implicit form and 128-sample groups");
-  __shared__ double s_red[NW][GS];
-  __shared__ double s_red2[NW][GS];
-  __shared__ T s_sc[GS];
-  __shared__ BMesh<T> s_meshes[kMaxMeshes];
-  __shared__ int s_flag;
+  double (*s_red)[GS] = sh.red;
+  double (*s_red2)[GS] = sh.red2;
+  T *s_sc = sh.sc;
+  BMesh<T> *s_meshes = sh.meshes;
   // the mesh descriptors, once per launch
   for (int i = threadIdx.x; i < A.nmesh * (int)(sizeof(BMesh<T>) / sizeof(int)); i += blockDim.x)
     reinterpret_cast<int *>(s_meshes)[i] = reinterpret_cast<const int *>(A.meshes)[i];
@@ -1628,84 +1801,9 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
   }
   long k;
   for (k = 1;; k++) {
-    const int par = (int)(k & 1), parm1 = (int)((k - 1) & 1);
-    const bool first = (k == 1);
+    const int par = (int)(k & 1);
     // ---- phase S: convergence on true residuals, beta, q = A p -------------
-    prof_begin(kPhS);
-    for (int t = claim(A.wctr + kPhS); t < A.ntiles; t = claim(A.wctr + kPhS)) {
-      const int4 ti = A.tiles[t];
-      const BMesh<T> &M = s_meshes[ti.x];
-      if (threadIdx.x == 0) s_flag = __ldcg(M.gtrue + ti.y);
-      __syncthreads();
-      const int g = ti.y;
-      const bool is_true = s_flag != 0;
-      int upd = 0, near = 0, wait = 0;
-      if (threadIdx.x < GS) {
-        const int sl = threadIdx.x, s = g * GS + sl;
-        const double rr = __ldcg(M.tot_rr + (size_t)parm1 * M.S + s);
-        const double rzn = __ldcg(M.tot_rz + (size_t)parm1 * M.S + s);
-        const double rzo = first ? 1.0 : __ldcg(M.rho + (size_t)parm1 * M.S + s);
-        const double tol2 = M.tol2[s];
-        const int st = __ldcg(M.state + s);
-        // A sample whose recursive residual reaches tol / 2 is frozen until
-        // the group's next true-residual pass confirms it (or it resumes).
-        // FP32 inner iterations too: the residual is replaced every time it
-        // has dropped by replace_near, so the recursive residual's drift is
-        // small against tol when it gets there.
-        constexpr bool kFreeze = true;
-        int nst = st;
-        if (st == ST_ACTIVE || st == ST_CAND) {
-          if (!(rr == rr) || isinf(rr)) nst = ST_NAN;
-          else if (is_true && (double)rr <= tol2) nst = ST_CONV;
-          else if (k > A.maxit) nst = ST_MAXIT;
-          else if (is_true) nst = ST_ACTIVE;  // a candidate that failed its check resumes
-          else if (kFreeze && rr <= 0.25 * tol2) nst = ST_CAND;
-        }
-        upd = (nst == ST_ACTIVE);
-        wait = (nst == ST_CAND);
-        // replace once the recursive residual has dropped by the factor
-        // near since the last replacement (FP32: also to verify convergence)
-        near = upd && !is_true &&
-               (rr <= A.near2 * __ldcg(M.rrlast + s) || (!kFreeze && rr <= 0.25 * tol2));
-        s_sc[sl] = upd ? (first ? T(0) : (T)(rzn / rzo)) : T(0);
-        if (ti.z == 0) {  // the group's first tile records per-sample results
-          if (sl == 0 && M.cmodes) M.gcz[g] = 0;  // z was formed in the last coarse phase
-          if (nst != st) {
-            M.state[s] = nst;
-            // a verified candidate keeps the count of the iterate it froze at
-            if (!(st == ST_CAND && nst == ST_CONV)) M.iters[s] = (int)(k - 1);
-          }
-          M.rho[(size_t)par * M.S + s] = rzn;
-          if (is_true) M.rrlast[s] = rr;
-        }
-      }
-      upd = __syncthreads_or(upd);
-      near = __syncthreads_or(near);
-      wait = __syncthreads_or(wait);
-      if (ti.z == 0 && threadIdx.x == 0) {
-        if (!upd && !wait && M.gactive[g]) {
-          M.gactive[g] = 0;
-          atomicSub(A.active_count, 1);
-        }
-        // a true-residual pass.  FP32: on the residual drop and every
-        // rr_every iterations -- both only on every kRepAlign-th iteration,
-        // so that the groups' replacements share passes (a pass over few
-        // groups leaves most SMs idle) -- and at once to verify candidates
-        // once no sample of the group still iterates.  FP64 (no drift to
-        // correct): only to verify candidates, once no sample of the group
-        // still iterates or rr_every iterations after the last pass.
-        const bool due = (k - M.glast[g] >= A.rr_every);
-        if (sizeof(T) == 8) M.gneed[g] = wait && (!upd || due);
-        else M.gneed[g] = (upd && (near || due) && (k % kRepAlign) == 0) || (wait && !upd);
-      }
-      if (!upd) {
-        __syncthreads();
-        continue;
-      }
-      const T *pold = (k & 1) ? M.p0 : M.p1;
-      T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_spmv<T, B, IMP, UN, VN, NW, F32P>(M, g, ti.z, s_sc, first, pold, pnew, s_red);
-    }
+    phase_S<T, B, IMP, UN, VN, NW, F32P>(A, s_meshes, k, s_red, s_sc);
     prof_end();
     if (!grid_barrier(A.bar)) return;
     release_counter(A.wctr + kPhS);
@@ -1713,67 +1811,14 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
     // every block takes the same exit decision.
     const int remaining = atomicAdd(A.active_count, 0);
     // ---- phase U: alpha, x += alpha p, r -= alpha q, z = r / M --------------
-    prof_begin(kPhU);
-    for (int t = claim(A.wctr + kPhU); t < A.ntiles; t = claim(A.wctr + kPhU)) {
-      const int4 ti = A.tiles[t];
-      const BMesh<T> &M = s_meshes[ti.x];
-      __syncthreads();
-      const int g = ti.y;
-      int upd = 0;
-      if (threadIdx.x < GS) {
-        const int sl = threadIdx.x, s = g * GS + sl;
-        const int st = __ldcg(M.state + s);
-        T alpha = 0;
-        if (st == ST_ACTIVE) {
-          const double pq = __ldcg(M.tot_pq + s);
-          const double rho = __ldcg(M.rho + (size_t)par * M.S + s);
-          if (pq > 0.0 && isfinite(pq)) {
-            alpha = (T)(rho / pq);
-            upd = 1;
-          } else if (ti.z == 0) {
-            M.state[s] = isfinite(pq) ? ST_BREAK : ST_NAN;  // p.q <= 0 or not finite: the sample is frozen
-            M.iters[s] = (int)k;
-          }
-        }
-        s_sc[sl] = alpha;
-      }
-      upd = __syncthreads_or(upd);
-      int live = 0;
-      if (threadIdx.x < GS) live = (__ldcg(M.state + g * GS + threadIdx.x) == ST_ACTIVE);
-      live = __syncthreads_or(live) | upd;
-      // groups due for a true-residual pass are counted whether or not they
-      // update (a group of frozen candidates only waits for that pass)
-      if (ti.z == 0 && threadIdx.x == 0 && __ldcg(M.gneed + g)) atomicAdd(A.rcount, 1);
-      if (!live) continue;
-      const T *pnew = (k & 1) ? M.p1 : M.p0;
-      tile_update<T, B, VN, NW>(M, g, ti.z, s_sc, pnew, par, s_red, s_red2);
-      if (ti.z == 0 && threadIdx.x == 0) M.gtrue[g] = 0;
-      if (M.cmodes && threadIdx.x == 0) M.gcz[g] = 1;
-    }
+    phase_U<T, B, VN, NW>(A, s_meshes, k, s_red, s_red2, s_sc);
     prof_end();
     if (!grid_barrier(A.bar)) return;
     release_counter(A.wctr + kPhU);
     // ---- phase R (when a group asked): replace the recursive residual -------
     const int nrep = atomicAdd(A.rcount, 0);  // changes only in phase U
     if (nrep > 0) {
-      prof_begin(kPhR);
-      if (blockIdx.x == 0 && threadIdx.x == 0 && A.prof) A.prof[2 * kProfWall] += 1;
-      for (int t = claim(A.wctr + kPhR); t < A.ntiles; t = claim(A.wctr + kPhR)) {
-        const int4 ti = A.tiles[t];
-        const BMesh<T> &M = s_meshes[ti.x];
-        if (threadIdx.x == 0) s_flag = __ldcg(M.gneed + ti.y);
-        __syncthreads();
-        if (!s_flag) {
-          __syncthreads();  // thread 0 rewrites s_flag for the next tile
-          continue;
-        }
-        tile_true_residual<T, B, IMP, UN, VN, NW>(M, ti.y, ti.z, par, s_red, s_red2);
-        if (ti.z == 0 && threadIdx.x == 0) {
-          M.gtrue[ti.y] = 1;
-          M.glast[ti.y] = (int)k;
-        }
-        if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
-      }
+      phase_R<T, B, IMP, UN, VN, NW>(A, s_meshes, k, s_red, s_red2);
       prof_end();
       if (!grid_barrier(A.bar)) return;
       release_counter(A.wctr + kPhR);
@@ -1787,6 +1832,99 @@ __device__ __forceinline__ void pcg_body(const BArgs<T> A) {
   }
   prof_flush(A.prof);
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
+}
+
+// One iteration of the split form (A.kstep = k >= 1): phases U, R, C1, C3
+// after the k_batch_s launch that ran phase S; A.kstep = 0: the initial
+// residual and coarse correction.  The grid barriers inside the launch are
+// those of pcg_body; the launch boundaries replace the barrier after S.
+template <typename T, int B, bool IMP, int UN, int VN, int NW, bool F32P>
+__device__ __forceinline__ void pcg_step(const BArgs<T> A, PcgShared<T, NW, 32 * VN> &sh) {
+  constexpr int GS = 32 * VN;
+  double (*s_red)[GS] = sh.red;
+  double (*s_red2)[GS] = sh.red2;
+  T *s_sc = sh.sc;
+  BMesh<T> *s_meshes = sh.meshes;
+  // every block reads the flag before the first barrier; block 0 sets it
+  // only after the launch's barriers
+  if (__ldcg(A.done)) return;
+  for (int i = threadIdx.x; i < A.nmesh * (int)(sizeof(BMesh<T>) / sizeof(int)); i += blockDim.x)
+    reinterpret_cast<int *>(s_meshes)[i] = reinterpret_cast<const int *>(A.meshes)[i];
+  prof_init();
+  __syncthreads();
+  const long k = A.kstep;
+  if (k == 0) {
+    for (int t = claim(A.wctr + kPhInit); t < A.ntiles; t = claim(A.wctr + kPhInit)) {
+      const int4 ti = A.tiles[t];
+      const BMesh<T> &M = s_meshes[ti.x];
+      int any = 0;
+      if (threadIdx.x < GS) any = (M.state[ti.y * GS + threadIdx.x] == ST_ACTIVE);
+      any = __syncthreads_or(any);
+      if (any) {
+        tile_true_residual<T, B, IMP, UN, VN, NW>(M, ti.y, ti.z, 0, s_red, s_red2);
+        if (ti.z == 0 && threadIdx.x == 0) {
+          M.gtrue[ti.y] = 1;
+          M.glast[ti.y] = 0;
+        }
+        if (M.cmodes && threadIdx.x == 0) M.gcz[ti.y] = 1;
+      }
+      __syncthreads();
+    }
+    prof_end();
+    if (!grid_barrier(A.bar)) return;
+    release_counter(A.wctr + kPhInit);
+    if (A.coarse && !coarse_phases<T>(A, s_meshes, 0)) return;
+    prof_flush(A.prof);
+    return;
+  }
+  const int par = (int)(k & 1);
+  release_counter(A.wctr + kPhS);  // k_batch_s has finished with it
+  // the group counter changes only in phase S (the previous launch)
+  const int remaining = atomicAdd(A.active_count, 0);
+  phase_U<T, B, VN, NW>(A, s_meshes, k, s_red, s_red2, s_sc);
+  prof_end();
+  if (!grid_barrier(A.bar)) return;
+  release_counter(A.wctr + kPhU);
+  const int nrep = atomicAdd(A.rcount, 0);  // changes only in phase U
+  if (nrep > 0) {
+    phase_R<T, B, IMP, UN, VN, NW>(A, s_meshes, k, s_red, s_red2);
+    prof_end();
+    if (!grid_barrier(A.bar)) return;
+    release_counter(A.wctr + kPhR);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(A.rcount, 0);
+  }
+  if (remaining <= 0 || k > A.maxit + 1) {
+    prof_flush(A.prof);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      *A.iter_out = k;
+      atomicExch(A.done, 1);
+    }
+    return;
+  }
+  if (A.coarse && !coarse_phases<T>(A, s_meshes, par)) return;
+  prof_flush(A.prof);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *A.iter_out = k;
+}
+
+// Phase S of iteration k for the split form, with more warps per SM than
+// the coarse instance's 16 (the gathers are latency-bound; the other phases
+// keep their 128 registers a thread in k_batch_pcg).  Ordinary launch, one
+// block per SM.
+constexpr int kSplitThreads = 768;
+template <typename T, int B, int UN, int VN, bool F32P>
+__global__ void __launch_bounds__(kSplitThreads, 1) k_batch_s(BArgs<T> A, long k) {
+  constexpr int GS = 32 * VN, NW = kSplitThreads / 32;
+  __shared__ double s_red[NW][GS];
+  __shared__ T s_sc[GS];
+  __shared__ BMesh<T> s_meshes[kMaxMeshes];
+  if (__ldcg(A.done)) return;
+  for (int i = threadIdx.x; i < A.nmesh * (int)(sizeof(BMesh<T>) / sizeof(int)); i += blockDim.x)
+    reinterpret_cast<int *>(s_meshes)[i] = reinterpret_cast<const int *>(A.meshes)[i];
+  prof_init();
+  __syncthreads();
+  phase_S<T, B, true, UN, VN, NW, F32P>(A, s_meshes, k, s_red, s_sc);
+  prof_end();
+  prof_flush(A.prof);
 }
 
 // UN: contributions whose gathers are issued together (implicit form);
@@ -1815,7 +1953,14 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
       tc::fence_after_sync();
     }
   }
-  pcg_body<T, B, IMP, UN, VN, CO, (CO ? kCoarseThreads : kThreads) / 32, F32P>(A);
+  constexpr int NW = (CO ? kCoarseThreads : kThreads) / 32;
+  __shared__ PcgShared<T, NW, 32 * VN> sh;
+  if constexpr (CO && sizeof(T) == 4) {
+    if (A.kstep >= 0) pcg_step<T, B, IMP, UN, VN, NW, F32P>(A, sh);
+    else pcg_body<T, B, IMP, UN, VN, CO, NW, F32P>(A, sh);
+  } else {
+    pcg_body<T, B, IMP, UN, VN, CO, NW, F32P>(A, sh);
+  }
   if constexpr (kCoarse) {
     if (A.coarse) {
       tc::fence_before_sync();
@@ -1947,6 +2092,7 @@ struct LaunchBufs {
   DBuf<long> itout;
   DBuf<unsigned long long> prof;
   DBuf<int> wctr;
+  DBuf<int> done;
 };
 template <typename T>
 LaunchBufs<T> &launch_bufs() {
@@ -2335,9 +2481,11 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   const int zero = 0;
   if ((rv = d_meshes.upload(hm.data(), hm.size())) || (rv = d_tiles.upload(tiles.data(), tiles.size())) ||
       (rv = bar.ensure(1)) || (rv = cnt.upload(&active_groups, 1)) || (rv = rcnt.upload(&zero, 1)) ||
-      (rv = itout.ensure(1)) || (rv = LB.prof.ensure(2 * kProfWall + 1)) || (rv = LB.wctr.ensure(kPhN)))
+      (rv = itout.ensure(1)) || (rv = LB.prof.ensure(2 * kProfWall + 1)) || (rv = LB.wctr.ensure(kPhN)) ||
+      (rv = LB.done.ensure(1)))
     return rv;
   UFEM_CUDA_TRY(cudaMemsetAsync(LB.wctr.p, 0, kPhN * sizeof(int)));
+  UFEM_CUDA_TRY(cudaMemsetAsync(LB.done.p, 0, sizeof(int)));
   UFEM_CUDA_TRY(cudaMemsetAsync(LB.prof.p, 0, (2 * kProfWall + 1) * sizeof(unsigned long long)));
   if (!c1items.empty() && ((rv = d_c1.upload(c1items.data(), c1items.size())) ||
                            (rv = d_c3.upload(c3items.data(), c3items.size()))))
@@ -2362,15 +2510,58 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   a.nc3 = (int)c3items.size();
   a.prof = LB.prof.p;
   a.wctr = LB.wctr.p;
+  a.kstep = -1;
+  a.done = LB.done.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
+  // The coarse-corrected FP32 kernels run each iteration as two launches:
+  // phase S in k_batch_s (24 warps per SM), the other phases in this
+  // kernel; every 4 iterations the host reads whether the iterations ended
+  // (later launches return at once).
+  bool split = false;
+  void (*skern)(BArgs<T>, long) = nullptr;
+  int sgrid = 0;
+  size_t sdsmem = 0;
+  if constexpr (IMP && VN == 4 && sizeof(T) == 4) {
+    if (coarse && B == 3) {
+      const int un = opt.unroll > 0 ? opt.unroll : 2;
+      skern = un <= 2 ? k_batch_s<T, 3, 2, VN, F32P> : k_batch_s<T, 3, 4, VN, F32P>;
+      sdsmem = smult ? mult_bytes : 0;
+      if (sdsmem) UFEM_CUDA_TRY(cudaFuncSetAttribute(skern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sdsmem));
+      int socc = 0;
+      UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&socc, skern, kSplitThreads, sdsmem));
+      if (socc >= 1) {
+        split = true;
+        sgrid = std::min<int>(nsm * socc, (int)tiles.size());
+      }
+    }
+  }
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0);
-  UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
+  if (!split) {
+    UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
+    g_stats.kernel_launches += 1;
+  } else {
+    a.kstep = 0;
+    UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
+    g_stats.kernel_launches += 1;
+    int hdone = 0;
+    for (long k = 1; k <= opt.max_iters + 2; k++) {
+      skern<<<sgrid, kSplitThreads, sdsmem>>>(a, k);
+      a.kstep = k;
+      UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
+      g_stats.kernel_launches += 2;
+      if ((k & 3) == 0) {
+        GridBar hb0;
+        UFEM_CUDA_TRY(cudaMemcpy(&hdone, LB.done.p, sizeof(int), cudaMemcpyDeviceToHost));
+        UFEM_CUDA_TRY(cudaMemcpy(&hb0, bar.p, sizeof(hb0), cudaMemcpyDeviceToHost));
+        if (hdone || hb0.err) break;
+      }
+    }
+  }
   cudaEventRecord(ev1);
-  g_stats.kernel_launches += 1;
   long its = 0;
   GridBar hb;
   UFEM_CUDA_TRY(cudaMemcpy(&its, itout.p, sizeof(long), cudaMemcpyDeviceToHost));
