@@ -1909,8 +1909,9 @@ __device__ __forceinline__ void pcg_step(const BArgs<T> A, PcgShared<T, NW, 32 *
 // Phase S of iteration k for the split form, with more warps per SM than
 // the coarse instance's 16 (the gathers are latency-bound; the other phases
 // keep their 128 registers a thread in k_batch_pcg).  Ordinary launch, one
-// block per SM.
-constexpr int kSplitThreads = 768;
+// block per SM.  28 warps (72 registers) measured best: S 85.0 ms per step
+// at 24 warps, 83.2 at 28, 84.8 at 32 (8,192 samples of the 40x10x10 beam).
+constexpr int kSplitThreads = 896;
 template <typename T, int B, int UN, int VN, bool F32P>
 __global__ void __launch_bounds__(kSplitThreads, 1) k_batch_s(BArgs<T> A, long k) {
   constexpr int GS = 32 * VN, NW = kSplitThreads / 32;
@@ -1955,9 +1956,8 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
   }
   constexpr int NW = (CO ? kCoarseThreads : kThreads) / 32;
   __shared__ PcgShared<T, NW, 32 * VN> sh;
-  if constexpr (CO && sizeof(T) == 4) {
-    if (A.kstep >= 0) pcg_step<T, B, IMP, UN, VN, NW, F32P>(A, sh);
-    else pcg_body<T, B, IMP, UN, VN, CO, NW, F32P>(A, sh);
+  if constexpr (CO && sizeof(T) == 4 && B == 3) {
+    pcg_step<T, B, IMP, UN, VN, NW, F32P>(A, sh);  // always split (run_pcg)
   } else {
     pcg_body<T, B, IMP, UN, VN, CO, NW, F32P>(A, sh);
   }
@@ -2514,10 +2514,10 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   a.done = LB.done.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
-  // The coarse-corrected FP32 kernels run each iteration as two launches:
-  // phase S in k_batch_s (24 warps per SM), the other phases in this
-  // kernel; every 4 iterations the host reads whether the iterations ended
-  // (later launches return at once).
+  // The coarse-corrected FP32 kernels of the brick family run each
+  // iteration as two launches: phase S in k_batch_s (28 warps per SM), the
+  // other phases in this kernel; every 4 iterations the host reads whether
+  // the iterations ended (later launches return at once).
   bool split = false;
   void (*skern)(BArgs<T>, long) = nullptr;
   int sgrid = 0;
@@ -2530,10 +2530,12 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
       if (sdsmem) UFEM_CUDA_TRY(cudaFuncSetAttribute(skern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sdsmem));
       int socc = 0;
       UFEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&socc, skern, kSplitThreads, sdsmem));
-      if (socc >= 1) {
-        split = true;
-        sgrid = std::min<int>(nsm * socc, (int)tiles.size());
+      if (socc < 1) {
+        set_error("batched PCG: the q = A z kernel does not fit on an SM");
+        return UFEM_AF_ERR;
       }
+      split = true;
+      sgrid = std::min<int>(nsm * socc, (int)tiles.size());
     }
   }
   cudaEvent_t ev0, ev1;
