@@ -1956,7 +1956,7 @@ __global__ void __launch_bounds__(CO ? kCoarseThreads : kThreads, CO ? 1 : (IMP 
   }
   constexpr int NW = (CO ? kCoarseThreads : kThreads) / 32;
   __shared__ PcgShared<T, NW, 32 * VN> sh;
-  if constexpr (CO && sizeof(T) == 4 && B == 3) {
+  if constexpr (CO && sizeof(T) == 4 && B == 3 && F32P) {
     pcg_step<T, B, IMP, UN, VN, NW, F32P>(A, sh);  // always split (run_pcg)
   } else {
     pcg_body<T, B, IMP, UN, VN, CO, NW, F32P>(A, sh);
@@ -2514,15 +2514,17 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   a.done = LB.done.p;
   void *args[] = {&a};
   const int grid = std::min<int>(G, (int)tiles.size());
-  // The coarse-corrected FP32 kernels of the brick family run each
+  // The coarse-corrected precision-4 kernels of the brick family run each
   // iteration as two launches: phase S in k_batch_s (28 warps per SM), the
   // other phases in this kernel; every 4 iterations the host reads whether
-  // the iterations ended (later launches return at once).
+  // the iterations ended (later launches return at once).  (Precision 3's
+  // FP64 products need more registers than 28 warps leave: 35,858 ->
+  // 24,961 solves/s split, so it keeps the persistent kernel.)
   bool split = false;
   void (*skern)(BArgs<T>, long) = nullptr;
   int sgrid = 0;
   size_t sdsmem = 0;
-  if constexpr (IMP && VN == 4 && sizeof(T) == 4) {
+  if constexpr (IMP && VN == 4 && sizeof(T) == 4 && F32P) {
     if (coarse && B == 3) {
       const int un = opt.unroll > 0 ? opt.unroll : 2;
       skern = un <= 2 ? k_batch_s<T, 3, 2, VN, F32P> : k_batch_s<T, 3, 4, VN, F32P>;
