@@ -2554,6 +2554,7 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
     int hdone = 0;
     for (long k = 1; k <= opt.max_iters + 2; k++) {
       skern<<<sgrid, kSplitThreads, sdsmem>>>(a, k);
+      UFEM_CUDA_TRY(cudaGetLastError());
       a.kstep = k;
       UFEM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(nthreads), args, dsmem, 0));
       g_stats.kernel_launches += 2;
