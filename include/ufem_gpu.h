@@ -321,7 +321,9 @@ typedef struct ufem_mc_stats {
   double pcg_bytes;          /* algorithmic bytes of all PCG iterations */
   double spmv_bytes;         /* algorithmic bytes of the SpMV phases only */
   long kernel_launches;
-  long pcg_launches;         /* persistent PCG launches (one per refinement step) */
+  long pcg_launches;         /* PCG solves launched (one per refinement step; a precision-4
+                                coarse-corrected solve runs as two kernel launches per
+                                iteration and counts once here, each launch in kernel_launches) */
   double pcg_launch_ms[16];  /* their durations (CUDA events around each launch) */
   int tiles_per_block, unroll, lane_samples;  /* the launch shape used */
   int coarse_modes;          /* modes of the coarse correction applied (0: Jacobi alone) */
