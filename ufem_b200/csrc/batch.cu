@@ -2329,11 +2329,14 @@ int run_pcg(int nmesh, ufem_model *const *models, std::vector<McWork *> &W, cons
   // rows per tile: about tiles_per_block tiles per block over the whole batch
   long total_rows = 0;
   for (int k = 0; k < nmesh; k++) total_rows += (long)models[k]->nbr * (W[k]->S / GS);
-  // measured best on B200: 12 for both forms (2 x 256-thread blocks per SM),
-  // 16 for the coarse-corrected instance (1 x 512; 8,192 samples of the
-  // 40x10x10 beam, precision 4: 201.2 ms per step against 206.1 at 24 and
+  // measured best on B200: 12 for both forms (2 x 256-thread blocks per SM)
+  // and for the coarse-corrected precision-4 solve with its split launches
+  // (8,192 samples of the 40x10x10 beam: 182.5 / 180.4 / 182.5 / 184.4 /
+  // 184.9 ms per step at 8 / 10 / 12 / 16 / 20 tiles per block); 16 for the
+  // one-kernel coarse-corrected instance (201.2 ms against 206.1 at 24 and
   // 202.7 at 12)
-  const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : (coarse ? 16 : 12);
+  const bool split_form = coarse && F32P && sizeof(T) == 4 && IMP && VN == 4 && B == 3;
+  const long tpb = opt.tiles_per_block > 0 ? opt.tiles_per_block : (coarse && !split_form ? 16 : 12);
   g_stats.tiles_per_block = (int)tpb;
   g_stats.unroll = IMP ? (opt.unroll > 0 ? opt.unroll : 2) : 0;
   g_stats.lane_samples = VN;
